@@ -1,0 +1,255 @@
+/*
+ * dycg.h -- C ABI of the B200 streaming delta-repair engine.
+ *
+ * One engine handle owns one graph (a paged adjacency held in pinned, mapped
+ * host memory, with an HBM page cache capped by a byte budget), the per-vertex
+ * results of one algorithm (SSSP, BFS, directed min-label CC or PageRank) and
+ * the CUDA stream everything runs on. After every snapshot of edge deletions
+ * and insertions the engine repairs the results incrementally on the GPU.
+ *
+ * Conventions
+ *  - Every function returns an int status: DYCG_OK (0) or a negative DYCG_E*
+ *    code. Nothing aborts the process; after an error, dycg_last_error() holds
+ *    a one-line description and the handle stays usable for gather/destroy.
+ *  - Input arrays are borrowed for the duration of the call only. Output
+ *    buffers are allocated by the caller.
+ *  - One host thread per handle; calls on one handle are not re-entrant.
+ *  - Vertex ids are uint32 and must be < 2^31 (bit 31 of an adjacency slot
+ *    marks a deleted occurrence).
+ *
+ * Each entry point cites the reference interface it replaces
+ * (MriMouse/DyCGraph, paths relative to that project).
+ */
+#ifndef DYCG_H
+#define DYCG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define DYCG_OK 0
+#define DYCG_EINVAL (-1)      /* bad argument                                 */
+#define DYCG_ECUDA (-2)       /* a CUDA runtime call failed                   */
+#define DYCG_ENOMEM (-3)      /* host or device allocation failed             */
+#define DYCG_ESTATE (-4)      /* call out of order (e.g. batch before init)   */
+#define DYCG_ECAPACITY (-5)   /* adjacency arena or a queue is exhausted      */
+#define DYCG_ELIMIT (-6)      /* a bounded device loop hit its iteration cap  */
+#define DYCG_EIO (-7)         /* file could not be read or parsed             */
+#define DYCG_ENOGPU (-8)      /* no CUDA device is available                  */
+
+/* ---- algorithms (the reference's four hybrid_* operators) -------------- */
+#define DYCG_ALGO_SSSP 0      /* samples/hybrid_sssp/hybrid_sssp.cu:51-204     */
+#define DYCG_ALGO_BFS 1       /* samples/hybrid_bfs/hybrid_bfs.cu (weight 1)   */
+#define DYCG_ALGO_CC 2        /* samples/hybrid_cc/hybrid_cc.cu:51-200         */
+#define DYCG_ALGO_PR 3        /* samples/hybrid_pr/hybrid_pr.cu:36-124         */
+
+/* ---- edge weights (SSSP) ----------------------------------------------- */
+/* HASH128: w(u,v) = (u+v) % 128 + 1, the reference's TraversalEdgeWeight
+ * (include/framework/variants/api.cuh:26-28); file weights are ignored.
+ * STORED: every adjacency slot carries the weight given at load/insert time. */
+#define DYCG_WEIGHT_HASH128 0
+#define DYCG_WEIGHT_STORED 1
+
+/* ---- cache admission policy -------------------------------------------- */
+#define DYCG_CACHE_NONE 0     /* no page is staged in HBM (reference -cache=0) */
+#define DYCG_CACHE_HOTNESS 1  /* decayed per-page access counts, top-K pages   */
+
+#define DYCG_INFINITY 0xFFFFFFFFu /* unreachable distance / no parent        */
+
+/* One update record, layout-compatible with the reference's 12-byte
+ * WEdgePair<uint32_t> (include/framework/edgepair.h:17-31). */
+typedef struct dycg_edge {
+  uint32_t u;
+  uint32_t v;
+  uint32_t w;
+} dycg_edge;
+
+typedef struct dycg_options {
+  uint32_t algo;          /* DYCG_ALGO_*                                      */
+  uint32_t weight_mode;   /* DYCG_WEIGHT_* (SSSP only)                        */
+  uint32_t source;        /* SSSP/BFS root (reference -source_node)           */
+  uint32_t segments;      /* reference -SEGMENT: edge-balanced vertex ranges  */
+                          /* used to bin each update batch                    */
+  uint64_t hbm_graph_budget_bytes; /* cap on adjacency bytes resident in HBM  */
+  uint32_t cache_policy;  /* DYCG_CACHE_*                                     */
+  uint32_t symmetric;     /* 1: graph and every batch are symmetric, the      */
+                          /* incoming adjacency aliases the outgoing one      */
+  float epsilon;          /* PR push threshold (reference -error)             */
+  float alpha;            /* PR damping factor (0.85)                         */
+  uint32_t max_rounds;    /* PR rounds per batch (reference -pr_max_rounds)   */
+  int32_t device;         /* CUDA device ordinal                              */
+  uint32_t page_shift;    /* log2 of adjacency slots per cache page (0: 12)   */
+  uint32_t reserved[7];
+} dycg_options;
+
+/* Per-call counters. Byte counts are algorithmic: every adjacency slot read
+ * or written is charged once, to the host link when its page is not resident
+ * in HBM and to HBM otherwise. */
+typedef struct dycg_batch_stats {
+  uint64_t deletions;          /* delete records received                    */
+  uint64_t insertions;         /* insert records received                    */
+  uint64_t missing_deletes;    /* deletes that matched no live occurrence    */
+  uint64_t invalid_updates;    /* records with an endpoint >= n              */
+  uint64_t touched_sources;    /* distinct sources of valid records          */
+  uint64_t relocated_rows;     /* rows moved to a larger block               */
+  uint64_t affected;           /* vertices invalidated by deletions          */
+  uint64_t expanded;           /* row expansions in the repair closures      */
+  uint64_t edges_scanned;      /* adjacency slots read by the repair         */
+  uint64_t improvements;       /* successful relaxations / residual pushes   */
+  uint64_t waves;              /* frontier waves (all closures)              */
+  uint64_t link_bytes;         /* adjacency bytes read/written over the host link */
+  uint64_t hbm_adj_bytes;      /* adjacency bytes read/written in the HBM cache   */
+  uint64_t state_bytes;        /* vertex-state bytes read/written (HBM)      */
+  uint64_t cache_pages_loaded; /* pages staged into HBM by maintenance       */
+  uint64_t cache_pages_evicted;
+  uint64_t kernel_launches;    /* CUDA kernels launched by the call          */
+  double ms_ingest;            /* device time per stage (CUDA events)        */
+  double ms_mutate;
+  double ms_repair;
+  double ms_cache;
+  double ms_total;
+  uint64_t reserved[8];
+} dycg_batch_stats;
+
+typedef struct dycg_graph_info {
+  uint64_t nodes;
+  uint64_t live_edges;
+  uint64_t arena_slots;        /* slots allocated in the host arena          */
+  uint64_t arena_used;         /* slots handed out (rows + relocations)      */
+  uint64_t pages;              /* pages over both adjacency directions       */
+  uint64_t cache_slots;        /* pages the HBM budget can hold              */
+  uint64_t cached_pages;       /* pages resident now                         */
+  uint64_t host_bytes;         /* pinned host bytes held by the arenas       */
+  uint64_t device_bytes;       /* device bytes held by the engine            */
+  uint32_t page_shift;
+  uint32_t has_incoming;       /* 1 if a separate incoming adjacency exists  */
+  uint64_t reserved[6];
+} dycg_graph_info;
+
+typedef struct dycg_engine dycg_engine;
+
+/* Fill *opt with the reference's defaults (SSSP, HASH128, source 0,
+ * SEGMENT 1, no cache, epsilon 1e-6, alpha 0.85, 100 rounds). */
+int dycg_options_default(dycg_options *opt);
+
+/* Replaces Engine::Engine(AlgoType) + SetOptions
+ * (include/framework/framework.cuh:1158, :1245). */
+int dycg_create(const dycg_options *opt, dycg_engine **out);
+
+/* Releases every device and pinned host allocation of the handle. */
+void dycg_destroy(dycg_engine *e);
+
+/* Replaces Engine::LoadGraph (include/framework/framework.cuh:1569-1798):
+ * builds the outgoing (and, unless symmetric, incoming) adjacency from a host
+ * CSR. offsets has n+1 entries; w may be NULL (weights then follow the weight
+ * mode). Rows keep their multiset of occurrences (duplicates are kept). */
+int dycg_load_graph_csr(dycg_engine *e, uint32_t n, const uint64_t *offsets,
+                        const uint32_t *dst, const uint32_t *w);
+
+/* Replaces Context's market_big reader (src/utils/parser.cpp:296-406): text
+ * lines "u v [w]"; n = max(max id + 1, min_nodes). */
+int dycg_load_graph_file(dycg_engine *e, const char *path, uint32_t min_nodes,
+                         int weighted);
+
+/* Synthetic workloads built on the GPU straight into the engine. R-MAT:
+ * 2^scale vertices, edge_factor*2^scale draws with quadrant probabilities
+ * (a,b,c,1-a-b-c), self-loops and duplicates removed; weights uniform in
+ * [wlo,whi] as a hash of (seed,u,v). symmetrize adds the reverse of every
+ * edge before de-duplication. */
+int dycg_load_graph_rmat(dycg_engine *e, uint32_t scale, uint32_t edge_factor,
+                         double a, double b, double c, uint64_t seed,
+                         uint32_t wlo, uint32_t whi, int symmetrize);
+
+/* 2D grid side x side, 4-neighbour edges in both directions, plus
+ * shortcut_permille/1000 * side^2 random shortcuts within radius (Chebyshev),
+ * inserted in both directions; weights uniform in [wlo,whi]. */
+int dycg_load_graph_grid(dycg_engine *e, uint32_t side, uint32_t shortcut_permille,
+                         uint32_t radius, uint64_t seed, uint32_t wlo, uint32_t whi);
+
+/* Replaces Engine::InitGraph + Engine::Start / StartPageRank
+ * (include/framework/framework.cuh:1803, :1963-2005, :2681) and the initial
+ * compute_hot_vertices/confirm_candidate_batch/LoadCache sequence
+ * (samples/hybrid_sssp/hybrid_sssp.cu:412-416): static solve on the GPU,
+ * then the first cache admission. */
+int dycg_init(dycg_engine *e);
+
+/* Replaces Engine::del_edge (include/framework/framework.cuh:2595-2618 ->
+ * update_tree_del :4811-4957): remove one occurrence per record, repair. */
+int dycg_delete_edges(dycg_engine *e, const dycg_edge *dels, size_t nd,
+                      dycg_batch_stats *stats);
+
+/* Replaces Engine::add_edge (include/framework/framework.cuh:2419 ->
+ * update_tree_add :3525-3756): append each record, repair. */
+int dycg_insert_edges(dycg_engine *e, const dycg_edge *adds, size_t na,
+                      dycg_batch_stats *stats);
+
+/* Replaces Engine::compute_hot_vertices_sssp + confirm_candidate_batch +
+ * CacheRefreshRequired + evication_cache + compact_cache + LoadCache
+ * (include/framework/framework.cuh:1264-1567, :2978-3061). */
+int dycg_cache_maintenance(dycg_engine *e, dycg_batch_stats *stats);
+
+/* One snapshot: all deletions, then all insertions (the reference's order,
+ * include/framework/topology_replay.h:71-72), one fused repair, then cache
+ * maintenance -- the unit the reference's batch timer measures
+ * (samples/hybrid_sssp/hybrid_sssp.cu:444-548). PR follows
+ * Engine::UpdatePageRank (include/framework/framework.cuh:2692-2736).
+ * Host arrays; the copies to the device are part of the call. */
+int dycg_apply_batch(dycg_engine *e, const dycg_edge *dels, size_t nd,
+                     const dycg_edge *adds, size_t na, dycg_batch_stats *stats);
+
+/* Same as dycg_apply_batch with the records already in device memory. */
+int dycg_apply_batch_device(dycg_engine *e, const dycg_edge *d_dels, size_t nd,
+                            const dycg_edge *d_adds, size_t na,
+                            dycg_batch_stats *stats);
+
+/* Replaces Engine::GatherValue/GatherParent (include/framework/framework.cuh:
+ * 4959-4984). values/parents: n entries each (either may be NULL). SSSP/BFS:
+ * distance/level, DYCG_INFINITY if unreachable; CC: label; parent is
+ * DYCG_INFINITY for roots and unreachable vertices. */
+int dycg_gather(dycg_engine *e, uint32_t *values, uint32_t *parents);
+
+/* PR: ranks x and residuals r (n floats each, either may be NULL). */
+int dycg_gather_ranks(dycg_engine *e, float *ranks, float *residuals);
+
+/* Current live row of v (outgoing, or incoming when incoming != 0), in slot
+ * order; *deg receives the live degree even when it exceeds cap. */
+int dycg_get_row(dycg_engine *e, uint32_t v, int incoming, uint32_t *dst,
+                 uint32_t *w, uint32_t cap, uint32_t *deg);
+
+/* Whole live outgoing adjacency as CSR (offsets n+1, dst/w live_edges). */
+int dycg_export_csr(dycg_engine *e, uint64_t *offsets, uint32_t *dst, uint32_t *w);
+
+int dycg_graph_info_get(dycg_engine *e, dycg_graph_info *info);
+
+/* Sample `count` distinct live edges uniformly (by occurrence) from the
+ * current outgoing adjacency, with their weights; deterministic in seed. */
+int dycg_sample_edges(dycg_engine *e, uint64_t count, uint64_t seed, dycg_edge *out);
+
+/* R-MAT edge draws (no de-duplication), computed on the host; identical to
+ * the draws dycg_load_graph_rmat makes for the same arguments at indices
+ * [first, first+count). Used for insertion batches. */
+int dycg_gen_rmat_edges(uint32_t scale, double a, double b, double c, uint64_t seed,
+                        uint64_t first, uint64_t count, uint32_t wlo, uint32_t whi,
+                        dycg_edge *out);
+
+/* Weight of edge (u,v) under the seeded uniform rule used by the loaders. */
+uint32_t dycg_hash_weight(uint64_t seed, uint32_t u, uint32_t v, uint32_t wlo,
+                          uint32_t whi);
+
+/* cudaStream_t the engine launches on (for CUDA-event timing by callers). */
+int dycg_stream(dycg_engine *e, void **stream);
+
+/* Copy of the last error message into buf (always NUL-terminated). */
+int dycg_last_error(dycg_engine *e, char *buf, size_t len);
+
+/* Library version string. */
+const char *dycg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DYCG_H */

@@ -1,0 +1,215 @@
+"""Generate the golden fixtures in tests/golden/ from the reference's own tests.
+
+Run in a container that has the reference checkout (default /root/reference):
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+What it records (all small JSON, committed):
+  smoke_bfs_sssp.json  -- the graph/update stream that tests/bfs_dynamic_smoke.py
+                          and tests/i22_ordered_insertion_test.py build, with
+                          per-phase distance checksums from that file's own
+                          oracle() (FIFO BFS and Dijkstra, weight (u+v)%128+1).
+  smoke_cc.json        -- tests/cc_dynamic_smoke.py's multigraph and 20 batches
+                          (6 random ones from its seed), checksums from its
+                          directed-reachability oracle().
+  smoke_pr.json        -- tests/pr_dynamic_smoke.py's graph and batches with the
+                          FP64 Jacobi ranks from its oracle().
+  pr_probe.json        -- paper/evaluation/audit_20261004/pr_probe: graph,
+                          updates, sizes and the FP64 reference ranks stored in
+                          its result.json.
+  topology_replay.json -- tests/fixtures/topology_replay_* with the output of
+                          the reference's topology_replay tool (built from the
+                          reference sources by oracle/Makefile).
+The reference is only read here; nothing at test time touches it.
+"""
+import argparse
+import importlib.util
+import json
+import os
+import random
+import re
+import subprocess
+import sys
+from collections import Counter
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent.parent
+
+
+def load_module(path, name):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def bfs_sssp_case(ref):
+    """The n=2048 stream of bfs_dynamic_smoke.py:59-77 (also i22:49-68)."""
+    mod = load_module(ref / "tests/bfs_dynamic_smoke.py", "ref_bfs_smoke")
+    n = 2048
+    edges = {(u, (u + 1) % n) for u in range(n)}
+    edges |= {(u, 1024) for u in range(1024)} | {(0, 0), (0, 2), (1, 3)}
+    graph = sorted(edges)
+    deleted = [(0, 1024), (20, 21), (700, 701), (1200, 1201)]
+    added = [(1, 1900), (500, 1700), (900, 2000), (3, 1500)]
+    batches, expect = [], {"bfs": [], "sssp": []}
+    for dels, adds in [(deleted, added), (added, deleted), (deleted, added)]:
+        for u, v in dels:
+            edges.remove((u, v))
+        for algo, weighted in (("bfs", False), ("sssp", True)):
+            expect[algo].append({"phase": "delete", "checksum": mod.oracle(edges, n, weighted)[1]})
+        for u, v in adds:
+            edges.add((u, v))
+        for algo, weighted in (("bfs", False), ("sssp", True)):
+            expect[algo].append({"phase": "batch", "checksum": mod.oracle(edges, n, weighted)[1]})
+        batches.append({"dels": [list(e) for e in dels], "adds": [list(e) for e in adds]})
+    final = {algo: mod.oracle(edges, n, algo == "sssp")[0] for algo in ("bfs", "sssp")}
+    return {"n": n, "source": 0, "graph": [list(e) for e in graph], "batches": batches,
+            "expected": expect, "final_values": final,
+            "origin": "tests/bfs_dynamic_smoke.py:59-77 oracle() :16-44"}
+
+
+def cc_case(ref):
+    """The n=256 multigraph and batches of cc_dynamic_smoke.py:58-88."""
+    mod = load_module(ref / "tests/cc_dynamic_smoke.py", "ref_cc_smoke")
+    nodes = 256
+    base = [(0, 0), (11, 11), (255, 255)]
+    base += [(0, 1), (1, 2), (2, 0), (2, 3), (3, 4), (4, 5), (5, 3)]
+    base += [(8, 9), (8, 9), (130, 140), (140, 150), (150, 130)]
+    base += [(u, u + 1) for u in range(160, 200)]
+    base += [(31, 30), (32, 30), (40, 41), (41, 42), (42, 41)]
+    base += [(0, 220), (220, 210), (210, 211), (211, 210)]
+    base += [(50, 51), (50, 52), (51, 53), (52, 53), (53, 54), (54, 53)]
+    base += [(60, 61), (60, 62), (61, 63), (62, 63), (63, 64), (64, 63)]
+    original = Counter(base)
+    graph = []
+    for (u, v), count in sorted(original.items()):
+        graph += [[u, v]] * count
+    batches = [([], []), ([(2, 3), (40, 41), (220, 210)], []), ([(0, 1)], []),
+               ([(8, 9)], []), ([(8, 9)], [(5, 8)]),
+               ([(3, 4), (3, 5)], [(2, 4), (9, 130)]),
+               ([(180, 181)], [(150, 190)]),
+               ([(210, 211), (11, 11)], [(10, 11)]),
+               ([], [(5, 8)]), ([(5, 8)], [(2, 3)])]
+    batches += [([(51, 53)], []), ([(50, 52), (61, 63), (62, 63)], []),
+                ([], [(49, 53)]), ([(49, 53)], [])]
+    rng = random.Random(20260923)
+    for _ in range(6):
+        batches.append(([(rng.randrange(nodes), rng.randrange(nodes)) for _ in range(8)],
+                        [(rng.randrange(nodes), rng.randrange(nodes)) for _ in range(8)]))
+    edges = original.copy()
+    expect, out = [], []
+    for deleted, added in batches:
+        for u, v in deleted:
+            edges[u, v] = max(0, edges[u, v] - 1)
+        expect.append({"phase": "delete", "checksum": mod.oracle(edges, nodes)[1]})
+        for u, v in added:
+            edges[u, v] += 1
+        expect.append({"phase": "batch", "checksum": mod.oracle(edges, nodes)[1]})
+        out.append({"dels": [list(e) for e in deleted], "adds": [list(e) for e in added]})
+    return {"n": nodes, "graph": graph, "batches": out, "expected": expect,
+            "final_labels": mod.oracle(edges, nodes)[0],
+            "origin": "tests/cc_dynamic_smoke.py:58-88 oracle() :17-41"}
+
+
+def pr_case(ref):
+    """The n=4096 graph and batches of pr_dynamic_smoke.py:44-64."""
+    mod = load_module(ref / "tests/pr_dynamic_smoke.py", "ref_pr_smoke")
+    n = 4096
+    base = [(0, 1), (1, 2), (2, 0), (3, 4), (4, 3), (8, 9), (8, 9), (10, 10), (n - 1, n - 1)]
+    base += [(20, v) for v in range(21, 1800)]
+    base += [(v, 20) for v in range(21, 1800)]
+    base += [(v, v + 1) for v in range(2000, 2020)]
+    original = Counter(base)
+    batches = [([], []), ([(2, 0)], []), ([], [(2, 3)]),
+               ([(3, 4)], [(3, 4)]), ([(8, 9)], []),
+               ([(8, 9), (10, 10)], [(9, 8)]),
+               ([(20, v) for v in range(21, 1800, 3)], [(20, 2000), (2020, 20)]),
+               ([(2000, 2001), (4000, 4001)], [(0, 8), (3, 10)]),
+               ([], [(10, 10), (10, 3), (8, 9), (8, 9)]),
+               ([(20, 2000), (2020, 20)], [(2000, 2001)])]
+    edges = original.copy()
+    out = []
+    for deleted, added in batches:
+        for u, v in deleted:
+            edges[u, v] = max(0, edges[u, v] - 1)
+        for u, v in added:
+            edges[u, v] += 1
+        out.append({"dels": [list(e) for e in deleted], "adds": [list(e) for e in added]})
+    return {"n": n, "graph": [list(e) for e in sorted(base)], "batches": out,
+            "initial_ranks": mod.oracle(original, n), "final_ranks": mod.oracle(edges, n),
+            "origin": "tests/pr_dynamic_smoke.py:44-64 oracle() :16-31"}
+
+
+def read_pairs(path):
+    rows = []
+    for line in Path(path).read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2:
+            rows.append([int(parts[0]), int(parts[1])])
+    return rows
+
+
+def read_updates(path):
+    rows = []
+    for line in Path(path).read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3:
+            rows.append([parts[0], int(parts[1]), int(parts[2])])
+    return rows
+
+
+def read_sizes(path):
+    return [[int(x) for x in line.split()[:2]] for line in Path(path).read_text().splitlines()
+            if line.strip()]
+
+
+def pr_probe_case(ref):
+    d = ref / "paper/evaluation/audit_20261004/pr_probe"
+    result = json.loads((d / "result.json").read_text())
+    return {"graph": read_pairs(d / "graph"), "updates": read_updates(d / "updates"),
+            "sizes": read_sizes(d / "sizes"), "reference_ranks": result["reference"],
+            "gpu_max_error": result["results"][0]["max_error"],
+            "origin": "paper/evaluation/audit_20261004/pr_probe (result.json 'reference')"}
+
+
+def topology_case(ref):
+    fx = ref / "tests/fixtures"
+    subprocess.run(["make", "-s", "-C", str(REPO / "oracle"), f"REF={ref}"], check=True)
+    tool = REPO / "oracle/_ref/topology_replay"
+    text = subprocess.run([str(tool), "--graph", str(fx / "topology_replay_graph.txt"),
+                           "--updates", str(fx / "topology_replay_updates.txt"),
+                           "--batch-sizes", str(fx / "topology_replay_batch_sizes.txt"),
+                           "--dump-sources"], check=True, capture_output=True, text=True).stdout
+    batches = [dict((k, int(v)) for k, v in re.findall(r"(\w+)=(\d+)", line))
+               for line in text.splitlines() if line.startswith("[TOPOLOGY-REPLAY-BATCH]")]
+    sources = [dict((k, int(v)) for k, v in re.findall(r"(\w+)=(\d+)", line))
+               for line in text.splitlines() if line.startswith("[TOPOLOGY-REPLAY-SOURCE]")]
+    return {"graph": read_pairs(fx / "topology_replay_graph.txt"),
+            "updates": read_updates(fx / "topology_replay_updates.txt"),
+            "sizes": read_sizes(fx / "topology_replay_batch_sizes.txt"),
+            "replay_batches": batches, "replay_sources": sources,
+            "ctest_regex": "batch=1 additions=1 deletions=1 touched_sources=2 changed_sources=1 "
+                           "missing_deletes=1 invalid_additions=0 graph_edges=6",
+            "origin": "tests/fixtures/topology_replay_*, CMakeLists.txt:134-145, "
+                      "src/topology_replay.cpp"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=os.environ.get("DYCG_REFERENCE", "/root/reference"))
+    args = ap.parse_args()
+    ref = Path(args.ref)
+    if not (ref / "tests/bfs_dynamic_smoke.py").exists():
+        sys.exit(f"reference checkout not found at {ref}")
+    cases = {"smoke_bfs_sssp.json": bfs_sssp_case(ref), "smoke_cc.json": cc_case(ref),
+             "smoke_pr.json": pr_case(ref), "pr_probe.json": pr_probe_case(ref),
+             "topology_replay.json": topology_case(ref)}
+    for name, data in cases.items():
+        (HERE / name).write_text(json.dumps(data, separators=(",", ":")) + "\n")
+        print(name, (HERE / name).stat().st_size, "bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,116 @@
+"""The CPU oracle against the reference's own golden vectors (no GPU)."""
+import numpy as np
+import pytest
+
+import oracle
+from tests import cases
+
+
+def _phase_checksums(algo, case):
+    n = case["n"]
+    off, dst, _ = cases.csr(n, case["graph"])
+    orc = oracle.Oracle(algo, n, off, dst, source=0)
+    orc.init()
+    out = []
+    for b in case["batches"]:
+        orc.delete_edges(cases.triples(b["dels"], algo))
+        out.append(("delete", oracle.checksum(orc.values()[0])))
+        orc.insert_edges(cases.triples(b["adds"], algo))
+        out.append(("batch", oracle.checksum(orc.values()[0])))
+    return out, orc
+
+
+@pytest.mark.parametrize("algo,name", [(oracle.BFS, "bfs"), (oracle.SSSP, "sssp")])
+def test_smoke_bfs_sssp_phase_checksums(algo, name):
+    case = cases.load("smoke_bfs_sssp.json")
+    got, orc = _phase_checksums(algo, case)
+    want = [(e["phase"], e["checksum"]) for e in case["expected"][name]]
+    assert got == want
+    vals, par = orc.values()
+    assert list(vals) == case["final_values"][name]
+    # parents are tight witnesses of existing edges
+    off, dst, _ = orc.csr()
+    for v in range(case["n"]):
+        if v == 0 or vals[v] == oracle.INF:
+            continue
+        p = int(par[v])
+        row = dst[int(off[p]):int(off[p + 1])]
+        assert v in row
+        assert vals[p] + cases.rule_w(algo, p, v) == vals[v]
+
+
+def test_smoke_cc_phase_checksums():
+    case = cases.load("smoke_cc.json")
+    got, orc = _phase_checksums(oracle.CC, case)
+    want = [(e["phase"], e["checksum"]) for e in case["expected"]]
+    assert got == want
+    assert list(orc.values()[0]) == case["final_labels"]
+
+
+def test_static_recompute_matches_golden():
+    case = cases.load("smoke_bfs_sssp.json")
+    n = case["n"]
+    edges = {tuple(e) for e in case["graph"]}
+    for b in case["batches"]:
+        edges -= {tuple(e) for e in b["dels"]}
+        edges |= {tuple(e) for e in b["adds"]}
+    off, dst, _ = cases.csr(n, sorted(edges))
+    assert list(oracle.static_bfs(n, off, dst, 0)) == case["final_values"]["bfs"]
+    assert list(oracle.static_sssp(n, off, dst, None, oracle.WEIGHT_HASH128, 0)) == \
+        case["final_values"]["sssp"]
+
+
+def test_pr_smoke_static_and_incremental():
+    case = cases.load("smoke_pr.json")
+    n = case["n"]
+    off, dst, _ = cases.csr(n, case["graph"])
+    x0 = oracle.static_pr(n, off, dst)
+    assert np.max(np.abs(x0 - np.array(case["initial_ranks"]))) < 1e-9
+    eps = 1e-9
+    orc = oracle.Oracle(oracle.PR, n, off, dst, epsilon=eps, max_rounds=100000)
+    orc.init()
+    for b in case["batches"]:
+        orc.apply_batch(cases.triples(b["dels"]), cases.triples(b["adds"]))
+    x, r = orc.ranks()
+    fin = np.array(case["final_ranks"])
+    # residual push leaves |r| <= eps per vertex: error <= sum|r| / (1 - alpha)
+    bound = np.sum(np.abs(r)) / 0.15 + 1e-9
+    assert np.max(np.abs(x - fin)) <= bound
+    sx = oracle.static_pr(n, *orc.csr()[:2])
+    assert np.max(np.abs(sx - fin)) < 1e-9
+
+
+def test_pr_probe_reference_ranks():
+    case = cases.load("pr_probe.json")
+    ref = np.array(case["reference_ranks"])
+    n = len(ref)
+    off, dst, _ = cases.csr(n, case["graph"])
+    batches = cases.replay_batches(case["updates"], case["sizes"])
+    orc = oracle.Oracle(oracle.PR, n, off, dst, epsilon=1e-10, max_rounds=100000)
+    orc.init()
+    for dels, adds in batches:
+        orc.apply_batch(cases.triples(dels), cases.triples(adds))
+    x, _ = orc.ranks()
+    assert np.max(np.abs(x - ref)) < 1e-8
+    off2, dst2, _ = orc.csr()
+    assert np.max(np.abs(oracle.static_pr(n, off2, dst2) - ref)) < 1e-9
+
+
+def test_topology_replay_fixture():
+    case = cases.load("topology_replay.json")
+    # n spans the update ids too (the replay model accepts dst 5)
+    n = 1 + max(max(max(e) for e in case["graph"]), max(max(u, v) for _, u, v in case["updates"]))
+    off, dst, _ = cases.csr(n, case["graph"])
+    orc = oracle.Oracle(oracle.SSSP, n, off, dst)
+    batches = cases.replay_batches(case["updates"], case["sizes"])
+    for bi, (dels, adds) in enumerate(batches):
+        orc.mutate(cases.triples(dels), cases.triples(adds))
+        st = orc.stats()
+        want = case["replay_batches"][bi]
+        assert st["missing_deletes"] == want["missing_deletes"]
+        assert orc.live_edges() == want["graph_edges"]
+        assert st["changed_sources"] == want["changed_sources"]
+        for s in case["replay_sources"]:
+            if s["batch"] == bi:
+                assert orc.row_degree(s["source"]) == s["after_degree"]
+                assert orc.row_multiset_hash(s["source"]) == s["multiset_hash"]

@@ -1,0 +1,153 @@
+// cache.cu -- HBM page cache: hotness scores, top-K admission, eviction and
+// page staging.
+//
+// Replaces the reference's per-vertex edge cache maintenance
+// (compute_hot_vertices_sssp / confirm_candidate_batch / evication_cache /
+// compact_cache / LoadCache, include/framework/framework.cuh:1264-1567,
+// :2978-3061; comp_hotness_sssp, include/framework/variants/driver.cuh:486-515;
+// cache_refresh_gate.h:9-31). The unit is a fixed-size page of the host arena
+// instead of a vertex row: a page's score is a decayed count of the slots the
+// kernels read from it (the reference sums four uint8 activity windows per
+// vertex); the resident set is the top-K pages by score (stable: ties go to
+// the smaller page id, as the reference's stable CUB sort does,
+// tests/hotness_pairing_test.cu:30-55); a refresh happens only when enough
+// top-K pages are missing (the refresh gate). Because every write goes to both
+// copies, eviction is a page-table update and compaction is never needed.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace dycg {
+
+__global__ void score_kernel(uint32_t *hits, float *score, uint32_t *ids, uint32_t npages,
+                             float decay) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npages;
+       p += gridDim.x * blockDim.x) {
+    score[p] = score[p] * decay + (float)hits[p];
+    hits[p] = 0;
+    ids[p] = p;
+  }
+}
+
+// flags in sorted (descending score) order: admit candidates among the top K,
+// eviction candidates among the rest.
+__global__ void flag_kernel(const uint32_t *ids, const float *sc, uint32_t npages, uint32_t K,
+                            const uint32_t *page_slot, uint32_t *fa, uint32_t *fe) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npages;
+       i += gridDim.x * blockDim.x) {
+    const bool top = i < K && sc[i] > 0.f;
+    const bool res = page_slot[ids[i]] != PAGE_NONE;
+    fa[i] = top && !res;
+    fe[i] = !top && res;
+  }
+}
+
+__global__ void evict_kernel(const uint32_t *ids, uint32_t npages, const uint32_t *fe,
+                             const uint32_t *se, uint32_t first_rank, uint32_t *page_slot,
+                             uint32_t *free_list, uint32_t free_base) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npages;
+       i += gridDim.x * blockDim.x) {
+    if (!fe[i] || se[i] < first_rank) continue;
+    const uint32_t p = ids[i];
+    free_list[free_base + (se[i] - first_rank)] = page_slot[p];
+    page_slot[p] = PAGE_NONE;
+  }
+}
+
+__global__ void admit_list_kernel(const uint32_t *ids, uint32_t npages, const uint32_t *fa,
+                                  const uint32_t *sa, uint32_t limit, uint32_t *admit) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npages;
+       i += gridDim.x * blockDim.x)
+    if (fa[i] && sa[i] < limit) admit[sa[i]] = ids[i];
+}
+
+// CTA per page: copy the page from the host arena into its cache slot with
+// 16-byte loads, then publish it in the page table.
+__global__ void fill_kernel(const uint32_t *admit, uint32_t count, const uint32_t *free_list,
+                            uint32_t free_top, uint32_t *page_slot, const uint32_t *h_out_dst,
+                            const uint32_t *h_out_w, const uint32_t *h_in_dst,
+                            const uint32_t *h_in_w, uint32_t pages_out, uint32_t page_shift,
+                            uint32_t *cdst, uint32_t *cw) {
+  for (uint32_t j = blockIdx.x; j < count; j += gridDim.x) {
+    const uint32_t p = admit[j];
+    const uint32_t slot = free_list[free_top - 1 - j];
+    const bool in_dir = p >= pages_out;
+    const u64 first = (u64)(in_dir ? p - pages_out : p) << page_shift;
+    const uint4 *sd = reinterpret_cast<const uint4 *>((in_dir ? h_in_dst : h_out_dst) + first);
+    const uint32_t *swp = in_dir ? h_in_w : h_out_w;
+    uint4 *dd = reinterpret_cast<uint4 *>(cdst + ((u64)slot << page_shift));
+    const uint32_t nv = (1u << page_shift) / 4;
+    for (uint32_t t = threadIdx.x; t < nv; t += blockDim.x) dd[t] = sd[t];
+    if (swp) {
+      const uint4 *sw = reinterpret_cast<const uint4 *>(swp + first);
+      uint4 *dw = reinterpret_cast<uint4 *>(cw + ((u64)slot << page_shift));
+      for (uint32_t t = threadIdx.x; t < nv; t += blockDim.x) dw[t] = sw[t];
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) page_slot[p] = slot;
+  }
+}
+
+static int grid_for(u64 threads) {
+  u64 b = (threads + BLOCK - 1) / BLOCK;
+  if (b < 1) b = 1;
+  if (b > 148ull * 32) b = 148ull * 32;
+  return (int)b;
+}
+
+cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay,
+                       const uint32_t *page_slot, cudaStream_t s) {
+  score_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.hits, W.score, W.ids, npages, decay);
+  size_t bytes = W.temp_bytes;
+  cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(
+      W.temp, bytes, W.score, W.score_sorted, W.ids, W.ids_sorted, (int)npages, 0, 32, s);
+  if (e != cudaSuccess) return e;
+  flag_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, W.score_sorted, npages, K,
+                                                 page_slot, W.fa, W.fe);
+  bytes = W.temp_bytes;
+  e = cub::DeviceScan::ExclusiveSum(W.temp, bytes, W.fa, W.sa, (int)npages, s);
+  if (e != cudaSuccess) return e;
+  bytes = W.temp_bytes;
+  e = cub::DeviceScan::ExclusiveSum(W.temp, bytes, W.fe, W.se, (int)npages, s);
+  if (e != cudaSuccess) return e;
+  // totals = last scan value + last flag
+  cudaMemcpyAsync(W.h_counts + 0, W.sa + npages - 1, 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(W.h_counts + 1, W.fa + npages - 1, 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(W.h_counts + 2, W.se + npages - 1, 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(W.h_counts + 3, W.fe + npages - 1, 4, cudaMemcpyDeviceToHost, s);
+  return cudaGetLastError();
+}
+
+size_t cache_temp_bytes(uint32_t npages) {
+  size_t a = 0, b = 0;
+  cub::DeviceRadixSort::SortPairsDescending(nullptr, a, (const float *)nullptr, (float *)nullptr,
+                                            (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                            (int)npages, 0, 32);
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                (int)npages);
+  return a > b ? a : b;
+}
+
+cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t n_evict_cand, uint32_t evict,
+                        uint32_t admit, uint32_t *page_slot, uint32_t *free_list,
+                        uint32_t free_count, const CachePages &pg, cudaStream_t s) {
+  if (evict) {
+    evict_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, npages, W.fe, W.se,
+                                                    n_evict_cand - evict, page_slot, free_list,
+                                                    free_count);
+  }
+  if (admit) {
+    admit_list_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, npages, W.fa, W.sa,
+                                                         admit, W.admit);
+    const uint32_t top = free_count + evict;
+    fill_kernel<<<(int)std::min<uint32_t>(admit, 148 * 8), BLOCK, 0, s>>>(
+        W.admit, admit, free_list, top, page_slot, pg.h_out_dst, pg.h_out_w, pg.h_in_dst,
+        pg.h_in_w, pg.pages_out, pg.page_shift, pg.cdst, pg.cw);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace dycg

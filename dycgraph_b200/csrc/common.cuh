@@ -1,0 +1,252 @@
+// common.cuh -- shared device types and helpers of the B200 delta-repair engine.
+//
+// Adjacency layout (one arena per direction, pinned + mapped host memory):
+//   dst[slot]  uint32 neighbour id; bit 31 set = deleted occurrence (tombstone)
+//   w[slot]    uint32 weight (only when weights are stored)
+// Each vertex owns a block [off, off+cap) of slots; [0,len) is in use, of which
+// [0,srt) is sorted by neighbour id (tombstones keep their id bits, so binary
+// search still works) and [srt,len) holds appended occurrences in insertion
+// order; live = occurrences in use minus tombstones.
+//
+// The arena is split into pages of 2^page_shift slots. page_slot[page] names
+// the HBM cache slot holding a copy of the page, or PAGE_NONE. Every write goes
+// to the host arena and, when the page is resident, to its cached copy, so the
+// host copy is always authoritative and eviction never writes back.
+//
+// Vertex state for SSSP/BFS/CC is one 64-bit key per vertex:
+//   key = (value << 32) | (parent + 1), parent field 0 = no parent.
+// atomicMin on the key keeps value and parent consistent and breaks ties
+// toward the smaller parent id.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dycg {
+
+typedef unsigned long long u64;
+
+constexpr uint32_t PAGE_NONE = 0xFFFFFFFFu;
+constexpr uint32_t TOMB = 0x80000000u;
+constexpr uint32_t VMASK = 0x7FFFFFFFu;
+constexpr uint32_t INF32 = 0xFFFFFFFFu;
+constexpr u64 KEY_INF = ~0ull;
+
+constexpr uint32_t ALGO_SSSP = 0, ALGO_BFS = 1, ALGO_CC = 2, ALGO_PR = 3;
+constexpr uint32_t WEIGHT_HASH128 = 0, WEIGHT_STORED = 1;
+
+// Rows longer than HEAVY are split into TILE-slot tiles processed by whole CTAs.
+constexpr uint32_t HEAVY = 1024;
+constexpr uint32_t TILE = 4096;
+constexpr int BLOCK = 256;
+
+// Error codes written to Ctl::err by device code (never trap).
+constexpr uint32_t ERR_BARRIER = 1;   // a grid barrier waited past its time limit
+constexpr uint32_t ERR_WAVES = 2;     // a closure exceeded its wave cap
+constexpr uint32_t ERR_TILES = 3;     // tile queue full
+constexpr uint32_t ERR_ARENA = 4;     // adjacency arena exhausted
+constexpr uint32_t ERR_QUEUE = 5;     // a vertex queue overflowed
+constexpr uint32_t ERR_NONFINITE = 6; // PR produced a non-finite value
+
+__host__ __device__ inline u64 pack_key(uint32_t value, uint32_t parent_plus1) {
+  return ((u64)value << 32) | parent_plus1;
+}
+__host__ __device__ inline uint32_t key_value(u64 k) { return (uint32_t)(k >> 32); }
+__host__ __device__ inline uint32_t key_parent1(u64 k) { return (uint32_t)k; }
+
+// SplitMix64 finalizer (Steele, Lea, Flood 2014): counter-based randomness for
+// the workload generators, identical on host and device.
+__host__ __device__ inline u64 mix64(u64 z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__host__ __device__ inline uint32_t hash_weight(u64 seed, uint32_t u, uint32_t v,
+                                                uint32_t wlo, uint32_t whi) {
+  u64 r = mix64(seed ^ mix64(((u64)u << 32) | v));
+  return wlo + (uint32_t)(r % (u64)(whi - wlo + 1));
+}
+
+// R-MAT draw number idx: quadrant a=(0,0) b=(0,1) c=(1,0) d=(1,1) per level,
+// three levels per 64-bit hash (21-bit uniform fields).
+__host__ __device__ inline void rmat_draw(u64 seed, u64 idx, uint32_t scale, uint32_t ta,
+                                          uint32_t tab, uint32_t tabc, uint32_t &u,
+                                          uint32_t &v) {
+  uint32_t uu = 0, vv = 0;
+  for (uint32_t level = 0; level < scale; level += 3) {
+    u64 r = mix64(seed ^ mix64(idx * 0x9E3779B97F4A7C15ull + level + 1));
+    for (uint32_t j = 0; j < 3 && level + j < scale; j++) {
+      uint32_t x = (uint32_t)(r >> (21 * j)) & ((1u << 21) - 1);
+      uint32_t bu = x >= tab;
+      uint32_t bv = (x >= ta && x < tab) || x >= tabc;
+      uu = (uu << 1) | bu;
+      vv = (vv << 1) | bv;
+    }
+  }
+  u = uu;
+  v = vv;
+}
+
+// Device view of one adjacency direction.
+struct Adj {
+  uint32_t *hdst;        // host arena (device-mapped pointer)
+  uint32_t *hw;          // host weights or nullptr
+  uint32_t *cdst;        // HBM page cache, slot-major (shared by both directions)
+  uint32_t *cw;          // cached weights or nullptr
+  const uint32_t *page_slot;
+  uint32_t *page_hits;   // per-page slot-access counters (hotness)
+  uint32_t page_base;    // global id of this arena's first page
+  uint32_t page_shift;
+  u64 *off;
+  uint32_t *len;
+  uint32_t *cap;
+  uint32_t *srt;
+  uint32_t *live;
+  u64 *top;              // arena bump pointer (slots)
+  u64 arena;             // arena size (slots)
+};
+
+// Per-launch control block in device memory: barrier, queues, counters.
+struct Ctl {
+  uint32_t bar_count;
+  uint32_t bar_gen;
+  uint32_t err;
+  uint32_t err_info;
+  uint32_t n_aff;        // affected list length
+  uint32_t q_count[2];   // wave queue lengths
+  uint32_t tile_count;
+  // snapshots taken by the last block to arrive at a barrier
+  uint32_t snap_aff;
+  uint32_t snap_q[2];
+  uint32_t snap_tiles;
+  uint32_t wave_tag;     // running wave tag (never reused)
+  uint32_t waves;        // waves run in this launch
+  uint32_t pad[2];
+  u64 stat[16];
+};
+
+enum StatIdx {
+  ST_LINK_BYTES = 0,
+  ST_HBM_ADJ_BYTES,
+  ST_STATE_BYTES,
+  ST_EXPANDED,
+  ST_SCANNED,
+  ST_IMPROVED,
+  ST_AFFECTED,
+  ST_MISSING,
+  ST_RELOCATED,
+  ST_INVALID,
+  ST_TOUCHED,
+  ST_PAGES_LOADED,
+  ST_PAGES_EVICTED,
+  ST_COUNT
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+__device__ __forceinline__ u64 globaltimer_ns() {
+  u64 t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Warp-aggregated append of `val` by the lanes with want=true. The calling
+// code keeps the warp converged (loops are warp-uniform).
+__device__ __forceinline__ bool warp_append(uint32_t *q, uint32_t *count, uint32_t cap,
+                                            bool want, uint32_t val, uint32_t *err) {
+  unsigned mask = __activemask();
+  unsigned m = __ballot_sync(mask, want);
+  if (!m) return true;
+  int leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if ((int)lane_id() == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+  base = __shfl_sync(mask, base, leader);
+  uint32_t rank = __popc(m & ((1u << lane_id()) - 1));
+  if (base + __popc(m) > cap) {
+    if ((int)lane_id() == leader) atomicExch(err, ERR_QUEUE);
+    return false;
+  }
+  if (want) q[base + rank] = val;
+  return true;
+}
+
+__device__ __forceinline__ u64 warp_sum(u64 x) {
+  for (int o = 16; o; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+  return x;
+}
+
+__device__ __forceinline__ u64 warp_min(u64 x) {
+  for (int o = 16; o; o >>= 1) {
+    u64 y = __shfl_down_sync(0xffffffffu, x, o);
+    x = y < x ? y : x;
+  }
+  return x;
+}
+
+// Slot address through the page table.
+__device__ __forceinline__ uint32_t page_of(const Adj &a, u64 p) {
+  return a.page_base + (uint32_t)(p >> a.page_shift);
+}
+
+__device__ __forceinline__ u64 cache_index(const Adj &a, uint32_t cslot, u64 p) {
+  return ((u64)cslot << a.page_shift) | (p & ((1ull << a.page_shift) - 1));
+}
+
+// Read dst (and optionally weight) of slot p; reports whether it came from HBM.
+__device__ __forceinline__ uint32_t read_dst(const Adj &a, u64 p, bool &cached) {
+  uint32_t cs = __ldg(a.page_slot + page_of(a, p));
+  cached = cs != PAGE_NONE;
+  return cached ? __ldg(a.cdst + cache_index(a, cs, p)) : __ldg(a.hdst + p);
+}
+
+__device__ __forceinline__ uint32_t read_w(const Adj &a, u64 p, bool cached) {
+  if (cached) {
+    uint32_t cs = __ldg(a.page_slot + page_of(a, p));
+    return __ldg(a.cw + cache_index(a, cs, p));
+  }
+  return __ldg(a.hw + p);
+}
+
+// Coherent read for kernels that also write the arena.
+__device__ __forceinline__ uint32_t read_dst_rw(const Adj &a, u64 p) {
+  uint32_t cs = a.page_slot[page_of(a, p)];
+  return cs != PAGE_NONE ? a.cdst[cache_index(a, cs, p)] : a.hdst[p];
+}
+
+__device__ __forceinline__ uint32_t read_w_rw(const Adj &a, u64 p) {
+  uint32_t cs = a.page_slot[page_of(a, p)];
+  return cs != PAGE_NONE ? a.cw[cache_index(a, cs, p)] : a.hw[p];
+}
+
+// Write-through store of one slot (host arena + resident cached copy).
+__device__ __forceinline__ bool write_slot(const Adj &a, u64 p, uint32_t d, uint32_t w,
+                                           bool with_w) {
+  uint32_t cs = a.page_slot[page_of(a, p)];
+  a.hdst[p] = d;
+  if (with_w) a.hw[p] = w;
+  if (cs != PAGE_NONE) {
+    u64 ci = cache_index(a, cs, p);
+    a.cdst[ci] = d;
+    if (with_w) a.cw[ci] = w;
+  }
+  return cs != PAGE_NONE;
+}
+
+__device__ __forceinline__ bool write_dst(const Adj &a, u64 p, uint32_t d) {
+  uint32_t cs = a.page_slot[page_of(a, p)];
+  a.hdst[p] = d;
+  if (cs != PAGE_NONE) a.cdst[cache_index(a, cs, p)] = d;
+  return cs != PAGE_NONE;
+}
+
+// Edge weight by algorithm: BFS 1, CC 0, SSSP stored or (u+v)%128+1
+// (the reference's TraversalEdgeWeight, include/framework/variants/api.cuh:26-28).
+template <uint32_t ALGO>
+__device__ __forceinline__ uint32_t rule_weight(uint32_t u, uint32_t v) {
+  if (ALGO == ALGO_BFS) return 1;
+  if (ALGO == ALGO_CC) return 0;
+  return (uint32_t)(((u64)u + v) % 128 + 1);
+}
+
+}  // namespace dycg

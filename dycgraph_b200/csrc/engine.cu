@@ -1,0 +1,939 @@
+// engine.cu -- host orchestration of the B200 delta-repair engine.
+//
+// The Engine mirrors the reference's sepgraph::engine::Engine
+// (include/framework/framework.cuh:780-6112) for one path: load a graph into
+// the paged pinned store, solve once, then per snapshot ingest + mutate +
+// repair + cache maintenance, all on one CUDA stream with one host
+// synchronisation at the end of a batch (two when the cache refreshes).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <unordered_set>
+
+#include "engine.h"
+
+namespace dycg {
+
+#define CK(x)                                                                              \
+  do {                                                                                     \
+    cudaError_t _e = (x);                                                                  \
+    if (_e != cudaSuccess)                                                                 \
+      throw Error(_e == cudaErrorMemoryAllocation ? DYCG_ENOMEM : DYCG_ECUDA,              \
+                  std::string(#x) + ": " + cudaGetErrorString(_e));                        \
+  } while (0)
+
+static u64 round_up(u64 x, u64 m) { return (x + m - 1) / m * m; }
+
+Engine::Engine(const dycg_options &opt) : opt_(opt) {
+  if (opt_.algo > DYCG_ALGO_PR) throw Error(DYCG_EINVAL, "unknown algorithm");
+  if (opt_.page_shift == 0) opt_.page_shift = 12;
+  if (opt_.page_shift < 8 || opt_.page_shift > 20) throw Error(DYCG_EINVAL, "page_shift out of range");
+  if (opt_.max_rounds == 0) opt_.max_rounds = 100;
+  if (!(opt_.alpha > 0.f && opt_.alpha < 1.f)) opt_.alpha = 0.85f;
+  page_shift_ = opt_.page_shift;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    throw Error(DYCG_ENOGPU, "no CUDA device available");
+  dev_ = opt_.device;
+  if (dev_ < 0 || dev_ >= ndev) throw Error(DYCG_EINVAL, "device ordinal out of range");
+  CK(cudaSetDevice(dev_));
+  CK(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev_));
+  int coop = 0;
+  CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev_));
+  if (!coop) throw Error(DYCG_ENOGPU, "device lacks cooperative launch");
+  CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  for (auto &e : ev_) CK(cudaEventCreate(&e));
+  stored_ = opt_.algo == DYCG_ALGO_SSSP && opt_.weight_mode == DYCG_WEIGHT_STORED;
+  has_in_ = !opt_.symmetric && opt_.algo != DYCG_ALGO_PR;
+}
+
+Engine::~Engine() {
+  if (st_) cudaStreamSynchronize(st_);
+  dfree_all();
+  for (void *p : hallocs_) cudaFreeHost(p);
+  for (auto &e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (st_) cudaStreamDestroy(st_);
+}
+
+void *Engine::dmalloc(size_t bytes) {
+  void *p = nullptr;
+  CK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+  dallocs_.push_back(p);
+  return p;
+}
+
+void Engine::dfree_all() {
+  for (void *p : dallocs_) cudaFree(p);
+  dallocs_.clear();
+  for (void *p : batch_allocs_) cudaFree(p);
+  batch_allocs_.clear();
+}
+
+void Engine::sync_check(const char *where) {
+  CK(cudaStreamSynchronize(st_));
+  CK(cudaGetLastError());
+  (void)where;
+}
+
+void Engine::check_loaded() const {
+  if (!loaded_) throw Error(DYCG_ESTATE, "no graph loaded");
+}
+
+Adj Engine::adj(const Arena &A) const {
+  Adj a;
+  a.hdst = A.d_dst;
+  a.hw = A.d_w;
+  a.cdst = cdst_;
+  a.cw = cw_;
+  a.page_slot = page_slot_;
+  a.page_hits = page_hits_;
+  a.page_base = A.page_base;
+  a.page_shift = page_shift_;
+  a.off = A.off;
+  a.len = A.len;
+  a.cap = A.cap;
+  a.srt = A.srt;
+  a.live = A.live;
+  a.top = A.top;
+  a.arena = A.slots;
+  return a;
+}
+
+// ---- graph construction ---------------------------------------------------
+
+// keys: sorted (row << 32 | neighbour), m of them, no KEY_INF among them.
+void Engine::build_direction(Arena &A, const u64 *keys, const uint32_t *wv, u64 m,
+                             bool weight_from_hash, u64 wseed, uint32_t wlo, uint32_t whi,
+                             bool swapped) {
+  const uint32_t n = n_;
+  uint32_t *deg = (uint32_t *)dmalloc((n + 1ull) * 4);
+  u64 *cap64 = (u64 *)dmalloc((n + 1ull) * 8);
+  u64 *rowstart = (u64 *)dmalloc((n + 1ull) * 8);
+  CK(cudaMemsetAsync(deg, 0, (n + 1ull) * 4, st_));
+  CK(cudaMemsetAsync(cap64, 0, (n + 1ull) * 8, st_));
+  A.off = (u64 *)dmalloc((n + 1ull) * 8);
+  A.len = (uint32_t *)dmalloc((n + 1ull) * 4);
+  A.cap = (uint32_t *)dmalloc((n + 1ull) * 4);
+  A.srt = (uint32_t *)dmalloc((n + 1ull) * 4);
+  A.live = (uint32_t *)dmalloc((n + 1ull) * 4);
+  A.top = (u64 *)dmalloc(8);
+  CK(build_degrees(keys, m, deg, st_));
+  CK(build_caps(deg, n, cap64, A.cap, A.len, A.srt, A.live, st_));
+  size_t tb = 0;
+  CK(build_scan_u64(nullptr, tb, cap64, A.off, n + 1ull, st_));
+  size_t tb2 = 0;
+  CK(build_scan_u32_to_u64(nullptr, tb2, deg, rowstart, n + 1ull, st_));
+  void *temp = dmalloc(std::max(tb, tb2));
+  CK(build_scan_u64(temp, tb, cap64, A.off, n + 1ull, st_));
+  CK(build_scan_u32_to_u64(temp, tb2, deg, rowstart, n + 1ull, st_));
+  u64 total = 0;
+  CK(cudaMemcpyAsync(&total, A.off + n, 8, cudaMemcpyDeviceToHost, st_));
+  sync_check("layout");
+  const u64 page = 1ull << page_shift_;
+  const u64 head = std::max<u64>(total / 8, 1ull << 20);
+  A.slots = round_up(total + head, page);
+  A.pages = (uint32_t)(A.slots >> page_shift_);
+  void *hd = nullptr;
+  CK(cudaHostAlloc(&hd, A.slots * 4, cudaHostAllocMapped | cudaHostAllocPortable));
+  hallocs_.push_back(hd);
+  A.h_dst = (uint32_t *)hd;
+  CK(cudaHostGetDevicePointer((void **)&A.d_dst, hd, 0));
+  if (stored_) {
+    void *hw = nullptr;
+    CK(cudaHostAlloc(&hw, A.slots * 4, cudaHostAllocMapped | cudaHostAllocPortable));
+    hallocs_.push_back(hw);
+    A.h_w = (uint32_t *)hw;
+    CK(cudaHostGetDevicePointer((void **)&A.d_w, hw, 0));
+  }
+  CK(cudaMemcpyAsync(A.top, &total, 8, cudaMemcpyHostToDevice, st_));
+  CK(build_scatter(keys, wv, m, A.off, rowstart, A.d_dst, A.d_w, wseed, wlo, whi,
+                   weight_from_hash ? 1 : 0, swapped ? 1 : 0, st_));
+  sync_check("scatter");
+  // free the temporaries (they are the last allocations made)
+  for (void *p : {temp, (void *)rowstart, (void *)cap64, (void *)deg}) {
+    auto it = std::find(dallocs_.begin(), dallocs_.end(), p);
+    if (it != dallocs_.end()) dallocs_.erase(it);
+    cudaFree(p);
+  }
+}
+
+// keys/wv: device arrays holding m sorted out-keys (and weights); scratch
+// buffers of the same size are used to build the incoming direction.
+void Engine::build_from_sorted_keys(u64 *keys, uint32_t *wv, u64 m, bool weight_from_hash,
+                                    u64 wseed, uint32_t wlo, uint32_t whi, u64 *scratch_keys,
+                                    uint32_t *scratch_w) {
+  build_direction(out_, keys, wv, m, weight_from_hash, wseed, wlo, whi, false);
+  if (has_in_) {
+    CK(build_swap_keys(keys, scratch_keys, m, st_));
+    size_t tb = 0;
+    CK(build_sort(nullptr, tb, scratch_keys, keys, wv ? wv : nullptr, wv ? scratch_w : nullptr, m,
+                  st_));
+    void *temp = nullptr;
+    CK(cudaMalloc(&temp, std::max<size_t>(tb, 16)));
+    // wv holds the weights in out-key order; sort them along with the swapped keys
+    cudaError_t e = build_sort(temp, tb, scratch_keys, keys, wv ? wv : nullptr,
+                               wv ? scratch_w : nullptr, m, st_);
+    cudaStreamSynchronize(st_);
+    cudaFree(temp);
+    CK(e);
+    build_direction(in_, keys, wv ? scratch_w : nullptr, m, weight_from_hash, wseed, wlo, whi,
+                    true);
+    in_.page_base = out_.pages;
+  }
+  finish_load();
+}
+
+void Engine::finish_load() {
+  const uint32_t n = n_;
+  npages_ = out_.pages + (has_in_ ? in_.pages : 0);
+  page_slot_ = (uint32_t *)dmalloc((u64)npages_ * 4);
+  page_hits_ = (uint32_t *)dmalloc((u64)npages_ * 4);
+  CK(cudaMemsetAsync(page_slot_, 0xFF, (u64)npages_ * 4, st_));
+  CK(cudaMemsetAsync(page_hits_, 0, (u64)npages_ * 4, st_));
+  const u64 page_bytes = (4ull << page_shift_) * (stored_ ? 2 : 1);
+  u64 slots = opt_.cache_policy == DYCG_CACHE_NONE ? 0 : opt_.hbm_graph_budget_bytes / page_bytes;
+  slots = std::min<u64>(slots, npages_);
+  cache_slots_ = (uint32_t)slots;
+  if (cache_slots_) {
+    cdst_ = (uint32_t *)dmalloc(((u64)cache_slots_ << page_shift_) * 4);
+    if (stored_) cw_ = (uint32_t *)dmalloc(((u64)cache_slots_ << page_shift_) * 4);
+    free_list_ = (uint32_t *)dmalloc((u64)cache_slots_ * 4);
+    std::vector<uint32_t> fl(cache_slots_);
+    for (uint32_t i = 0; i < cache_slots_; i++) fl[i] = cache_slots_ - 1 - i;
+    CK(cudaMemcpyAsync(free_list_, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice, st_));
+    free_count_ = cache_slots_;
+    cwk_.hits = page_hits_;
+    cwk_.score = (float *)dmalloc((u64)npages_ * 4);
+    cwk_.score_sorted = (float *)dmalloc((u64)npages_ * 4);
+    cwk_.ids = (uint32_t *)dmalloc((u64)npages_ * 4);
+    cwk_.ids_sorted = (uint32_t *)dmalloc((u64)npages_ * 4);
+    cwk_.fa = (uint32_t *)dmalloc((u64)npages_ * 4);
+    cwk_.fe = (uint32_t *)dmalloc((u64)npages_ * 4);
+    cwk_.sa = (uint32_t *)dmalloc((u64)npages_ * 4);
+    cwk_.se = (uint32_t *)dmalloc((u64)npages_ * 4);
+    cwk_.admit = (uint32_t *)dmalloc((u64)npages_ * 4);
+    CK(cudaMemsetAsync(cwk_.score, 0, (u64)npages_ * 4, st_));
+    cwk_.temp_bytes = cache_temp_bytes(npages_);
+    cwk_.temp = dmalloc(cwk_.temp_bytes);
+    void *hc = nullptr;
+    CK(cudaHostAlloc(&hc, 64, cudaHostAllocDefault));
+    hallocs_.push_back(hc);
+    cwk_.h_counts = (uint32_t *)hc;
+  }
+  // vertex state
+  key_ = (u64 *)dmalloc((n + 1ull) * 8);
+  mark_ = (uint32_t *)dmalloc((n + 1ull) * 4);
+  wtag_ = (uint32_t *)dmalloc((n + 1ull) * 4);
+  touch_ = (uint32_t *)dmalloc((n + 1ull) * 4);
+  aff_ = (uint32_t *)dmalloc((n + 1ull) * 4);
+  q0_ = (uint32_t *)dmalloc((n + 1ull) * 4);
+  q1_ = (uint32_t *)dmalloc((n + 1ull) * 4);
+  CK(cudaMemsetAsync(mark_, 0, (n + 1ull) * 4, st_));
+  CK(cudaMemsetAsync(wtag_, 0, (n + 1ull) * 4, st_));
+  CK(cudaMemsetAsync(touch_, 0, (n + 1ull) * 4, st_));
+  const u64 maxslots = std::max(out_.slots, in_.slots);
+  const u64 tcap = maxslots / TILE + maxslots / HEAVY + 4096;
+  tile_cap_ = (uint32_t)std::min<u64>(tcap, 0x7FFFFFFFull);
+  tiles_ = (uint4 *)dmalloc((u64)tile_cap_ * sizeof(uint4));
+  ctl_ = (Ctl *)dmalloc(sizeof(Ctl));
+  void *hc = nullptr;
+  CK(cudaHostAlloc(&hc, sizeof(Ctl), cudaHostAllocDefault));
+  hallocs_.push_back(hc);
+  h_ctl_ = (Ctl *)hc;
+  if (opt_.algo == DYCG_ALGO_PR) {
+    x_ = (float *)dmalloc((n + 1ull) * 4);
+    r_ = (float *)dmalloc((n + 1ull) * 4);
+    delta_ = (float *)dmalloc((n + 1ull) * 4);
+    queued_ = (uint32_t *)dmalloc((n + 1ull) * 4);
+    CK(cudaMemsetAsync(delta_, 0, (n + 1ull) * 4, st_));
+  }
+  sync_check("state");
+  loaded_ = true;
+}
+
+void Engine::load_csr(uint32_t n, const uint64_t *off, const uint32_t *dst, const uint32_t *w) {
+  if (loaded_) throw Error(DYCG_ESTATE, "graph already loaded");
+  if (n == 0 || n >= 0x7FFFFFFFu) throw Error(DYCG_EINVAL, "vertex count out of range");
+  if (!off || (!dst && off[n] != 0)) throw Error(DYCG_EINVAL, "null CSR array");
+  n_ = n;
+  const u64 m = off[n];
+  for (u64 e = 0; e < m; e++)
+    if (dst[e] >= n) throw Error(DYCG_EINVAL, "CSR neighbour id out of range");
+  const bool with_w = stored_;
+  u64 *d_off = nullptr;
+  uint32_t *d_dst = nullptr, *d_w = nullptr, *d_w2 = nullptr;
+  u64 *k1 = nullptr, *k2 = nullptr;
+  CK(cudaMalloc(&d_off, (n + 1ull) * 8));
+  CK(cudaMalloc(&d_dst, std::max<u64>(m, 1) * 4));
+  CK(cudaMalloc(&k1, std::max<u64>(m, 1) * 8));
+  CK(cudaMalloc(&k2, std::max<u64>(m, 1) * 8));
+  CK(cudaMemcpyAsync(d_off, off, (n + 1ull) * 8, cudaMemcpyHostToDevice, st_));
+  if (m) CK(cudaMemcpyAsync(d_dst, dst, m * 4, cudaMemcpyHostToDevice, st_));
+  if (with_w) {
+    CK(cudaMalloc(&d_w, std::max<u64>(m, 1) * 4));
+    CK(cudaMalloc(&d_w2, std::max<u64>(m, 1) * 4));
+    if (w && m) {
+      CK(cudaMemcpyAsync(d_w, w, m * 4, cudaMemcpyHostToDevice, st_));
+    } else {
+      std::vector<uint32_t> ones(std::max<u64>(m, 1), 1u);
+      CK(cudaMemcpyAsync(d_w, ones.data(), m * 4, cudaMemcpyHostToDevice, st_));
+      sync_check("ones");
+    }
+  }
+  CK(build_csr_keys(d_off, d_dst, n, k1, st_));
+  size_t tb = 0;
+  CK(build_sort(nullptr, tb, k1, k2, with_w ? d_w : nullptr, with_w ? d_w2 : nullptr, m, st_));
+  void *temp = nullptr;
+  CK(cudaMalloc(&temp, std::max<size_t>(tb, 16)));
+  CK(build_sort(temp, tb, k1, k2, with_w ? d_w : nullptr, with_w ? d_w2 : nullptr, m, st_));
+  sync_check("csr sort");
+  cudaFree(temp);
+  cudaFree(d_off);
+  cudaFree(d_dst);
+  // k2 / d_w2: sorted keys and weights; k1 / d_w are free for scratch
+  build_from_sorted_keys(k2, with_w ? d_w2 : nullptr, m, false, 0, 1, 1, k1, d_w);
+  cudaFree(k1);
+  cudaFree(k2);
+  if (d_w) cudaFree(d_w);
+  if (d_w2) cudaFree(d_w2);
+}
+
+void Engine::load_file(const char *path, uint32_t min_nodes, int weighted) {
+  std::ifstream in(path);
+  if (!in) throw Error(DYCG_EIO, std::string("cannot open graph file ") + path);
+  std::vector<uint32_t> us, vs, ws;
+  std::string line;
+  uint64_t maxid = 0;
+  while (std::getline(in, line)) {
+    if (line.empty() || line[0] == '#' || line[0] == '%') continue;
+    std::istringstream ss(line);
+    uint64_t u, v, w = 1;
+    if (!(ss >> u >> v)) continue;
+    if (weighted && !(ss >> w)) w = 1;
+    if (u >= 0x7FFFFFFFull || v >= 0x7FFFFFFFull) throw Error(DYCG_EIO, "vertex id too large");
+    us.push_back((uint32_t)u);
+    vs.push_back((uint32_t)v);
+    ws.push_back((uint32_t)w);
+    maxid = std::max(maxid, std::max(u, v));
+  }
+  const uint32_t n = std::max<uint32_t>(us.empty() ? 1u : (uint32_t)(maxid + 1), min_nodes);
+  std::vector<uint64_t> off(n + 1ull, 0);
+  for (uint32_t u : us) off[u + 1]++;
+  for (uint32_t v = 0; v < n; v++) off[v + 1] += off[v];
+  std::vector<uint32_t> dst(us.size() + 1), wt(us.size() + 1);
+  std::vector<uint64_t> fill(off.begin(), off.end() - 1);
+  for (size_t i = 0; i < us.size(); i++) {
+    const uint64_t p = fill[us[i]]++;
+    dst[p] = vs[i];
+    wt[p] = ws[i];
+  }
+  load_csr(n, off.data(), dst.data(), weighted ? wt.data() : nullptr);
+}
+
+void Engine::load_rmat(uint32_t scale, uint32_t ef, double a, double b, double c, uint64_t seed,
+                       uint32_t wlo, uint32_t whi, int symmetrize) {
+  if (loaded_) throw Error(DYCG_ESTATE, "graph already loaded");
+  if (scale < 1 || scale > 30 || ef == 0) throw Error(DYCG_EINVAL, "bad R-MAT size");
+  if (!(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0)) throw Error(DYCG_EINVAL, "bad R-MAT probabilities");
+  if (wlo == 0 || whi < wlo) throw Error(DYCG_EINVAL, "bad weight range");
+  n_ = 1u << scale;
+  const u64 draws = (u64)ef << scale;
+  const u64 total = draws * (symmetrize ? 2 : 1);
+  u64 *k1 = nullptr, *k2 = nullptr;
+  uint32_t *flag = nullptr;
+  u64 *pos = nullptr;
+  CK(cudaMalloc(&k1, total * 8));
+  CK(cudaMalloc(&k2, total * 8));
+  CK(build_gen_rmat(k1, draws, seed, scale, a, b, c, symmetrize, st_));
+  size_t tb = build_temp_bytes(total, false);
+  void *temp = nullptr;
+  CK(cudaMalloc(&temp, std::max<size_t>(tb, 16)));
+  CK(build_sort(temp, tb, k1, k2, nullptr, nullptr, total, st_));
+  CK(cudaMalloc(&flag, total * 4));
+  CK(cudaMalloc(&pos, total * 8));
+  CK(build_unique(k2, nullptr, total, 1, flag, pos, k1, nullptr, temp, tb, st_));
+  u64 last_pos = 0;
+  uint32_t last_flag = 0;
+  CK(cudaMemcpyAsync(&last_pos, pos + total - 1, 8, cudaMemcpyDeviceToHost, st_));
+  CK(cudaMemcpyAsync(&last_flag, flag + total - 1, 4, cudaMemcpyDeviceToHost, st_));
+  sync_check("rmat unique");
+  const u64 m = last_pos + last_flag;
+  cudaFree(flag);
+  cudaFree(pos);
+  cudaFree(temp);
+  build_from_sorted_keys(k1, nullptr, m, stored_, seed ^ 0x5745494748545321ull, wlo, whi, k2,
+                         nullptr);
+  cudaFree(k1);
+  cudaFree(k2);
+}
+
+void Engine::load_grid(uint32_t side, uint32_t permille, uint32_t radius, uint64_t seed,
+                       uint32_t wlo, uint32_t whi) {
+  if (loaded_) throw Error(DYCG_ESTATE, "graph already loaded");
+  if (side < 2 || (u64)side * side >= 0x7FFFFFFFull || radius == 0)
+    throw Error(DYCG_EINVAL, "bad grid size");
+  if (wlo == 0 || whi < wlo) throw Error(DYCG_EINVAL, "bad weight range");
+  n_ = side * side;
+  const u64 nshort = (u64)n_ * permille / 1000;
+  const u64 total = (u64)n_ * 4 + nshort * 2;
+  u64 *k1 = nullptr, *k2 = nullptr, *pos = nullptr;
+  uint32_t *flag = nullptr;
+  CK(cudaMalloc(&k1, total * 8));
+  CK(cudaMalloc(&k2, total * 8));
+  CK(build_gen_grid(k1, side, nshort, radius, seed, st_));
+  size_t tb = build_temp_bytes(total, false);
+  void *temp = nullptr;
+  CK(cudaMalloc(&temp, std::max<size_t>(tb, 16)));
+  CK(build_sort(temp, tb, k1, k2, nullptr, nullptr, total, st_));
+  CK(cudaMalloc(&flag, total * 4));
+  CK(cudaMalloc(&pos, total * 8));
+  CK(build_unique(k2, nullptr, total, 1, flag, pos, k1, nullptr, temp, tb, st_));
+  u64 last_pos = 0;
+  uint32_t last_flag = 0;
+  CK(cudaMemcpyAsync(&last_pos, pos + total - 1, 8, cudaMemcpyDeviceToHost, st_));
+  CK(cudaMemcpyAsync(&last_flag, flag + total - 1, 4, cudaMemcpyDeviceToHost, st_));
+  sync_check("grid unique");
+  const u64 m = last_pos + last_flag;
+  cudaFree(flag);
+  cudaFree(pos);
+  cudaFree(temp);
+  build_from_sorted_keys(k1, nullptr, m, stored_, seed ^ 0x5745494748545321ull, wlo, whi, k2,
+                         nullptr);
+  cudaFree(k1);
+  cudaFree(k2);
+}
+
+// ---- solve / batches -------------------------------------------------------
+
+void Engine::init() {
+  check_loaded();
+  CK(cudaMemsetAsync(ctl_, 0, sizeof(Ctl), st_));
+  const u64 timeout = 120ull * 1000000000ull;
+  if (opt_.algo == DYCG_ALGO_PR) {
+    CK(launch_pr_init(x_, r_, queued_, q0_, n_, 1.f - opt_.alpha, ctl_, st_));
+    PrLaunch L{};
+    L.out = adj(out_);
+    L.x = x_;
+    L.r = r_;
+    L.delta = delta_;
+    L.queued = queued_;
+    L.q0 = q0_;
+    L.q1 = q1_;
+    L.sources = touched_ ? touched_ : q0_;
+    L.n_sources = counts_ ? counts_ + 4 : nullptr;
+    L.tiles = tiles_;
+    L.tile_cap = tile_cap_;
+    L.ctl = ctl_;
+    L.n = n_;
+    L.cur = 0;
+    L.phases = PR_CONVERGE;
+    L.sign = 1.f;
+    L.eps = opt_.epsilon;
+    L.alpha = opt_.alpha;
+    L.max_rounds = opt_.max_rounds;
+    L.timeout_ns = timeout;
+    L.num_sms = num_sms_;
+    CK(launch_pr(L, st_));
+    launches_ += 2;
+  } else {
+    CK(launch_init_state(opt_.algo, key_, n_, opt_.source, q0_, ctl_, st_));
+    RepairLaunch L{};
+    L.out = adj(out_);
+    L.in = has_in_ ? adj(in_) : adj(out_);
+    L.key = key_;
+    L.mark = mark_;
+    L.wtag = wtag_;
+    L.aff = aff_;
+    L.q0 = q0_;
+    L.q1 = q1_;
+    L.tiles = tiles_;
+    L.tile_cap = tile_cap_;
+    L.ctl = ctl_;
+    L.n = n_;
+    L.source = opt_.source;
+    L.epoch = ++epoch_;
+    L.tag_base = tag_base_;
+    L.phases = PH_CLOSE;
+    L.max_waves = (uint32_t)std::min<u64>(4ull * n_ + 1024, 0x7FFFFFFFull);
+    L.timeout_ns = timeout;
+    L.algo = opt_.algo;
+    L.stored = stored_;
+    L.num_sms = num_sms_;
+    CK(launch_repair(L, st_));
+    launches_ += 2;
+  }
+  CK(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
+  sync_check("init");
+  if (h_ctl_->err) {
+    failed = true;
+    throw Error(h_ctl_->err == ERR_WAVES || h_ctl_->err == ERR_BARRIER ? DYCG_ELIMIT : DYCG_ECAPACITY,
+                "static solve failed on the device (error code " + std::to_string(h_ctl_->err) + ")");
+  }
+  tag_base_ += h_ctl_->waves + 2;
+  if (opt_.algo == DYCG_ALGO_PR) {
+    pr_cur_ = h_ctl_->pad[0];
+    pr_count_ = h_ctl_->pad[1];
+  }
+  inited_ = true;
+  cache_maintenance(true, nullptr);
+}
+
+void Engine::ensure_batch(size_t cnt) {
+  if (cnt <= bcap_) return;
+  for (void *p : batch_allocs_) cudaFree(p);
+  batch_allocs_.clear();
+  size_t c = std::max<size_t>(cnt, 1024);
+  c = std::max(c, bcap_ * 2);
+  auto al = [&](size_t bytes) {
+    void *p = nullptr;
+    CK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+    batch_allocs_.push_back(p);
+    return p;
+  };
+  k_tmp_out_ = (u64 *)al(c * 8);
+  k_tmp_in_ = (u64 *)al(c * 8);
+  k_del_out_ = (u64 *)al(c * 8);
+  k_del_in_ = (u64 *)al(c * 8);
+  k_add_out_ = (u64 *)al(c * 8);
+  k_add_in_ = (u64 *)al(c * 8);
+  w_tmp_ = (uint32_t *)al(c * 4);
+  w_add_out_ = (uint32_t *)al(c * 4);
+  w_add_in_ = (uint32_t *)al(c * 4);
+  uv_out_ = (uint2 *)al(c * 8);
+  uv_in_ = (uint2 *)al(c * 8);
+  mult_out_ = (uint32_t *)al(c * 4);
+  mult_in_ = (uint32_t *)al(c * 4);
+  found_out_ = (uint32_t *)al(c * 4);
+  seg_out_ = (uint3 *)al(c * 12);
+  seg_in_ = (uint3 *)al(c * 12);
+  add_uvw_ = (uint3 *)al(c * 12);
+  touched_ = (uint32_t *)al(c * 2 * 4);
+  counts_ = (uint32_t *)al(64);
+  d_edges_ = (dycg_edge_dev *)al(c * 2 * sizeof(dycg_edge_dev));
+  size_t a = 0, b = 0;
+  CK(sort_keys(nullptr, a, k_tmp_out_, k_del_out_, (uint32_t)c, st_));
+  CK(sort_pairs(nullptr, b, k_tmp_out_, k_add_out_, w_tmp_, w_add_out_, (uint32_t)c, st_));
+  cub_bytes_ = std::max(a, b);
+  cub_temp_ = al(cub_bytes_);
+  if (h_stage_) {
+    cudaFreeHost(h_stage_);
+    hallocs_.erase(std::find(hallocs_.begin(), hallocs_.end(), (void *)h_stage_));
+  }
+  void *hs = nullptr;
+  CK(cudaHostAlloc(&hs, c * 2 * sizeof(dycg_edge), cudaHostAllocDefault));
+  hallocs_.push_back(hs);
+  h_stage_ = (dycg_edge *)hs;
+  bcap_ = c;
+}
+
+void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na,
+                   bool device_ptrs, int mode, bool maintenance, dycg_batch_stats *stats) {
+  check_loaded();
+  if (!inited_) throw Error(DYCG_ESTATE, "dycg_init must run before batches");
+  if (failed) throw Error(DYCG_ESTATE, "engine is in a failed state");
+  if ((nd && !dels) || (na && !adds)) throw Error(DYCG_EINVAL, "null update array");
+  if (nd > 0x3FFFFFFFull || na > 0x3FFFFFFFull) throw Error(DYCG_EINVAL, "batch too large");
+  if (mode == 1) na = 0;
+  if (mode == 2) nd = 0;
+  ensure_batch(std::max(nd, na));
+  const uint64_t l0 = launches_;
+  CK(cudaEventRecord(ev_[0], st_));
+  const dycg_edge_dev *d_dels = (const dycg_edge_dev *)dels;
+  const dycg_edge_dev *d_adds = (const dycg_edge_dev *)adds;
+  if (!device_ptrs) {
+    if (nd) std::memcpy(h_stage_, dels, nd * sizeof(dycg_edge));
+    if (na) std::memcpy(h_stage_ + nd, adds, na * sizeof(dycg_edge));
+    if (nd + na)
+      CK(cudaMemcpyAsync(d_edges_, h_stage_, (nd + na) * sizeof(dycg_edge),
+                         cudaMemcpyHostToDevice, st_));
+    d_dels = d_edges_;
+    d_adds = d_edges_ + nd;
+  }
+  CK(cudaMemsetAsync(ctl_, 0, sizeof(Ctl), st_));
+  CK(cudaMemsetAsync(counts_, 0, 64, st_));
+  if (opt_.algo == DYCG_ALGO_PR) {
+    // carried frontier length
+    h_ctl_->q_count[pr_cur_] = pr_count_;
+    CK(cudaMemcpyAsync(&ctl_->q_count[pr_cur_], &h_ctl_->q_count[pr_cur_], 4,
+                       cudaMemcpyHostToDevice, st_));
+  }
+  launches_ += 2;
+  // ---- ingest
+  u64 *invalid = &ctl_->stat[ST_INVALID];
+  size_t tb = cub_bytes_;
+  if (nd) {
+    CK(launch_prep_keys(d_dels, (uint32_t)nd, n_, k_tmp_out_, has_in_ ? k_tmp_in_ : nullptr,
+                        nullptr, invalid, st_));
+    CK(sort_keys(cub_temp_, tb, k_tmp_out_, k_del_out_, (uint32_t)nd, st_));
+    CK(launch_unique_runs(k_del_out_, (uint32_t)nd, uv_out_, mult_out_, counts_ + 0,
+                          (uint32_t)bcap_, &ctl_->err, st_));
+    launches_ += 3;
+    if (has_in_) {
+      tb = cub_bytes_;
+      CK(sort_keys(cub_temp_, tb, k_tmp_in_, k_del_in_, (uint32_t)nd, st_));
+      CK(launch_unique_runs(k_del_in_, (uint32_t)nd, uv_in_, mult_in_, counts_ + 1,
+                            (uint32_t)bcap_, &ctl_->err, st_));
+      launches_ += 2;
+    }
+  }
+  if (na) {
+    tb = cub_bytes_;
+    CK(launch_prep_keys(d_adds, (uint32_t)na, n_, k_tmp_out_, has_in_ ? k_tmp_in_ : nullptr,
+                        w_tmp_, invalid, st_));
+    CK(sort_pairs(cub_temp_, tb, k_tmp_out_, k_add_out_, w_tmp_, w_add_out_, (uint32_t)na, st_));
+    CK(launch_row_segments(k_add_out_, (uint32_t)na, seg_out_, counts_ + 2, st_));
+    CK(launch_keys_to_uvw(k_add_out_, w_add_out_, (uint32_t)na, add_uvw_, st_));
+    launches_ += 4;
+    if (has_in_) {
+      tb = cub_bytes_;
+      CK(sort_pairs(cub_temp_, tb, k_tmp_in_, k_add_in_, w_tmp_, w_add_in_, (uint32_t)na, st_));
+      CK(launch_row_segments(k_add_in_, (uint32_t)na, seg_in_, counts_ + 3, st_));
+      launches_ += 2;
+    }
+  }
+  ++touch_epoch_;
+  if (nd) CK(launch_touched(k_del_out_, (uint32_t)nd, touch_, touch_epoch_, touched_, counts_ + 4,
+                            ctl_, st_));
+  if (na) CK(launch_touched(k_add_out_, (uint32_t)na, touch_, touch_epoch_, touched_, counts_ + 4,
+                            ctl_, st_));
+  launches_ += (nd ? 1 : 0) + (na ? 1 : 0);
+  CK(cudaEventRecord(ev_[1], st_));
+  const u64 timeout = 60ull * 1000000000ull;
+  PrLaunch PL{};
+  if (opt_.algo == DYCG_ALGO_PR) {
+    PL.out = adj(out_);
+    PL.x = x_;
+    PL.r = r_;
+    PL.delta = delta_;
+    PL.queued = queued_;
+    PL.q0 = q0_;
+    PL.q1 = q1_;
+    PL.sources = touched_;
+    PL.n_sources = counts_ + 4;
+    PL.tiles = tiles_;
+    PL.tile_cap = tile_cap_;
+    PL.ctl = ctl_;
+    PL.n = n_;
+    PL.cur = pr_cur_;
+    PL.phases = PR_AMEND;
+    PL.sign = -1.f;
+    PL.eps = opt_.epsilon;
+    PL.alpha = opt_.alpha;
+    PL.max_rounds = opt_.max_rounds;
+    PL.timeout_ns = timeout;
+    PL.num_sms = num_sms_;
+    if (nd + na) {
+      CK(launch_pr(PL, st_));
+      launches_++;
+    }
+  }
+  // ---- mutation
+  const Adj A_out = adj(out_);
+  const Adj A_in = has_in_ ? adj(in_) : A_out;
+  if (nd) {
+    CK(launch_delete_rows(A_out, uv_out_, mult_out_, counts_ + 0, (uint32_t)nd, found_out_, ctl_,
+                          1, st_));
+    launches_++;
+    if (has_in_) {
+      CK(launch_delete_rows(A_in, uv_in_, mult_in_, counts_ + 1, (uint32_t)nd, nullptr, ctl_, 0,
+                            st_));
+      launches_++;
+    }
+  }
+  if (na) {
+    CK(launch_add_rows(A_out, k_add_out_, w_add_out_, seg_out_, counts_ + 2, (uint32_t)na,
+                       stored_ ? 1 : 0, ctl_, st_));
+    launches_++;
+    if (has_in_) {
+      CK(launch_add_rows(A_in, k_add_in_, w_add_in_, seg_in_, counts_ + 3, (uint32_t)na,
+                         stored_ ? 1 : 0, ctl_, st_));
+      launches_++;
+    }
+  }
+  CK(cudaEventRecord(ev_[2], st_));
+  // ---- repair
+  if (opt_.algo == DYCG_ALGO_PR) {
+    PL.phases = (nd + na) ? (PR_AMEND | PR_CONVERGE) : PR_CONVERGE;
+    PL.sign = 1.f;
+    CK(launch_pr(PL, st_));
+    launches_++;
+  } else {
+    RepairLaunch L{};
+    L.out = A_out;
+    L.in = A_in;
+    L.key = key_;
+    L.mark = mark_;
+    L.wtag = wtag_;
+    L.aff = aff_;
+    L.q0 = q0_;
+    L.q1 = q1_;
+    L.tiles = tiles_;
+    L.tile_cap = tile_cap_;
+    L.ctl = ctl_;
+    L.del_uv = uv_out_;
+    L.del_found = found_out_;
+    L.n_del_ptr = counts_ + 0;
+    L.add_uvw = add_uvw_;
+    L.n_add = (uint32_t)na;
+    L.n = n_;
+    L.source = opt_.source;
+    L.epoch = ++epoch_;
+    L.tag_base = tag_base_;
+    L.phases = (nd ? PH_DELETE : 0) | (na ? PH_INSERT : 0) | PH_CLOSE;
+    L.max_waves = (uint32_t)std::min<u64>(4ull * n_ + 1024, 0x7FFFFFFFull);
+    L.timeout_ns = timeout;
+    L.algo = opt_.algo;
+    L.stored = stored_;
+    L.num_sms = num_sms_;
+    CK(launch_repair(L, st_));
+    launches_++;
+  }
+  CK(cudaEventRecord(ev_[3], st_));
+  CK(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
+  sync_check("batch");
+  Ctl c = *h_ctl_;
+  if (c.err) {
+    failed = true;
+    const int code = (c.err == ERR_WAVES || c.err == ERR_BARRIER) ? DYCG_ELIMIT : DYCG_ECAPACITY;
+    throw Error(code, "batch failed on the device (error code " + std::to_string(c.err) + ")");
+  }
+  tag_base_ += c.waves + 2;
+  if (opt_.algo == DYCG_ALGO_PR) {
+    pr_cur_ = c.pad[0];
+    pr_count_ = c.pad[1];
+  }
+  float ms[4] = {0, 0, 0, 0};
+  cudaEventElapsedTime(&ms[0], ev_[0], ev_[1]);
+  cudaEventElapsedTime(&ms[1], ev_[1], ev_[2]);
+  cudaEventElapsedTime(&ms[2], ev_[2], ev_[3]);
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->deletions = nd;
+    stats->insertions = na;
+    stats->missing_deletes = c.stat[ST_MISSING];
+    stats->invalid_updates = c.stat[ST_INVALID];
+    stats->touched_sources = c.stat[ST_TOUCHED];
+    stats->relocated_rows = c.stat[ST_RELOCATED];
+    stats->affected = c.stat[ST_AFFECTED];
+    stats->expanded = c.stat[ST_EXPANDED];
+    stats->edges_scanned = c.stat[ST_SCANNED];
+    stats->improvements = c.stat[ST_IMPROVED];
+    stats->waves = c.waves;
+    stats->link_bytes = c.stat[ST_LINK_BYTES];
+    stats->hbm_adj_bytes = c.stat[ST_HBM_ADJ_BYTES];
+    stats->ms_ingest = ms[0];
+    stats->ms_mutate = ms[1];
+    stats->ms_repair = ms[2];
+  }
+  if (maintenance) cache_maintenance(false, stats);
+  if (stats) {
+    stats->kernel_launches = launches_ - l0;
+    float tot = 0;
+    cudaEventElapsedTime(&tot, ev_[0], maintenance && cache_slots_ ? ev_[5] : ev_[3]);
+    stats->ms_total = tot;
+    // vertex-state bytes: per expanded row 8 B key + per scanned slot 8 B key
+    // read; per improvement 8 B atomic + 4 B tag + 4 B queue slot
+    stats->state_bytes = stats->expanded * 8 + stats->edges_scanned * 8 + stats->improvements * 16;
+  }
+}
+
+void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
+  check_loaded();
+  if (!cache_slots_) {
+    CK(cudaMemsetAsync(page_hits_, 0, (u64)npages_ * 4, st_));
+    return;
+  }
+  CK(cudaEventRecord(ev_[4], st_));
+  CK(cache_rank(cwk_, npages_, cache_slots_, 0.5f, page_slot_, st_));
+  sync_check("cache rank");
+  const uint32_t n_admit = cwk_.h_counts[0] + cwk_.h_counts[1];
+  const uint32_t n_evict_cand = cwk_.h_counts[2] + cwk_.h_counts[3];
+  // refresh gate: skip unless enough top-K pages are missing
+  const uint32_t gate = initial ? 1u : std::max<uint32_t>(1u, cache_slots_ / 1024);
+  uint32_t admit = 0, evict = 0;
+  if (n_admit >= gate) {
+    const uint32_t cap = initial ? cache_slots_ : std::max<uint32_t>(cache_slots_ / 16, 64u);
+    admit = std::min(n_admit, cap);
+    const uint32_t need = admit > free_count_ ? admit - free_count_ : 0u;
+    evict = std::min(n_evict_cand, need);
+    admit = std::min(admit, free_count_ + evict);
+    CachePages pg{out_.d_dst, out_.d_w, has_in_ ? in_.d_dst : nullptr,
+                  has_in_ ? in_.d_w : nullptr, out_.pages, page_shift_, cdst_, cw_};
+    CK(cache_apply(cwk_, npages_, n_evict_cand, evict, admit, page_slot_, free_list_, free_count_,
+                   pg, st_));
+    free_count_ = free_count_ + evict - admit;
+    pages_loaded_ += admit;
+    pages_evicted_ += evict;
+    launches_ += 3;
+  }
+  launches_ += 5;
+  CK(cudaEventRecord(ev_[5], st_));
+  sync_check("cache apply");
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev_[4], ev_[5]);
+    stats->ms_cache = ms;
+    stats->cache_pages_loaded = admit;
+    stats->cache_pages_evicted = evict;
+    const u64 page_bytes = (4ull << page_shift_) * (stored_ ? 2 : 1);
+    stats->link_bytes += (u64)admit * page_bytes;
+    stats->hbm_adj_bytes += (u64)admit * page_bytes;
+  }
+}
+
+void Engine::gather(uint32_t *values, uint32_t *parents) {
+  check_loaded();
+  if (opt_.algo == DYCG_ALGO_PR) throw Error(DYCG_EINVAL, "PR results: use dycg_gather_ranks");
+  std::vector<u64> k(n_);
+  CK(cudaMemcpyAsync(k.data(), key_, (u64)n_ * 8, cudaMemcpyDeviceToHost, st_));
+  sync_check("gather");
+  for (uint32_t v = 0; v < n_; v++) {
+    const uint32_t val = key_value(k[v]);
+    const uint32_t p1 = key_parent1(k[v]);
+    if (values) values[v] = val;
+    if (parents) parents[v] = (val == INF32 || p1 == 0) ? INF32 : p1 - 1;
+  }
+}
+
+void Engine::gather_ranks(float *ranks, float *residuals) {
+  check_loaded();
+  if (opt_.algo != DYCG_ALGO_PR) throw Error(DYCG_EINVAL, "not a PageRank engine");
+  if (ranks) CK(cudaMemcpyAsync(ranks, x_, (u64)n_ * 4, cudaMemcpyDeviceToHost, st_));
+  if (residuals) CK(cudaMemcpyAsync(residuals, r_, (u64)n_ * 4, cudaMemcpyDeviceToHost, st_));
+  sync_check("gather ranks");
+}
+
+void Engine::get_row(uint32_t v, int incoming, uint32_t *dst, uint32_t *w, uint32_t cap,
+                     uint32_t *deg) {
+  check_loaded();
+  if (v >= n_) throw Error(DYCG_EINVAL, "vertex out of range");
+  const Arena &A = (incoming && has_in_) ? in_ : out_;
+  u64 off = 0;
+  uint32_t len = 0;
+  CK(cudaMemcpyAsync(&off, A.off + v, 8, cudaMemcpyDeviceToHost, st_));
+  CK(cudaMemcpyAsync(&len, A.len + v, 4, cudaMemcpyDeviceToHost, st_));
+  sync_check("row");
+  uint32_t k = 0;
+  for (uint32_t s = 0; s < len; s++) {
+    const uint32_t d = A.h_dst[off + s];
+    if (d & TOMB) continue;
+    if (k < cap) {
+      if (dst) dst[k] = d;
+      if (w) w[k] = A.h_w ? A.h_w[off + s] : 0u;
+    }
+    k++;
+  }
+  if (deg) *deg = k;
+}
+
+void Engine::export_csr(uint64_t *off, uint32_t *dst, uint32_t *w) {
+  check_loaded();
+  std::vector<u64> o(n_);
+  std::vector<uint32_t> l(n_);
+  CK(cudaMemcpyAsync(o.data(), out_.off, (u64)n_ * 8, cudaMemcpyDeviceToHost, st_));
+  CK(cudaMemcpyAsync(l.data(), out_.len, (u64)n_ * 4, cudaMemcpyDeviceToHost, st_));
+  sync_check("export");
+  u64 p = 0;
+  for (uint32_t v = 0; v < n_; v++) {
+    off[v] = p;
+    for (uint32_t s = 0; s < l[v]; s++) {
+      const uint32_t d = out_.h_dst[o[v] + s];
+      if (d & TOMB) continue;
+      if (dst) dst[p] = d;
+      if (w) w[p] = out_.h_w ? out_.h_w[o[v] + s] : 0u;
+      p++;
+    }
+  }
+  off[n_] = p;
+}
+
+void Engine::info(dycg_graph_info *out) {
+  check_loaded();
+  std::memset(out, 0, sizeof(*out));
+  out->nodes = n_;
+  std::vector<uint32_t> l(n_);
+  CK(cudaMemcpyAsync(l.data(), out_.live, (u64)n_ * 4, cudaMemcpyDeviceToHost, st_));
+  u64 top_out = 0, top_in = 0;
+  CK(cudaMemcpyAsync(&top_out, out_.top, 8, cudaMemcpyDeviceToHost, st_));
+  if (has_in_) CK(cudaMemcpyAsync(&top_in, in_.top, 8, cudaMemcpyDeviceToHost, st_));
+  sync_check("info");
+  u64 m = 0;
+  for (uint32_t x : l) m += x;
+  out->live_edges = m;
+  out->arena_slots = out_.slots + (has_in_ ? in_.slots : 0);
+  out->arena_used = top_out + top_in;
+  out->pages = npages_;
+  out->cache_slots = cache_slots_;
+  out->cached_pages = cache_slots_ - free_count_;
+  out->host_bytes = out->arena_slots * 4 * (stored_ ? 2 : 1);
+  out->device_bytes = (u64)n_ * (8 + 4 * 6) + (u64)n_ * (has_in_ ? 48 : 24) +
+                      ((u64)cache_slots_ << page_shift_) * 4 * (stored_ ? 2 : 1);
+  out->page_shift = page_shift_;
+  out->has_incoming = has_in_ ? 1 : 0;
+}
+
+void Engine::sample_edges(uint64_t count, uint64_t seed, dycg_edge *out) {
+  check_loaded();
+  if (!count) return;
+  const uint32_t n = n_;
+  u64 *pre = nullptr;
+  CK(cudaMalloc(&pre, (n + 1ull) * 8));
+  size_t tb = 0;
+  CK(build_scan_u32_to_u64(nullptr, tb, out_.live, pre, n, st_));
+  void *temp = nullptr;
+  CK(cudaMalloc(&temp, std::max<size_t>(tb, 16)));
+  CK(build_scan_u32_to_u64(temp, tb, out_.live, pre, n, st_));
+  u64 last_pre = 0;
+  uint32_t last_live = 0;
+  CK(cudaMemcpyAsync(&last_pre, pre + n - 1, 8, cudaMemcpyDeviceToHost, st_));
+  CK(cudaMemcpyAsync(&last_live, out_.live + n - 1, 4, cudaMemcpyDeviceToHost, st_));
+  sync_check("sample scan");
+  cudaFree(temp);
+  const u64 total = last_pre + last_live;
+  if (count > total) {
+    cudaFree(pre);
+    throw Error(DYCG_EINVAL, "more samples requested than live edges");
+  }
+  // draw with oversampling, keep the first `count` distinct ranks in draw order
+  std::vector<u64> chosen;
+  chosen.reserve(count);
+  std::unordered_set<u64> seen;
+  seen.reserve(count * 2);
+  u64 round = 0;
+  while (chosen.size() < count) {
+    const u64 draws = (count - chosen.size()) + (count - chosen.size()) / 16 + 64;
+    u64 *pos = nullptr;
+    CK(cudaMalloc(&pos, draws * 8));
+    CK(sample_draw(pos, draws, mix64(seed + round * 0x9E37ull), total, st_));
+    std::vector<u64> h(draws);
+    CK(cudaMemcpyAsync(h.data(), pos, draws * 8, cudaMemcpyDeviceToHost, st_));
+    sync_check("sample draw");
+    cudaFree(pos);
+    for (u64 r : h) {
+      if (chosen.size() >= count) break;
+      if (seen.insert(r).second) chosen.push_back(r);
+    }
+    if (++round > 64) break;
+  }
+  const u64 k = chosen.size();
+  u64 *pos = nullptr;
+  uint32_t *res = nullptr;
+  CK(cudaMalloc(&pos, k * 8));
+  CK(cudaMalloc(&res, k * 12));
+  CK(cudaMemcpyAsync(pos, chosen.data(), k * 8, cudaMemcpyHostToDevice, st_));
+  CK(sample_resolve(pos, k, pre, n, adj(out_), res, st_));
+  CK(cudaMemcpyAsync(out, res, k * 12, cudaMemcpyDeviceToHost, st_));
+  sync_check("sample resolve");
+  cudaFree(pos);
+  cudaFree(res);
+  cudaFree(pre);
+  if (k < count) throw Error(DYCG_ELIMIT, "could not draw enough distinct edges");
+}
+
+}  // namespace dycg

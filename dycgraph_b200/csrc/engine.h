@@ -1,0 +1,117 @@
+// engine.h -- host-side engine behind the C ABI (include/dycg.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/dycg.h"
+#include "internal.h"
+
+namespace dycg {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+// One adjacency direction: a pinned, mapped host arena plus its descriptors.
+struct Arena {
+  uint32_t *h_dst = nullptr, *h_w = nullptr;  // host addresses
+  uint32_t *d_dst = nullptr, *d_w = nullptr;  // device-mapped addresses
+  u64 slots = 0;
+  uint32_t pages = 0, page_base = 0;
+  u64 *off = nullptr;
+  uint32_t *len = nullptr, *cap = nullptr, *srt = nullptr, *live = nullptr;
+  u64 *top = nullptr;
+};
+
+class Engine {
+ public:
+  explicit Engine(const dycg_options &opt);
+  ~Engine();
+
+  void load_csr(uint32_t n, const uint64_t *off, const uint32_t *dst, const uint32_t *w);
+  void load_file(const char *path, uint32_t min_nodes, int weighted);
+  void load_rmat(uint32_t scale, uint32_t ef, double a, double b, double c, uint64_t seed,
+                 uint32_t wlo, uint32_t whi, int symmetrize);
+  void load_grid(uint32_t side, uint32_t permille, uint32_t radius, uint64_t seed, uint32_t wlo,
+                 uint32_t whi);
+  void init();
+  // mode: 0 fused batch, 1 deletions only, 2 insertions only
+  void apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na, bool device_ptrs,
+             int mode, bool maintenance, dycg_batch_stats *stats);
+  void cache_maintenance(bool initial, dycg_batch_stats *stats);
+  void gather(uint32_t *values, uint32_t *parents);
+  void gather_ranks(float *ranks, float *residuals);
+  void get_row(uint32_t v, int incoming, uint32_t *dst, uint32_t *w, uint32_t cap, uint32_t *deg);
+  void export_csr(uint64_t *off, uint32_t *dst, uint32_t *w);
+  void info(dycg_graph_info *out);
+  void sample_edges(uint64_t count, uint64_t seed, dycg_edge *out);
+  cudaStream_t stream() const { return st_; }
+
+  std::string last_error;
+  bool failed = false;
+
+ private:
+  void check_loaded() const;
+  void build_from_sorted_keys(u64 *keys, uint32_t *wv, u64 m, bool weight_from_hash, u64 wseed,
+                              uint32_t wlo, uint32_t whi, u64 *scratch_keys, uint32_t *scratch_w);
+  void build_direction(Arena &A, const u64 *keys, const uint32_t *wv, u64 m, bool weight_from_hash,
+                       u64 wseed, uint32_t wlo, uint32_t whi, bool swapped);
+  void finish_load();
+  void ensure_batch(size_t cnt);
+  Adj adj(const Arena &A) const;
+  void sync_check(const char *where);
+  void fill_stats(dycg_batch_stats *s, float ms[4]);
+  void *dmalloc(size_t bytes);
+  void dfree_all();
+
+  dycg_options opt_;
+  int dev_ = 0, num_sms_ = 148;
+  cudaStream_t st_ = nullptr;
+  cudaEvent_t ev_[6] = {};
+  uint32_t n_ = 0;
+  bool loaded_ = false, inited_ = false, has_in_ = false, stored_ = false;
+  Arena out_, in_;
+  std::vector<void *> dallocs_;
+  std::vector<void *> hallocs_;
+
+  // cache
+  uint32_t page_shift_ = 12, npages_ = 0, cache_slots_ = 0, free_count_ = 0;
+  uint32_t *page_slot_ = nullptr, *page_hits_ = nullptr, *cdst_ = nullptr, *cw_ = nullptr,
+           *free_list_ = nullptr;
+  CacheWork cwk_{};
+  uint64_t pages_loaded_ = 0, pages_evicted_ = 0;
+
+  // vertex state
+  u64 *key_ = nullptr;
+  uint32_t *mark_ = nullptr, *wtag_ = nullptr, *aff_ = nullptr, *q0_ = nullptr, *q1_ = nullptr,
+           *touch_ = nullptr;
+  uint4 *tiles_ = nullptr;
+  uint32_t tile_cap_ = 0;
+  Ctl *ctl_ = nullptr, *h_ctl_ = nullptr;
+  float *x_ = nullptr, *r_ = nullptr, *delta_ = nullptr;
+  uint32_t *queued_ = nullptr;
+  uint32_t pr_cur_ = 0, pr_count_ = 0;
+  uint32_t epoch_ = 0, tag_base_ = 1, touch_epoch_ = 0;
+
+  // batch buffers
+  size_t bcap_ = 0;
+  u64 *k_tmp_out_ = nullptr, *k_tmp_in_ = nullptr, *k_del_out_ = nullptr, *k_del_in_ = nullptr,
+      *k_add_out_ = nullptr, *k_add_in_ = nullptr;
+  uint32_t *w_tmp_ = nullptr, *w_add_out_ = nullptr, *w_add_in_ = nullptr;
+  uint2 *uv_out_ = nullptr, *uv_in_ = nullptr;
+  uint32_t *mult_out_ = nullptr, *mult_in_ = nullptr, *found_out_ = nullptr;
+  uint3 *seg_out_ = nullptr, *seg_in_ = nullptr, *add_uvw_ = nullptr;
+  uint32_t *touched_ = nullptr, *counts_ = nullptr;
+  dycg_edge_dev *d_edges_ = nullptr;
+  dycg_edge *h_stage_ = nullptr;
+  void *cub_temp_ = nullptr;
+  size_t cub_bytes_ = 0;
+  std::vector<void *> batch_allocs_;
+  uint64_t launches_ = 0;
+};
+
+}  // namespace dycg

@@ -1,0 +1,180 @@
+// frontier.cuh -- bounded grid barrier and the row-expansion engine shared by
+// the persistent repair kernels (SSSP/BFS/CC closures and PageRank pushes).
+//
+// Work distribution (the B200 form of the reference's degree-aware CTA/warp
+// scheduler, include/groute/device/cta_scheduler_hybrid.cuh:60-240): one warp
+// per frontier vertex walks its row 32 slots at a time (coalesced 128-byte
+// reads, from the HBM page cache or zero-copy from the host arena); rows
+// longer than HEAVY are cut into TILE-slot tiles that whole CTAs process after
+// a grid barrier, so a million-edge hub row spreads over the whole GPU.
+#pragma once
+#include "common.cuh"
+
+namespace dycg {
+
+constexpr uint32_t SYNC_RESET_TILES = 1;
+constexpr uint32_t SYNC_RESET_Q0 = 2;
+constexpr uint32_t SYNC_RESET_Q1 = 4;
+
+// Grid-wide barrier for cooperative launches. Every wait is bounded: past
+// timeout_ns the waiting block records ERR_BARRIER and all blocks leave at
+// their next barrier. The last block to arrive snapshots the queue counters
+// and applies the requested resets while every other block is waiting.
+__device__ __forceinline__ bool grid_sync(Ctl *c, uint32_t flags, u64 timeout_ns) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t *vgen = &c->bar_gen;
+    volatile uint32_t *verr = &c->err;
+    uint32_t g = *vgen;
+    __threadfence();
+    uint32_t arrived = atomicAdd(&c->bar_count, 1u) + 1;
+    int ok = 1;
+    if (arrived == gridDim.x) {
+      if (flags & SYNC_RESET_TILES) c->tile_count = 0;
+      if (flags & SYNC_RESET_Q0) c->q_count[0] = 0;
+      if (flags & SYNC_RESET_Q1) c->q_count[1] = 0;
+      c->snap_aff = *(volatile uint32_t *)&c->n_aff;
+      c->snap_q[0] = *(volatile uint32_t *)&c->q_count[0];
+      c->snap_q[1] = *(volatile uint32_t *)&c->q_count[1];
+      c->snap_tiles = *(volatile uint32_t *)&c->tile_count;
+      atomicExch(&c->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&c->bar_gen, 1u);
+    } else {
+      u64 t0 = globaltimer_ns();
+      while (*vgen == g) {
+        if (*verr) {
+          ok = 0;
+          break;
+        }
+        if (globaltimer_ns() - t0 > timeout_ns) {
+          atomicCAS(&c->err, 0u, ERR_BARRIER);
+          ok = 0;
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+    s_ok = ok && (*verr == 0);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Per-thread traffic counters, flushed once per kernel.
+struct Acc {
+  u64 link;
+  u64 hbm;
+  u64 scanned;
+  u64 expanded;
+  u64 improved;
+  __device__ void flush(Ctl *c) {
+    u64 a = warp_sum(link), b = warp_sum(hbm), s = warp_sum(scanned), e = warp_sum(expanded),
+        i = warp_sum(improved);
+    if (lane_id() == 0) {
+      if (a) atomicAdd(&c->stat[ST_LINK_BYTES], a);
+      if (b) atomicAdd(&c->stat[ST_HBM_ADJ_BYTES], b);
+      if (s) atomicAdd(&c->stat[ST_SCANNED], s);
+      if (e) atomicAdd(&c->stat[ST_EXPANDED], e);
+      if (i) atomicAdd(&c->stat[ST_IMPROVED], i);
+    }
+  }
+};
+
+// Walk slots [b, e) of row v; this lane handles s0 + lane for s0 = b, b+stride...
+// Op interface (all lanes call every member, keeping the warp converged):
+//   bool begin(uint32_t v, Row&)                  -- false: skip the row
+//   void edge(uint32_t v, uint32_t nb, uint32_t w, bool valid, Row&, Acc&)
+//   void end(uint32_t v, Row&)
+template <bool WITH_W, class Op>
+__device__ __forceinline__ void warp_slots(const Adj &A, uint32_t v, u64 off, uint32_t b,
+                                           uint32_t e, uint32_t stride, Op &op, Acc &acc) {
+  typename Op::Row r;
+  if (!op.begin(v, r)) return;
+  const uint32_t lane = lane_id();
+  uint32_t hit_pg = PAGE_NONE, hit_n = 0;  // lane 0: pending hotness count
+  const uint32_t bytes = WITH_W ? 8u : 4u;
+  for (uint32_t s0 = b; s0 < e; s0 += stride) {
+    const uint32_t s = s0 + lane;
+    const bool in = s < e;
+    bool valid = in, cached = false;
+    uint32_t d = 0, w = 0;
+    const u64 p = off + s;
+    uint32_t pg = PAGE_NONE;
+    if (in) {
+      pg = page_of(A, p);
+      d = read_dst(A, p, cached);
+      if (d & TOMB) valid = false;
+      if (WITH_W && valid) w = read_w(A, p, cached);
+      if (cached) acc.hbm += valid ? bytes : 4u;
+      else acc.link += valid ? bytes : 4u;
+      acc.scanned++;
+    }
+    // hotness: lane 0 accumulates the warp's slots that share its page
+    const uint32_t pg0 = __shfl_sync(0xffffffffu, pg, 0);
+    const unsigned same = __ballot_sync(0xffffffffu, in && pg == pg0);
+    if (lane == 0) {
+      if (pg0 != hit_pg) {
+        if (hit_n) atomicAdd(A.page_hits + hit_pg, hit_n);
+        hit_pg = pg0;
+        hit_n = 0;
+      }
+      hit_n += __popc(same);
+    }
+    if (in && pg != pg0) atomicAdd(A.page_hits + pg, 1u);
+    op.edge(v, d & VMASK, w, valid, r, acc);
+  }
+  if (lane == 0 && hit_n) atomicAdd(A.page_hits + hit_pg, hit_n);
+  op.end(v, r);
+}
+
+struct Tiles {
+  uint4 *tiles;
+  uint32_t cap;
+};
+
+// Expand the rows of items[0..cnt) over adjacency A. Ends with a grid barrier
+// that also applies `reset_flags` (with the tile reset). Returns false when
+// the launch has failed (error flag set).
+template <bool WITH_W, class Op>
+__device__ bool expand_rows(const Adj &A, const uint32_t *items, uint32_t cnt, Op &op,
+                            Acc &acc, Tiles T, Ctl *ctl, uint32_t reset_flags,
+                            u64 timeout_ns) {
+  const uint32_t lane = lane_id();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = gw; i < cnt; i += nw) {
+    const uint32_t v = items[i];
+    const uint32_t len = A.len[v];
+    if (len > HEAVY) {
+      if (lane == 0) {
+        const uint32_t nt = (len + TILE - 1) / TILE;
+        const uint32_t base = atomicAdd(&ctl->tile_count, nt);
+        if (base + nt > T.cap) {
+          atomicCAS(&ctl->err, 0u, ERR_TILES);
+        } else {
+          for (uint32_t t = 0; t < nt; t++)
+            T.tiles[base + t] = make_uint4(v, t * TILE, min(len, (t + 1) * TILE), 0);
+        }
+      }
+      continue;
+    }
+    warp_slots<WITH_W>(A, v, A.off[v], 0, len, 32, op, acc);
+  }
+  if (!grid_sync(ctl, 0, timeout_ns)) return false;
+  const uint32_t nt = min(*(volatile uint32_t *)&ctl->snap_tiles, T.cap);
+  const uint32_t wib = threadIdx.x >> 5;
+  for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
+    const uint4 tl = T.tiles[t];
+    warp_slots<WITH_W>(A, tl.x, A.off[tl.x], tl.y + wib * 32, tl.z, blockDim.x, op, acc);
+  }
+  return grid_sync(ctl, SYNC_RESET_TILES | reset_flags, timeout_ns);
+}
+
+__device__ __forceinline__ u64 ld_key(const u64 *p) {
+  return *(const volatile u64 *)p;
+}
+
+}  // namespace dycg

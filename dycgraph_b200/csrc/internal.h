@@ -1,0 +1,131 @@
+// internal.h -- launcher declarations shared between the kernel files and the
+// host engine.
+#pragma once
+#include <algorithm>
+#include <cstddef>
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace dycg {
+
+struct dycg_edge_dev {
+  uint32_t u, v, w;
+};
+
+constexpr uint32_t PH_DELETE = 1, PH_INSERT = 2, PH_CLOSE = 4;
+constexpr uint32_t PR_AMEND = 1, PR_CONVERGE = 2;
+
+struct RepairLaunch {
+  Adj out, in;
+  u64 *key;
+  uint32_t *mark, *wtag, *aff, *q0, *q1;
+  uint4 *tiles;
+  uint32_t tile_cap;
+  Ctl *ctl;
+  const uint2 *del_uv;
+  const uint32_t *del_found;
+  const uint32_t *n_del_ptr;
+  const uint3 *add_uvw;
+  uint32_t n_add;
+  uint32_t n, source, epoch, tag_base, phases, max_waves;
+  u64 timeout_ns;
+  uint32_t algo;
+  bool stored;
+  int num_sms;
+};
+cudaError_t launch_repair(const RepairLaunch &L, cudaStream_t s);
+cudaError_t launch_init_state(uint32_t algo, u64 *key, uint32_t n, uint32_t source,
+                              uint32_t *q0, Ctl *ctl, cudaStream_t s);
+
+struct PrLaunch {
+  Adj out;
+  float *x, *r, *delta;
+  uint32_t *queued, *q0, *q1;
+  const uint32_t *sources, *n_sources;
+  uint4 *tiles;
+  uint32_t tile_cap;
+  Ctl *ctl;
+  uint32_t n, cur, phases;
+  float sign, eps, alpha;
+  uint32_t max_rounds;
+  u64 timeout_ns;
+  int num_sms;
+};
+cudaError_t launch_pr(const PrLaunch &L, cudaStream_t s);
+cudaError_t launch_pr_init(float *x, float *r, uint32_t *queued, uint32_t *q0, uint32_t n,
+                           float base, Ctl *ctl, cudaStream_t s);
+
+// ingest + mutation
+cudaError_t launch_prep_keys(const dycg_edge_dev *e, uint32_t cnt, uint32_t n, u64 *kout,
+                             u64 *kin, uint32_t *w, u64 *invalid, cudaStream_t s);
+cudaError_t sort_keys(void *temp, size_t &temp_bytes, const u64 *in, u64 *out, uint32_t cnt,
+                      cudaStream_t s);
+cudaError_t sort_pairs(void *temp, size_t &temp_bytes, const u64 *kin, u64 *kout,
+                       const uint32_t *vin, uint32_t *vout, uint32_t cnt, cudaStream_t s);
+cudaError_t launch_unique_runs(const u64 *k, uint32_t cnt, uint2 *uv, uint32_t *mult,
+                               uint32_t *n_out, uint32_t cap, uint32_t *err, cudaStream_t s);
+cudaError_t launch_row_segments(const u64 *k, uint32_t cnt, uint3 *seg, uint32_t *n_out,
+                                cudaStream_t s);
+cudaError_t launch_delete_rows(const Adj &A, const uint2 *uv, const uint32_t *mult,
+                               const uint32_t *n_ptr, uint32_t max_n, uint32_t *found, Ctl *ctl,
+                               int count_missing, cudaStream_t s);
+cudaError_t launch_add_rows(const Adj &A, const u64 *k, const uint32_t *w, const uint3 *seg,
+                            const uint32_t *n_ptr, uint32_t max_n, int with_w, Ctl *ctl,
+                            cudaStream_t s);
+cudaError_t launch_keys_to_uvw(const u64 *k, const uint32_t *w, uint32_t cnt, uint3 *out,
+                               cudaStream_t s);
+cudaError_t launch_touched(const u64 *k, uint32_t cnt, uint32_t *tag, uint32_t epoch,
+                           uint32_t *list, uint32_t *n_out, Ctl *ctl, cudaStream_t s);
+
+// cache
+struct CacheWork {
+  uint32_t *hits;        // == page_hits
+  float *score, *score_sorted;
+  uint32_t *ids, *ids_sorted, *fa, *fe, *sa, *se, *admit;
+  void *temp;
+  size_t temp_bytes;
+  uint32_t *h_counts;    // pinned host [4]
+};
+struct CachePages {
+  const uint32_t *h_out_dst, *h_out_w, *h_in_dst, *h_in_w;
+  uint32_t pages_out, page_shift;
+  uint32_t *cdst, *cw;
+};
+size_t cache_temp_bytes(uint32_t npages);
+cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay,
+                       const uint32_t *page_slot, cudaStream_t s);
+cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t n_evict_cand, uint32_t evict,
+                        uint32_t admit, uint32_t *page_slot, uint32_t *free_list,
+                        uint32_t free_count, const CachePages &pg, cudaStream_t s);
+
+// build
+cudaError_t build_gen_rmat(u64 *keys, u64 draws, u64 seed, uint32_t scale, double a, double b,
+                           double c, int symmetrize, cudaStream_t s);
+cudaError_t build_gen_grid(u64 *keys, uint32_t side, u64 nshort, uint32_t radius, u64 seed,
+                           cudaStream_t s);
+cudaError_t build_csr_keys(const u64 *off, const uint32_t *dst, uint32_t n, u64 *keys,
+                           cudaStream_t s);
+cudaError_t build_swap_keys(const u64 *in, u64 *out, u64 count, cudaStream_t s);
+cudaError_t build_sort(void *temp, size_t &bytes, u64 *k_in, u64 *k_out, uint32_t *v_in,
+                       uint32_t *v_out, u64 count, cudaStream_t s);
+cudaError_t build_scan_u32_to_u64(void *temp, size_t &bytes, const uint32_t *in, u64 *out,
+                                  u64 count, cudaStream_t s);
+cudaError_t build_scan_u64(void *temp, size_t &bytes, const u64 *in, u64 *out, u64 count,
+                           cudaStream_t s);
+cudaError_t build_unique(const u64 *k, const uint32_t *vin, u64 count, int dedup,
+                         uint32_t *flag, u64 *pos, u64 *out, uint32_t *vout, void *temp,
+                         size_t temp_bytes, cudaStream_t s);
+cudaError_t build_degrees(const u64 *k, u64 m, uint32_t *deg, cudaStream_t s);
+cudaError_t build_caps(const uint32_t *deg, uint32_t n, u64 *cap64, uint32_t *cap,
+                       uint32_t *len, uint32_t *srt, uint32_t *live, cudaStream_t s);
+cudaError_t build_scatter(const u64 *k, const uint32_t *wv, u64 m, const u64 *off,
+                          const u64 *rowstart, uint32_t *hdst, uint32_t *hw, u64 wseed,
+                          uint32_t wlo, uint32_t whi, int weight_from_hash, int swapped,
+                          cudaStream_t s);
+size_t build_temp_bytes(u64 count, bool pairs);
+cudaError_t sample_draw(u64 *pos, u64 count, u64 seed, u64 total, cudaStream_t s);
+cudaError_t sample_resolve(const u64 *pos, u64 count, const u64 *pre, uint32_t n, const Adj &A,
+                           uint32_t *out, cudaStream_t s);
+
+}  // namespace dycg

@@ -1,0 +1,363 @@
+"""ctypes binding of libdycg.so and the reference-shaped Engine class.
+
+Method names follow sepgraph::engine::Engine (include/framework/framework.cuh:
+LoadGraph :1569, InitGraph :1803, Start :1963, del_edge :2595, add_edge :2419,
+compute_hot_vertices_sssp :1264, confirm_candidate_batch :1364, LoadCache :1509,
+evication_cache :3038, compact_cache :2978, GatherValue/GatherParent :4959-4984,
+StartPageRank :2681, UpdatePageRank :2692). Errors raise DycgError with the
+library's status code and message, where the reference would abort.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+ALGOS = {"sssp": 0, "bfs": 1, "cc": 2, "pr": 3}
+WEIGHTS = {"hash128": 0, "stored": 1}
+CACHE = {"none": 0, "hotness": 1}
+STATUS = {0: "DYCG_OK", -1: "DYCG_EINVAL", -2: "DYCG_ECUDA", -3: "DYCG_ENOMEM",
+          -4: "DYCG_ESTATE", -5: "DYCG_ECAPACITY", -6: "DYCG_ELIMIT", -7: "DYCG_EIO",
+          -8: "DYCG_ENOGPU"}
+INF = 0xFFFFFFFF
+
+
+class DycgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Edge(ctypes.Structure):
+    _fields_ = [("u", ctypes.c_uint32), ("v", ctypes.c_uint32), ("w", ctypes.c_uint32)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("algo", ctypes.c_uint32), ("weight_mode", ctypes.c_uint32),
+                ("source", ctypes.c_uint32), ("segments", ctypes.c_uint32),
+                ("hbm_graph_budget_bytes", ctypes.c_uint64), ("cache_policy", ctypes.c_uint32),
+                ("symmetric", ctypes.c_uint32), ("epsilon", ctypes.c_float),
+                ("alpha", ctypes.c_float), ("max_rounds", ctypes.c_uint32),
+                ("device", ctypes.c_int32), ("page_shift", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 7)]
+
+
+_STAT_U64 = ["deletions", "insertions", "missing_deletes", "invalid_updates", "touched_sources",
+             "relocated_rows", "affected", "expanded", "edges_scanned", "improvements", "waves",
+             "link_bytes", "hbm_adj_bytes", "state_bytes", "cache_pages_loaded",
+             "cache_pages_evicted", "kernel_launches"]
+_STAT_F64 = ["ms_ingest", "ms_mutate", "ms_repair", "ms_cache", "ms_total"]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = ([(k, ctypes.c_uint64) for k in _STAT_U64] + [(k, ctypes.c_double) for k in _STAT_F64]
+                + [("reserved", ctypes.c_uint64 * 8)])
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k in _STAT_U64 + _STAT_F64}
+
+
+class GraphInfo(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in (
+        "nodes", "live_edges", "arena_slots", "arena_used", "pages", "cache_slots",
+        "cached_pages", "host_bytes", "device_bytes")] + [
+        ("page_shift", ctypes.c_uint32), ("has_incoming", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint64 * 6)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+def library_path():
+    return os.environ.get("DYCG_LIBRARY", os.path.join(_HERE, "libdycg.so"))
+
+
+def lib():
+    """Load libdycg.so (built in-tree by `make -C dycgraph_b200`)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise ImportError(f"libdycg.so not built at {path}: run `make -C dycgraph_b200` "
+                          "(there is no CPU fallback)")
+    L = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    I = ctypes.c_int
+    u32, u64, sz = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_size_t
+    u32p, u64p = ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)
+    ep = ctypes.POINTER(Edge)
+    sp = ctypes.POINTER(BatchStats)
+    sig = {
+        "dycg_options_default": (I, [ctypes.POINTER(Options)]),
+        "dycg_create": (I, [ctypes.POINTER(Options), ctypes.POINTER(P)]),
+        "dycg_destroy": (None, [P]),
+        "dycg_load_graph_csr": (I, [P, u32, u64p, u32p, u32p]),
+        "dycg_load_graph_file": (I, [P, ctypes.c_char_p, u32, I]),
+        "dycg_load_graph_rmat": (I, [P, u32, u32, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, u64, u32, u32, I]),
+        "dycg_load_graph_grid": (I, [P, u32, u32, u32, u64, u32, u32]),
+        "dycg_init": (I, [P]),
+        "dycg_delete_edges": (I, [P, ep, sz, sp]),
+        "dycg_insert_edges": (I, [P, ep, sz, sp]),
+        "dycg_cache_maintenance": (I, [P, sp]),
+        "dycg_apply_batch": (I, [P, ep, sz, ep, sz, sp]),
+        "dycg_apply_batch_device": (I, [P, P, sz, P, sz, sp]),
+        "dycg_gather": (I, [P, u32p, u32p]),
+        "dycg_gather_ranks": (I, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+        "dycg_get_row": (I, [P, u32, I, u32p, u32p, u32, u32p]),
+        "dycg_export_csr": (I, [P, u64p, u32p, u32p]),
+        "dycg_graph_info_get": (I, [P, ctypes.POINTER(GraphInfo)]),
+        "dycg_sample_edges": (I, [P, u64, u64, ep]),
+        "dycg_gen_rmat_edges": (I, [u32, ctypes.c_double, ctypes.c_double, ctypes.c_double, u64,
+                                    u64, u64, u32, u32, ep]),
+        "dycg_hash_weight": (u32, [u64, u32, u32, u32, u32]),
+        "dycg_stream": (I, [P, ctypes.POINTER(P)]),
+        "dycg_last_error": (I, [P, ctypes.c_char_p, sz]),
+        "dycg_version": (ctypes.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = L
+    return L
+
+
+def _ptr(a, t):
+    return None if a is None else a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def edges_array(edges):
+    """(k,3) uint32 array from a list of (u, v[, w]) or an array."""
+    if isinstance(edges, np.ndarray):
+        arr = np.ascontiguousarray(edges, dtype=np.uint32)
+        if arr.ndim == 1:
+            arr = arr.reshape(-1, 3)
+        if arr.shape[1] == 2:
+            arr = np.concatenate([arr, np.ones((arr.shape[0], 1), np.uint32)], axis=1)
+        return np.ascontiguousarray(arr)
+    rows = [(e[0], e[1], e[2] if len(e) > 2 else 1) for e in edges]
+    return np.asarray(rows, dtype=np.uint32).reshape(-1, 3)
+
+
+def gen_rmat_edges(scale, count, seed, first=0, a=0.57, b=0.19, c=0.19, wlo=1, whi=64):
+    out = np.empty((count, 3), np.uint32)
+    rc = lib().dycg_gen_rmat_edges(scale, a, b, c, seed, first, count, wlo, whi,
+                                   out.ctypes.data_as(ctypes.POINTER(Edge)))
+    if rc:
+        raise DycgError(rc, "dycg_gen_rmat_edges")
+    return out
+
+
+def hash_weight(seed, u, v, wlo=1, whi=64):
+    return lib().dycg_hash_weight(seed, u, v, wlo, whi)
+
+
+class Engine:
+    """One graph + one algorithm on one GPU (reference: sepgraph::engine::Engine)."""
+
+    def __init__(self, algo="sssp", weight_mode="hash128", source=0, segments=1,
+                 hbm_graph_budget_bytes=0, cache_policy=None, symmetric=False, epsilon=1e-6,
+                 alpha=0.85, max_rounds=100, device=0, page_shift=12):
+        L = lib()
+        opt = Options()
+        L.dycg_options_default(ctypes.byref(opt))
+        opt.algo = ALGOS[algo] if isinstance(algo, str) else int(algo)
+        opt.weight_mode = WEIGHTS[weight_mode] if isinstance(weight_mode, str) else int(weight_mode)
+        opt.source = source
+        opt.segments = segments
+        opt.hbm_graph_budget_bytes = int(hbm_graph_budget_bytes)
+        if cache_policy is None:
+            cache_policy = "hotness" if hbm_graph_budget_bytes else "none"
+        opt.cache_policy = CACHE[cache_policy] if isinstance(cache_policy, str) else int(cache_policy)
+        opt.symmetric = int(bool(symmetric))
+        opt.epsilon = epsilon
+        opt.alpha = alpha
+        opt.max_rounds = max_rounds
+        opt.device = device
+        opt.page_shift = page_shift
+        self.algo = opt.algo
+        self.options = opt
+        self._h = ctypes.c_void_p()
+        rc = L.dycg_create(ctypes.byref(opt), ctypes.byref(self._h))
+        if rc:
+            self._h = None
+            raise DycgError(rc, "dycg_create failed (is a CUDA device visible?)")
+        self.n = 0
+        self.last_stats = None
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().dycg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc:
+            buf = ctypes.create_string_buffer(512)
+            lib().dycg_last_error(self._h, buf, 512)
+            raise DycgError(rc, f"{what}: {buf.value.decode(errors='replace')}")
+
+    # -- loading (Engine::LoadGraph) ------------------------------------------
+    def load_csr(self, n, offsets, dst, w=None):
+        off = np.ascontiguousarray(offsets, np.uint64)
+        d = np.ascontiguousarray(dst, np.uint32)
+        ww = None if w is None else np.ascontiguousarray(w, np.uint32)
+        self._check(lib().dycg_load_graph_csr(self._h, n, _ptr(off, ctypes.c_uint64),
+                                              _ptr(d, ctypes.c_uint32), _ptr(ww, ctypes.c_uint32)),
+                    "load_csr")
+        self.n = n
+
+    def load_file(self, path, min_nodes=0, weighted=False):
+        self._check(lib().dycg_load_graph_file(self._h, path.encode(), min_nodes, int(weighted)),
+                    "load_file")
+        self.n = self.info()["nodes"]
+
+    def load_rmat(self, scale, edge_factor=16, seed=1, a=0.57, b=0.19, c=0.19, wlo=1, whi=64,
+                  symmetrize=False):
+        self._check(lib().dycg_load_graph_rmat(self._h, scale, edge_factor, a, b, c, seed, wlo,
+                                               whi, int(symmetrize)), "load_rmat")
+        self.n = 1 << scale
+
+    def load_grid(self, side, shortcut_permille=10, radius=8, seed=1, wlo=1, whi=1000):
+        self._check(lib().dycg_load_graph_grid(self._h, side, shortcut_permille, radius, seed,
+                                               wlo, whi), "load_grid")
+        self.n = side * side
+
+    LoadGraph = load_csr
+
+    # -- solve (InitGraph + Start / StartPageRank) ----------------------------
+    def start(self):
+        self._check(lib().dycg_init(self._h), "init")
+
+    Start = start
+    StartPageRank = start
+
+    def InitGraph(self, source=None):
+        """The source is fixed at construction (dycg_options.source)."""
+        if source is not None and source != self.options.source:
+            raise DycgError(-1, "source differs from the engine's configured source")
+
+    # -- batches ---------------------------------------------------------------
+    def delete_edges(self, dels):
+        arr = edges_array(dels)
+        st = BatchStats()
+        self._check(lib().dycg_delete_edges(self._h, arr.ctypes.data_as(ctypes.POINTER(Edge)),
+                                            arr.shape[0], ctypes.byref(st)), "delete_edges")
+        self.last_stats = st.as_dict()
+        return self.last_stats
+
+    def insert_edges(self, adds):
+        arr = edges_array(adds)
+        st = BatchStats()
+        self._check(lib().dycg_insert_edges(self._h, arr.ctypes.data_as(ctypes.POINTER(Edge)),
+                                            arr.shape[0], ctypes.byref(st)), "insert_edges")
+        self.last_stats = st.as_dict()
+        return self.last_stats
+
+    del_edge = delete_edges
+    add_edge = insert_edges
+
+    def apply_batch(self, dels, adds):
+        d = edges_array(dels)
+        a = edges_array(adds)
+        st = BatchStats()
+        self._check(lib().dycg_apply_batch(self._h, d.ctypes.data_as(ctypes.POINTER(Edge)),
+                                           d.shape[0], a.ctypes.data_as(ctypes.POINTER(Edge)),
+                                           a.shape[0], ctypes.byref(st)), "apply_batch")
+        self.last_stats = st.as_dict()
+        return self.last_stats
+
+    UpdatePageRank = apply_batch
+
+    def apply_batch_device(self, d_dels_ptr, nd, d_adds_ptr, na, stats=None):
+        """Records already in device memory (raw device addresses)."""
+        st = stats if stats is not None else BatchStats()
+        self._check(lib().dycg_apply_batch_device(self._h, ctypes.c_void_p(d_dels_ptr), nd,
+                                                  ctypes.c_void_p(d_adds_ptr), na,
+                                                  ctypes.byref(st)), "apply_batch_device")
+        return st
+
+    def cache_maintenance(self):
+        st = BatchStats()
+        self._check(lib().dycg_cache_maintenance(self._h, ctypes.byref(st)), "cache_maintenance")
+        return st.as_dict()
+
+    # The reference's separate hotness/candidate/eviction/compaction/load steps
+    # are one call here: the page cache has no compaction step.
+    compute_hot_vertices_sssp = cache_maintenance
+    LoadCache = cache_maintenance
+
+    # -- results ---------------------------------------------------------------
+    def gather(self):
+        v = np.empty(self.n, np.uint32)
+        p = np.empty(self.n, np.uint32)
+        self._check(lib().dycg_gather(self._h, _ptr(v, ctypes.c_uint32), _ptr(p, ctypes.c_uint32)),
+                    "gather")
+        return v, p
+
+    def GatherValue(self):
+        return self.gather()[0]
+
+    def GatherParent(self):
+        return self.gather()[1]
+
+    def gather_ranks(self):
+        x = np.empty(self.n, np.float32)
+        r = np.empty(self.n, np.float32)
+        self._check(lib().dycg_gather_ranks(self._h, _ptr(x, ctypes.c_float),
+                                            _ptr(r, ctypes.c_float)), "gather_ranks")
+        return x, r
+
+    def row(self, v, incoming=False, cap=None):
+        deg = ctypes.c_uint32(0)
+        self._check(lib().dycg_get_row(self._h, v, int(incoming), None, None, 0, ctypes.byref(deg)),
+                    "get_row")
+        n = deg.value
+        d = np.empty(max(n, 1), np.uint32)
+        w = np.empty(max(n, 1), np.uint32)
+        self._check(lib().dycg_get_row(self._h, v, int(incoming), _ptr(d, ctypes.c_uint32),
+                                       _ptr(w, ctypes.c_uint32), n, ctypes.byref(deg)), "get_row")
+        return d[:n], w[:n]
+
+    def csr(self):
+        m = self.info()["live_edges"]
+        off = np.empty(self.n + 1, np.uint64)
+        dst = np.empty(max(m, 1), np.uint32)
+        w = np.empty(max(m, 1), np.uint32)
+        self._check(lib().dycg_export_csr(self._h, _ptr(off, ctypes.c_uint64),
+                                          _ptr(dst, ctypes.c_uint32), _ptr(w, ctypes.c_uint32)),
+                    "export_csr")
+        return off, dst[:m], w[:m]
+
+    def info(self):
+        gi = GraphInfo()
+        self._check(lib().dycg_graph_info_get(self._h, ctypes.byref(gi)), "graph_info")
+        return gi.as_dict()
+
+    def sample_edges(self, count, seed):
+        out = np.empty((count, 3), np.uint32)
+        self._check(lib().dycg_sample_edges(self._h, count, seed,
+                                            out.ctypes.data_as(ctypes.POINTER(Edge))),
+                    "sample_edges")
+        return out
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(lib().dycg_stream(self._h, ctypes.byref(s)), "stream")
+        return s.value

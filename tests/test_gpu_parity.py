@@ -1,0 +1,346 @@
+"""GPU parity: libdycg (through the C ABI) against the CPU oracle and the
+reference's golden vectors. SSSP distances, BFS levels and CC labels must be
+bit-exact; parents must be tight witnesses of live edges; PageRank is
+compared with an FP64 oracle within the bound stated in each test."""
+import numpy as np
+import pytest
+
+import dycgraph_b200 as dg
+import oracle
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+ALGO = {"sssp": oracle.SSSP, "bfs": oracle.BFS, "cc": oracle.CC, "pr": oracle.PR}
+
+
+def engine_for(algo, n, off, dst, w=None, **kw):
+    e = dg.Engine(algo, **kw)
+    e.load_csr(n, off, dst, w)
+    e.start()
+    return e
+
+
+def check_parents(e, algo, vals, par, source=0, stored=False):
+    """Every reachable non-root vertex names a parent with a live edge that is tight."""
+    off, dst, w = e.csr()
+    n = len(vals)
+    bad = 0
+    for v in range(n):
+        if vals[v] == dg.engine.INF:
+            assert par[v] == dg.engine.INF
+            continue
+        if algo == "cc":
+            if vals[v] == v:
+                continue
+        elif v == source:
+            continue
+        p = int(par[v])
+        assert p < n, (v, p)
+        row = dst[int(off[p]):int(off[p + 1])]
+        wr = w[int(off[p]):int(off[p + 1])]
+        hits = np.nonzero(row == v)[0]
+        if len(hits) == 0:
+            bad += 1
+            continue
+        if algo == "cc":
+            ok = vals[p] == vals[v]
+        else:
+            wt = [int(wr[i]) if stored else cases.rule_w(ALGO[algo], p, v) for i in hits]
+            ok = any(int(vals[p]) + x == int(vals[v]) for x in wt)
+        bad += not ok
+    assert bad == 0
+
+
+# ---- golden vectors from the reference's own smoke tests --------------------
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp"])
+@pytest.mark.parametrize("budget", [0, 1 << 16])
+def test_golden_smoke_bfs_sssp(algo, budget):
+    case = cases.load("smoke_bfs_sssp.json")
+    n = case["n"]
+    off, dst, _ = cases.csr(n, case["graph"])
+    e = engine_for(algo, n, off, dst, hbm_graph_budget_bytes=budget, page_shift=8)
+    got = []
+    for b in case["batches"]:
+        e.delete_edges(cases.triples(b["dels"], ALGO[algo]))
+        got.append(("delete", oracle.checksum(e.gather()[0])))
+        e.insert_edges(cases.triples(b["adds"], ALGO[algo]))
+        if budget:
+            e.cache_maintenance()
+        got.append(("batch", oracle.checksum(e.gather()[0])))
+    want = [(x["phase"], x["checksum"]) for x in case["expected"][algo]]
+    assert got == want
+    vals, par = e.gather()
+    assert list(vals) == case["final_values"][algo]
+    check_parents(e, algo, vals, par)
+
+
+def test_golden_smoke_cc():
+    case = cases.load("smoke_cc.json")
+    n = case["n"]
+    off, dst, _ = cases.csr(n, case["graph"])
+    e = engine_for("cc", n, off, dst)
+    got = []
+    for b in case["batches"]:
+        e.delete_edges(cases.triples(b["dels"], oracle.CC))
+        got.append(("delete", oracle.checksum(e.gather()[0])))
+        e.insert_edges(cases.triples(b["adds"], oracle.CC))
+        got.append(("batch", oracle.checksum(e.gather()[0])))
+    assert got == [(x["phase"], x["checksum"]) for x in case["expected"]]
+    vals, par = e.gather()
+    assert list(vals) == case["final_labels"]
+    check_parents(e, "cc", vals, par)
+
+
+def test_golden_smoke_cc_fused_batches():
+    case = cases.load("smoke_cc.json")
+    n = case["n"]
+    off, dst, _ = cases.csr(n, case["graph"])
+    e = engine_for("cc", n, off, dst)
+    for b in case["batches"]:
+        e.apply_batch(cases.triples(b["dels"], oracle.CC), cases.triples(b["adds"], oracle.CC))
+    assert oracle.checksum(e.gather()[0]) == case["expected"][-1]["checksum"]
+
+
+def test_golden_topology_replay_mutation():
+    """Chunk-store occurrence semantics against the reference's topology_replay output."""
+    case = cases.load("topology_replay.json")
+    n = 1 + max(max(max(x) for x in case["graph"]), max(max(u, v) for _, u, v in case["updates"]))
+    off, dst, _ = cases.csr(n, case["graph"])
+    e = engine_for("sssp", n, off, dst)
+    for bi, (dels, adds) in enumerate(cases.replay_batches(case["updates"], case["sizes"])):
+        st = e.apply_batch(cases.triples(dels), cases.triples(adds))
+        want = case["replay_batches"][bi]
+        assert st["missing_deletes"] == want["missing_deletes"]
+        assert e.info()["live_edges"] == want["graph_edges"]
+        for s in case["replay_sources"]:
+            if s["batch"] == bi:
+                row, _ = e.row(s["source"])
+                assert len(row) == s["after_degree"]
+                h = 1469598103934665603
+                for d in sorted(int(x) for x in row):
+                    h = ((h ^ d) * 1099511628211) & (2**64 - 1)
+                h = ((h ^ len(row)) * 1099511628211) & (2**64 - 1)
+                assert h == s["multiset_hash"]
+
+
+def _pr_bound(r_gpu, n, alpha=0.85):
+    # x* - x = (I - alpha P^T)^{-1} r: |x* - x|_inf <= |r|_1 / (1 - alpha); plus FP32
+    # rounding of ranks of order 1 (relative 2^-23 per accumulation, a few hundred deep)
+    return float(np.sum(np.abs(r_gpu.astype(np.float64)))) / (1 - alpha) + 1e-4
+
+
+def test_golden_pr_smoke():
+    case = cases.load("smoke_pr.json")
+    n = case["n"]
+    off, dst, _ = cases.csr(n, case["graph"])
+    e = engine_for("pr", n, off, dst, epsilon=1e-7, max_rounds=100000)
+    x, r = e.gather_ranks()
+    assert np.max(np.abs(x - np.array(case["initial_ranks"]))) <= _pr_bound(r, n)
+    for b in case["batches"]:
+        e.apply_batch(cases.triples(b["dels"]), cases.triples(b["adds"]))
+    x, r = e.gather_ranks()
+    fin = np.array(case["final_ranks"])
+    err = np.max(np.abs(x.astype(np.float64) - fin))
+    assert err <= _pr_bound(r, n), err
+    assert np.max(np.abs(r)) <= 1e-7 * 1.0001
+
+
+def test_golden_pr_probe():
+    case = cases.load("pr_probe.json")
+    ref = np.array(case["reference_ranks"])
+    n = len(ref)
+    off, dst, _ = cases.csr(n, case["graph"])
+    e = engine_for("pr", n, off, dst, epsilon=1e-7, max_rounds=100000)
+    for dels, adds in cases.replay_batches(case["updates"], case["sizes"]):
+        e.apply_batch(cases.triples(dels), cases.triples(adds))
+    x, r = e.gather_ranks()
+    err = float(np.max(np.abs(x.astype(np.float64) - ref)))
+    # the reference's own GPU result on this probe is within 1.39e-6
+    assert err < 2e-6, err
+
+
+# ---- seeded random workloads vs the oracle restatement ----------------------
+
+def run_random(algo, scale, batches, nd, na, seed, budget=0, stored=False, symmetric=False,
+               split=False, page_shift=8):
+    n, off, dst, w = cases.small_rmat(scale, 8, seed)
+    if symmetric:
+        src = np.repeat(np.arange(n), np.diff(off).astype(np.int64))
+        pairs = np.unique(np.concatenate([np.stack([src, dst], 1), np.stack([dst, src], 1)]), axis=0)
+        off, dst, _ = cases.csr(n, pairs)
+        w = cases.hw(np.repeat(np.arange(n), np.diff(off).astype(np.int64)), dst)
+    wmode = "stored" if stored else "hash128"
+    e = engine_for(algo, n, off, dst, w if stored else None, weight_mode=wmode,
+                   hbm_graph_budget_bytes=budget, page_shift=page_shift, symmetric=symmetric)
+    orc = oracle.Oracle(ALGO[algo], n, off, dst, w if stored else None,
+                        weight_mode=oracle.WEIGHT_STORED if stored else oracle.WEIGHT_HASH128,
+                        symmetric=symmetric)
+    orc.init()
+    assert (e.gather()[0] == orc.values()[0]).all()
+    cur_off, cur_dst, cur_w = off, dst, w
+    for bi in range(batches):
+        dels, adds = cases.random_batch(n, cur_off, cur_dst, cur_w, nd, na, seed * 100 + bi)
+        if not stored:
+            dels = [(u, v, cases.rule_w(ALGO[algo], u, v)) for u, v, _ in dels]
+            adds = [(u, v, cases.rule_w(ALGO[algo], u, v)) for u, v, _ in adds]
+        if symmetric:
+            dels = dels + [(v, u, x) for u, v, x in dels]
+            adds = adds + [(v, u, x) for u, v, x in adds]
+        if split:
+            e.delete_edges(dels)
+            orc.delete_edges(dels)
+            assert (e.gather()[0] == orc.values()[0]).all(), ("delete stage", bi)
+            e.insert_edges(adds)
+            orc.insert_edges(adds)
+        else:
+            st = e.apply_batch(dels, adds)
+            orc.apply_batch(dels, adds)
+            assert st["missing_deletes"] == orc.stats()["missing_deletes"]
+        vals, par = e.gather()
+        ovals = orc.values()[0]
+        assert (vals == ovals).all(), (bi, int(np.sum(vals != ovals)))
+        cur_off, cur_dst, cur_w = orc.csr()
+    # static recompute of the final graph
+    if algo == "sssp":
+        ref = oracle.static_sssp(n, cur_off, cur_dst, cur_w if stored else None,
+                                 oracle.WEIGHT_STORED if stored else oracle.WEIGHT_HASH128, 0)
+    elif algo == "bfs":
+        ref = oracle.static_bfs(n, cur_off, cur_dst, 0)
+    else:
+        ref = oracle.static_cc(n, cur_off, cur_dst)
+    assert (vals == ref).all()
+    check_parents(e, algo, vals, par, stored=stored)
+    return e
+
+
+@pytest.mark.parametrize("algo", ["sssp", "bfs", "cc"])
+def test_random_fused_uncached(algo):
+    run_random(algo, 10, 4, 300, 300, seed=3)
+
+
+@pytest.mark.parametrize("algo", ["sssp", "bfs", "cc"])
+def test_random_split_phases(algo):
+    run_random(algo, 9, 3, 200, 200, seed=5, split=True)
+
+
+def test_random_sssp_stored_weights_cached():
+    e = run_random("sssp", 11, 4, 500, 500, seed=11, budget=1 << 18, stored=True)
+    assert e.info()["cached_pages"] > 0
+
+
+def test_random_cc_symmetric():
+    run_random("cc", 10, 3, 200, 200, seed=13, symmetric=True)
+
+
+def test_random_heavy_rows_tiles():
+    # scale 14 R-MAT hubs exceed the 1024-slot heavy threshold: exercises tiles
+    n, off, dst, _ = cases.small_rmat(14, 16, 17)
+    assert int(np.max(np.diff(off))) > 4096
+    run_random("sssp", 14, 2, 2000, 2000, seed=17, budget=1 << 20)
+
+
+def test_random_pr_fused():
+    n, off, dst, _ = cases.small_rmat(10, 8, 19)
+    e = engine_for("pr", n, off, dst, epsilon=1e-7, max_rounds=100000)
+    orc = oracle.Oracle(oracle.PR, n, off, dst)
+    cur_off, cur_dst = off, dst
+    for bi in range(3):
+        dels, adds = cases.random_batch(n, cur_off, cur_dst, None, 200, 200, 900 + bi)
+        e.apply_batch(dels, adds)
+        orc.mutate(dels, adds)
+        cur_off, cur_dst, _ = orc.csr()
+    x, r = e.gather_ranks()
+    ref = oracle.static_pr(n, cur_off, cur_dst)
+    err = float(np.max(np.abs(x.astype(np.float64) - ref)))
+    assert err <= _pr_bound(r, n), err
+
+
+# ---- edge cases ---------------------------------------------------------------
+
+def test_empty_batches_and_invalid_ids():
+    case = cases.load("smoke_bfs_sssp.json")
+    n = case["n"]
+    off, dst, _ = cases.csr(n, case["graph"])
+    e = engine_for("sssp", n, off, dst)
+    before = e.gather()[0].copy()
+    st = e.apply_batch([], [])
+    assert st["deletions"] == 0 and st["insertions"] == 0
+    st = e.apply_batch([(n + 5, 1, 1), (1, n, 1)], [(n, 0, 1), (0, n + 1, 1)])
+    assert st["invalid_updates"] == 4
+    assert (e.gather()[0] == before).all()
+    # missing delete and duplicate delete of a single occurrence
+    st = e.apply_batch([(5, 900, 1), (0, 1, 1), (0, 1, 1)], [])
+    assert st["missing_deletes"] == 2
+    vals = e.gather()[0]
+    assert vals[0] == 0
+
+
+def test_delete_all_source_edges_then_reinsert():
+    case = cases.load("smoke_bfs_sssp.json")
+    n = case["n"]
+    off, dst, _ = cases.csr(n, case["graph"])
+    e = engine_for("bfs", n, off, dst)
+    row, _ = e.row(0)
+    e.apply_batch([(0, int(v), 1) for v in row], [])
+    vals = e.gather()[0]
+    assert vals[0] == 0 and (vals[1:] == dg.engine.INF).all()
+    e.apply_batch([], [(0, int(v), 1) for v in row])
+    assert list(e.gather()[0]) == list(oracle.static_bfs(n, off, dst, 0))
+
+
+def test_self_loops_and_multigraph():
+    pairs = [(0, 1), (0, 1), (1, 1), (1, 2), (2, 0), (2, 3)]
+    off, dst, _ = cases.csr(4, pairs)
+    e = engine_for("sssp", 4, off, dst)
+    e.apply_batch([(0, 1, 0)], [])
+    assert e.gather()[0][1] == (0 + 1) % 128 + 1  # one copy of 0->1 survives
+    e.apply_batch([(0, 1, 0)], [(1, 1, 0)])
+    vals = e.gather()[0]
+    assert vals[1] == dg.engine.INF and vals[3] == dg.engine.INF
+
+
+def test_row_growth_relocation():
+    # star growth beyond every power-of-two block: rows relocate, stay exact
+    off, dst, _ = cases.csr(2000, [(0, 1), (1, 2)])
+    e = engine_for("sssp", 2000, off, dst)
+    st_total = 0
+    for k in range(5):
+        adds = [(0, v, 1) for v in range(3 + k * 300, 3 + (k + 1) * 300)]
+        st = e.apply_batch([], adds)
+        st_total += st["relocated_rows"]
+    assert st_total >= 3
+    row, _ = e.row(0)
+    assert len(row) == 1501
+    off2, dst2, _ = e.csr()
+    assert list(e.gather()[0]) == list(oracle.static_sssp(2000, off2, dst2, None, 0, 0))
+
+
+def test_gpu_rmat_loader_matches_host_draws():
+    """dycg_load_graph_rmat builds exactly the de-duplicated draws of dycg_gen_rmat_edges."""
+    scale, ef, seed = 12, 8, 99
+    e = dg.Engine("sssp", weight_mode="stored")
+    e.load_rmat(scale, ef, seed=seed)
+    d = dg.gen_rmat_edges(scale, ef << scale, seed)
+    keys = np.unique(d[d[:, 0] != d[:, 1], 0].astype(np.uint64) << np.uint64(32) |
+                     d[d[:, 0] != d[:, 1], 1].astype(np.uint64))
+    off, dst, w = e.csr()
+    src = np.repeat(np.arange(1 << scale, dtype=np.uint64), np.diff(off).astype(np.int64))
+    got = np.sort((src << np.uint64(32)) | dst.astype(np.uint64))
+    assert (got == keys).all()
+    assert all(dg.hash_weight(seed, int(s), int(t)) == x for s, t, x in zip(src[:200], dst[:200], w[:200]))
+    e.start()
+    vals = e.gather()[0]
+    ref = oracle.static_sssp(1 << scale, off, dst, w, oracle.WEIGHT_STORED, 0)
+    assert (vals == ref).all()
+
+
+def test_sample_edges_distinct_and_live():
+    n, off, dst, w = cases.small_rmat(10, 8, 23)
+    e = engine_for("sssp", n, off, dst, w, weight_mode="stored")
+    s = e.sample_edges(500, 5)
+    assert len({(int(a), int(b)) for a, b, _ in s}) == 500
+    src = np.repeat(np.arange(n), np.diff(off).astype(np.int64))
+    live = {(int(a), int(b)): int(c) for a, b, c in zip(src, dst, w)}
+    assert all(live[(int(a), int(b))] == int(c) for a, b, c in s)

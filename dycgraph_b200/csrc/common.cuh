@@ -15,8 +15,10 @@
 //
 // Vertex state for SSSP/BFS/CC is one 64-bit key per vertex:
 //   key = (value << 32) | (parent + 1), parent field 0 = no parent.
-// atomicMin on the key keeps value and parent consistent and breaks ties
-// toward the smaller parent id.
+// One 64-bit atomic keeps value and parent consistent. With weights >= 1
+// (BFS, the (u+v)%128+1 rule) atomicMin is used and equal values break toward
+// the smaller parent id; where zero weights can occur (CC, stored weights) the
+// parent only moves on a strict value decrease (see repair.cu).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>

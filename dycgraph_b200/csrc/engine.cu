@@ -541,7 +541,7 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
   if (nd > 0x3FFFFFFFull || na > 0x3FFFFFFFull) throw Error(DYCG_EINVAL, "batch too large");
   if (mode == 1) na = 0;
   if (mode == 2) nd = 0;
-  ensure_batch(std::max(nd, na));
+  ensure_batch(std::max<size_t>(std::max(nd, na), 1));
   const uint64_t l0 = launches_;
   CK(cudaEventRecord(ev_[0], st_));
   const dycg_edge_dev *d_dels = (const dycg_edge_dev *)dels;

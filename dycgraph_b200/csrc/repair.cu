@@ -52,6 +52,27 @@ __device__ __forceinline__ u64 reset_key(uint32_t v) {
   return ALGO == ALGO_CC ? pack_key(v, 0) : KEY_INF;
 }
 
+// Lower key[v] to cand only when the value strictly decreases. With
+// zero-weight edges (CC labels; stored weights may be 0) an equal value must
+// not move the parent: a switch to a smaller-id parent of equal value can
+// close a cycle in the parent forest, and deletion repair follows parents.
+// Returns true when this call lowered the value.
+__device__ __forceinline__ bool strict_lower(u64 *addr, u64 cand) {
+  u64 old = ld_key(addr);
+  while (key_value(cand) < key_value(old)) {
+    const u64 prev = atomicCAS(addr, old, cand);
+    if (prev == old) return true;
+    old = prev;
+  }
+  return false;
+}
+
+// Zero-weight edges possible: strict value decrease only.
+template <uint32_t ALGO, bool STORED>
+struct Strict {
+  static constexpr bool value = ALGO == ALGO_CC || STORED;
+};
+
 // Children of an affected vertex become affected.
 template <uint32_t ALGO>
 struct InvalidateOp {
@@ -92,7 +113,10 @@ struct PullOp {
   }
   __device__ void end(uint32_t v, Row &r) {
     const u64 m = warp_min(r.best);
-    if (lane_id() == 0 && m != KEY_INF) atomicMin(P->key + v, m);
+    if (lane_id() == 0 && m != KEY_INF) {
+      if (Strict<ALGO, STORED>::value) strict_lower(P->key + v, m);
+      else atomicMin(P->key + v, m);
+    }
   }
 };
 
@@ -117,12 +141,15 @@ struct RelaxOp {
       const u64 c = (u64)r.dv + (STORED ? w : rule_weight<ALGO>(x, y));
       if (c < INF32) {
         const u64 cand = pack_key((uint32_t)c, x + 1u);
-        if (cand < ld_key(P->key + y)) {
-          const u64 old = atomicMin(P->key + y, cand);
-          if (key_value(old) > (uint32_t)c) {
-            acc.improved++;
-            want = atomicExch(P->wtag + y, tag) != tag;
-          }
+        bool lowered = false;
+        if (Strict<ALGO, STORED>::value) {
+          lowered = strict_lower(P->key + y, cand);
+        } else if (cand < ld_key(P->key + y)) {
+          lowered = key_value(atomicMin(P->key + y, cand)) > (uint32_t)c;
+        }
+        if (lowered) {
+          acc.improved++;
+          want = atomicExch(P->wtag + y, tag) != tag;
         }
       }
     }
@@ -209,11 +236,13 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
           const u64 c = (u64)du + (STORED ? e.z : rule_weight<ALGO>(e.x, e.y));
           if (c < INF32) {
             const u64 cand = pack_key((uint32_t)c, e.x + 1u);
-            if (cand < ld_key(P.key + v)) {
-              const u64 old = atomicMin(P.key + v, cand);
-              if (key_value(old) > (uint32_t)c)
-                want = atomicExch(P.wtag + v, P.tag_base) != P.tag_base;
+            bool lowered = false;
+            if (Strict<ALGO, STORED>::value) {
+              lowered = strict_lower(P.key + v, cand);
+            } else if (cand < ld_key(P.key + v)) {
+              lowered = key_value(atomicMin(P.key + v, cand)) > (uint32_t)c;
             }
+            if (lowered) want = atomicExch(P.wtag + v, P.tag_base) != P.tag_base;
           }
         }
       }

@@ -1,0 +1,402 @@
+"""Benchmark: per-snapshot delta repair on an out-of-memory R-MAT graph.
+
+Workload (the headline configuration): R-MAT scale 26 (67.1M vertices, edge
+factor 16, a=.57 b=.19 c=.19, self-loops and duplicates removed, ~1.07B
+directed edges), uint32 weights uniform in [1,64] stored with every
+adjacency slot, SSSP from vertex 0, the graph held in pinned host memory with
+its HBM residency capped at 4 GB, snapshots of 100K updates (50K deletions
+sampled uniformly from live edges, 50K R-MAT insertions). Synthetic data: the
+reference's datasets are not available, seeded R-MAT stands in for them.
+
+One step = one snapshot (deletions, insertions, repair, cache maintenance).
+  value: updates/s with the snapshot's records already resident in HBM
+         (dycg_apply_batch_device), timed with CUDA events on the engine stream.
+  e2e:   the same through dycg_apply_batch with host buffers (H2D of the
+         records and D2H of the batch counters inside the timed region).
+N > 1 GPUs run independent replicas (a snapshot repair does not shard).
+
+`--impl reference` times the reference's repair algorithm on the host cores
+(the CPU oracle restatement; the reference's own engine cannot be built here)
+on the same workload.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "batch-repair edges/s (updates applied and repaired per second)"
+UNIT = "updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dycg", choices=["dycg", "reference"])
+    ap.add_argument("--algo", default="sssp", choices=["sssp", "bfs", "cc", "pr"])
+    ap.add_argument("--scale", type=int, default=26)
+    ap.add_argument("--edge-factor", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=100_000, help="updates per snapshot (50/50)")
+    ap.add_argument("--budget-gb", type=float, default=4.0)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--cpu-baseline-batches", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--json-out", default=None)
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def make_batches(scale, total_batches, nd, na, seed, sample_fn):
+    """Deletions: nd distinct live edges per snapshot, disjoint across snapshots
+    (sampled once from the initial graph); insertions: R-MAT draws."""
+    import dycgraph_b200 as dg
+    dels = sample_fn(total_batches * nd, seed)
+    adds = dg.gen_rmat_edges(scale, total_batches * na, seed + 1, first=0)
+    return [(dels[i * nd:(i + 1) * nd], adds[i * na:(i + 1) * na]) for i in range(total_batches)]
+
+
+# ----------------------------------------------------------------------------
+def run_dycg(args):
+    import torch
+    import dycgraph_b200 as dg
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    K, W = args.steps, max(args.warmup, 3)
+    E = args.e2e_steps if args.e2e_steps is not None else K
+    nd = args.batch // 2
+    na = args.batch - nd
+    algo = args.algo
+    budget = int(args.budget_gb * (1 << 30))
+
+    t0 = time.time()
+    eng = dg.Engine(algo, weight_mode="stored" if algo == "sssp" else "hash128",
+                    hbm_graph_budget_bytes=budget, symmetric=(algo == "cc"), epsilon=1e-4,
+                    device=local)
+    eng.load_rmat(args.scale, args.edge_factor, seed=args.seed, wlo=1, whi=64,
+                  symmetrize=(algo == "cc"))
+    t_load = time.time() - t0
+    t0 = time.time()
+    eng.start()
+    t_init = time.time() - t0
+    info = eng.info()
+    batches = make_batches(args.scale, W + K + E, nd, na, args.seed + 17 + 1000 * rank,
+                           eng.sample_edges)
+    if algo == "cc":  # symmetric updates on the symmetrised graph
+        batches = [(np.concatenate([d, d[:, [1, 0, 2]]]), np.concatenate([a, a[:, [1, 0, 2]]]))
+                   for d, a in batches]
+    per_step_updates = sum(len(d) + len(a) for d, a in batches[:1])
+    dev_batches = [(torch.from_numpy(d.astype(np.int32)).cuda(), torch.from_numpy(a.astype(np.int32)).cuda())
+                   for d, a in batches[:W + K]]
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(eng.stream())
+
+    def dev_step(i, st):
+        d, a = dev_batches[i]
+        eng.apply_batch_device(d.data_ptr(), d.shape[0], a.data_ptr(), a.shape[0], st)
+
+    stats = dg.BatchStats()
+    for i in range(W):
+        dev_step(i, stats)
+    # timed region: device-resident records
+    clocks = Clocks(local)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    per = []
+    ev0.record(stream)
+    for i in range(W, W + K):
+        dev_step(i, stats)
+        per.append(stats.as_dict())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        torch.distributed.barrier()
+    # e2e: host buffers through the public C ABI
+    e2e_ms = None
+    if E:
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(W + K, W + K + E):
+            d, a = batches[i]
+            eng.apply_batch(d, a)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+    times = torch.tensor([ms, e2e_ms or 0.0], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
+    ms, e2e_ms = float(times[0]), float(times[1])
+    total_updates = per_step_updates * K * world
+    value = total_updates / (ms / 1e3)
+    e2e_value = per_step_updates * E * world / (e2e_ms / 1e3) if E else None
+
+    # roofline of the dominant kernel (the persistent repair kernel; one launch
+    # per snapshot): algorithmic bytes from the kernel's own counters
+    page_bytes = 4 << 12
+    page_bytes *= 2 if algo == "sssp" else 1
+    rep_ms = np.mean([p["ms_repair"] for p in per])
+    rep_link = np.mean([p["link_bytes"] - p["mutate_link_bytes"] - p["cache_pages_loaded"] * page_bytes
+                        for p in per])
+    rep_hbm = np.mean([p["hbm_adj_bytes"] - p["mutate_hbm_bytes"] - p["cache_pages_loaded"] * page_bytes
+                       + p["state_bytes"] for p in per])
+    mut_ms = np.mean([p["ms_mutate"] for p in per])
+    mut_bytes_link = np.mean([p["mutate_link_bytes"] for p in per])
+    mut_bytes_hbm = np.mean([p["mutate_hbm_bytes"] for p in per])
+    hbm_peak, peak_kind = peaks()
+    link_h2d, link_zc = dg.measure_host_link(local, 1 << 30)
+    ach_hbm = rep_hbm / (rep_ms * 1e6)
+    ach_link = rep_link / (rep_ms * 1e6)
+    t_bound = max(rep_hbm / (hbm_peak * 1e9), rep_link / (link_zc * 1e9))
+    roofline = {
+        "kernel": f"repair_kernel<{algo}>",
+        "bound": "hbm", "achieved": round(ach_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
+        "frac": round(ach_hbm / hbm_peak, 5), "traffic": None,
+        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",
+        "algorithmic_bytes_per_launch": {"hbm": int(rep_hbm), "host_link": int(rep_link)},
+        "launch_ms": round(float(rep_ms), 4),
+        "host_link": {"achieved": round(ach_link, 2), "peak_zero_copy": round(link_zc, 2),
+                      "peak_h2d_copy": round(link_h2d, 2), "unit": "GB/s",
+                      "frac": round(ach_link / link_zc, 5)},
+        "roofline_time_frac": round(t_bound / (rep_ms / 1e3), 5),
+        "mutation_kernels": {"ms": round(float(mut_ms), 4), "link_bytes": int(mut_bytes_link),
+                             "hbm_bytes": int(mut_bytes_hbm)},
+    }
+    launches = int(sum(p["kernel_launches"] for p in per))
+    out = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": round(ms / K, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32" if algo != "pr" else "f32",
+        "data": "synthetic (seeded R-MAT; the reference's real graphs are not available)",
+        "config": {"workload": f"rmat{args.scale}-ef{args.edge_factor} {algo} "
+                               f"{args.batch // 1000}K-update snapshots, HBM graph budget "
+                               f"{args.budget_gb:g} GB",
+                   "vertices": info["nodes"], "edges": info["live_edges"],
+                   "updates_per_step": per_step_updates, "deletes_per_step": nd,
+                   "inserts_per_step": na, "weights": "uint32 uniform [1,64] stored"
+                   if algo == "sssp" else "rule", "graph_host_bytes": info["host_bytes"],
+                   "cached_pages": info["cached_pages"], "cache_slots": info["cache_slots"],
+                   "l2": "inputs larger than L2 (graph in pinned host memory, vertex state "
+                         f"{info['nodes'] * 40 / 1e9:.1f} GB in HBM)",
+                   "parallelism": f"replicas x{world}", "load_s": round(t_load, 2),
+                   "static_solve_s": round(t_init, 2)},
+        "clocks": clk,
+        "e2e": {"value": round(e2e_value, 1) if e2e_value else None, "unit": UNIT,
+                "h2d_bytes_per_step": per_step_updates * 12, "d2h_bytes_per_step": 256,
+                "steps": E},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "per_step": {k: round(float(np.mean([p[k] for p in per])), 4) for k in
+                     ("ms_ingest", "ms_mutate", "ms_repair", "ms_cache", "ms_total", "affected",
+                      "expanded", "edges_scanned", "improvements", "waves", "relocated_rows",
+                      "missing_deletes", "cache_pages_loaded")},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and algo in ("sssp", "bfs", "cc"):
+        out["cpu_baseline"] = cpu_baseline(eng, args, algo, nd, na)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    eng.close()
+    return out if rank == 0 else None
+
+
+def cpu_baseline(eng, args, algo, nd, na):
+    """Time the CPU restatement of the reference's repair on a bounded sample
+    of the same workload (the next snapshot(s), from the engine's state), and
+    check the GPU's results on those snapshots against it."""
+    import oracle
+    t0 = time.time()
+    off, dst, w = eng.csr()
+    vals, par = eng.gather()
+    threads = os.cpu_count() or 1
+    orc = oracle.Oracle({"sssp": oracle.SSSP, "bfs": oracle.BFS, "cc": oracle.CC}[algo],
+                        eng.n, off, dst, w if algo == "sssp" else None,
+                        weight_mode=oracle.WEIGHT_STORED if algo == "sssp" else oracle.WEIGHT_HASH128,
+                        symmetric=(algo == "cc"), threads=threads)
+    orc.set_state(vals, par)
+    del off, dst, w
+    setup_s = time.time() - t0
+    nb = max(1, args.cpu_baseline_batches)
+    batches = make_batches(args.scale, nb, nd, na, args.seed + 999, eng.sample_edges)
+    cpu_s = 0.0
+    parity = True
+    for d, a in batches:
+        t = time.perf_counter()
+        orc.apply_batch(d, a)
+        cpu_s += time.perf_counter() - t
+        eng.apply_batch(d, a)
+        parity &= bool((eng.gather()[0] == orc.values()[0]).all())
+    upd = sum(len(d) + len(a) for d, a in batches)
+    return {"value": round(upd / cpu_s, 1), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{nb} snapshot(s) of {upd // nb} updates on the same rmat{args.scale} graph "
+                      f"and state as the GPU run ({cpu_s:.1f} s CPU; mutation parallel over "
+                      f"sources, closures serial as in the reference's CPU-owner mode)",
+            "setup_s": round(setup_s, 1), "gpu_matches_oracle": parity}
+
+
+# ----------------------------------------------------------------------------
+def run_reference(args):
+    """The reference's repair algorithm (CPU oracle restatement) on host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    import oracle
+    K, W = args.steps, max(args.warmup, 3)
+    nd = args.batch // 2
+    na = args.batch - nd
+    algo = args.algo
+    if algo == "pr":
+        return {"impl": "reference", "unavailable": "reference arm is wired for SSSP/BFS/CC"}
+    threads = os.cpu_count() or 1
+    t0 = time.time()
+    n, off, dst, w = oracle.rmat_csr(args.scale, args.edge_factor, args.seed, wlo=1, whi=64,
+                                     with_w=(algo == "sssp"))
+    code = {"sssp": oracle.SSSP, "bfs": oracle.BFS, "cc": oracle.CC}[algo]
+    wmode = oracle.WEIGHT_STORED if algo == "sssp" else oracle.WEIGHT_HASH128
+    orc = oracle.Oracle(code, n, off, dst, w, weight_mode=wmode, threads=threads)
+    if algo == "cc":
+        orc.init()
+    else:
+        vals, par = oracle.parallel_sssp(n, off, dst, w, code, wmode, 0)
+        orc.set_state(vals, par)
+    setup_s = time.time() - t0
+    rng = np.random.default_rng(args.seed + 17)
+    m = len(dst)
+    pick = rng.choice(m, size=(W + K) * nd, replace=False)
+    src = np.searchsorted(off, pick, side="right") - 1
+    dels = np.stack([src.astype(np.uint32), dst[pick], w[pick] if w is not None else np.ones(len(pick), np.uint32)], 1)
+    adds = oracle.gen_rmat_edges(args.scale, (W + K) * na, args.seed + 18)
+    del off, dst, w
+    # a step is a bounded sample: a full snapshot, or a fixed slice of it when
+    # one snapshot would take too long on these cores
+    frac = 1.0
+    d0, a0 = dels[:nd], adds[:na]
+    t = time.perf_counter()
+    orc.apply_batch(d0, a0)
+    first = time.perf_counter() - t
+    if first > 20.0:
+        frac = max(0.05, 20.0 / first)
+    sub_d, sub_a = int(nd * frac), int(na * frac)
+    for i in range(1, W):
+        orc.apply_batch(dels[i * nd:i * nd + sub_d], adds[i * na:i * na + sub_a])
+    t = time.perf_counter()
+    for i in range(W, W + K):
+        orc.apply_batch(dels[i * nd:i * nd + sub_d], adds[i * na:i * na + sub_a])
+    el = time.perf_counter() - t
+    upd = (sub_d + sub_a) * K
+    value = upd / el
+    sample = (f"{K} steps of {sub_d + sub_a} updates ({frac:.0%} of a {args.batch}-update snapshot) "
+              f"on rmat{args.scale}-ef{args.edge_factor}; CPU restatement of the reference's repair "
+              f"(reference engine itself not buildable without its CMake deps)")
+    return {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT,
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": K, "warmup": W,
+            "ms_per_step": round(el * 1e3 / K, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded R-MAT)",
+            "config": {"workload": f"rmat{args.scale}-ef{args.edge_factor} {algo} "
+                                   f"{args.batch // 1000}K-update snapshots",
+                       "setup_s": round(setup_s, 1), "first_snapshot_s": round(first, 2)},
+            "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    out = run_reference(args) if args.impl == "reference" else run_dycg(args)
+    if out is not None:
+        line = json.dumps(out)
+        print(line, flush=True)
+        if args.json_out:
+            with open(args.json_out, "w") as f:
+                f.write(line + "\n")
+
+
+if __name__ == "__main__":
+    main()

@@ -10,7 +10,7 @@ a CUDA device is missing.
 """
 from .engine import (  # noqa: F401
     Engine, DycgError, BatchStats, GraphInfo, Edge, lib, library_path, edges_array,
-    gen_rmat_edges, hash_weight, ALGOS, STATUS,
+    gen_rmat_edges, hash_weight, measure_host_link, ALGOS, STATUS,
 )
 from . import operators  # noqa: F401
 

@@ -142,6 +142,8 @@ enum StatIdx {
   ST_TOUCHED,
   ST_PAGES_LOADED,
   ST_PAGES_EVICTED,
+  ST_MUT_LINK_BYTES,   // mutation kernels' adjacency bytes over the host link
+  ST_MUT_HBM_BYTES,    // mutation kernels' adjacency bytes in the HBM cache
   ST_COUNT
 };
 

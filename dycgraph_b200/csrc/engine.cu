@@ -725,8 +725,10 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     stats->edges_scanned = c.stat[ST_SCANNED];
     stats->improvements = c.stat[ST_IMPROVED];
     stats->waves = c.waves;
-    stats->link_bytes = c.stat[ST_LINK_BYTES];
-    stats->hbm_adj_bytes = c.stat[ST_HBM_ADJ_BYTES];
+    stats->link_bytes = c.stat[ST_LINK_BYTES] + c.stat[ST_MUT_LINK_BYTES];
+    stats->hbm_adj_bytes = c.stat[ST_HBM_ADJ_BYTES] + c.stat[ST_MUT_HBM_BYTES];
+    stats->mutate_link_bytes = c.stat[ST_MUT_LINK_BYTES];
+    stats->mutate_hbm_bytes = c.stat[ST_MUT_HBM_BYTES];
     stats->ms_ingest = ms[0];
     stats->ms_mutate = ms[1];
     stats->ms_repair = ms[2];
@@ -737,9 +739,10 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     float tot = 0;
     cudaEventElapsedTime(&tot, ev_[0], maintenance && cache_slots_ ? ev_[5] : ev_[3]);
     stats->ms_total = tot;
-    // vertex-state bytes: per expanded row 8 B key + per scanned slot 8 B key
-    // read; per improvement 8 B atomic + 4 B tag + 4 B queue slot
-    stats->state_bytes = stats->expanded * 8 + stats->edges_scanned * 8 + stats->improvements * 16;
+    // repair kernels' vertex-state bytes (algorithmic): per expanded row its
+    // 16-byte descriptor and 8-byte key, per scanned slot the neighbour's
+    // 8-byte key, per improvement 8 B key atomic + 4 B tag + 4 B queue slot
+    stats->state_bytes = stats->expanded * 24 + stats->edges_scanned * 8 + stats->improvements * 16;
   }
 }
 

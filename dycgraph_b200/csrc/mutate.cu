@@ -171,8 +171,8 @@ __global__ void delete_rows_kernel(Adj A, const uint2 *uv, const uint32_t *mult,
   link = warp_sum(link);
   hbm = warp_sum(hbm);
   if (lane == 0) {
-    if (link) atomicAdd(&ctl->stat[ST_LINK_BYTES], link);
-    if (hbm) atomicAdd(&ctl->stat[ST_HBM_ADJ_BYTES], hbm);
+    if (link) atomicAdd(&ctl->stat[ST_MUT_LINK_BYTES], link);
+    if (hbm) atomicAdd(&ctl->stat[ST_MUT_HBM_BYTES], hbm);
     if (count_missing && missing) atomicAdd(&ctl->stat[ST_MISSING], missing);
   }
 }
@@ -264,8 +264,8 @@ __global__ void add_rows_kernel(Adj A, const u64 *k, const uint32_t *wv, const u
   link = warp_sum(link);
   hbm = warp_sum(hbm);
   if (lane == 0) {
-    if (link) atomicAdd(&ctl->stat[ST_LINK_BYTES], link);
-    if (hbm) atomicAdd(&ctl->stat[ST_HBM_ADJ_BYTES], hbm);
+    if (link) atomicAdd(&ctl->stat[ST_MUT_LINK_BYTES], link);
+    if (hbm) atomicAdd(&ctl->stat[ST_MUT_HBM_BYTES], hbm);
     if (reloc) atomicAdd(&ctl->stat[ST_RELOCATED], reloc);
   }
 }

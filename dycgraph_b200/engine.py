@@ -49,14 +49,15 @@ _STAT_U64 = ["deletions", "insertions", "missing_deletes", "invalid_updates", "t
              "link_bytes", "hbm_adj_bytes", "state_bytes", "cache_pages_loaded",
              "cache_pages_evicted", "kernel_launches"]
 _STAT_F64 = ["ms_ingest", "ms_mutate", "ms_repair", "ms_cache", "ms_total"]
+_STAT_TAIL = ["mutate_link_bytes", "mutate_hbm_bytes"]
 
 
 class BatchStats(ctypes.Structure):
     _fields_ = ([(k, ctypes.c_uint64) for k in _STAT_U64] + [(k, ctypes.c_double) for k in _STAT_F64]
-                + [("reserved", ctypes.c_uint64 * 8)])
+                + [(k, ctypes.c_uint64) for k in _STAT_TAIL] + [("reserved", ctypes.c_uint64 * 6)])
 
     def as_dict(self):
-        return {k: getattr(self, k) for k in _STAT_U64 + _STAT_F64}
+        return {k: getattr(self, k) for k in _STAT_U64 + _STAT_F64 + _STAT_TAIL}
 
 
 class GraphInfo(ctypes.Structure):
@@ -115,6 +116,8 @@ def lib():
                                     u64, u64, u32, u32, ep]),
         "dycg_hash_weight": (u32, [u64, u32, u32, u32, u32]),
         "dycg_stream": (I, [P, ctypes.POINTER(P)]),
+        "dycg_measure_host_link": (I, [I, u64, ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_double)]),
         "dycg_last_error": (I, [P, ctypes.c_char_p, sz]),
         "dycg_version": (ctypes.c_char_p, []),
     }
@@ -150,6 +153,15 @@ def gen_rmat_edges(scale, count, seed, first=0, a=0.57, b=0.19, c=0.19, wlo=1, w
     if rc:
         raise DycgError(rc, "dycg_gen_rmat_edges")
     return out
+
+
+def measure_host_link(device=0, nbytes=1 << 30):
+    """(h2d copy GB/s, zero-copy read GB/s) over the host link of `device`."""
+    a, b = ctypes.c_double(0), ctypes.c_double(0)
+    rc = lib().dycg_measure_host_link(device, nbytes, ctypes.byref(a), ctypes.byref(b))
+    if rc:
+        raise DycgError(rc, "dycg_measure_host_link")
+    return a.value, b.value
 
 
 def hash_weight(seed, u, v, wlo=1, whi=64):

@@ -112,7 +112,9 @@ typedef struct dycg_batch_stats {
   double ms_repair;
   double ms_cache;
   double ms_total;
-  uint64_t reserved[8];
+  uint64_t mutate_link_bytes;  /* mutation kernels' share of link_bytes      */
+  uint64_t mutate_hbm_bytes;   /* mutation kernels' share of hbm_adj_bytes    */
+  uint64_t reserved[6];
 } dycg_batch_stats;
 
 typedef struct dycg_graph_info {
@@ -239,6 +241,12 @@ int dycg_gen_rmat_edges(uint32_t scale, double a, double b, double c, uint64_t s
 /* Weight of edge (u,v) under the seeded uniform rule used by the loaders. */
 uint32_t dycg_hash_weight(uint64_t seed, uint32_t u, uint32_t v, uint32_t wlo,
                           uint32_t whi);
+
+/* Measurement helper (no reference counterpart): host-link bandwidth on
+ * `device` with a `bytes`-sized pinned buffer -- a host-to-device copy-engine
+ * transfer and a kernel reading the mapped buffer zero-copy with 16-byte
+ * loads (best of 5 each, GB/s). */
+int dycg_measure_host_link(int device, uint64_t bytes, double *h2d_gbs, double *zero_copy_gbs);
 
 /* cudaStream_t the engine launches on (for CUDA-event timing by callers). */
 int dycg_stream(dycg_engine *e, void **stream);

@@ -82,6 +82,17 @@ def lib():
         L.orc_distance_checksum.argtypes = [u32p, ctypes.c_uint32]
         L.orc_rule_weight.restype = ctypes.c_uint32
         L.orc_rule_weight.argtypes = [ctypes.c_uint32] * 3
+        L.orc_gen_rmat_edges.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64,
+                                         ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ep]
+        L.orc_rmat_csr.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
+                                   ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                   ctypes.POINTER(u64p), ctypes.POINTER(u32p),
+                                   ctypes.POINTER(u32p), u64p]
+        L.orc_free.argtypes = [P]
+        L.orc_parallel_sssp.argtypes = [ctypes.c_uint32, u64p, u32p, u32p, ctypes.c_uint32,
+                                        ctypes.c_uint32, ctypes.c_uint32, u32p, u32p]
         _LIB = L
     return _LIB
 
@@ -259,3 +270,43 @@ def csr_from_edges(n, edges):
     off = np.cumsum(off).astype(np.uint64)
     dst = e[order, 1].astype(np.uint32) if len(e) else np.zeros(0, np.uint32)
     return off, dst, w[order] if len(e) else np.zeros(0, np.uint32)
+
+
+def gen_rmat_edges(scale, count, seed, first=0, a=0.57, b=0.19, c=0.19, wlo=1, whi=64):
+    out = np.empty((count, 3), np.uint32)
+    lib().orc_gen_rmat_edges(scale, a, b, c, seed, first, count, wlo, whi,
+                             out.ctypes.data_as(ctypes.POINTER(Edge)))
+    return out
+
+
+def rmat_csr(scale, ef, seed, a=0.57, b=0.19, c=0.19, wlo=1, whi=64, with_w=True):
+    """De-duplicated R-MAT CSR built on the host cores (numpy views over C arrays,
+    copied so the C allocations can be released)."""
+    L = lib()
+    po = ctypes.POINTER(ctypes.c_uint64)()
+    pd = ctypes.POINTER(ctypes.c_uint32)()
+    pw = ctypes.POINTER(ctypes.c_uint32)()
+    m = ctypes.c_uint64(0)
+    if L.orc_rmat_csr(scale, ef, a, b, c, seed, wlo, whi, int(with_w), ctypes.byref(po),
+                      ctypes.byref(pd), ctypes.byref(pw), ctypes.byref(m)):
+        raise MemoryError("rmat_csr failed")
+    n = 1 << scale
+    off = np.ctypeslib.as_array(po, shape=(n + 1,)).copy()
+    dst = np.ctypeslib.as_array(pd, shape=(max(m.value, 1),))[:m.value].copy()
+    w = np.ctypeslib.as_array(pw, shape=(max(m.value, 1),))[:m.value].copy() if with_w else None
+    for p in (po, pd, pw):
+        if p:
+            L.orc_free(ctypes.cast(p, ctypes.c_void_p))
+    return n, off, dst, w
+
+
+def parallel_sssp(n, off, dst, w, algo, weight_mode, source=0):
+    dist = np.empty(n, np.uint32)
+    par = np.empty(n, np.uint32)
+    off = np.ascontiguousarray(off, np.uint64)
+    dst = np.ascontiguousarray(dst, np.uint32)
+    w = None if w is None else np.ascontiguousarray(w, np.uint32)
+    lib().orc_parallel_sssp(n, _p(off, ctypes.c_uint64), _p(dst, ctypes.c_uint32),
+                            _p(w, ctypes.c_uint32), algo, weight_mode, source,
+                            _p(dist, ctypes.c_uint32), _p(par, ctypes.c_uint32))
+    return dist, par

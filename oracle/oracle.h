@@ -103,6 +103,18 @@ uint64_t orc_bellman_check(uint32_t n, const uint64_t *off, const uint32_t *dst,
                            uint32_t source, const uint32_t *dist,
                            uint64_t *missing);
 
+/* ---- workload synthesis for the CPU side of the benchmark (gen.c) ------- */
+void orc_gen_rmat_edges(uint32_t scale, double a, double b, double c, uint64_t seed,
+                        uint64_t first, uint64_t count, uint32_t wlo, uint32_t whi,
+                        orc_edge *out);
+int orc_rmat_csr(uint32_t scale, uint32_t ef, double a, double b, double c, uint64_t seed,
+                 uint32_t wlo, uint32_t whi, int with_w, uint64_t **off, uint32_t **dst,
+                 uint32_t **w, uint64_t *m);
+void orc_free(void *p);
+int orc_parallel_sssp(uint32_t n, const uint64_t *off, const uint32_t *dst, const uint32_t *w,
+                      uint32_t algo, uint32_t weight_mode, uint32_t source, uint32_t *dist,
+                      uint32_t *parent);
+
 /* samples/hybrid_sssp/hybrid_sssp.cu:335-347 (DistanceChecksum). */
 uint64_t orc_distance_checksum(const uint32_t *values, uint32_t n);
 

@@ -40,7 +40,7 @@ UNIT = "updates/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dycg", choices=["dycg", "reference"])
     ap.add_argument("--algo", default="sssp", choices=["sssp", "bfs", "cc", "pr"])
@@ -66,25 +66,35 @@ class Clocks:
         self.index = index
         self.proc = None
         self.lines = []
+        self.window = (0.0, 0.0)
 
     def start(self):
+        """Start sampling and wait for the first sample (the sampler must be
+        running when the timed region opens)."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.reader = threading.Thread(target=self._read, daemon=True)
             self.reader.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, t_begin, t_end):
+        self.window = (t_begin, t_end)
 
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.06)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -92,7 +102,9 @@ class Clocks:
             self.proc.kill()
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        b, e = self.window
+        inside = [ln for t, ln in self.lines if b - 0.05 <= t <= e + 0.05]
+        for ln in inside or [ln for _, ln in self.lines[-2:]]:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -105,7 +117,8 @@ class Clocks:
                 if val.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "samples_inside_timed_region": len(inside)}
 
 
 def peaks():
@@ -184,12 +197,14 @@ def run_dycg(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     per = []
+    t_begin = time.time()
     ev0.record(stream)
     for i in range(W, W + K):
         dev_step(i, stats)
         per.append(stats.as_dict())
     ev1.record(stream)
     torch.cuda.synchronize()
+    clocks.mark(t_begin, time.time())
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     if world > 1:

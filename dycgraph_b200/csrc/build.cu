@@ -105,8 +105,11 @@ __global__ void degree_kernel(const u64 *k, u64 m, uint32_t *deg) {
 __global__ void caps_kernel(const uint32_t *deg, uint32_t n, u64 *cap64, uint32_t *cap,
                             uint32_t *len, uint32_t *srt, uint32_t *live) {
   for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    // power-of-two blocks with headroom: a row of exactly 2^k occurrences
+    // still has room to grow before it must move
     const uint32_t d = deg[v];
-    const uint32_t c = d == 0 ? 0u : (d <= 1 ? 1u : 1u << (32 - __clz(d - 1)));
+    const uint32_t need = d + d / 16 + 1;
+    const uint32_t c = d == 0 ? 0u : (need <= 1 ? 1u : 1u << (32 - __clz(need - 1)));
     cap64[v] = c;
     cap[v] = c;
     len[v] = d;
@@ -117,14 +120,16 @@ __global__ void caps_kernel(const uint32_t *deg, uint32_t n, u64 *cap64, uint32_
 
 // Rows are contiguous in the sorted key array: slot = off[u] + (i - rowstart[u]).
 __global__ void scatter_kernel(const u64 *k, const uint32_t *wv, u64 m, const u64 *off,
-                               const u64 *rowstart, uint32_t *hdst, uint32_t *hw, u64 wseed,
-                               uint32_t wlo, uint32_t whi, int weight_from_hash, int swapped) {
+                               const u64 *rowstart, uint32_t *hdst, uint32_t *hw, uint32_t *fence,
+                               u64 wseed, uint32_t wlo, uint32_t whi, int weight_from_hash,
+                               int swapped) {
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < m;
        i += (u64)gridDim.x * blockDim.x) {
     const u64 key = k[i];
     const uint32_t u = (uint32_t)(key >> 32), v = (uint32_t)key;
     const u64 slot = off[u] + (i - rowstart[u]);
     hdst[slot] = v;
+    if ((slot & 31) == 0) fence[slot >> 5] = v;
     if (hw) {
       // weights are a property of the directed edge (source, target)
       const uint32_t s = swapped ? v : u, t = swapped ? u : v;
@@ -203,12 +208,12 @@ cudaError_t build_caps(const uint32_t *deg, uint32_t n, u64 *cap64, uint32_t *ca
 }
 
 cudaError_t build_scatter(const u64 *k, const uint32_t *wv, u64 m, const u64 *off,
-                          const u64 *rowstart, uint32_t *hdst, uint32_t *hw, u64 wseed,
-                          uint32_t wlo, uint32_t whi, int weight_from_hash, int swapped,
-                          cudaStream_t s) {
+                          const u64 *rowstart, uint32_t *hdst, uint32_t *hw, uint32_t *fence,
+                          u64 wseed, uint32_t wlo, uint32_t whi, int weight_from_hash,
+                          int swapped, cudaStream_t s) {
   if (!m) return cudaSuccess;
-  scatter_kernel<<<grid_for(m), BLOCK, 0, s>>>(k, wv, m, off, rowstart, hdst, hw, wseed, wlo,
-                                               whi, weight_from_hash, swapped);
+  scatter_kernel<<<grid_for(m), BLOCK, 0, s>>>(k, wv, m, off, rowstart, hdst, hw, fence, wseed,
+                                               wlo, whi, weight_from_hash, swapped);
   return cudaGetLastError();
 }
 

@@ -34,12 +34,13 @@ __global__ void score_kernel(uint32_t *hits, float *score, uint32_t *ids, uint32
 // flags in sorted (descending score) order: admit candidates among the top K,
 // eviction candidates among the rest.
 __global__ void flag_kernel(const uint32_t *ids, const float *sc, uint32_t npages, uint32_t K,
-                            const uint32_t *page_slot, uint32_t *fa, uint32_t *fe) {
+                            float min_score, const uint32_t *page_slot, uint32_t *fa,
+                            uint32_t *fe) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npages;
        i += gridDim.x * blockDim.x) {
     const bool top = i < K && sc[i] > 0.f;
     const bool res = page_slot[ids[i]] != PAGE_NONE;
-    fa[i] = top && !res;
+    fa[i] = top && !res && sc[i] >= min_score;
     fe[i] = !top && res;
   }
 }
@@ -98,7 +99,7 @@ static int grid_for(u64 threads) {
   return (int)b;
 }
 
-cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay,
+cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay, float min_score,
                        const uint32_t *page_slot, cudaStream_t s) {
   score_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.hits, W.score, W.ids, npages, decay);
   size_t bytes = W.temp_bytes;
@@ -106,7 +107,7 @@ cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay,
       W.temp, bytes, W.score, W.score_sorted, W.ids, W.ids_sorted, (int)npages, 0, 32, s);
   if (e != cudaSuccess) return e;
   flag_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, W.score_sorted, npages, K,
-                                                 page_slot, W.fa, W.fe);
+                                                 min_score, page_slot, W.fa, W.fe);
   bytes = W.temp_bytes;
   e = cub::DeviceScan::ExclusiveSum(W.temp, bytes, W.fa, W.sa, (int)npages, s);
   if (e != cudaSuccess) return e;

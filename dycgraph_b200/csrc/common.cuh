@@ -107,6 +107,7 @@ struct Adj {
   uint32_t *live;
   u64 *top;              // arena bump pointer (slots)
   u64 arena;             // arena size (slots)
+  uint32_t *fence;       // HBM fence index: fence[f] = id bits of slot 32*f
 };
 
 // Per-launch control block in device memory: barrier, queues, counters.
@@ -223,12 +224,14 @@ __device__ __forceinline__ uint32_t read_w_rw(const Adj &a, u64 p) {
   return cs != PAGE_NONE ? a.cw[cache_index(a, cs, p)] : a.hw[p];
 }
 
-// Write-through store of one slot (host arena + resident cached copy).
+// Write-through store of one slot (host arena + resident cached copy + the
+// HBM fence entry when the slot starts a 32-slot group).
 __device__ __forceinline__ bool write_slot(const Adj &a, u64 p, uint32_t d, uint32_t w,
                                            bool with_w) {
   uint32_t cs = a.page_slot[page_of(a, p)];
   a.hdst[p] = d;
   if (with_w) a.hw[p] = w;
+  if ((p & 31) == 0) a.fence[p >> 5] = d & VMASK;
   if (cs != PAGE_NONE) {
     u64 ci = cache_index(a, cs, p);
     a.cdst[ci] = d;
@@ -237,6 +240,7 @@ __device__ __forceinline__ bool write_slot(const Adj &a, u64 p, uint32_t d, uint
   return cs != PAGE_NONE;
 }
 
+// Tombstone/flag update of one slot: the id bits (and so the fence) are unchanged.
 __device__ __forceinline__ bool write_dst(const Adj &a, u64 p, uint32_t d) {
   uint32_t cs = a.page_slot[page_of(a, p)];
   a.hdst[p] = d;

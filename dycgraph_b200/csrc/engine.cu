@@ -102,6 +102,7 @@ Adj Engine::adj(const Arena &A) const {
   a.live = A.live;
   a.top = A.top;
   a.arena = A.slots;
+  a.fence = A.fence;
   return a;
 }
 
@@ -151,8 +152,9 @@ void Engine::build_direction(Arena &A, const u64 *keys, const uint32_t *wv, u64 
     A.h_w = (uint32_t *)hw;
     CK(cudaHostGetDevicePointer((void **)&A.d_w, hw, 0));
   }
+  A.fence = (uint32_t *)dmalloc((A.slots >> 5) * 4);
   CK(cudaMemcpyAsync(A.top, &total, 8, cudaMemcpyHostToDevice, st_));
-  CK(build_scatter(keys, wv, m, A.off, rowstart, A.d_dst, A.d_w, wseed, wlo, whi,
+  CK(build_scatter(keys, wv, m, A.off, rowstart, A.d_dst, A.d_w, A.fence, wseed, wlo, whi,
                    weight_from_hash ? 1 : 0, swapped ? 1 : 0, st_));
   sync_check("scatter");
   // free the temporaries (they are the last allocations made)
@@ -196,8 +198,11 @@ void Engine::finish_load() {
   page_hits_ = (uint32_t *)dmalloc((u64)npages_ * 4);
   CK(cudaMemsetAsync(page_slot_, 0xFF, (u64)npages_ * 4, st_));
   CK(cudaMemsetAsync(page_hits_, 0, (u64)npages_ * 4, st_));
+  // the HBM graph budget covers the fence index and the cached pages
   const u64 page_bytes = (4ull << page_shift_) * (stored_ ? 2 : 1);
-  u64 slots = opt_.cache_policy == DYCG_CACHE_NONE ? 0 : opt_.hbm_graph_budget_bytes / page_bytes;
+  const u64 fence_bytes = ((out_.slots >> 5) + (has_in_ ? (in_.slots >> 5) : 0)) * 4;
+  const u64 avail = opt_.hbm_graph_budget_bytes > fence_bytes ? opt_.hbm_graph_budget_bytes - fence_bytes : 0;
+  u64 slots = opt_.cache_policy == DYCG_CACHE_NONE ? 0 : avail / page_bytes;
   slots = std::min<u64>(slots, npages_);
   cache_slots_ = (uint32_t)slots;
   if (cache_slots_) {
@@ -515,6 +520,20 @@ void Engine::ensure_batch(size_t cnt) {
   add_uvw_ = (uint3 *)al(c * 12);
   touched_ = (uint32_t *)al(c * 2 * 4);
   counts_ = (uint32_t *)al(64);
+  reloc_.rec = (RelocRec *)al(c * sizeof(RelocRec));
+  reloc_.cap = (uint32_t)c;
+  {
+    const u64 maxslots = std::max(out_.slots, in_.slots);
+    const u64 cc = std::min<u64>(maxslots / RELOC_CHUNK + c + 1024, 0x7FFFFFFFull);
+    reloc_.chunks = (uint2 *)al(cc * sizeof(uint2));
+    reloc_.chunk_cap = (uint32_t)cc;
+  }
+  reloc_.n_reloc = counts_ + 8;
+  reloc_.n_chunks = counts_ + 9;
+  tombs_.pos = (u64 *)al(c * 8);
+  tombs_.val = (uint32_t *)al(c * 4);
+  tombs_.count = counts_ + 10;
+  tombs_.cap = (uint32_t)c;
   d_edges_ = (dycg_edge_dev *)al(c * 2 * sizeof(dycg_edge_dev));
   size_t a = 0, b = 0;
   CK(sort_keys(nullptr, a, k_tmp_out_, k_del_out_, (uint32_t)c, st_));
@@ -638,22 +657,22 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
   const Adj A_in = has_in_ ? adj(in_) : A_out;
   if (nd) {
     CK(launch_delete_rows(A_out, uv_out_, mult_out_, counts_ + 0, (uint32_t)nd, found_out_, ctl_,
-                          1, st_));
-    launches_++;
+                          1, tombs_, st_));
+    launches_ += 2;
     if (has_in_) {
       CK(launch_delete_rows(A_in, uv_in_, mult_in_, counts_ + 1, (uint32_t)nd, nullptr, ctl_, 0,
-                            st_));
-      launches_++;
+                            tombs_, st_));
+      launches_ += 2;
     }
   }
   if (na) {
     CK(launch_add_rows(A_out, k_add_out_, w_add_out_, seg_out_, counts_ + 2, (uint32_t)na,
-                       stored_ ? 1 : 0, ctl_, st_));
-    launches_++;
+                       stored_ ? 1 : 0, reloc_, ctl_, st_));
+    launches_ += 3;
     if (has_in_) {
       CK(launch_add_rows(A_in, k_add_in_, w_add_in_, seg_in_, counts_ + 3, (uint32_t)na,
-                         stored_ ? 1 : 0, ctl_, st_));
-      launches_++;
+                         stored_ ? 1 : 0, reloc_, ctl_, st_));
+      launches_ += 3;
     }
   }
   CK(cudaEventRecord(ev_[2], st_));
@@ -753,7 +772,10 @@ void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
     return;
   }
   CK(cudaEventRecord(ev_[4], st_));
-  CK(cache_rank(cwk_, npages_, cache_slots_, 0.5f, page_slot_, st_));
+  // a page must have been read at least kMinScore times (decayed) before it
+  // displaces a resident one: single random probes do not churn the cache
+  const float kMinScore = initial ? 0.f : 64.f;
+  CK(cache_rank(cwk_, npages_, cache_slots_, 0.75f, kMinScore, page_slot_, st_));
   sync_check("cache rank");
   const uint32_t n_admit = cwk_.h_counts[0] + cwk_.h_counts[1];
   const uint32_t n_evict_cand = cwk_.h_counts[2] + cwk_.h_counts[3];
@@ -761,7 +783,7 @@ void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
   const uint32_t gate = initial ? 1u : std::max<uint32_t>(1u, cache_slots_ / 1024);
   uint32_t admit = 0, evict = 0;
   if (n_admit >= gate) {
-    const uint32_t cap = initial ? cache_slots_ : std::max<uint32_t>(cache_slots_ / 16, 64u);
+    const uint32_t cap = initial ? cache_slots_ : std::max<uint32_t>(cache_slots_ / 512, 64u);
     admit = std::min(n_admit, cap);
     const uint32_t need = admit > free_count_ ? admit - free_count_ : 0u;
     evict = std::min(n_evict_cand, need);

@@ -25,6 +25,7 @@ struct Arena {
   u64 *off = nullptr;
   uint32_t *len = nullptr, *cap = nullptr, *srt = nullptr, *live = nullptr;
   u64 *top = nullptr;
+  uint32_t *fence = nullptr;  // HBM fence index (id of every 32nd slot)
 };
 
 class Engine {
@@ -106,6 +107,8 @@ class Engine {
   uint32_t *mult_out_ = nullptr, *mult_in_ = nullptr, *found_out_ = nullptr;
   uint3 *seg_out_ = nullptr, *seg_in_ = nullptr, *add_uvw_ = nullptr;
   uint32_t *touched_ = nullptr, *counts_ = nullptr;
+  Reloc reloc_{};
+  Tombs tombs_{};
   dycg_edge_dev *d_edges_ = nullptr;
   dycg_edge *h_stage_ = nullptr;
   void *cub_temp_ = nullptr;

@@ -84,6 +84,8 @@ struct Acc {
 };
 
 // Walk slots [b, e) of row v; this lane handles s0 + lane for s0 = b, b+stride...
+// Loads are issued UNROLL iterations ahead of their use so that each lane keeps
+// several zero-copy reads in flight (a host-link read costs ~1-2 us).
 // Op interface (all lanes call every member, keeping the warp converged):
 //   bool begin(uint32_t v, Row&)                  -- false: skip the row
 //   void edge(uint32_t v, uint32_t nb, uint32_t w, bool valid, Row&, Acc&)
@@ -91,40 +93,54 @@ struct Acc {
 template <bool WITH_W, class Op>
 __device__ __forceinline__ void warp_slots(const Adj &A, uint32_t v, u64 off, uint32_t b,
                                            uint32_t e, uint32_t stride, Op &op, Acc &acc) {
+  constexpr int UNROLL = 4;
   typename Op::Row r;
   if (!op.begin(v, r)) return;
   const uint32_t lane = lane_id();
+  if (lane == 0 && b == 0) acc.expanded++;
   uint32_t hit_pg = PAGE_NONE, hit_n = 0;  // lane 0: pending hotness count
   const uint32_t bytes = WITH_W ? 8u : 4u;
-  for (uint32_t s0 = b; s0 < e; s0 += stride) {
-    const uint32_t s = s0 + lane;
-    const bool in = s < e;
-    bool valid = in, cached = false;
-    uint32_t d = 0, w = 0;
-    const u64 p = off + s;
-    uint32_t pg = PAGE_NONE;
-    if (in) {
-      pg = page_of(A, p);
-      d = read_dst(A, p, cached);
-      if (d & TOMB) valid = false;
-      if (WITH_W && valid) w = read_w(A, p, cached);
-      if (cached) acc.hbm += valid ? bytes : 4u;
-      else acc.link += valid ? bytes : 4u;
-      acc.scanned++;
-    }
-    // hotness: lane 0 accumulates the warp's slots that share its page
-    const uint32_t pg0 = __shfl_sync(0xffffffffu, pg, 0);
-    const unsigned same = __ballot_sync(0xffffffffu, in && pg == pg0);
-    if (lane == 0) {
-      if (pg0 != hit_pg) {
-        if (hit_n) atomicAdd(A.page_hits + hit_pg, hit_n);
-        hit_pg = pg0;
-        hit_n = 0;
+  for (uint32_t s0 = b; s0 < e; s0 += stride * UNROLL) {
+    uint32_t d[UNROLL], w[UNROLL], pg[UNROLL];
+    bool in[UNROLL], cached[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; u++) {
+      const uint32_t s = s0 + u * stride + lane;
+      in[u] = s < e;
+      d[u] = TOMB;
+      w[u] = 0;
+      pg[u] = PAGE_NONE;
+      cached[u] = false;
+      if (in[u]) {
+        const u64 p = off + s;
+        pg[u] = page_of(A, p);
+        d[u] = read_dst(A, p, cached[u]);
+        if (WITH_W) w[u] = read_w(A, p, cached[u]);
       }
-      hit_n += __popc(same);
     }
-    if (in && pg != pg0) atomicAdd(A.page_hits + pg, 1u);
-    op.edge(v, d & VMASK, w, valid, r, acc);
+#pragma unroll
+    for (int u = 0; u < UNROLL; u++) {
+      if (s0 + u * stride >= e) break;  // warp-uniform
+      const bool valid = in[u] && !(d[u] & TOMB);
+      if (in[u]) {
+        if (cached[u]) acc.hbm += valid ? bytes : 4u;
+        else acc.link += valid ? bytes : 4u;
+        acc.scanned++;
+      }
+      // hotness: lane 0 accumulates the warp's slots that share its page
+      const uint32_t pg0 = __shfl_sync(0xffffffffu, pg[u], 0);
+      const unsigned same = __ballot_sync(0xffffffffu, in[u] && pg[u] == pg0);
+      if (lane == 0) {
+        if (pg0 != hit_pg) {
+          if (hit_n) atomicAdd(A.page_hits + hit_pg, hit_n);
+          hit_pg = pg0;
+          hit_n = 0;
+        }
+        hit_n += __popc(same);
+      }
+      if (in[u] && pg[u] != pg0) atomicAdd(A.page_hits + pg[u], 1u);
+      op.edge(v, d[u] & VMASK, w[u], valid, r, acc);
+    }
   }
   if (lane == 0 && hit_n) atomicAdd(A.page_hits + hit_pg, hit_n);
   op.end(v, r);

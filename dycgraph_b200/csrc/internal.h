@@ -67,12 +67,31 @@ cudaError_t launch_unique_runs(const u64 *k, uint32_t cnt, uint2 *uv, uint32_t *
                                uint32_t *n_out, uint32_t cap, uint32_t *err, cudaStream_t s);
 cudaError_t launch_row_segments(const u64 *k, uint32_t cnt, uint3 *seg, uint32_t *n_out,
                                 cudaStream_t s);
+// Deleted occurrences found by the read-only search, written afterwards.
+struct Tombs {
+  u64 *pos;
+  uint32_t *val;
+  uint32_t *count;
+  uint32_t cap;
+};
 cudaError_t launch_delete_rows(const Adj &A, const uint2 *uv, const uint32_t *mult,
                                const uint32_t *n_ptr, uint32_t max_n, uint32_t *found, Ctl *ctl,
-                               int count_missing, cudaStream_t s);
+                               int count_missing, const Tombs &T, cudaStream_t s);
+// Relocation bookkeeping for rows that outgrow their block.
+constexpr uint32_t RELOC_CHUNK = 1024;
+struct RelocRec {
+  uint32_t row, seg, len, pad;
+  u64 old_off, new_off;
+};
+struct Reloc {
+  RelocRec *rec;
+  uint2 *chunks;
+  uint32_t *n_reloc, *n_chunks;
+  uint32_t cap, chunk_cap;
+};
 cudaError_t launch_add_rows(const Adj &A, const u64 *k, const uint32_t *w, const uint3 *seg,
-                            const uint32_t *n_ptr, uint32_t max_n, int with_w, Ctl *ctl,
-                            cudaStream_t s);
+                            const uint32_t *n_ptr, uint32_t max_n, int with_w, const Reloc &R,
+                            Ctl *ctl, cudaStream_t s);
 cudaError_t launch_keys_to_uvw(const u64 *k, const uint32_t *w, uint32_t cnt, uint3 *out,
                                cudaStream_t s);
 cudaError_t launch_touched(const u64 *k, uint32_t cnt, uint32_t *tag, uint32_t epoch,
@@ -93,7 +112,7 @@ struct CachePages {
   uint32_t *cdst, *cw;
 };
 size_t cache_temp_bytes(uint32_t npages);
-cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay,
+cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay, float min_score,
                        const uint32_t *page_slot, cudaStream_t s);
 cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t n_evict_cand, uint32_t evict,
                         uint32_t admit, uint32_t *page_slot, uint32_t *free_list,
@@ -120,9 +139,9 @@ cudaError_t build_degrees(const u64 *k, u64 m, uint32_t *deg, cudaStream_t s);
 cudaError_t build_caps(const uint32_t *deg, uint32_t n, u64 *cap64, uint32_t *cap,
                        uint32_t *len, uint32_t *srt, uint32_t *live, cudaStream_t s);
 cudaError_t build_scatter(const u64 *k, const uint32_t *wv, u64 m, const u64 *off,
-                          const u64 *rowstart, uint32_t *hdst, uint32_t *hw, u64 wseed,
-                          uint32_t wlo, uint32_t whi, int weight_from_hash, int swapped,
-                          cudaStream_t s);
+                          const u64 *rowstart, uint32_t *hdst, uint32_t *hw, uint32_t *fence,
+                          u64 wseed, uint32_t wlo, uint32_t whi, int weight_from_hash,
+                          int swapped, cudaStream_t s);
 size_t build_temp_bytes(u64 count, bool pairs);
 cudaError_t sample_draw(u64 *pos, u64 count, u64 seed, u64 total, cudaStream_t s);
 cudaError_t sample_resolve(const u64 *pos, u64 count, const u64 *pre, uint32_t n, const Adj &A,

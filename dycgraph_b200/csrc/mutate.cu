@@ -87,37 +87,67 @@ __global__ void row_segments_kernel(const u64 *k, uint32_t cnt, uint3 *seg, uint
   }
 }
 
-// First index in [lo, hi) of the sorted prefix whose id is >= target
-// (32-ary search: each step narrows the window 32-fold with one warp read).
-__device__ uint32_t warp_lower_bound(const Adj &A, u64 off, uint32_t lo, uint32_t hi,
-                                     uint32_t target, uint32_t &reads) {
+// First index (row-relative) in the sorted prefix [0, srt) of the row at
+// arena offset off whose id is >= target; all lanes return the same index.
+// The HBM fence index holds the id of every 32nd arena slot, so a 32-ary warp
+// search over the row's fences (HBM reads) narrows the answer to one 32-slot
+// window, read from the row with a single coalesced request.
+__device__ uint32_t warp_lower_bound(const Adj &A, u64 off, uint32_t srt, uint32_t target,
+                                     uint32_t &reads) {
   const uint32_t lane = lane_id();
+  // fences inside the prefix: arena slots 32*f with off <= 32*f < off + srt
+  u64 flo = (off + 31) >> 5;
+  u64 fhi = srt ? ((off + srt - 1) >> 5) + 1 : flo;  // exclusive
+  if (fhi < flo) fhi = flo;
+  // first fence index f in [flo, fhi) with fence[f] >= target (fhi if none)
+  u64 lo = flo, hi = fhi;
   while (hi - lo > 32) {
-    const uint32_t step = (hi - lo + 31) / 32;
-    uint32_t pos = lo + (lane + 1) * step - 1;
-    if (pos >= hi) pos = hi - 1;
-    const uint32_t val = read_dst_rw(A, off + pos) & VMASK;
-    reads++;
-    const unsigned ge = __ballot_sync(0xffffffffu, val >= target);
-    if (!ge) return hi;
-    const uint32_t f = __ffs(ge) - 1;
-    const uint32_t nlo = lo + f * step;
-    const uint32_t nhi = min(lo + (f + 1) * step, hi);
+    const u64 step = (hi - lo + 31) / 32;
+    u64 f = lo + (lane + 1) * step - 1;
+    if (f >= hi) f = hi - 1;
+    const unsigned ge = __ballot_sync(0xffffffffu, A.fence[f] >= target);
+    if (!ge) {
+      lo = hi;
+      break;
+    }
+    const uint32_t k = __ffs(ge) - 1;
+    const u64 nlo = lo + k * step;
+    hi = min(lo + (k + 1) * step, hi);
     lo = nlo;
-    hi = nhi;
   }
-  const uint32_t pos = lo + lane;
-  const bool in = pos < hi;
-  const uint32_t val = in ? (read_dst_rw(A, off + pos) & VMASK) : 0xFFFFFFFFu;
-  if (in) reads++;
-  const unsigned ge = __ballot_sync(0xffffffffu, in && val >= target);
-  return ge ? lo + __ffs(ge) - 1 : hi;
+  if (hi > lo) {
+    const u64 f = lo + lane;
+    const unsigned ge = __ballot_sync(0xffffffffu, f < hi && A.fence[f] >= target);
+    lo = ge ? lo + __ffs(ge) - 1 : hi;
+  }
+  // the answer lies in (32*(lo-1), 32*lo] clipped to the prefix
+  const u64 pend = off + srt;
+  u64 wbeg = lo > flo ? ((lo - 1) << 5) + 1 : off;
+  u64 wend = lo < fhi ? (lo << 5) + 1 : pend;
+  if (wbeg < off) wbeg = off;
+  if (wend > pend) wend = pend;
+  uint32_t ans = (uint32_t)(wend - off);
+  for (u64 b = wbeg; b < wend; b += 32) {
+    const u64 p = b + lane;
+    const bool in = p < wend;
+    const uint32_t val = in ? (read_dst_rw(A, p) & VMASK) : 0xFFFFFFFFu;
+    reads += in;
+    const unsigned ge = __ballot_sync(0xffffffffu, in && val >= target);
+    if (ge) {
+      ans = (uint32_t)(b + __ffs(ge) - 1 - off);
+      break;
+    }
+  }
+  return ans;
 }
 
-// Warp per unique deletion record: tombstone up to mult live occurrences.
+// Warp per unique deletion record: find up to mult live occurrences (reads
+// only) and record them; the tombstones are written by tombstone_kernel after
+// every search of the batch has finished, so no host-link read waits behind
+// this batch's posted writes.
 __global__ void delete_rows_kernel(Adj A, const uint2 *uv, const uint32_t *mult,
                                    const uint32_t *n_ptr, uint32_t *found_out, Ctl *ctl,
-                                   int count_missing) {
+                                   int count_missing, Tombs T) {
   const uint32_t lane = lane_id();
   const uint32_t nrec = *n_ptr;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -129,43 +159,40 @@ __global__ void delete_rows_kernel(Adj A, const uint2 *uv, const uint32_t *mult,
     uint32_t remaining = mult[i], found = 0, reads = 0;
     const u64 off = A.off[row];
     const uint32_t len = A.len[row], srt = A.srt[row];
-    const uint32_t pos = warp_lower_bound(A, off, 0, srt, target, reads);
-    for (uint32_t s0 = pos; s0 < srt && remaining; s0 += 32) {
-      const uint32_t s = s0 + lane;
-      const bool in = s < srt;
-      const uint32_t d = in ? read_dst_rw(A, off + s) : 0xFFFFFFFFu;
-      reads += in;
-      const bool live = in && (d & VMASK) == target && !(d & TOMB);
-      const unsigned lm = __ballot_sync(0xffffffffu, live);
-      const uint32_t rank = __popc(lm & ((1u << lane) - 1));
-      if (live && rank < remaining) write_dst(A, off + s, d | TOMB);
-      const uint32_t take = min((uint32_t)__popc(lm), remaining);
-      remaining -= take;
-      found += take;
-      if (__ballot_sync(0xffffffffu, in && (d & VMASK) != target)) break;
-    }
-    for (uint32_t s0 = srt; s0 < len && remaining; s0 += 32) {
-      const uint32_t s = s0 + lane;
-      const bool in = s < len;
-      const uint32_t d = in ? read_dst_rw(A, off + s) : 0xFFFFFFFFu;
-      reads += in;
-      const bool live = in && (d & VMASK) == target && !(d & TOMB);
-      const unsigned lm = __ballot_sync(0xffffffffu, live);
-      const uint32_t rank = __popc(lm & ((1u << lane) - 1));
-      if (live && rank < remaining) write_dst(A, off + s, d | TOMB);
-      const uint32_t take = min((uint32_t)__popc(lm), remaining);
-      remaining -= take;
-      found += take;
+    const uint32_t pos = warp_lower_bound(A, off, srt, target, reads);
+    for (uint32_t pass = 0; pass < 2; pass++) {
+      // pass 0: the run of target in the sorted prefix; pass 1: the unsorted suffix
+      const uint32_t b = pass ? srt : pos, e2 = pass ? len : srt;
+      for (uint32_t s0 = b; s0 < e2 && remaining; s0 += 32) {
+        const uint32_t s = s0 + lane;
+        const bool in = s < e2;
+        const uint32_t d = in ? read_dst_rw(A, off + s) : 0xFFFFFFFFu;
+        reads += in;
+        const bool live = in && (d & VMASK) == target && !(d & TOMB);
+        const unsigned lm = __ballot_sync(0xffffffffu, live);
+        const uint32_t rank = __popc(lm & ((1u << lane) - 1));
+        const uint32_t take = min((uint32_t)__popc(lm), remaining);
+        uint32_t base = 0;
+        if (lane == 0 && take) base = atomicAdd(T.count, take);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (live && rank < remaining && base + rank < T.cap) {
+          T.pos[base + rank] = off + s;
+          T.val[base + rank] = d | TOMB;
+        }
+        remaining -= take;
+        found += take;
+        if (!pass && __ballot_sync(0xffffffffu, in && (d & VMASK) != target)) break;
+      }
     }
     const bool cached = len && A.page_slot[page_of(A, off)] != PAGE_NONE;
-    const u64 bytes = 4ull * reads + (lane == 0 ? 4ull * found : 0ull);
+    const u64 bytes = 4ull * reads;
     if (cached) hbm += bytes; else link += bytes;
     const u64 total_reads = warp_sum(reads);
     if (lane == 0) {
       if (found) atomicSub(A.live + row, found);
       if (found_out) found_out[i] = found;
       missing += mult[i] - found;
-      if (total_reads) atomicAdd(A.page_hits + page_of(A, off), (uint32_t)total_reads);
+      if (total_reads) atomicAdd(A.page_hits + page_of(A, off + pos), (uint32_t)total_reads);
     }
   }
   link = warp_sum(link);
@@ -177,14 +204,35 @@ __global__ void delete_rows_kernel(Adj A, const uint2 *uv, const uint32_t *mult,
   }
 }
 
+__global__ void tombstone_kernel(Adj A, Tombs T, Ctl *ctl) {
+  const uint32_t n = min(*T.count, T.cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && *T.count > T.cap) atomicCAS(&ctl->err, 0u, ERR_QUEUE);
+  u64 link = 0, hbm = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const bool c = write_dst(A, T.pos[i], T.val[i]);
+    link += 4;
+    if (c) hbm += 4;
+  }
+  link = warp_sum(link);
+  hbm = warp_sum(hbm);
+  if (lane_id() == 0) {
+    if (link) atomicAdd(&ctl->stat[ST_MUT_LINK_BYTES], link);
+    if (hbm) atomicAdd(&ctl->stat[ST_MUT_HBM_BYTES], hbm);
+  }
+}
+
 __device__ __forceinline__ uint32_t next_pow2_u32(uint32_t x) {
   return x <= 1 ? 1u : 1u << (32 - __clz(x - 1));
 }
 
-// Warp per row segment: append the segment's occurrences, relocating the row
-// to a new power-of-two block when it does not fit.
+// Warp per row segment: append the segment's occurrences in place when they
+// fit. A row that does not fit gets a new power-of-two block (with headroom)
+// at the arena tail; its descriptor moves at once, while the copy of the old
+// slots and the append are deferred to relocate_copy_kernel and
+// relocate_append_kernel, so a large row is copied by many warps instead of
+// one.
 __global__ void add_rows_kernel(Adj A, const u64 *k, const uint32_t *wv, const uint3 *seg,
-                                const uint32_t *n_ptr, int with_w, Ctl *ctl) {
+                                const uint32_t *n_ptr, int with_w, Reloc R, Ctl *ctl) {
   const uint32_t lane = lane_id();
   const uint32_t nseg = *n_ptr;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -197,7 +245,6 @@ __global__ void add_rows_kernel(Adj A, const u64 *k, const uint32_t *wv, const u
     const uint32_t len = A.len[row], cap = A.cap[row], srt = A.srt[row];
     const uint32_t live = A.live[row];
     const u64 off = A.off[row];
-    const uint32_t first_new = (uint32_t)k[start];
     if ((u64)len + count <= cap) {
       for (uint32_t j = lane; j < count; j += 32) {
         const bool c = write_slot(A, off + len + j, (uint32_t)k[start + j],
@@ -205,11 +252,9 @@ __global__ void add_rows_kernel(Adj A, const u64 *k, const uint32_t *wv, const u
         link += bytes;
         if (c) hbm += bytes;
       }
-      uint32_t nsrt = srt;
-      if (srt == len) {
-        const uint32_t last = len ? (read_dst_rw(A, off + len - 1) & VMASK) : 0u;
-        if (len == 0 || last <= first_new) nsrt = len + count;
-      }
+      // appends stay in the unsorted suffix (no host-link read here); an
+      // empty row takes its sorted run of appends as its sorted prefix
+      const uint32_t nsrt = len == 0 ? count : srt;
       if (lane == 0) {
         A.len[row] = len + count;
         A.live[row] = live + count;
@@ -217,48 +262,22 @@ __global__ void add_rows_kernel(Adj A, const u64 *k, const uint32_t *wv, const u
       }
       continue;
     }
-    // relocation
-    const uint32_t ncap = max(4u, next_pow2_u32(live + count));
-    u64 noff = 0;
-    if (lane == 0) noff = atomicAdd(A.top, (u64)ncap);
-    noff = __shfl_sync(0xffffffffu, noff, 0);
-    if (noff + ncap > A.arena) {
-      if (lane == 0) atomicCAS(&ctl->err, 0u, ERR_ARENA);
-      continue;
-    }
-    uint32_t wpos = 0, nsrt = 0, last_val = 0;
-    for (uint32_t s0 = 0; s0 < len; s0 += 32) {
-      const uint32_t s = s0 + lane;
-      const bool in = s < len;
-      const uint32_t d = in ? read_dst_rw(A, off + s) : TOMB;
-      const uint32_t w = (with_w && in && !(d & TOMB)) ? read_w_rw(A, off + s) : 0u;
-      const bool keep = in && !(d & TOMB);
-      const unsigned m = __ballot_sync(0xffffffffu, keep);
-      const unsigned ms = __ballot_sync(0xffffffffu, keep && s < srt);
-      if (keep) {
-        const bool c = write_slot(A, noff + wpos + __popc(m & ((1u << lane) - 1)), d, w, with_w);
-        link += bytes;
-        if (c) hbm += bytes;
-      }
-      if (in) link += bytes;
-      if (m) last_val = __shfl_sync(0xffffffffu, d, 31 - __clz(m)) & VMASK;
-      wpos += __popc(m);
-      nsrt += __popc(ms);
-    }
-    for (uint32_t j = lane; j < count; j += 32) {
-      const bool c = write_slot(A, noff + wpos + j, (uint32_t)k[start + j],
-                                with_w ? wv[start + j] : 0u, with_w);
-      link += bytes;
-      if (c) hbm += bytes;
-    }
-    if (nsrt == wpos && (wpos == 0 || last_val <= first_new)) nsrt = wpos + count;
     if (lane == 0) {
-      A.off[row] = noff;
-      A.cap[row] = ncap;
-      A.len[row] = wpos + count;
-      A.live[row] = wpos + count;
-      A.srt[row] = nsrt;
-      reloc++;
+      const u64 need = (u64)len + count;
+      const uint32_t ncap = next_pow2_u32((uint32_t)(need + need / 8 + 1));
+      const u64 noff = atomicAdd(A.top, (u64)ncap);
+      const uint32_t r = atomicAdd(R.n_reloc, 1u);
+      const uint32_t nchunk = (len + RELOC_CHUNK - 1) / RELOC_CHUNK;
+      const uint32_t cb = atomicAdd(R.n_chunks, nchunk);
+      if (noff + ncap > A.arena || r >= R.cap || cb + nchunk > R.chunk_cap) {
+        atomicCAS(&ctl->err, 0u, ERR_ARENA);
+      } else {
+        R.rec[r] = RelocRec{row, i, len, 0u, off, noff};
+        for (uint32_t c = 0; c < nchunk; c++) R.chunks[cb + c] = make_uint2(r, c);
+        A.off[row] = noff;
+        A.cap[row] = ncap;
+        reloc++;
+      }
     }
   }
   link = warp_sum(link);
@@ -267,6 +286,74 @@ __global__ void add_rows_kernel(Adj A, const u64 *k, const uint32_t *wv, const u
     if (link) atomicAdd(&ctl->stat[ST_MUT_LINK_BYTES], link);
     if (hbm) atomicAdd(&ctl->stat[ST_MUT_HBM_BYTES], hbm);
     if (reloc) atomicAdd(&ctl->stat[ST_RELOCATED], reloc);
+  }
+}
+
+// Warp per RELOC_CHUNK slots of a relocated row: verbatim copy (tombstones
+// included, so the sorted prefix and the live count stay valid). Each lane
+// keeps RELOC_CHUNK/32 loads in flight before storing.
+__global__ void relocate_copy_kernel(Adj A, Reloc R, int with_w, Ctl *ctl) {
+  const uint32_t lane = lane_id();
+  const uint32_t nch = min(*R.n_chunks, R.chunk_cap);
+  const uint32_t nrec = min(*R.n_reloc, R.cap);
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  constexpr uint32_t PER = RELOC_CHUNK / 32;
+  u64 link = 0, hbm = 0;
+  for (uint32_t i = gw; i < nch; i += nw) {
+    const uint2 ch = R.chunks[i];
+    if (ch.x >= nrec) continue;
+    const RelocRec rec = R.rec[ch.x];
+    const uint32_t b = ch.y * RELOC_CHUNK;
+    const uint32_t e = min(rec.len, b + RELOC_CHUNK);
+    uint32_t d[PER], w[PER];
+#pragma unroll
+    for (uint32_t t = 0; t < PER; t++) {
+      const uint32_t s = b + t * 32 + lane;
+      if (s < e) {
+        d[t] = read_dst_rw(A, rec.old_off + s);
+        w[t] = with_w ? read_w_rw(A, rec.old_off + s) : 0u;
+      }
+    }
+#pragma unroll
+    for (uint32_t t = 0; t < PER; t++) {
+      const uint32_t s = b + t * 32 + lane;
+      if (s < e) {
+        const bool c = write_slot(A, rec.new_off + s, d[t], w[t], with_w);
+        const uint32_t bytes = with_w ? 8u : 4u;
+        link += 2 * bytes;
+        if (c) hbm += bytes;
+      }
+    }
+  }
+  link = warp_sum(link);
+  hbm = warp_sum(hbm);
+  if (lane == 0) {
+    if (link) atomicAdd(&ctl->stat[ST_MUT_LINK_BYTES], link);
+    if (hbm) atomicAdd(&ctl->stat[ST_MUT_HBM_BYTES], hbm);
+  }
+}
+
+// Warp per relocated row: append its segment after the copied slots.
+__global__ void relocate_append_kernel(Adj A, const u64 *k, const uint32_t *wv,
+                                       const uint3 *seg, Reloc R, int with_w) {
+  const uint32_t lane = lane_id();
+  const uint32_t nrec = min(*R.n_reloc, R.cap);
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = gw; i < nrec; i += nw) {
+    const RelocRec rec = R.rec[i];
+    const uint3 sg = seg[rec.seg];
+    const uint32_t start = sg.y, count = sg.z, len = rec.len;
+    for (uint32_t j = lane; j < count; j += 32)
+      write_slot(A, rec.new_off + len + j, (uint32_t)k[start + j], with_w ? wv[start + j] : 0u,
+                 with_w);
+    if (lane == 0) {
+      const uint32_t nsrt = len == 0 ? count : A.srt[rec.row];
+      A.srt[rec.row] = nsrt;
+      A.len[rec.row] = len + count;
+      A.live[rec.row] += count;
+    }
   }
 }
 
@@ -339,18 +426,25 @@ cudaError_t launch_row_segments(const u64 *k, uint32_t cnt, uint3 *seg, uint32_t
 
 cudaError_t launch_delete_rows(const Adj &A, const uint2 *uv, const uint32_t *mult,
                                const uint32_t *n_ptr, uint32_t max_n, uint32_t *found, Ctl *ctl,
-                               int count_missing, cudaStream_t s) {
+                               int count_missing, const Tombs &T, cudaStream_t s) {
   if (!max_n) return cudaSuccess;
+  cudaMemsetAsync(T.count, 0, 4, s);
   delete_rows_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, uv, mult, n_ptr, found, ctl,
-                                                                 count_missing);
+                                                                 count_missing, T);
+  tombstone_kernel<<<grid_for(max_n), BLOCK, 0, s>>>(A, T, ctl);
   return cudaGetLastError();
 }
 
 cudaError_t launch_add_rows(const Adj &A, const u64 *k, const uint32_t *w, const uint3 *seg,
-                            const uint32_t *n_ptr, uint32_t max_n, int with_w, Ctl *ctl,
-                            cudaStream_t s) {
+                            const uint32_t *n_ptr, uint32_t max_n, int with_w, const Reloc &R,
+                            Ctl *ctl, cudaStream_t s) {
   if (!max_n) return cudaSuccess;
-  add_rows_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, k, w, seg, n_ptr, with_w, ctl);
+  cudaMemsetAsync(R.n_reloc, 0, 4, s);
+  cudaMemsetAsync(R.n_chunks, 0, 4, s);
+  add_rows_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, k, w, seg, n_ptr, with_w, R,
+                                                              ctl);
+  relocate_copy_kernel<<<148 * 16, BLOCK, 0, s>>>(A, R, with_w, ctl);
+  relocate_append_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, k, w, seg, R, with_w);
   return cudaGetLastError();
 }
 

@@ -237,7 +237,7 @@ def test_random_split_phases(algo):
 
 
 def test_random_sssp_stored_weights_cached():
-    e = run_random("sssp", 11, 4, 500, 500, seed=11, budget=1 << 18, stored=True)
+    e = run_random("sssp", 11, 4, 500, 500, seed=11, budget=1 << 20, stored=True)
     assert e.info()["cached_pages"] > 0
 
 

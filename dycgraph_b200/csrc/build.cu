@@ -120,21 +120,23 @@ __global__ void caps_kernel(const uint32_t *deg, uint32_t n, u64 *cap64, uint32_
 
 // Rows are contiguous in the sorted key array: slot = off[u] + (i - rowstart[u]).
 __global__ void scatter_kernel(const u64 *k, const uint32_t *wv, u64 m, const u64 *off,
-                               const u64 *rowstart, uint32_t *hdst, uint32_t *hw, uint32_t *fence,
-                               u64 wseed, uint32_t wlo, uint32_t whi, int weight_from_hash,
-                               int swapped) {
+                               const u64 *rowstart, uint32_t *hwords, uint32_t stride,
+                               uint32_t *fence, uint32_t fence_shift, u64 wseed, uint32_t wlo,
+                               uint32_t whi, int weight_from_hash, int swapped) {
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < m;
        i += (u64)gridDim.x * blockDim.x) {
     const u64 key = k[i];
     const uint32_t u = (uint32_t)(key >> 32), v = (uint32_t)key;
     const u64 slot = off[u] + (i - rowstart[u]);
-    hdst[slot] = v;
-    if ((slot & 31) == 0) fence[slot >> 5] = v;
-    if (hw) {
+    if (stride == 2) {
       // weights are a property of the directed edge (source, target)
       const uint32_t s = swapped ? v : u, t = swapped ? u : v;
-      hw[slot] = weight_from_hash ? hash_weight(wseed, s, t, wlo, whi) : wv[i];
+      const uint32_t w = weight_from_hash ? hash_weight(wseed, s, t, wlo, whi) : wv[i];
+      *reinterpret_cast<uint2 *>(hwords + slot * 2) = make_uint2(v, w);
+    } else {
+      hwords[slot] = v;
     }
+    if ((slot & ((1ull << fence_shift) - 1)) == 0) fence[slot >> fence_shift] = v;
   }
 }
 
@@ -208,12 +210,13 @@ cudaError_t build_caps(const uint32_t *deg, uint32_t n, u64 *cap64, uint32_t *ca
 }
 
 cudaError_t build_scatter(const u64 *k, const uint32_t *wv, u64 m, const u64 *off,
-                          const u64 *rowstart, uint32_t *hdst, uint32_t *hw, uint32_t *fence,
-                          u64 wseed, uint32_t wlo, uint32_t whi, int weight_from_hash,
-                          int swapped, cudaStream_t s) {
+                          const u64 *rowstart, uint32_t *hwords, uint32_t stride, uint32_t *fence,
+                          uint32_t fence_shift, u64 wseed, uint32_t wlo, uint32_t whi,
+                          int weight_from_hash, int swapped, cudaStream_t s) {
   if (!m) return cudaSuccess;
-  scatter_kernel<<<grid_for(m), BLOCK, 0, s>>>(k, wv, m, off, rowstart, hdst, hw, fence, wseed,
-                                               wlo, whi, weight_from_hash, swapped);
+  scatter_kernel<<<grid_for(m), BLOCK, 0, s>>>(k, wv, m, off, rowstart, hwords, stride, fence,
+                                               fence_shift, wseed, wlo, whi, weight_from_hash,
+                                               swapped);
   return cudaGetLastError();
 }
 
@@ -258,17 +261,18 @@ __global__ void resolve_positions_kernel(const u64 *pos, u64 count, const u64 *p
     const u64 off = A.off[u];
     const uint32_t len = A.len[u];
     uint32_t v = 0, w = 0;
-    if (A.live[u] == len && k < len) {  // no tombstones: direct index
-      v = read_dst_rw(A, off + k) & VMASK;
-      w = A.hw ? read_w_rw(A, off + k) : 0u;
+    if (A.live[u] == len && k < len) {  // no deleted slot: direct index
+      const uint2 pr = read_pair_rw(A, off + k);
+      v = pr.x & VMASK;
+      w = pr.y;
       k = len;  // skip the scan
     }
     for (uint32_t s = 0; s < len && k < len; s++) {
-      const uint32_t d = read_dst_rw(A, off + s);
-      if (d & TOMB) continue;
+      const uint2 pr = read_pair_rw(A, off + s);
+      if (slot_deleted_rw(A, off + s, pr.x)) continue;
       if (k == 0) {
-        v = d;
-        w = A.hw ? read_w_rw(A, off + s) : 0u;
+        v = pr.x;
+        w = pr.y;
         break;
       }
       k--;

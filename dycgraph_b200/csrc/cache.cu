@@ -64,28 +64,21 @@ __global__ void admit_list_kernel(const uint32_t *ids, uint32_t npages, const ui
     if (fa[i] && sa[i] < limit) admit[sa[i]] = ids[i];
 }
 
-// CTA per page: copy the page from the host arena into its cache slot with
-// 16-byte loads, then publish it in the page table.
+// CTA per page: copy the page's slot words from the host arena into its cache
+// slot with 16-byte loads, then publish it in the page table.
 __global__ void fill_kernel(const uint32_t *admit, uint32_t count, const uint32_t *free_list,
-                            uint32_t free_top, uint32_t *page_slot, const uint32_t *h_out_dst,
-                            const uint32_t *h_out_w, const uint32_t *h_in_dst,
-                            const uint32_t *h_in_w, uint32_t pages_out, uint32_t page_shift,
-                            uint32_t *cdst, uint32_t *cw) {
+                            uint32_t free_top, uint32_t *page_slot, const uint32_t *h_out,
+                            const uint32_t *h_in, uint32_t pages_out, uint32_t page_shift,
+                            uint32_t stride, uint32_t *cdst) {
+  const u64 words = (u64)stride << page_shift;
   for (uint32_t j = blockIdx.x; j < count; j += gridDim.x) {
     const uint32_t p = admit[j];
     const uint32_t slot = free_list[free_top - 1 - j];
     const bool in_dir = p >= pages_out;
-    const u64 first = (u64)(in_dir ? p - pages_out : p) << page_shift;
-    const uint4 *sd = reinterpret_cast<const uint4 *>((in_dir ? h_in_dst : h_out_dst) + first);
-    const uint32_t *swp = in_dir ? h_in_w : h_out_w;
-    uint4 *dd = reinterpret_cast<uint4 *>(cdst + ((u64)slot << page_shift));
-    const uint32_t nv = (1u << page_shift) / 4;
-    for (uint32_t t = threadIdx.x; t < nv; t += blockDim.x) dd[t] = sd[t];
-    if (swp) {
-      const uint4 *sw = reinterpret_cast<const uint4 *>(swp + first);
-      uint4 *dw = reinterpret_cast<uint4 *>(cw + ((u64)slot << page_shift));
-      for (uint32_t t = threadIdx.x; t < nv; t += blockDim.x) dw[t] = sw[t];
-    }
+    const u64 first = (u64)(in_dir ? p - pages_out : p) * words;
+    const uint4 *sd = reinterpret_cast<const uint4 *>((in_dir ? h_in : h_out) + first);
+    uint4 *dd = reinterpret_cast<uint4 *>(cdst + (u64)slot * words);
+    for (uint32_t t = threadIdx.x; t < words / 4; t += blockDim.x) dd[t] = sd[t];
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) page_slot[p] = slot;
@@ -145,8 +138,8 @@ cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t n_evict_cand, ui
                                                          admit, W.admit);
     const uint32_t top = free_count + evict;
     fill_kernel<<<(int)std::min<uint32_t>(admit, 148 * 8), BLOCK, 0, s>>>(
-        W.admit, admit, free_list, top, page_slot, pg.h_out_dst, pg.h_out_w, pg.h_in_dst,
-        pg.h_in_w, pg.pages_out, pg.page_shift, pg.cdst, pg.cw);
+        W.admit, admit, free_list, top, page_slot, pg.h_out, pg.h_in, pg.pages_out,
+        pg.page_shift, pg.stride, pg.cdst);
   }
   return cudaGetLastError();
 }

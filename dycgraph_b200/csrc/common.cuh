@@ -90,16 +90,18 @@ __host__ __device__ inline void rmat_draw(u64 seed, u64 idx, uint32_t scale, uin
   v = vv;
 }
 
-// Device view of one adjacency direction.
+// Device view of one adjacency direction. Slot p occupies `stride` 32-bit
+// words at word index p*stride: the neighbour id, then (stride 2) its weight,
+// so one 8-byte access moves both.
 struct Adj {
-  uint32_t *hdst;        // host arena (device-mapped pointer)
-  uint32_t *hw;          // host weights or nullptr
-  uint32_t *cdst;        // HBM page cache, slot-major (shared by both directions)
-  uint32_t *cw;          // cached weights or nullptr
+  uint32_t *hdst;        // host arena words (device-mapped pointer)
+  uint32_t *cdst;        // HBM page cache words, slot-major (shared by both directions)
   const uint32_t *page_slot;
   uint32_t *page_hits;   // per-page slot-access counters (hotness)
   uint32_t page_base;    // global id of this arena's first page
   uint32_t page_shift;
+  uint32_t stride;       // 1: id only, 2: (id, weight)
+  uint32_t fence_shift;  // one fence per 128 bytes of slots: 5 (stride 1) or 4 (stride 2)
   u64 *off;
   uint32_t *len;
   uint32_t *cap;
@@ -107,7 +109,8 @@ struct Adj {
   uint32_t *live;
   u64 *top;              // arena bump pointer (slots)
   u64 arena;             // arena size (slots)
-  uint32_t *fence;       // HBM fence index: fence[f] = id bits of slot 32*f
+  uint32_t *fence;       // HBM fence index: id bits of slot (f << fence_shift)
+  uint32_t *tbits;       // HBM deletion bitmap, one bit per arena slot
 };
 
 // Per-launch control block in device memory: barrier, queues, counters.
@@ -198,53 +201,61 @@ __device__ __forceinline__ u64 cache_index(const Adj &a, uint32_t cslot, u64 p) 
   return ((u64)cslot << a.page_shift) | (p & ((1ull << a.page_shift) - 1));
 }
 
-// Read dst (and optionally weight) of slot p; reports whether it came from HBM.
-__device__ __forceinline__ uint32_t read_dst(const Adj &a, u64 p, bool &cached) {
-  uint32_t cs = __ldg(a.page_slot + page_of(a, p));
+// Word address of slot p (HBM copy when its page is resident) for readers.
+__device__ __forceinline__ const uint32_t *slot_ptr(const Adj &a, u64 p, bool &cached) {
+  const uint32_t cs = __ldg(a.page_slot + page_of(a, p));
   cached = cs != PAGE_NONE;
-  return cached ? __ldg(a.cdst + cache_index(a, cs, p)) : __ldg(a.hdst + p);
+  return cached ? a.cdst + cache_index(a, cs, p) * a.stride : a.hdst + p * a.stride;
 }
 
-__device__ __forceinline__ uint32_t read_w(const Adj &a, u64 p, bool cached) {
-  if (cached) {
-    uint32_t cs = __ldg(a.page_slot + page_of(a, p));
-    return __ldg(a.cw + cache_index(a, cs, p));
+// Same, for kernels that also write the arena (no read-only cache path).
+__device__ __forceinline__ const uint32_t *slot_ptr_rw(const Adj &a, u64 p) {
+  const uint32_t cs = a.page_slot[page_of(a, p)];
+  return cs != PAGE_NONE ? a.cdst + cache_index(a, cs, p) * a.stride : a.hdst + p * a.stride;
+}
+
+__device__ __forceinline__ uint32_t read_dst(const Adj &a, u64 p, bool &cached) {
+  return __ldg(slot_ptr(a, p, cached));
+}
+
+// (id, weight) of slot p in one access; weight 0 without stored weights.
+__device__ __forceinline__ uint2 read_pair(const Adj &a, u64 p, bool &cached) {
+  const uint32_t *q = slot_ptr(a, p, cached);
+  if (a.stride == 2) return __ldg(reinterpret_cast<const uint2 *>(q));
+  return make_uint2(__ldg(q), 0u);
+}
+
+__device__ __forceinline__ uint32_t read_dst_rw(const Adj &a, u64 p) { return *slot_ptr_rw(a, p); }
+
+__device__ __forceinline__ uint2 read_pair_rw(const Adj &a, u64 p) {
+  const uint32_t *q = slot_ptr_rw(a, p);
+  if (a.stride == 2) return *reinterpret_cast<const uint2 *>(q);
+  return make_uint2(*q, 0u);
+}
+
+// Deleted: tombstone bit in the slot (materialised by a row relocation) or the
+// slot's bit in the HBM deletion bitmap (set by the deletion kernels).
+__device__ __forceinline__ bool slot_deleted(const Adj &a, u64 p, uint32_t d) {
+  return (d & TOMB) || ((__ldg(a.tbits + (p >> 5)) >> (p & 31)) & 1u);
+}
+
+__device__ __forceinline__ bool slot_deleted_rw(const Adj &a, u64 p, uint32_t d) {
+  return (d & TOMB) || ((*(volatile uint32_t *)(a.tbits + (p >> 5)) >> (p & 31)) & 1u);
+}
+
+// Write-through store of one slot: host arena (one 8-byte store with
+// weights), the resident cached copy, and the fence entry when the slot opens
+// a 128-byte group. Returns whether the page is resident.
+__device__ __forceinline__ bool write_slot(const Adj &a, u64 p, uint32_t d, uint32_t w) {
+  const uint32_t cs = a.page_slot[page_of(a, p)];
+  if (a.stride == 2) {
+    *reinterpret_cast<uint2 *>(a.hdst + p * 2) = make_uint2(d, w);
+    if (cs != PAGE_NONE) *reinterpret_cast<uint2 *>(a.cdst + cache_index(a, cs, p) * 2) = make_uint2(d, w);
+  } else {
+    a.hdst[p] = d;
+    if (cs != PAGE_NONE) a.cdst[cache_index(a, cs, p)] = d;
   }
-  return __ldg(a.hw + p);
-}
-
-// Coherent read for kernels that also write the arena.
-__device__ __forceinline__ uint32_t read_dst_rw(const Adj &a, u64 p) {
-  uint32_t cs = a.page_slot[page_of(a, p)];
-  return cs != PAGE_NONE ? a.cdst[cache_index(a, cs, p)] : a.hdst[p];
-}
-
-__device__ __forceinline__ uint32_t read_w_rw(const Adj &a, u64 p) {
-  uint32_t cs = a.page_slot[page_of(a, p)];
-  return cs != PAGE_NONE ? a.cw[cache_index(a, cs, p)] : a.hw[p];
-}
-
-// Write-through store of one slot (host arena + resident cached copy + the
-// HBM fence entry when the slot starts a 32-slot group).
-__device__ __forceinline__ bool write_slot(const Adj &a, u64 p, uint32_t d, uint32_t w,
-                                           bool with_w) {
-  uint32_t cs = a.page_slot[page_of(a, p)];
-  a.hdst[p] = d;
-  if (with_w) a.hw[p] = w;
-  if ((p & 31) == 0) a.fence[p >> 5] = d & VMASK;
-  if (cs != PAGE_NONE) {
-    u64 ci = cache_index(a, cs, p);
-    a.cdst[ci] = d;
-    if (with_w) a.cw[ci] = w;
-  }
-  return cs != PAGE_NONE;
-}
-
-// Tombstone/flag update of one slot: the id bits (and so the fence) are unchanged.
-__device__ __forceinline__ bool write_dst(const Adj &a, u64 p, uint32_t d) {
-  uint32_t cs = a.page_slot[page_of(a, p)];
-  a.hdst[p] = d;
-  if (cs != PAGE_NONE) a.cdst[cache_index(a, cs, p)] = d;
+  if ((p & ((1ull << a.fence_shift) - 1)) == 0) a.fence[p >> a.fence_shift] = d & VMASK;
   return cs != PAGE_NONE;
 }
 

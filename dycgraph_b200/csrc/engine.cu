@@ -88,9 +88,10 @@ void Engine::check_loaded() const {
 Adj Engine::adj(const Arena &A) const {
   Adj a;
   a.hdst = A.d_dst;
-  a.hw = A.d_w;
   a.cdst = cdst_;
-  a.cw = cw_;
+  a.stride = A.stride;
+  a.fence_shift = A.fence_shift;
+  a.tbits = A.tbits;
   a.page_slot = page_slot_;
   a.page_hits = page_hits_;
   a.page_base = A.page_base;
@@ -140,22 +141,19 @@ void Engine::build_direction(Arena &A, const u64 *keys, const uint32_t *wv, u64 
   const u64 head = std::max<u64>(total / 8, 1ull << 20);
   A.slots = round_up(total + head, page);
   A.pages = (uint32_t)(A.slots >> page_shift_);
+  A.stride = stored_ ? 2 : 1;
+  A.fence_shift = stored_ ? 4 : 5;
   void *hd = nullptr;
-  CK(cudaHostAlloc(&hd, A.slots * 4, cudaHostAllocMapped | cudaHostAllocPortable));
+  CK(cudaHostAlloc(&hd, A.slots * 4 * A.stride, cudaHostAllocMapped | cudaHostAllocPortable));
   hallocs_.push_back(hd);
   A.h_dst = (uint32_t *)hd;
   CK(cudaHostGetDevicePointer((void **)&A.d_dst, hd, 0));
-  if (stored_) {
-    void *hw = nullptr;
-    CK(cudaHostAlloc(&hw, A.slots * 4, cudaHostAllocMapped | cudaHostAllocPortable));
-    hallocs_.push_back(hw);
-    A.h_w = (uint32_t *)hw;
-    CK(cudaHostGetDevicePointer((void **)&A.d_w, hw, 0));
-  }
-  A.fence = (uint32_t *)dmalloc((A.slots >> 5) * 4);
+  A.fence = (uint32_t *)dmalloc((A.slots >> A.fence_shift) * 4);
+  A.tbits = (uint32_t *)dmalloc((A.slots >> 5) * 4);
+  CK(cudaMemsetAsync(A.tbits, 0, (A.slots >> 5) * 4, st_));
   CK(cudaMemcpyAsync(A.top, &total, 8, cudaMemcpyHostToDevice, st_));
-  CK(build_scatter(keys, wv, m, A.off, rowstart, A.d_dst, A.d_w, A.fence, wseed, wlo, whi,
-                   weight_from_hash ? 1 : 0, swapped ? 1 : 0, st_));
+  CK(build_scatter(keys, wv, m, A.off, rowstart, A.d_dst, A.stride, A.fence, A.fence_shift, wseed,
+                   wlo, whi, weight_from_hash ? 1 : 0, swapped ? 1 : 0, st_));
   sync_check("scatter");
   // free the temporaries (they are the last allocations made)
   for (void *p : {temp, (void *)rowstart, (void *)cap64, (void *)deg}) {
@@ -198,16 +196,19 @@ void Engine::finish_load() {
   page_hits_ = (uint32_t *)dmalloc((u64)npages_ * 4);
   CK(cudaMemsetAsync(page_slot_, 0xFF, (u64)npages_ * 4, st_));
   CK(cudaMemsetAsync(page_hits_, 0, (u64)npages_ * 4, st_));
-  // the HBM graph budget covers the fence index and the cached pages
-  const u64 page_bytes = (4ull << page_shift_) * (stored_ ? 2 : 1);
-  const u64 fence_bytes = ((out_.slots >> 5) + (has_in_ ? (in_.slots >> 5) : 0)) * 4;
-  const u64 avail = opt_.hbm_graph_budget_bytes > fence_bytes ? opt_.hbm_graph_budget_bytes - fence_bytes : 0;
+  // the HBM graph budget covers the fence index, the deletion bitmap and the
+  // cached pages
+  const u64 page_bytes = (4ull << page_shift_) * out_.stride;
+  const u64 index_bytes =
+      ((out_.slots >> out_.fence_shift) + (out_.slots >> 5)) * 4 +
+      (has_in_ ? ((in_.slots >> in_.fence_shift) + (in_.slots >> 5)) * 4 : 0);
+  index_bytes_ = index_bytes;
+  const u64 avail = opt_.hbm_graph_budget_bytes > index_bytes ? opt_.hbm_graph_budget_bytes - index_bytes : 0;
   u64 slots = opt_.cache_policy == DYCG_CACHE_NONE ? 0 : avail / page_bytes;
   slots = std::min<u64>(slots, npages_);
   cache_slots_ = (uint32_t)slots;
   if (cache_slots_) {
-    cdst_ = (uint32_t *)dmalloc(((u64)cache_slots_ << page_shift_) * 4);
-    if (stored_) cw_ = (uint32_t *)dmalloc(((u64)cache_slots_ << page_shift_) * 4);
+    cdst_ = (uint32_t *)dmalloc(((u64)cache_slots_ << page_shift_) * 4 * out_.stride);
     free_list_ = (uint32_t *)dmalloc((u64)cache_slots_ * 4);
     std::vector<uint32_t> fl(cache_slots_);
     for (uint32_t i = 0; i < cache_slots_; i++) fl[i] = cache_slots_ - 1 - i;
@@ -531,7 +532,6 @@ void Engine::ensure_batch(size_t cnt) {
   reloc_.n_reloc = counts_ + 8;
   reloc_.n_chunks = counts_ + 9;
   tombs_.pos = (u64 *)al(c * 8);
-  tombs_.val = (uint32_t *)al(c * 4);
   tombs_.count = counts_ + 10;
   tombs_.cap = (uint32_t)c;
   d_edges_ = (dycg_edge_dev *)al(c * 2 * sizeof(dycg_edge_dev));
@@ -667,11 +667,11 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
   }
   if (na) {
     CK(launch_add_rows(A_out, k_add_out_, w_add_out_, seg_out_, counts_ + 2, (uint32_t)na,
-                       stored_ ? 1 : 0, reloc_, ctl_, st_));
+                       reloc_, ctl_, st_));
     launches_ += 3;
     if (has_in_) {
-      CK(launch_add_rows(A_in, k_add_in_, w_add_in_, seg_in_, counts_ + 3, (uint32_t)na,
-                         stored_ ? 1 : 0, reloc_, ctl_, st_));
+      CK(launch_add_rows(A_in, k_add_in_, w_add_in_, seg_in_, counts_ + 3, (uint32_t)na, reloc_,
+                         ctl_, st_));
       launches_ += 3;
     }
   }
@@ -788,8 +788,8 @@ void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
     const uint32_t need = admit > free_count_ ? admit - free_count_ : 0u;
     evict = std::min(n_evict_cand, need);
     admit = std::min(admit, free_count_ + evict);
-    CachePages pg{out_.d_dst, out_.d_w, has_in_ ? in_.d_dst : nullptr,
-                  has_in_ ? in_.d_w : nullptr, out_.pages, page_shift_, cdst_, cw_};
+    CachePages pg{out_.d_dst, has_in_ ? in_.d_dst : nullptr, out_.pages, page_shift_,
+                  out_.stride, cdst_};
     CK(cache_apply(cwk_, npages_, n_evict_cand, evict, admit, page_slot_, free_list_, free_count_,
                    pg, st_));
     free_count_ = free_count_ + evict - admit;
@@ -806,7 +806,7 @@ void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
     stats->ms_cache = ms;
     stats->cache_pages_loaded = admit;
     stats->cache_pages_evicted = evict;
-    const u64 page_bytes = (4ull << page_shift_) * (stored_ ? 2 : 1);
+    const u64 page_bytes = (4ull << page_shift_) * out_.stride;
     stats->link_bytes += (u64)admit * page_bytes;
     stats->hbm_adj_bytes += (u64)admit * page_bytes;
   }
@@ -834,6 +834,14 @@ void Engine::gather_ranks(float *ranks, float *residuals) {
   sync_check("gather ranks");
 }
 
+// Host bitmap words covering slots [first, first + count) of arena A.
+static std::vector<uint32_t> fetch_bits(const Arena &A, u64 first, u64 count, cudaStream_t st) {
+  const u64 w0 = first >> 5, w1 = (first + count + 31) >> 5;
+  std::vector<uint32_t> b(w1 - w0 + 1, 0);
+  if (w1 > w0) cudaMemcpyAsync(b.data(), A.tbits + w0, (w1 - w0) * 4, cudaMemcpyDeviceToHost, st);
+  return b;
+}
+
 void Engine::get_row(uint32_t v, int incoming, uint32_t *dst, uint32_t *w, uint32_t cap,
                      uint32_t *deg) {
   check_loaded();
@@ -844,13 +852,17 @@ void Engine::get_row(uint32_t v, int incoming, uint32_t *dst, uint32_t *w, uint3
   CK(cudaMemcpyAsync(&off, A.off + v, 8, cudaMemcpyDeviceToHost, st_));
   CK(cudaMemcpyAsync(&len, A.len + v, 4, cudaMemcpyDeviceToHost, st_));
   sync_check("row");
+  std::vector<uint32_t> bits = fetch_bits(A, off, len, st_);
+  sync_check("row bits");
+  const u64 w0 = off >> 5;
   uint32_t k = 0;
   for (uint32_t s = 0; s < len; s++) {
-    const uint32_t d = A.h_dst[off + s];
-    if (d & TOMB) continue;
+    const u64 p = off + s;
+    const uint32_t d = A.h_dst[p * A.stride];
+    if ((d & TOMB) || ((bits[(p >> 5) - w0] >> (p & 31)) & 1u)) continue;
     if (k < cap) {
       if (dst) dst[k] = d;
-      if (w) w[k] = A.h_w ? A.h_w[off + s] : 0u;
+      if (w) w[k] = A.stride == 2 ? A.h_dst[p * 2 + 1] : 0u;
     }
     k++;
   }
@@ -863,19 +875,21 @@ void Engine::export_csr(uint64_t *off, uint32_t *dst, uint32_t *w) {
   std::vector<uint32_t> l(n_);
   CK(cudaMemcpyAsync(o.data(), out_.off, (u64)n_ * 8, cudaMemcpyDeviceToHost, st_));
   CK(cudaMemcpyAsync(l.data(), out_.len, (u64)n_ * 4, cudaMemcpyDeviceToHost, st_));
+  std::vector<uint32_t> bits = fetch_bits(out_, 0, out_.slots, st_);
   sync_check("export");
-  u64 p = 0;
+  u64 q = 0;
   for (uint32_t v = 0; v < n_; v++) {
-    off[v] = p;
+    off[v] = q;
     for (uint32_t s = 0; s < l[v]; s++) {
-      const uint32_t d = out_.h_dst[o[v] + s];
-      if (d & TOMB) continue;
-      if (dst) dst[p] = d;
-      if (w) w[p] = out_.h_w ? out_.h_w[o[v] + s] : 0u;
-      p++;
+      const u64 p = o[v] + s;
+      const uint32_t d = out_.h_dst[p * out_.stride];
+      if ((d & TOMB) || ((bits[p >> 5] >> (p & 31)) & 1u)) continue;
+      if (dst) dst[q] = d;
+      if (w) w[q] = out_.stride == 2 ? out_.h_dst[p * 2 + 1] : 0u;
+      q++;
     }
   }
-  off[n_] = p;
+  off[n_] = q;
 }
 
 void Engine::info(dycg_graph_info *out) {
@@ -896,9 +910,10 @@ void Engine::info(dycg_graph_info *out) {
   out->pages = npages_;
   out->cache_slots = cache_slots_;
   out->cached_pages = cache_slots_ - free_count_;
-  out->host_bytes = out->arena_slots * 4 * (stored_ ? 2 : 1);
+  out->host_bytes = out->arena_slots * 4 * out_.stride;
   out->device_bytes = (u64)n_ * (8 + 4 * 6) + (u64)n_ * (has_in_ ? 48 : 24) +
-                      ((u64)cache_slots_ << page_shift_) * 4 * (stored_ ? 2 : 1);
+                      ((u64)cache_slots_ << page_shift_) * 4 * out_.stride + index_bytes_;
+  out->reserved[0] = index_bytes_;  // fence index + deletion bitmap (part of the budget)
   out->page_shift = page_shift_;
   out->has_incoming = has_in_ ? 1 : 0;
 }

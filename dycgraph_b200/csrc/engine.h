@@ -18,8 +18,11 @@ struct Error : std::runtime_error {
 
 // One adjacency direction: a pinned, mapped host arena plus its descriptors.
 struct Arena {
-  uint32_t *h_dst = nullptr, *h_w = nullptr;  // host addresses
-  uint32_t *d_dst = nullptr, *d_w = nullptr;  // device-mapped addresses
+  uint32_t *h_dst = nullptr;  // host address of the slot words
+  uint32_t *d_dst = nullptr;  // device-mapped address of the same words
+  uint32_t stride = 1;        // words per slot: 1 (id) or 2 (id, weight)
+  uint32_t fence_shift = 5;   // one fence per 128 bytes of slots
+  uint32_t *tbits = nullptr;  // HBM deletion bitmap
   u64 slots = 0;
   uint32_t pages = 0, page_base = 0;
   u64 *off = nullptr;
@@ -81,10 +84,10 @@ class Engine {
 
   // cache
   uint32_t page_shift_ = 12, npages_ = 0, cache_slots_ = 0, free_count_ = 0;
-  uint32_t *page_slot_ = nullptr, *page_hits_ = nullptr, *cdst_ = nullptr, *cw_ = nullptr,
-           *free_list_ = nullptr;
+  uint32_t *page_slot_ = nullptr, *page_hits_ = nullptr, *cdst_ = nullptr, *free_list_ = nullptr;
   CacheWork cwk_{};
   uint64_t pages_loaded_ = 0, pages_evicted_ = 0;
+  u64 index_bytes_ = 0;
 
   // vertex state
   u64 *key_ = nullptr;

@@ -114,8 +114,14 @@ __device__ __forceinline__ void warp_slots(const Adj &A, uint32_t v, u64 off, ui
       if (in[u]) {
         const u64 p = off + s;
         pg[u] = page_of(A, p);
-        d[u] = read_dst(A, p, cached[u]);
-        if (WITH_W) w[u] = read_w(A, p, cached[u]);
+        if (WITH_W) {
+          const uint2 pr = read_pair(A, p, cached[u]);
+          d[u] = pr.x;
+          w[u] = pr.y;
+        } else {
+          d[u] = read_dst(A, p, cached[u]);
+        }
+        if (slot_deleted(A, p, d[u])) d[u] |= TOMB;
       }
     }
 #pragma unroll

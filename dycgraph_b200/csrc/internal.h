@@ -70,7 +70,6 @@ cudaError_t launch_row_segments(const u64 *k, uint32_t cnt, uint3 *seg, uint32_t
 // Deleted occurrences found by the read-only search, written afterwards.
 struct Tombs {
   u64 *pos;
-  uint32_t *val;
   uint32_t *count;
   uint32_t cap;
 };
@@ -90,8 +89,8 @@ struct Reloc {
   uint32_t cap, chunk_cap;
 };
 cudaError_t launch_add_rows(const Adj &A, const u64 *k, const uint32_t *w, const uint3 *seg,
-                            const uint32_t *n_ptr, uint32_t max_n, int with_w, const Reloc &R,
-                            Ctl *ctl, cudaStream_t s);
+                            const uint32_t *n_ptr, uint32_t max_n, const Reloc &R, Ctl *ctl,
+                            cudaStream_t s);
 cudaError_t launch_keys_to_uvw(const u64 *k, const uint32_t *w, uint32_t cnt, uint3 *out,
                                cudaStream_t s);
 cudaError_t launch_touched(const u64 *k, uint32_t cnt, uint32_t *tag, uint32_t epoch,
@@ -107,9 +106,9 @@ struct CacheWork {
   uint32_t *h_counts;    // pinned host [4]
 };
 struct CachePages {
-  const uint32_t *h_out_dst, *h_out_w, *h_in_dst, *h_in_w;
-  uint32_t pages_out, page_shift;
-  uint32_t *cdst, *cw;
+  const uint32_t *h_out, *h_in;  // host arena words (device-mapped)
+  uint32_t pages_out, page_shift, stride;
+  uint32_t *cdst;
 };
 size_t cache_temp_bytes(uint32_t npages);
 cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay, float min_score,
@@ -139,9 +138,9 @@ cudaError_t build_degrees(const u64 *k, u64 m, uint32_t *deg, cudaStream_t s);
 cudaError_t build_caps(const uint32_t *deg, uint32_t n, u64 *cap64, uint32_t *cap,
                        uint32_t *len, uint32_t *srt, uint32_t *live, cudaStream_t s);
 cudaError_t build_scatter(const u64 *k, const uint32_t *wv, u64 m, const u64 *off,
-                          const u64 *rowstart, uint32_t *hdst, uint32_t *hw, uint32_t *fence,
-                          u64 wseed, uint32_t wlo, uint32_t whi, int weight_from_hash,
-                          int swapped, cudaStream_t s);
+                          const u64 *rowstart, uint32_t *hwords, uint32_t stride, uint32_t *fence,
+                          uint32_t fence_shift, u64 wseed, uint32_t wlo, uint32_t whi,
+                          int weight_from_hash, int swapped, cudaStream_t s);
 size_t build_temp_bytes(u64 count, bool pairs);
 cudaError_t sample_draw(u64 *pos, u64 count, u64 seed, u64 total, cudaStream_t s);
 cudaError_t sample_resolve(const u64 *pos, u64 count, const u64 *pre, uint32_t n, const Adj &A,

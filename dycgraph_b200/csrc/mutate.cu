@@ -89,15 +89,18 @@ __global__ void row_segments_kernel(const u64 *k, uint32_t cnt, uint3 *seg, uint
 
 // First index (row-relative) in the sorted prefix [0, srt) of the row at
 // arena offset off whose id is >= target; all lanes return the same index.
-// The HBM fence index holds the id of every 32nd arena slot, so a 32-ary warp
-// search over the row's fences (HBM reads) narrows the answer to one 32-slot
-// window, read from the row with a single coalesced request.
+// The HBM fence index holds the id of the first slot of every 128-byte group
+// of slots (G = 32 slots without weights, 16 with), so a 32-ary warp search
+// over the row's fences (HBM reads) narrows the answer to one group, read
+// from the row with a single coalesced 128-byte request.
 __device__ uint32_t warp_lower_bound(const Adj &A, u64 off, uint32_t srt, uint32_t target,
                                      uint32_t &reads) {
   const uint32_t lane = lane_id();
-  // fences inside the prefix: arena slots 32*f with off <= 32*f < off + srt
-  u64 flo = (off + 31) >> 5;
-  u64 fhi = srt ? ((off + srt - 1) >> 5) + 1 : flo;  // exclusive
+  const uint32_t fs = A.fence_shift;
+  const u64 G = 1ull << fs;
+  // fences inside the prefix: groups f with off <= f*G < off + srt
+  const u64 flo = (off + G - 1) >> fs;
+  u64 fhi = srt ? ((off + srt - 1) >> fs) + 1 : flo;  // exclusive
   if (fhi < flo) fhi = flo;
   // first fence index f in [flo, fhi) with fence[f] >= target (fhi if none)
   u64 lo = flo, hi = fhi;
@@ -120,10 +123,10 @@ __device__ uint32_t warp_lower_bound(const Adj &A, u64 off, uint32_t srt, uint32
     const unsigned ge = __ballot_sync(0xffffffffu, f < hi && A.fence[f] >= target);
     lo = ge ? lo + __ffs(ge) - 1 : hi;
   }
-  // the answer lies in (32*(lo-1), 32*lo] clipped to the prefix
+  // the answer lies in ((lo-1)*G, lo*G] clipped to the prefix
   const u64 pend = off + srt;
-  u64 wbeg = lo > flo ? ((lo - 1) << 5) + 1 : off;
-  u64 wend = lo < fhi ? (lo << 5) + 1 : pend;
+  u64 wbeg = lo > flo ? ((lo - 1) << fs) + 1 : off;
+  u64 wend = lo < fhi ? (lo << fs) + 1 : pend;
   if (wbeg < off) wbeg = off;
   if (wend > pend) wend = pend;
   uint32_t ans = (uint32_t)(wend - off);
@@ -142,9 +145,8 @@ __device__ uint32_t warp_lower_bound(const Adj &A, u64 off, uint32_t srt, uint32
 }
 
 // Warp per unique deletion record: find up to mult live occurrences (reads
-// only) and record them; the tombstones are written by tombstone_kernel after
-// every search of the batch has finished, so no host-link read waits behind
-// this batch's posted writes.
+// only) and record their slots; tombstone_kernel then sets their bits in the
+// HBM deletion bitmap, so a deletion costs no host-link write.
 __global__ void delete_rows_kernel(Adj A, const uint2 *uv, const uint32_t *mult,
                                    const uint32_t *n_ptr, uint32_t *found_out, Ctl *ctl,
                                    int count_missing, Tombs T) {
@@ -168,17 +170,14 @@ __global__ void delete_rows_kernel(Adj A, const uint2 *uv, const uint32_t *mult,
         const bool in = s < e2;
         const uint32_t d = in ? read_dst_rw(A, off + s) : 0xFFFFFFFFu;
         reads += in;
-        const bool live = in && (d & VMASK) == target && !(d & TOMB);
+        const bool live = in && (d & VMASK) == target && !slot_deleted_rw(A, off + s, d);
         const unsigned lm = __ballot_sync(0xffffffffu, live);
         const uint32_t rank = __popc(lm & ((1u << lane) - 1));
         const uint32_t take = min((uint32_t)__popc(lm), remaining);
         uint32_t base = 0;
         if (lane == 0 && take) base = atomicAdd(T.count, take);
         base = __shfl_sync(0xffffffffu, base, 0);
-        if (live && rank < remaining && base + rank < T.cap) {
-          T.pos[base + rank] = off + s;
-          T.val[base + rank] = d | TOMB;
-        }
+        if (live && rank < remaining && base + rank < T.cap) T.pos[base + rank] = off + s;
         remaining -= take;
         found += take;
         if (!pass && __ballot_sync(0xffffffffu, in && (d & VMASK) != target)) break;
@@ -207,18 +206,14 @@ __global__ void delete_rows_kernel(Adj A, const uint2 *uv, const uint32_t *mult,
 __global__ void tombstone_kernel(Adj A, Tombs T, Ctl *ctl) {
   const uint32_t n = min(*T.count, T.cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && *T.count > T.cap) atomicCAS(&ctl->err, 0u, ERR_QUEUE);
-  u64 link = 0, hbm = 0;
+  u64 hbm = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const bool c = write_dst(A, T.pos[i], T.val[i]);
-    link += 4;
-    if (c) hbm += 4;
+    const u64 p = T.pos[i];
+    atomicOr(A.tbits + (p >> 5), 1u << (p & 31));
+    hbm += 4;
   }
-  link = warp_sum(link);
   hbm = warp_sum(hbm);
-  if (lane_id() == 0) {
-    if (link) atomicAdd(&ctl->stat[ST_MUT_LINK_BYTES], link);
-    if (hbm) atomicAdd(&ctl->stat[ST_MUT_HBM_BYTES], hbm);
-  }
+  if (lane_id() == 0 && hbm) atomicAdd(&ctl->stat[ST_MUT_HBM_BYTES], hbm);
 }
 
 __device__ __forceinline__ uint32_t next_pow2_u32(uint32_t x) {
@@ -232,13 +227,13 @@ __device__ __forceinline__ uint32_t next_pow2_u32(uint32_t x) {
 // relocate_append_kernel, so a large row is copied by many warps instead of
 // one.
 __global__ void add_rows_kernel(Adj A, const u64 *k, const uint32_t *wv, const uint3 *seg,
-                                const uint32_t *n_ptr, int with_w, Reloc R, Ctl *ctl) {
+                                const uint32_t *n_ptr, Reloc R, Ctl *ctl) {
   const uint32_t lane = lane_id();
   const uint32_t nseg = *n_ptr;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   u64 link = 0, hbm = 0, reloc = 0;
-  const uint32_t bytes = with_w ? 8u : 4u;
+  const uint32_t bytes = 4u * A.stride;
   for (uint32_t i = gw; i < nseg; i += nw) {
     const uint3 sg = seg[i];
     const uint32_t row = sg.x, start = sg.y, count = sg.z;
@@ -247,8 +242,7 @@ __global__ void add_rows_kernel(Adj A, const u64 *k, const uint32_t *wv, const u
     const u64 off = A.off[row];
     if ((u64)len + count <= cap) {
       for (uint32_t j = lane; j < count; j += 32) {
-        const bool c = write_slot(A, off + len + j, (uint32_t)k[start + j],
-                                  with_w ? wv[start + j] : 0u, with_w);
+        const bool c = write_slot(A, off + len + j, (uint32_t)k[start + j], wv ? wv[start + j] : 0u);
         link += bytes;
         if (c) hbm += bytes;
       }
@@ -292,13 +286,14 @@ __global__ void add_rows_kernel(Adj A, const u64 *k, const uint32_t *wv, const u
 // Warp per RELOC_CHUNK slots of a relocated row: verbatim copy (tombstones
 // included, so the sorted prefix and the live count stay valid). Each lane
 // keeps RELOC_CHUNK/32 loads in flight before storing.
-__global__ void relocate_copy_kernel(Adj A, Reloc R, int with_w, Ctl *ctl) {
+__global__ void relocate_copy_kernel(Adj A, Reloc R, Ctl *ctl) {
   const uint32_t lane = lane_id();
   const uint32_t nch = min(*R.n_chunks, R.chunk_cap);
   const uint32_t nrec = min(*R.n_reloc, R.cap);
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   constexpr uint32_t PER = RELOC_CHUNK / 32;
+  const uint32_t bytes = 4u * A.stride;
   u64 link = 0, hbm = 0;
   for (uint32_t i = gw; i < nch; i += nw) {
     const uint2 ch = R.chunks[i];
@@ -306,21 +301,21 @@ __global__ void relocate_copy_kernel(Adj A, Reloc R, int with_w, Ctl *ctl) {
     const RelocRec rec = R.rec[ch.x];
     const uint32_t b = ch.y * RELOC_CHUNK;
     const uint32_t e = min(rec.len, b + RELOC_CHUNK);
-    uint32_t d[PER], w[PER];
+    uint2 v[PER];
 #pragma unroll
     for (uint32_t t = 0; t < PER; t++) {
       const uint32_t s = b + t * 32 + lane;
       if (s < e) {
-        d[t] = read_dst_rw(A, rec.old_off + s);
-        w[t] = with_w ? read_w_rw(A, rec.old_off + s) : 0u;
+        v[t] = read_pair_rw(A, rec.old_off + s);
+        // a slot deleted through the bitmap keeps its deletion as a tombstone bit
+        if (slot_deleted_rw(A, rec.old_off + s, v[t].x)) v[t].x |= TOMB;
       }
     }
 #pragma unroll
     for (uint32_t t = 0; t < PER; t++) {
       const uint32_t s = b + t * 32 + lane;
       if (s < e) {
-        const bool c = write_slot(A, rec.new_off + s, d[t], w[t], with_w);
-        const uint32_t bytes = with_w ? 8u : 4u;
+        const bool c = write_slot(A, rec.new_off + s, v[t].x, v[t].y);
         link += 2 * bytes;
         if (c) hbm += bytes;
       }
@@ -336,7 +331,7 @@ __global__ void relocate_copy_kernel(Adj A, Reloc R, int with_w, Ctl *ctl) {
 
 // Warp per relocated row: append its segment after the copied slots.
 __global__ void relocate_append_kernel(Adj A, const u64 *k, const uint32_t *wv,
-                                       const uint3 *seg, Reloc R, int with_w) {
+                                       const uint3 *seg, Reloc R) {
   const uint32_t lane = lane_id();
   const uint32_t nrec = min(*R.n_reloc, R.cap);
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -346,8 +341,7 @@ __global__ void relocate_append_kernel(Adj A, const u64 *k, const uint32_t *wv,
     const uint3 sg = seg[rec.seg];
     const uint32_t start = sg.y, count = sg.z, len = rec.len;
     for (uint32_t j = lane; j < count; j += 32)
-      write_slot(A, rec.new_off + len + j, (uint32_t)k[start + j], with_w ? wv[start + j] : 0u,
-                 with_w);
+      write_slot(A, rec.new_off + len + j, (uint32_t)k[start + j], wv ? wv[start + j] : 0u);
     if (lane == 0) {
       const uint32_t nsrt = len == 0 ? count : A.srt[rec.row];
       A.srt[rec.row] = nsrt;
@@ -436,15 +430,15 @@ cudaError_t launch_delete_rows(const Adj &A, const uint2 *uv, const uint32_t *mu
 }
 
 cudaError_t launch_add_rows(const Adj &A, const u64 *k, const uint32_t *w, const uint3 *seg,
-                            const uint32_t *n_ptr, uint32_t max_n, int with_w, const Reloc &R,
-                            Ctl *ctl, cudaStream_t s) {
+                            const uint32_t *n_ptr, uint32_t max_n, const Reloc &R, Ctl *ctl,
+                            cudaStream_t s) {
   if (!max_n) return cudaSuccess;
   cudaMemsetAsync(R.n_reloc, 0, 4, s);
   cudaMemsetAsync(R.n_chunks, 0, 4, s);
-  add_rows_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, k, w, seg, n_ptr, with_w, R,
-                                                              ctl);
-  relocate_copy_kernel<<<148 * 16, BLOCK, 0, s>>>(A, R, with_w, ctl);
-  relocate_append_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, k, w, seg, R, with_w);
+  const uint32_t *wv = A.stride == 2 ? w : nullptr;
+  add_rows_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, k, wv, seg, n_ptr, R, ctl);
+  relocate_copy_kernel<<<148 * 16, BLOCK, 0, s>>>(A, R, ctl);
+  relocate_append_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, k, wv, seg, R);
   return cudaGetLastError();
 }
 

@@ -118,6 +118,7 @@ def lib():
         "dycg_stream": (I, [P, ctypes.POINTER(P)]),
         "dycg_measure_host_link": (I, [I, u64, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_double)]),
+        "dycg_group_updates": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
         "dycg_last_error": (I, [P, ctypes.c_char_p, sz]),
         "dycg_version": (ctypes.c_char_p, []),
     }

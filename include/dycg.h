@@ -248,6 +248,21 @@ uint32_t dycg_hash_weight(uint64_t seed, uint32_t u, uint32_t v, uint32_t wlo,
  * loads (best of 5 each, GB/s). */
 int dycg_measure_host_link(int device, uint64_t bytes, double *h2d_gbs, double *zero_copy_gbs);
 
+/* Replaces GroupedUpdateBatch (include/framework/effective_update_batch.h:
+ * 36-207) as a standalone device step. Device pointers throughout; stream is a
+ * cudaStream_t (NULL = default stream). Records with an endpoint >=
+ * num_vertices are dropped; the rest are sorted by (u, v) and each distinct
+ * (u, v) is written once, in ascending order, as d_out_uv[2i], d_out_uv[2i+1]
+ * with its multiplicity d_out_mult[i] (outputs sized n). d_counts[0] = distinct
+ * records, d_counts[1] = dropped records. When num_segments > 0, the distinct
+ * records are also counted per source segment: segment s holds sources in
+ * [d_segment_ends[s-1], d_segment_ends[s]) (ends ascending). Scratch memory is
+ * allocated on the stream and released before the call returns. */
+int dycg_group_updates(const dycg_edge *d_records, size_t n, uint32_t num_vertices,
+                       const uint32_t *d_segment_ends, uint32_t num_segments,
+                       uint32_t *d_out_uv, uint32_t *d_out_mult, uint32_t *d_segment_counts,
+                       uint32_t *d_counts, void *stream);
+
 /* cudaStream_t the engine launches on (for CUDA-event timing by callers). */
 int dycg_stream(dycg_engine *e, void **stream);
 

@@ -119,6 +119,7 @@ def lib():
         "dycg_measure_host_link": (I, [I, u64, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_double)]),
         "dycg_group_updates": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
+        "dycg_group_updates_noalloc": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
         "dycg_last_error": (I, [P, ctypes.c_char_p, sz]),
         "dycg_version": (ctypes.c_char_p, []),
     }

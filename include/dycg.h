@@ -263,6 +263,23 @@ int dycg_group_updates(const dycg_edge *d_records, size_t n, uint32_t num_vertic
                        uint32_t *d_out_uv, uint32_t *d_out_mult, uint32_t *d_segment_counts,
                        uint32_t *d_counts, void *stream);
 
+/* dycg_group_updates without any allocation -- no counterpart in the
+ * reference. Same inputs, outputs and results as dycg_group_updates, for
+ * callers that cannot allocate device memory at call time (code that must not
+ * synchronise the device, processes whose device memory is held by another
+ * allocator, hosts that must not own GPU allocations). Its scratch is a fixed
+ * file-scope device array sized for DYCG_GROUP_NOALLOC_MAX_RECORDS records
+ * (about 10 MiB, held on every GPU that loads the library until exit); larger
+ * batches return DYCG_ECAPACITY. All calls share that array: calls that
+ * overlap on the GPU race, calls ordered on one stream are safe. The first
+ * call on a device looks up the array's device address and should come
+ * before any stream capture. */
+#define DYCG_GROUP_NOALLOC_MAX_RECORDS 262144u
+int dycg_group_updates_noalloc(const dycg_edge *d_records, size_t n, uint32_t num_vertices,
+                               const uint32_t *d_segment_ends, uint32_t num_segments,
+                               uint32_t *d_out_uv, uint32_t *d_out_mult,
+                               uint32_t *d_segment_counts, uint32_t *d_counts, void *stream);
+
 /* cudaStream_t the engine launches on (for CUDA-event timing by callers). */
 int dycg_stream(dycg_engine *e, void **stream);
 

@@ -44,16 +44,28 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dycg", choices=["dycg", "reference"])
     ap.add_argument("--algo", default="sssp", choices=["sssp", "bfs", "cc", "pr"])
-    ap.add_argument("--scale", type=int, default=26)
+    ap.add_argument("--config", default="rmat26", choices=["rmat26", "rmat16", "grid"],
+                    help="rmat26: headline out-of-memory R-MAT; rmat16: the small CPU-runnable "
+                         "R-MAT; grid: 4096^2 road-like grid")
+    ap.add_argument("--scale", type=int, default=None)
     ap.add_argument("--edge-factor", type=int, default=16)
-    ap.add_argument("--batch", type=int, default=100_000, help="updates per snapshot (50/50)")
-    ap.add_argument("--budget-gb", type=float, default=4.0)
+    ap.add_argument("--batch", type=int, default=None, help="updates per snapshot (50/50)")
+    ap.add_argument("--budget-gb", type=float, default=None)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-baseline-batches", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--json-out", default=None)
-    return ap.parse_args()
+    args = ap.parse_args()
+    defaults = {"rmat26": (26, 100_000, 4.0), "rmat16": (16, 2_000, 0.0),
+                "grid": (12, 10_000, 0.25)}[args.config]
+    if args.scale is None:
+        args.scale = defaults[0]
+    if args.batch is None:
+        args.batch = defaults[1]
+    if args.budget_gb is None:
+        args.budget_gb = defaults[2]
+    return args
 
 
 class Clocks:
@@ -130,13 +142,59 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def make_batches(scale, total_batches, nd, na, seed, sample_fn):
+def make_batches(scale, total_batches, nd, na, seed, sample_fn, config="rmat26", wmax=64):
     """Deletions: nd distinct live edges per snapshot, disjoint across snapshots
-    (sampled once from the initial graph); insertions: R-MAT draws."""
+    (sampled once from the initial graph); insertions: R-MAT draws. On the grid:
+    70% of the deletions are 4-neighbour grid edges and 30% shortcuts, and the
+    insertions are new shortcuts within radius 8."""
     import dycgraph_b200 as dg
-    dels = sample_fn(total_batches * nd, seed)
-    adds = dg.gen_rmat_edges(scale, total_batches * na, seed + 1, first=0)
-    return [(dels[i * nd:(i + 1) * nd], adds[i * na:(i + 1) * na]) for i in range(total_batches)]
+    if config != "grid":
+        dels = sample_fn(total_batches * nd, seed)
+        adds = dg.gen_rmat_edges(scale, total_batches * na, seed + 1, first=0)
+        return [(dels[i * nd:(i + 1) * nd], adds[i * na:(i + 1) * na])
+                for i in range(total_batches)]
+    side = 1 << scale
+    # shortcuts are ~0.5% of the directed edges: sample a pool large enough to
+    # hold 30% of every snapshot's deletions as shortcuts
+    need = int(total_batches * nd * 0.3 / 0.004) + total_batches * nd
+    pool = sample_fn(min(need, 48_000_000), seed)
+    du = pool[:, 0].astype(np.int64)
+    dv = pool[:, 1].astype(np.int64)
+    is_grid = (np.abs(du - dv) == 1) | (np.abs(du - dv) == side)
+    g, sc = pool[is_grid], pool[~is_grid]
+    ns = min(nd - int(round(nd * 0.7)), len(sc) // total_batches)
+    ng = nd - ns
+    if len(g) < ng * total_batches:
+        raise RuntimeError("not enough grid edges sampled")
+    rng = np.random.default_rng(seed + 5)
+    n = side * side
+    u = rng.integers(0, n, size=total_batches * na)
+    dr = rng.integers(-8, 9, size=u.shape[0])
+    dc = rng.integers(-8, 9, size=u.shape[0])
+    r = np.clip(u // side + dr, 0, side - 1)
+    c = np.clip(u % side + dc, 0, side - 1)
+    v = r * side + c
+    v = np.where(v == u, (u + 1) % n, v)
+    w = (np.random.default_rng(seed + 9).integers(1, wmax + 1, size=u.shape[0])).astype(np.uint32)
+    adds = np.stack([u.astype(np.uint32), v.astype(np.uint32), w], 1)
+    out = []
+    for i in range(total_batches):
+        d = np.concatenate([g[i * ng:(i + 1) * ng], sc[i * ns:(i + 1) * ns]])
+        out.append((d, adds[i * na:(i + 1) * na]))
+    return out
+
+
+def replica_totals(ms, e2e_ms, per_step_updates, K, E, world, device):
+    """N GPUs run independent replicas: the job time is the maximum of the
+    ranks' device times, the throughput counts every rank's updates."""
+    import torch
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms, e2e_ms = float(t[0]), float(t[1])
+    value = per_step_updates * K * world / (ms / 1e3)
+    e2e_value = per_step_updates * E * world / (e2e_ms / 1e3) if E and e2e_ms > 0 else None
+    return ms, e2e_ms, value, e2e_value
 
 
 # ----------------------------------------------------------------------------
@@ -161,18 +219,23 @@ def run_dycg(args):
 
     t0 = time.time()
     eng = dg.Engine(algo, weight_mode="stored" if algo == "sssp" else "hash128",
-                    hbm_graph_budget_bytes=budget, symmetric=(algo == "cc"), epsilon=1e-4,
+                    hbm_graph_budget_bytes=budget,
+                    symmetric=(algo == "cc" and args.config != "grid"), epsilon=1e-4,
                     device=local)
-    eng.load_rmat(args.scale, args.edge_factor, seed=args.seed, wlo=1, whi=64,
-                  symmetrize=(algo == "cc"))
+    wmax = 1000 if args.config == "grid" else 64
+    if args.config == "grid":
+        eng.load_grid(1 << args.scale, 10, 8, seed=args.seed, wlo=1, whi=wmax)
+    else:
+        eng.load_rmat(args.scale, args.edge_factor, seed=args.seed, wlo=1, whi=wmax,
+                      symmetrize=(algo == "cc"))
     t_load = time.time() - t0
     t0 = time.time()
     eng.start()
     t_init = time.time() - t0
     info = eng.info()
     batches = make_batches(args.scale, W + K + E, nd, na, args.seed + 17 + 1000 * rank,
-                           eng.sample_edges)
-    if algo == "cc":  # symmetric updates on the symmetrised graph
+                           eng.sample_edges, args.config, wmax)
+    if algo == "cc" and args.config != "grid":  # symmetric updates on the symmetrised graph
         batches = [(np.concatenate([d, d[:, [1, 0, 2]]]), np.concatenate([a, a[:, [1, 0, 2]]]))
                    for d, a in batches]
     per_step_updates = sum(len(d) + len(a) for d, a in batches[:1])
@@ -224,13 +287,8 @@ def run_dycg(args):
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1)
-    times = torch.tensor([ms, e2e_ms or 0.0], device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
-    ms, e2e_ms = float(times[0]), float(times[1])
-    total_updates = per_step_updates * K * world
-    value = total_updates / (ms / 1e3)
-    e2e_value = per_step_updates * E * world / (e2e_ms / 1e3) if E else None
+    ms, e2e_ms, value, e2e_value = replica_totals(ms, e2e_ms or 0.0, per_step_updates, K, E,
+                                                  world, "cuda")
 
     # roofline of the dominant kernel (the persistent repair kernel; one launch
     # per snapshot): algorithmic bytes from the kernel's own counters
@@ -269,12 +327,14 @@ def run_dycg(args):
         "warmup": W, "ms_per_step": round(ms / K, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32" if algo != "pr" else "f32",
         "data": "synthetic (seeded R-MAT; the reference's real graphs are not available)",
-        "config": {"workload": f"rmat{args.scale}-ef{args.edge_factor} {algo} "
+        "config": {"workload": (f"grid{1 << args.scale}x{1 << args.scale}+1%shortcuts"
+                                if args.config == "grid" else
+                                f"rmat{args.scale}-ef{args.edge_factor}") + f" {algo} "
                                f"{args.batch // 1000}K-update snapshots, HBM graph budget "
                                f"{args.budget_gb:g} GB",
                    "vertices": info["nodes"], "edges": info["live_edges"],
                    "updates_per_step": per_step_updates, "deletes_per_step": nd,
-                   "inserts_per_step": na, "weights": "uint32 uniform [1,64] stored"
+                   "inserts_per_step": na, "weights": f"uint32 uniform [1,{wmax}] stored"
                    if algo == "sssp" else "rule", "graph_host_bytes": info["host_bytes"],
                    "cached_pages": info["cached_pages"], "cache_slots": info["cache_slots"],
                    "l2": "inputs larger than L2 (graph in pinned host memory, vertex state "
@@ -318,7 +378,8 @@ def cpu_baseline(eng, args, algo, nd, na):
     del off, dst, w
     setup_s = time.time() - t0
     nb = max(1, args.cpu_baseline_batches)
-    batches = make_batches(args.scale, nb, nd, na, args.seed + 999, eng.sample_edges)
+    batches = make_batches(args.scale, nb, nd, na, args.seed + 999, eng.sample_edges, args.config,
+                           1000 if args.config == "grid" else 64)
     cpu_s = 0.0
     parity = True
     for d, a in batches:
@@ -346,8 +407,9 @@ def run_reference(args):
     nd = args.batch // 2
     na = args.batch - nd
     algo = args.algo
-    if algo == "pr":
-        return {"impl": "reference", "unavailable": "reference arm is wired for SSSP/BFS/CC"}
+    if algo == "pr" or args.config == "grid":
+        return {"impl": "reference",
+                "unavailable": "the CPU reference arm is wired for SSSP/BFS/CC on R-MAT configs"}
     threads = os.cpu_count() or 1
     t0 = time.time()
     n, off, dst, w = oracle.rmat_csr(args.scale, args.edge_factor, args.seed, wlo=1, whi=64,

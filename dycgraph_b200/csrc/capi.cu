@@ -94,6 +94,11 @@ int dycg_load_graph_file(dycg_engine *e, const char *path, uint32_t min_nodes, i
   return guard(e, [&](Engine &g) { g.load_file(path, min_nodes, weighted); });
 }
 
+int dycg_load_graph_binary(dycg_engine *e, const char *path) {
+  if (!path) return DYCG_EINVAL;
+  return guard(e, [&](Engine &g) { g.load_binary(path); });
+}
+
 int dycg_load_graph_rmat(dycg_engine *e, uint32_t scale, uint32_t edge_factor, double a, double b,
                          double c, uint64_t seed, uint32_t wlo, uint32_t whi, int symmetrize) {
   return guard(e, [&](Engine &g) { g.load_rmat(scale, edge_factor, a, b, c, seed, wlo, whi, symmetrize); });

@@ -89,6 +89,27 @@ bool read_updates(const std::string &upd, const std::string &sizes, Updates &U) 
   return true;
 }
 
+// Binary stream "DYCGUPD1": sizes (adds, dels) per snapshot, then per snapshot
+// its deletions followed by its insertions (12-byte records).
+bool read_updates_binary(const std::string &path, Updates &U) {
+  std::ifstream f(path, std::ios::binary);
+  char magic[8];
+  uint64_t hdr[3];
+  if (!f.read(magic, 8) || std::memcmp(magic, "DYCGUPD1", 8) != 0) return false;
+  if (!f.read(reinterpret_cast<char *>(hdr), sizeof hdr)) return false;
+  std::vector<uint32_t> sz(hdr[0] * 2);
+  if (!f.read(reinterpret_cast<char *>(sz.data()), sz.size() * 4)) return false;
+  for (uint64_t b = 0; b < hdr[0]; b++) {
+    U.sizes.push_back({sz[2 * b], sz[2 * b + 1]});
+    std::vector<dycg_edge> d(sz[2 * b + 1]), a(sz[2 * b]);
+    if (!d.empty() && !f.read(reinterpret_cast<char *>(d.data()), d.size() * 12)) return false;
+    if (!a.empty() && !f.read(reinterpret_cast<char *>(a.data()), a.size() * 12)) return false;
+    U.dels.insert(U.dels.end(), d.begin(), d.end());
+    U.adds.insert(U.adds.end(), a.begin(), a.end());
+  }
+  return true;
+}
+
 uint64_t distance_checksum(const std::vector<uint32_t> &d) {
   // samples/hybrid_sssp/hybrid_sssp.cu:335-347
   uint64_t c = 1469598103934665603ull;
@@ -209,7 +230,9 @@ int main(int argc, char **argv) {
   dycg_engine *e = nullptr;
   int rc = dycg_create(&o, &e);
   if (rc) return fail(nullptr, "dycg_create", rc);
-  rc = dycg_load_graph_file(e, graphfile.c_str(), 0, 0);
+  const std::string fmt = flag("format", "market_big");
+  rc = fmt == "binary" ? dycg_load_graph_binary(e, graphfile.c_str())
+                       : dycg_load_graph_file(e, graphfile.c_str(), 0, 0);
   if (rc) return fail(e, "load graph", rc);
   dycg_graph_info gi;
   dycg_graph_info_get(e, &gi);
@@ -225,7 +248,12 @@ int main(int argc, char **argv) {
 
   Updates U;
   const std::string updfile = flag("updatefile", ""), sizefile = flag("update_size", "");
-  if (!updfile.empty() && !read_updates(updfile, sizefile, U)) {
+  const bool upd_bin = flag("update_format", "") == "binary";
+  if (!updfile.empty() && upd_bin && !read_updates_binary(updfile, U)) {
+    std::fprintf(stderr, "cannot read binary update file\n");
+    return 1;
+  }
+  if (!updfile.empty() && !upd_bin && !read_updates(updfile, sizefile, U)) {
     std::fprintf(stderr, "cannot read update files\n");
     return 1;
   }

@@ -15,6 +15,11 @@
 #include <sstream>
 #include <unordered_set>
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include "engine.h"
 
 namespace dycg {
@@ -340,6 +345,42 @@ void Engine::load_file(const char *path, uint32_t min_nodes, int weighted) {
     wt[p] = ws[i];
   }
   load_csr(n, off.data(), dst.data(), weighted ? wt.data() : nullptr);
+}
+
+// Binary CSR: header "DYCGCSR1", n, m, flags; offsets[n+1] (u64); dst[m] (u32);
+// w[m] (u32, flag bit 0). Mapped read-only; the arrays feed load_csr directly.
+void Engine::load_binary(const char *path) {
+  int fd = ::open(path, O_RDONLY);
+  if (fd < 0) throw Error(DYCG_EIO, std::string("cannot open graph file ") + path);
+  struct stat st;
+  if (fstat(fd, &st) != 0 || st.st_size < 32) {
+    ::close(fd);
+    throw Error(DYCG_EIO, "binary graph file too short");
+  }
+  void *map = mmap(nullptr, (size_t)st.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+  ::close(fd);
+  if (map == MAP_FAILED) throw Error(DYCG_EIO, "cannot map binary graph file");
+  const char *b = (const char *)map;
+  uint64_t hdr[3];
+  std::memcpy(hdr, b + 8, 24);
+  const uint64_t n = hdr[0], m = hdr[1], flags = hdr[2];
+  const uint64_t need = 32 + (n + 1) * 8 + m * 4 * ((flags & 1) ? 2 : 1);
+  if (std::memcmp(b, "DYCGCSR1", 8) != 0 || n == 0 || n >= 0x7FFFFFFFull ||
+      (uint64_t)st.st_size < need) {
+    munmap(map, (size_t)st.st_size);
+    throw Error(DYCG_EIO, "not a DYCGCSR1 file or truncated");
+  }
+  const uint64_t *off = (const uint64_t *)(b + 32);
+  const uint32_t *dst = (const uint32_t *)(b + 32 + (n + 1) * 8);
+  const uint32_t *w = (flags & 1) ? dst + m : nullptr;
+  try {
+    if (off[0] != 0 || off[n] != m) throw Error(DYCG_EIO, "inconsistent offsets");
+    load_csr((uint32_t)n, off, dst, w);
+  } catch (...) {
+    munmap(map, (size_t)st.st_size);
+    throw;
+  }
+  munmap(map, (size_t)st.st_size);
 }
 
 void Engine::load_rmat(uint32_t scale, uint32_t ef, double a, double b, double c, uint64_t seed,

@@ -38,6 +38,7 @@ class Engine {
 
   void load_csr(uint32_t n, const uint64_t *off, const uint32_t *dst, const uint32_t *w);
   void load_file(const char *path, uint32_t min_nodes, int weighted);
+  void load_binary(const char *path);
   void load_rmat(uint32_t scale, uint32_t ef, double a, double b, double c, uint64_t seed,
                  uint32_t wlo, uint32_t whi, int symmetrize);
   void load_grid(uint32_t side, uint32_t permille, uint32_t radius, uint64_t seed, uint32_t wlo,

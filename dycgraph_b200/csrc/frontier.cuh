@@ -185,14 +185,18 @@ __device__ bool expand_rows(const Adj &A, const uint32_t *items, uint32_t cnt, O
     }
     warp_slots<WITH_W>(A, v, A.off[v], 0, len, 32, op, acc);
   }
-  if (!grid_sync(ctl, 0, timeout_ns)) return false;
+  // The items have been consumed: the queue resets can apply here. When no row
+  // was heavy this barrier's snapshot already holds every append of the
+  // expansion and the tile phase (and its barrier) is skipped.
+  if (!grid_sync(ctl, reset_flags, timeout_ns)) return false;
   const uint32_t nt = min(*(volatile uint32_t *)&ctl->snap_tiles, T.cap);
+  if (nt == 0) return true;
   const uint32_t wib = threadIdx.x >> 5;
   for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
     const uint4 tl = T.tiles[t];
     warp_slots<WITH_W>(A, tl.x, A.off[tl.x], tl.y + wib * 32, tl.z, blockDim.x, op, acc);
   }
-  return grid_sync(ctl, SYNC_RESET_TILES | reset_flags, timeout_ns);
+  return grid_sync(ctl, SYNC_RESET_TILES, timeout_ns);
 }
 
 __device__ __forceinline__ u64 ld_key(const u64 *p) {

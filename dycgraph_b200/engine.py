@@ -97,6 +97,7 @@ def lib():
         "dycg_destroy": (None, [P]),
         "dycg_load_graph_csr": (I, [P, u32, u64p, u32p, u32p]),
         "dycg_load_graph_file": (I, [P, ctypes.c_char_p, u32, I]),
+        "dycg_load_graph_binary": (I, [P, ctypes.c_char_p]),
         "dycg_load_graph_rmat": (I, [P, u32, u32, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double, u64, u32, u32, I]),
         "dycg_load_graph_grid": (I, [P, u32, u32, u32, u64, u32, u32]),
@@ -240,6 +241,10 @@ class Engine:
     def load_file(self, path, min_nodes=0, weighted=False):
         self._check(lib().dycg_load_graph_file(self._h, path.encode(), min_nodes, int(weighted)),
                     "load_file")
+        self.n = self.info()["nodes"]
+
+    def load_binary(self, path):
+        self._check(lib().dycg_load_graph_binary(self._h, path.encode()), "load_binary")
         self.n = self.info()["nodes"]
 
     def load_rmat(self, scale, edge_factor=16, seed=1, a=0.57, b=0.19, c=0.19, wlo=1, whi=64,

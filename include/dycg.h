@@ -157,6 +157,13 @@ int dycg_load_graph_csr(dycg_engine *e, uint32_t n, const uint64_t *offsets,
 int dycg_load_graph_file(dycg_engine *e, const char *path, uint32_t min_nodes,
                          int weighted);
 
+/* Binary CSR graph file (replaces the market_big text parse,
+ * src/utils/parser.cpp:296-406, for large graphs): little-endian
+ *   char magic[8] = "DYCGCSR1"; uint64 n; uint64 m; uint64 flags (bit 0: weights)
+ *   uint64 offsets[n+1]; uint32 dst[m]; uint32 w[m] (when bit 0 is set)
+ * read with one pass over a memory map. */
+int dycg_load_graph_binary(dycg_engine *e, const char *path);
+
 /* Synthetic workloads built on the GPU straight into the engine. R-MAT:
  * 2^scale vertices, edge_factor*2^scale draws with quadrant probabilities
  * (a,b,c,1-a-b-c), self-loops and duplicates removed; weights uniform in

@@ -67,3 +67,20 @@ def test_rmat_draws_deterministic_and_skewed():
     # weights are a function of (u, v)
     for u, v, w in a[:50]:
         assert dg.hash_weight(7, int(u), int(v)) == w
+
+
+def test_binary_formats_round_trip(tmp_path):
+    from dycgraph_b200 import formats
+    off = np.array([0, 2, 2, 5], np.uint64)
+    dst = np.array([1, 2, 0, 1, 1], np.uint32)
+    w = np.array([3, 4, 5, 6, 7], np.uint32)
+    formats.write_graph(tmp_path / "g.bin", off, dst, w)
+    n, o2, d2, w2 = formats.read_graph(tmp_path / "g.bin")
+    assert n == 3 and (o2 == off).all() and (d2 == dst).all() and (w2 == w).all()
+    batches = [(np.array([[0, 1, 3]]), np.array([[2, 0, 9], [1, 2, 1]])), (np.zeros((0, 3)), np.array([[0, 2, 2]]))]
+    formats.write_updates(tmp_path / "u.bin", batches)
+    back = formats.read_updates(tmp_path / "u.bin")
+    assert len(back) == 2
+    for (d, a), (d2_, a2) in zip(batches, back):
+        assert (np.asarray(d, np.uint32).reshape(-1, 3) == d2_).all()
+        assert (np.asarray(a, np.uint32).reshape(-1, 3) == a2).all()

@@ -68,3 +68,22 @@ def test_cli_pr_smoke(tmp_path):
     x = np.array([float(line.split()[1]) for line in (tmp_path / "out").read_text().splitlines()])
     # the reference's acceptance bound (tests/pr_dynamic_smoke.py:96-98)
     assert float(np.mean(np.abs(x - np.array(case["final_ranks"])))) < 1e-5
+
+
+def test_cli_binary_formats(tmp_path):
+    """The same smoke stream through the binary graph and update files."""
+    from dycgraph_b200 import formats
+    case = cases.load("smoke_bfs_sssp.json")
+    n = case["n"]
+    off, dst, _ = cases.csr(n, case["graph"])
+    formats.write_graph(tmp_path / "graph", off, dst)
+    formats.write_updates(tmp_path / "updates", [
+        (np.array([(u, v, 77) for u, v in b["dels"]], np.uint32),
+         np.array([(u, v, 91) for u, v in b["adds"]], np.uint32)) for b in case["batches"]])
+    cmd = [os.path.join(BIN, "hybrid_sssp"), f"--graphfile={tmp_path / 'graph'}", "--format=binary",
+           f"--updatefile={tmp_path / 'updates'}", "--update_format=binary", "--check=true",
+           "--sssp_max_batches=3"]
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout[-2000:] + p.stderr[-2000:]
+    got = [int(v) for v in re.findall(r"\[SSSP-(?:DELETE-STAGE|BATCH)-CHECK\][^\n]*distance_checksum=(\d+)", p.stdout)]
+    assert got == [e["checksum"] for e in case["expected"]["sssp"]]

@@ -55,8 +55,13 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-baseline-batches", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ordered-delta", type=int, default=None,
+                    help="bucketed closure width (default: 0 on R-MAT, on the grid 256 for SSSP "
+                         "and 1 for BFS/CC)")
     ap.add_argument("--json-out", default=None)
     args = ap.parse_args()
+    if args.ordered_delta is None:
+        args.ordered_delta = 0 if args.config != "grid" else (256 if args.algo == "sssp" else 1)
     defaults = {"rmat26": (26, 100_000, 4.0), "rmat16": (16, 2_000, 0.0),
                 "grid": (12, 10_000, 0.25)}[args.config]
     if args.scale is None:
@@ -221,7 +226,7 @@ def run_dycg(args):
     eng = dg.Engine(algo, weight_mode="stored" if algo == "sssp" else "hash128",
                     hbm_graph_budget_bytes=budget,
                     symmetric=(algo == "cc" and args.config != "grid"), epsilon=1e-4,
-                    device=local)
+                    device=local, ordered_delta=args.ordered_delta if algo != "pr" else 0)
     wmax = 1000 if args.config == "grid" else 64
     if args.config == "grid":
         eng.load_grid(1 << args.scale, 10, 8, seed=args.seed, wlo=1, whi=wmax)
@@ -339,7 +344,8 @@ def run_dycg(args):
                    "cached_pages": info["cached_pages"], "cache_slots": info["cache_slots"],
                    "l2": "inputs larger than L2 (graph in pinned host memory, vertex state "
                          f"{info['nodes'] * 40 / 1e9:.1f} GB in HBM)",
-                   "parallelism": f"replicas x{world}", "load_s": round(t_load, 2),
+                   "parallelism": f"replicas x{world}", "ordered_delta": args.ordered_delta,
+                   "load_s": round(t_load, 2),
                    "static_solve_s": round(t_init, 2)},
         "clocks": clk,
         "e2e": {"value": round(e2e_value, 1) if e2e_value else None, "unit": UNIT,

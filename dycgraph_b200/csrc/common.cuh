@@ -120,12 +120,14 @@ struct Ctl {
   uint32_t err;
   uint32_t err_info;
   uint32_t n_aff;        // affected list length
-  uint32_t q_count[2];   // wave queue lengths
+  uint32_t q_count[3];   // wave queue lengths (q0/q1 alternate; q2: the ordered bucket)
   uint32_t tile_count;
+  uint32_t vmin;         // ordered closure: minimum frontier value of the wave
   // snapshots taken by the last block to arrive at a barrier
   uint32_t snap_aff;
-  uint32_t snap_q[2];
+  uint32_t snap_q[3];
   uint32_t snap_tiles;
+  uint32_t snap_vmin;
   uint32_t wave_tag;     // running wave tag (never reused)
   uint32_t waves;        // waves run in this launch
   uint32_t pad[2];

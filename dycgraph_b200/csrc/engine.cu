@@ -245,6 +245,7 @@ void Engine::finish_load() {
   aff_ = (uint32_t *)dmalloc((n + 1ull) * 4);
   q0_ = (uint32_t *)dmalloc((n + 1ull) * 4);
   q1_ = (uint32_t *)dmalloc((n + 1ull) * 4);
+  q2_ = opt_.ordered_delta ? (uint32_t *)dmalloc((n + 1ull) * 4) : nullptr;
   CK(cudaMemsetAsync(mark_, 0, (n + 1ull) * 4, st_));
   CK(cudaMemsetAsync(wtag_, 0, (n + 1ull) * 4, st_));
   CK(cudaMemsetAsync(touch_, 0, (n + 1ull) * 4, st_));
@@ -508,6 +509,8 @@ void Engine::init() {
     L.tag_base = tag_base_;
     L.phases = PH_CLOSE;
     L.max_waves = (uint32_t)std::min<u64>(4ull * n_ + 1024, 0x7FFFFFFFull);
+    L.delta = opt_.ordered_delta;
+    L.q2 = q2_;
     L.timeout_ns = timeout;
     L.algo = opt_.algo;
     L.stored = stored_;
@@ -747,6 +750,8 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     L.tag_base = tag_base_;
     L.phases = (nd ? PH_DELETE : 0) | (na ? PH_INSERT : 0) | PH_CLOSE;
     L.max_waves = (uint32_t)std::min<u64>(4ull * n_ + 1024, 0x7FFFFFFFull);
+    L.delta = opt_.ordered_delta;
+    L.q2 = q2_;
     L.timeout_ns = timeout;
     L.algo = opt_.algo;
     L.stored = stored_;

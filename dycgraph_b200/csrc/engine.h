@@ -93,7 +93,7 @@ class Engine {
   // vertex state
   u64 *key_ = nullptr;
   uint32_t *mark_ = nullptr, *wtag_ = nullptr, *aff_ = nullptr, *q0_ = nullptr, *q1_ = nullptr,
-           *touch_ = nullptr;
+           *q2_ = nullptr, *touch_ = nullptr;
   uint4 *tiles_ = nullptr;
   uint32_t tile_cap_ = 0;
   Ctl *ctl_ = nullptr, *h_ctl_ = nullptr;

@@ -15,6 +15,8 @@ namespace dycg {
 constexpr uint32_t SYNC_RESET_TILES = 1;
 constexpr uint32_t SYNC_RESET_Q0 = 2;
 constexpr uint32_t SYNC_RESET_Q1 = 4;
+constexpr uint32_t SYNC_RESET_Q2 = 8;
+constexpr uint32_t SYNC_RESET_VMIN = 16;
 
 // Grid-wide barrier for cooperative launches. Every wait is bounded: past
 // timeout_ns the waiting block records ERR_BARRIER and all blocks leave at
@@ -34,10 +36,14 @@ __device__ __forceinline__ bool grid_sync(Ctl *c, uint32_t flags, u64 timeout_ns
       if (flags & SYNC_RESET_TILES) c->tile_count = 0;
       if (flags & SYNC_RESET_Q0) c->q_count[0] = 0;
       if (flags & SYNC_RESET_Q1) c->q_count[1] = 0;
+      if (flags & SYNC_RESET_Q2) c->q_count[2] = 0;
       c->snap_aff = *(volatile uint32_t *)&c->n_aff;
       c->snap_q[0] = *(volatile uint32_t *)&c->q_count[0];
       c->snap_q[1] = *(volatile uint32_t *)&c->q_count[1];
+      c->snap_q[2] = *(volatile uint32_t *)&c->q_count[2];
       c->snap_tiles = *(volatile uint32_t *)&c->tile_count;
+      c->snap_vmin = *(volatile uint32_t *)&c->vmin;
+      if (flags & SYNC_RESET_VMIN) c->vmin = 0xFFFFFFFFu;
       atomicExch(&c->bar_count, 0u);
       __threadfence();
       atomicAdd(&c->bar_gen, 1u);

@@ -29,6 +29,8 @@ struct RepairLaunch {
   const uint3 *add_uvw;
   uint32_t n_add;
   uint32_t n, source, epoch, tag_base, phases, max_waves;
+  uint32_t delta;  // ordered closure bucket width (0: unordered)
+  uint32_t *q2;
   u64 timeout_ns;
   uint32_t algo;
   bool stored;

@@ -44,6 +44,8 @@ struct RepairParams {
   uint32_t tag_base;
   uint32_t phases;
   uint32_t max_waves;
+  uint32_t delta;           // ordered closure: expand values < wave min + delta (0: unordered)
+  uint32_t *q2;             // ordered closure: the wave's bucket
   u64 timeout_ns;
 };
 
@@ -249,9 +251,56 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
       warp_append(P.q[0], &ctl->q_count[0], P.n, want, v, &ctl->err);
     }
   }
-  if (!grid_sync(ctl, 0, P.timeout_ns)) goto done;
+  if (!grid_sync(ctl, SYNC_RESET_VMIN, P.timeout_ns)) goto done;
   // 6. closure waves
-  if (P.phases & PH_CLOSE) {
+  if ((P.phases & PH_CLOSE) && P.delta) {
+    // Ordered (bucketed) closure for high-diameter graphs, the B200 form of
+    // the reference's ordered insertion schedule (framework.cuh:537-556):
+    // each wave expands only the frontier vertices whose value is below the
+    // wave's minimum + delta and carries the rest to the next wave, so a
+    // vertex is expanded about once instead of once per improvement.
+    uint32_t cur = 0;
+    for (uint32_t wave = 0;; wave++) {
+      const uint32_t cnt = *(volatile uint32_t *)&ctl->snap_q[cur];
+      if (cnt == 0) break;
+      if (wave >= P.max_waves) {
+        if (gtid == 0) atomicCAS(&ctl->err, 0u, ERR_WAVES);
+        break;
+      }
+      const uint32_t tag = P.tag_base + 1 + wave;
+      uint32_t m = INF32;
+      for (uint32_t i = gtid; i < cnt; i += gstride)
+        m = min(m, key_value(ld_key(P.key + P.q[cur][i])));
+      for (int o = 16; o; o >>= 1) m = min(m, __shfl_down_sync(0xffffffffu, m, o));
+      if (lane == 0 && m != INF32) atomicMin(&ctl->vmin, m);
+      if (!grid_sync(ctl, 0, P.timeout_ns)) goto done;
+      const uint32_t vm = *(volatile uint32_t *)&ctl->snap_vmin;
+      const uint32_t thr = vm > INF32 - P.delta ? INF32 : vm + P.delta;
+      // split: values below thr form this wave's bucket, the rest carry over
+      for (uint32_t i0 = gtid - lane; i0 < cnt; i0 += gstride) {
+        const uint32_t i = i0 + lane;
+        uint32_t v = 0;
+        bool now = false, carry = false;
+        if (i < cnt) {
+          v = P.q[cur][i];
+          const uint32_t d = key_value(ld_key(P.key + v));
+          now = d < thr;
+          carry = !now && d != INF32 && atomicExch(P.wtag + v, tag) != tag;
+        }
+        warp_append(P.q2, &ctl->q_count[2], P.n, now, v, &ctl->err);
+        warp_append(P.q[cur ^ 1], &ctl->q_count[cur ^ 1], P.n, carry, v, &ctl->err);
+      }
+      if (!grid_sync(ctl, (cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0) | SYNC_RESET_VMIN, P.timeout_ns))
+        goto done;
+      const uint32_t nb = *(volatile uint32_t *)&ctl->snap_q[2];
+      RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag};
+      if (!expand_rows<STORED>(P.out, P.q2, nb, op, acc, P.tiles, ctl, SYNC_RESET_Q2,
+                               P.timeout_ns))
+        goto done;
+      if (gtid == 0) ctl->waves = wave + 1;
+      cur ^= 1;
+    }
+  } else if (P.phases & PH_CLOSE) {
     uint32_t cur = 0;
     for (uint32_t wave = 0;; wave++) {
       const uint32_t cnt = *(volatile uint32_t *)&ctl->snap_q[cur];
@@ -320,6 +369,8 @@ static cudaError_t launch_one(const RepairLaunch &L, cudaStream_t s) {
   P.tag_base = L.tag_base;
   P.phases = L.phases;
   P.max_waves = L.max_waves;
+  P.delta = L.delta;
+  P.q2 = L.q2;
   P.timeout_ns = L.timeout_ns;
   static int blocks_per_sm = -1;
   if (blocks_per_sm < 0) {

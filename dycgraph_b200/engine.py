@@ -41,7 +41,7 @@ class Options(ctypes.Structure):
                 ("symmetric", ctypes.c_uint32), ("epsilon", ctypes.c_float),
                 ("alpha", ctypes.c_float), ("max_rounds", ctypes.c_uint32),
                 ("device", ctypes.c_int32), ("page_shift", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 7)]
+                ("ordered_delta", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
 
 
 _STAT_U64 = ["deletions", "insertions", "missing_deletes", "invalid_updates", "touched_sources",
@@ -176,7 +176,7 @@ class Engine:
 
     def __init__(self, algo="sssp", weight_mode="hash128", source=0, segments=1,
                  hbm_graph_budget_bytes=0, cache_policy=None, symmetric=False, epsilon=1e-6,
-                 alpha=0.85, max_rounds=100, device=0, page_shift=12):
+                 alpha=0.85, max_rounds=100, device=0, page_shift=12, ordered_delta=0):
         L = lib()
         opt = Options()
         L.dycg_options_default(ctypes.byref(opt))
@@ -194,6 +194,7 @@ class Engine:
         opt.max_rounds = max_rounds
         opt.device = device
         opt.page_shift = page_shift
+        opt.ordered_delta = ordered_delta
         self.algo = opt.algo
         self.options = opt
         self._h = ctypes.c_void_p()

@@ -83,7 +83,11 @@ typedef struct dycg_options {
   uint32_t max_rounds;    /* PR rounds per batch (reference -pr_max_rounds)   */
   int32_t device;         /* CUDA device ordinal                              */
   uint32_t page_shift;    /* log2 of adjacency slots per cache page (0: 12)   */
-  uint32_t reserved[7];
+  uint32_t ordered_delta; /* SSSP/BFS/CC: 0 = unordered closure; d > 0 = each  */
+                          /* wave expands only values < wave min + d (the    */
+                          /* reference's ordered schedule, for high-diameter */
+                          /* graphs; 1 is exact-min order for BFS and CC)    */
+  uint32_t reserved[6];
 } dycg_options;
 
 /* Per-call counters. Byte counts are algorithmic: every adjacency slot read

@@ -353,3 +353,39 @@ def test_sample_edges_distinct_and_live():
     src = np.repeat(np.arange(n), np.diff(off).astype(np.int64))
     live = {(int(a), int(b)): int(c) for a, b, c in zip(src, dst, w)}
     assert all(live[(int(a), int(b))] == int(c) for a, b, c in s)
+
+
+# ---- ordered (bucketed) closure -------------------------------------------------
+
+@pytest.mark.parametrize("algo,delta", [("sssp", 64), ("bfs", 1), ("cc", 1), ("sssp", 1)])
+def test_ordered_closure_matches_oracle(algo, delta):
+    n, off, dst, w = cases.small_rmat(10, 8, 31)
+    e = engine_for(algo, n, off, dst, ordered_delta=delta, page_shift=8)
+    orc = oracle.Oracle(ALGO[algo], n, off, dst)
+    orc.init()
+    assert (e.gather()[0] == orc.values()[0]).all()
+    cur_off, cur_dst, cur_w = off, dst, w
+    for bi in range(3):
+        dels, adds = cases.random_batch(n, cur_off, cur_dst, cur_w, 200, 200, 700 + bi)
+        dels = [(u, v, cases.rule_w(ALGO[algo], u, v)) for u, v, _ in dels]
+        adds = [(u, v, cases.rule_w(ALGO[algo], u, v)) for u, v, _ in adds]
+        e.apply_batch(dels, adds)
+        orc.apply_batch(dels, adds)
+        assert (e.gather()[0] == orc.values()[0]).all()
+        cur_off, cur_dst, cur_w = orc.csr()
+    vals, par = e.gather()
+    check_parents(e, algo, vals, par)
+
+
+def test_ordered_closure_grid():
+    """High-diameter grid: the ordered closure gives the oracle's distances."""
+    e = dg.Engine("sssp", weight_mode="stored", ordered_delta=200, page_shift=8)
+    e.load_grid(64, 10, 8, seed=5, wlo=1, whi=1000)
+    e.start()
+    off, dst, w = e.csr()
+    n = 64 * 64
+    assert (e.gather()[0] == oracle.static_sssp(n, off, dst, w, oracle.WEIGHT_STORED, 0)).all()
+    s = e.sample_edges(300, 3)
+    e.apply_batch(s, [(int(u), int((u + 65) % n), 7) for u in range(0, n, 40)])
+    off, dst, w = e.csr()
+    assert (e.gather()[0] == oracle.static_sssp(n, off, dst, w, oracle.WEIGHT_STORED, 0)).all()

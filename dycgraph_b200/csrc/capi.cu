@@ -185,6 +185,19 @@ uint32_t dycg_hash_weight(uint64_t seed, uint32_t u, uint32_t v, uint32_t wlo, u
   return dycg::hash_weight(seed ^ 0x5745494748545321ull, u, v, wlo, whi);
 }
 
+int dycg_set_queries(dycg_engine *e, const uint32_t *sources, uint32_t count, uint32_t mode) {
+  if (!sources && count) return DYCG_EINVAL;
+  return guard(e, [&](Engine &g) { g.set_queries(sources, count, mode); });
+}
+
+int dycg_set_query_mapping(dycg_engine *e, uint32_t edge_lanes, uint32_t heavy, uint32_t tile) {
+  return guard(e, [&](Engine &g) { g.set_query_mapping(edge_lanes, heavy, tile); });
+}
+
+int dycg_gather_query(dycg_engine *e, uint32_t q, uint32_t *values, uint32_t *parents) {
+  return guard(e, [&](Engine &g) { g.gather_query(q, values, parents); });
+}
+
 int dycg_stream(dycg_engine *e, void **stream) {
   if (!stream) return DYCG_EINVAL;
   return guard(e, [&](Engine &g) { *stream = (void *)g.stream(); });

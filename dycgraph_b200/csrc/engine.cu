@@ -461,8 +461,15 @@ void Engine::load_grid(uint32_t side, uint32_t permille, uint32_t radius, uint64
 
 void Engine::init() {
   check_loaded();
+  if (inited_) throw Error(DYCG_ESTATE, "engine already initialised");
   CK(cudaMemsetAsync(ctl_, 0, sizeof(Ctl), st_));
   const u64 timeout = 120ull * 1000000000ull;
+  if (nq_) {
+    init_queries(timeout);
+    inited_ = true;
+    cache_maintenance(true, nullptr);
+    return;
+  }
   if (opt_.algo == DYCG_ALGO_PR) {
     CK(launch_pr_init(x_, r_, queued_, q0_, n_, 1.f - opt_.alpha, ctl_, st_));
     PrLaunch L{};
@@ -726,6 +733,8 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     PL.sign = 1.f;
     CK(launch_pr(PL, st_));
     launches_++;
+  } else if (nq_) {
+    repair_queries((uint32_t)nd, (uint32_t)na, timeout);
   } else {
     RepairLaunch L{};
     L.out = A_out;
@@ -761,8 +770,31 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
   }
   CK(cudaEventRecord(ev_[3], st_));
   CK(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
+  if (nq_) {
+    if (qmode_ == DYCG_QUERIES_PER_QUERY)
+      CK(cudaMemcpyAsync(h_qctl_, qctl_, (u64)nq_ * sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
+    CK(cudaMemcpyAsync(h_seq_, seq_, 8, cudaMemcpyDeviceToHost, st_));
+  }
   sync_check("batch");
   Ctl c = *h_ctl_;
+  if (nq_ && qmode_ == DYCG_QUERIES_PER_QUERY) {
+    // mutation counters are in ctl_, each query's repair counters in its own block
+    for (uint32_t q = 0; q < nq_; q++) {
+      const Ctl &r = h_qctl_[q];
+      if (!c.err) c.err = r.err;
+      for (int i : {ST_LINK_BYTES, ST_HBM_ADJ_BYTES, ST_EXPANDED, ST_SCANNED, ST_IMPROVED,
+                    ST_AFFECTED})
+        c.stat[i] += r.stat[i];
+      c.waves += r.waves;
+    }
+  }
+  if (nq_ && h_seq_[1] > 0xF0000000u) {
+    // wave tags are about to wrap: clear the tag array and restart the count
+    CK(cudaMemsetAsync(wtag_, 0, (n_ + 1ull) * 4, st_));
+    h_seq_[1] = 1;
+    CK(cudaMemcpyAsync(seq_ + 1, h_seq_ + 1, 4, cudaMemcpyHostToDevice, st_));
+    sync_check("tag reset");
+  }
   if (c.err) {
     failed = true;
     const int code = (c.err == ERR_WAVES || c.err == ERR_BARRIER) ? DYCG_ELIMIT : DYCG_ECAPACITY;
@@ -809,6 +841,239 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     // 8-byte key, per improvement 8 B key atomic + 4 B tag + 4 B queue slot
     stats->state_bytes = stats->expanded * 24 + stats->edges_scanned * 8 + stats->improvements * 16;
   }
+}
+
+// ---- many-query forms -------------------------------------------------------
+
+void Engine::set_queries(const uint32_t *sources, uint32_t count, uint32_t mode) {
+  check_loaded();
+  if (inited_) throw Error(DYCG_ESTATE, "queries must be set before dycg_init");
+  if (nq_) throw Error(DYCG_ESTATE, "queries already set");
+  if (opt_.algo != DYCG_ALGO_SSSP && opt_.algo != DYCG_ALGO_BFS)
+    throw Error(DYCG_EINVAL, "many-query forms support SSSP and BFS");
+  if (count == 0 || count > DYCG_MAX_QUERIES) throw Error(DYCG_EINVAL, "query count out of range");
+  if (mode != DYCG_QUERIES_BATCHED && mode != DYCG_QUERIES_PER_QUERY)
+    throw Error(DYCG_EINVAL, "unknown query mode");
+  if (opt_.ordered_delta && mode == DYCG_QUERIES_BATCHED)
+    throw Error(DYCG_EINVAL, "the batched form runs the unordered closure (ordered_delta 0)");
+  for (uint32_t q = 0; q < count; q++)
+    if (sources[q] >= n_) throw Error(DYCG_EINVAL, "query source out of range");
+  sources_.assign(sources, sources + count);
+  const u64 n = n_;
+  if (mode == DYCG_QUERIES_BATCHED) {
+    uint32_t nb = 1;
+    while (nb * 32 < count) nb *= 2;
+    const uint32_t Q = nb * 32;
+    std::vector<uint32_t> padded(Q, INF32);
+    std::copy(sources, sources + count, padded.begin());
+    d_sources_ = (uint32_t *)dmalloc((u64)Q * 4);
+    CK(cudaMemcpyAsync(d_sources_, padded.data(), (u64)Q * 4, cudaMemcpyHostToDevice, st_));
+    qkey_ = (u64 *)dmalloc(n * Q * 8);
+    uint32_t **masks[6] = {&affm_, &inew_[0], &inew_[1], &nmask_[0], &nmask_[1], &cmask_};
+    for (uint32_t **m : masks) {
+      *m = (uint32_t *)dmalloc(n * nb * 4);
+      CK(cudaMemsetAsync(*m, 0, n * nb * 4, st_));
+    }
+    // tiles for the smallest tile size the mapping accepts
+    const u64 maxslots = std::max(out_.slots, in_.slots);
+    mtile_cap_ = (uint32_t)std::min<u64>(2 * (maxslots / MULTI_MIN_TILE) + 4096, 0x7FFFFFFFull);
+    mtiles_ = (uint4 *)dmalloc((u64)mtile_cap_ * sizeof(uint4));
+    qnb_ = nb;
+    qbytes_ = (u64)Q * 4 + n * Q * 8 + 6 * n * nb * 4 + (u64)mtile_cap_ * sizeof(uint4);
+  } else {
+    d_sources_ = (uint32_t *)dmalloc((u64)count * 4);
+    CK(cudaMemcpyAsync(d_sources_, sources, (u64)count * 4, cudaMemcpyHostToDevice, st_));
+    qkey_ = (u64 *)dmalloc(n * count * 8);
+    qctl_ = (Ctl *)dmalloc((u64)count * sizeof(Ctl));
+    void *hq = nullptr;
+    CK(cudaHostAlloc(&hq, (u64)count * sizeof(Ctl), cudaHostAllocDefault));
+    hallocs_.push_back(hq);
+    h_qctl_ = (Ctl *)hq;
+    qbytes_ = (u64)count * 4 + n * count * 8 + (u64)count * sizeof(Ctl);
+  }
+  seq_ = (uint32_t *)dmalloc(8);
+  void *hs = nullptr;
+  CK(cudaHostAlloc(&hs, 8, cudaHostAllocDefault));
+  hallocs_.push_back(hs);
+  h_seq_ = (uint32_t *)hs;
+  h_seq_[0] = 1;  // epoch (mark_ starts at 0)
+  h_seq_[1] = 1;  // next wave tag (wtag_ starts at 0)
+  CK(cudaMemcpyAsync(seq_, h_seq_, 8, cudaMemcpyHostToDevice, st_));
+  qmode_ = mode;
+  nq_ = count;
+  sync_check("queries");
+}
+
+void Engine::set_query_mapping(uint32_t edge_lanes, uint32_t heavy, uint32_t tile) {
+  if (edge_lanes > MULTI_EDGE_LANES_MAX) throw Error(DYCG_EINVAL, "edge_lanes must be <= 8");
+  if (heavy < MULTI_MIN_TILE || tile < MULTI_MIN_TILE)
+    throw Error(DYCG_EINVAL, "heavy and tile must be >= 1024 slots");
+  edge_lanes_ = edge_lanes;
+  heavy_ = heavy;
+  tile_ = tile;
+}
+
+MultiLaunch Engine::multi_launch(uint32_t phases, uint32_t n_add, u64 timeout) {
+  MultiLaunch L{};
+  L.out = adj(out_);
+  L.in = has_in_ ? adj(in_) : L.out;
+  L.key = qkey_;
+  L.affm = affm_;
+  L.inew0 = inew_[0];
+  L.inew1 = inew_[1];
+  L.nmask0 = nmask_[0];
+  L.nmask1 = nmask_[1];
+  L.cmask = cmask_;
+  L.mark = mark_;
+  L.wtag = wtag_;
+  L.aff = aff_;
+  L.q0 = q0_;
+  L.q1 = q1_;
+  L.tiles = mtiles_;
+  L.tile_cap = mtile_cap_;
+  L.ctl = ctl_;
+  L.seq = seq_;
+  L.del_uv = uv_out_;
+  L.del_found = found_out_;
+  L.n_del_ptr = counts_;
+  L.add_uvw = add_uvw_;
+  L.n_add = n_add;
+  L.n = n_;
+  L.nb = qnb_;
+  L.phases = phases;
+  L.max_waves = (uint32_t)std::min<u64>(4ull * n_ + 1024, 0x7FFFFFFFull);
+  L.edge_lanes = edge_lanes_;
+  L.heavy = heavy_;
+  L.tile = tile_;
+  L.timeout_ns = timeout;
+  L.algo = opt_.algo;
+  L.stored = stored_;
+  L.num_sms = num_sms_;
+  return L;
+}
+
+// Single-source repair launch of query q (the per-query form).
+static RepairLaunch query_launch(const Adj &out, const Adj &in, u64 *key, uint32_t source) {
+  RepairLaunch L{};
+  L.out = out;
+  L.in = in;
+  L.key = key;
+  L.source = source;
+  return L;
+}
+
+// Static solve of every query.
+void Engine::init_queries(u64 timeout) {
+  if (qmode_ == DYCG_QUERIES_BATCHED) {
+    CK(launch_multi_init(qkey_, n_, qnb_, d_sources_, nmask_[0], q0_, wtag_, seq_, ctl_, st_));
+    CK(launch_multi(multi_launch(PH_CLOSE, 0, timeout), st_));
+    launches_ += 3;
+    CK(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
+    sync_check("init queries");
+    if (h_ctl_->err) {
+      failed = true;
+      throw Error(h_ctl_->err == ERR_WAVES || h_ctl_->err == ERR_BARRIER ? DYCG_ELIMIT : DYCG_ECAPACITY,
+                  "batched static solve failed on the device (error code " +
+                      std::to_string(h_ctl_->err) + ")");
+    }
+    return;
+  }
+  CK(cudaMemsetAsync(qctl_, 0, (u64)nq_ * sizeof(Ctl), st_));
+  const Adj A_out = adj(out_);
+  const Adj A_in = has_in_ ? adj(in_) : A_out;
+  for (uint32_t q = 0; q < nq_; q++) {
+    u64 *key = qkey_ + (u64)q * n_;
+    CK(launch_init_state(opt_.algo, key, n_, sources_[q], q0_, qctl_ + q, st_));
+    RepairLaunch L = query_launch(A_out, A_in, key, sources_[q]);
+    L.mark = mark_;
+    L.wtag = wtag_;
+    L.aff = aff_;
+    L.q0 = q0_;
+    L.q1 = q1_;
+    L.tiles = tiles_;
+    L.tile_cap = tile_cap_;
+    L.ctl = qctl_ + q;
+    L.n = n_;
+    L.epoch = ++epoch_;
+    L.phases = PH_CLOSE;
+    L.max_waves = (uint32_t)std::min<u64>(4ull * n_ + 1024, 0x7FFFFFFFull);
+    L.delta = opt_.ordered_delta;
+    L.q2 = q2_;
+    L.tag_dev = seq_ + 1;
+    L.timeout_ns = timeout;
+    L.algo = opt_.algo;
+    L.stored = stored_;
+    L.num_sms = num_sms_;
+    CK(launch_repair(L, st_));
+    launches_ += 2;
+  }
+  CK(cudaMemcpyAsync(h_qctl_, qctl_, (u64)nq_ * sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
+  sync_check("init queries");
+  for (uint32_t q = 0; q < nq_; q++)
+    if (h_qctl_[q].err) {
+      failed = true;
+      throw Error(h_qctl_[q].err == ERR_WAVES || h_qctl_[q].err == ERR_BARRIER ? DYCG_ELIMIT
+                                                                               : DYCG_ECAPACITY,
+                  "static solve of query " + std::to_string(q) + " failed (error code " +
+                      std::to_string(h_qctl_[q].err) + ")");
+    }
+}
+
+// Repair of every query after the snapshot's mutation (asynchronous).
+void Engine::repair_queries(uint32_t nd, uint32_t na, u64 timeout) {
+  const uint32_t phases = (nd ? PH_DELETE : 0) | (na ? PH_INSERT : 0) | PH_CLOSE;
+  if (qmode_ == DYCG_QUERIES_BATCHED) {
+    CK(launch_multi(multi_launch(phases, na, timeout), st_));
+    launches_++;
+    return;
+  }
+  CK(cudaMemsetAsync(qctl_, 0, (u64)nq_ * sizeof(Ctl), st_));
+  launches_++;
+  const Adj A_out = adj(out_);
+  const Adj A_in = has_in_ ? adj(in_) : A_out;
+  for (uint32_t q = 0; q < nq_; q++) {
+    RepairLaunch L = query_launch(A_out, A_in, qkey_ + (u64)q * n_, sources_[q]);
+    L.mark = mark_;
+    L.wtag = wtag_;
+    L.aff = aff_;
+    L.q0 = q0_;
+    L.q1 = q1_;
+    L.tiles = tiles_;
+    L.tile_cap = tile_cap_;
+    L.ctl = qctl_ + q;
+    L.del_uv = uv_out_;
+    L.del_found = found_out_;
+    L.n_del_ptr = counts_;
+    L.add_uvw = add_uvw_;
+    L.n_add = na;
+    L.n = n_;
+    L.epoch = ++epoch_;
+    L.phases = phases;
+    L.max_waves = (uint32_t)std::min<u64>(4ull * n_ + 1024, 0x7FFFFFFFull);
+    L.delta = opt_.ordered_delta;
+    L.q2 = q2_;
+    L.tag_dev = seq_ + 1;
+    L.timeout_ns = timeout;
+    L.algo = opt_.algo;
+    L.stored = stored_;
+    L.num_sms = num_sms_;
+    CK(launch_repair(L, st_));
+    launches_++;
+  }
+}
+
+void Engine::gather_query(uint32_t q, uint32_t *values, uint32_t *parents) {
+  check_loaded();
+  if (!nq_) throw Error(DYCG_ESTATE, "no queries set");
+  if (q >= nq_) throw Error(DYCG_EINVAL, "query index out of range");
+  // q0_/q1_ (n+1 entries each) are idle between calls: use them as staging
+  if (qmode_ == DYCG_QUERIES_BATCHED)
+    CK(launch_multi_gather(qkey_, n_, qnb_ * 32, q, q0_, q1_, st_));
+  else
+    CK(launch_multi_gather(qkey_ + (u64)q * n_, n_, 0, 0, q0_, q1_, st_));
+  if (values) CK(cudaMemcpyAsync(values, q0_, (u64)n_ * 4, cudaMemcpyDeviceToHost, st_));
+  if (parents) CK(cudaMemcpyAsync(parents, q1_, (u64)n_ * 4, cudaMemcpyDeviceToHost, st_));
+  sync_check("gather query");
 }
 
 void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
@@ -861,6 +1126,10 @@ void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
 void Engine::gather(uint32_t *values, uint32_t *parents) {
   check_loaded();
   if (opt_.algo == DYCG_ALGO_PR) throw Error(DYCG_EINVAL, "PR results: use dycg_gather_ranks");
+  if (nq_) {
+    gather_query(0, values, parents);
+    return;
+  }
   std::vector<u64> k(n_);
   CK(cudaMemcpyAsync(k.data(), key_, (u64)n_ * 8, cudaMemcpyDeviceToHost, st_));
   sync_check("gather");
@@ -958,7 +1227,8 @@ void Engine::info(dycg_graph_info *out) {
   out->cached_pages = cache_slots_ - free_count_;
   out->host_bytes = out->arena_slots * 4 * out_.stride;
   out->device_bytes = (u64)n_ * (8 + 4 * 6) + (u64)n_ * (has_in_ ? 48 : 24) +
-                      ((u64)cache_slots_ << page_shift_) * 4 * out_.stride + index_bytes_;
+                      ((u64)cache_slots_ << page_shift_) * 4 * out_.stride + index_bytes_ +
+                      qbytes_;
   out->reserved[0] = index_bytes_;  // fence index + deletion bitmap (part of the budget)
   out->page_shift = page_shift_;
   out->has_incoming = has_in_ ? 1 : 0;

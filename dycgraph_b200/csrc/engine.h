@@ -54,6 +54,11 @@ class Engine {
   void export_csr(uint64_t *off, uint32_t *dst, uint32_t *w);
   void info(dycg_graph_info *out);
   void sample_edges(uint64_t count, uint64_t seed, dycg_edge *out);
+  // many-query forms (SSSP/BFS): set after loading, before init
+  void set_queries(const uint32_t *sources, uint32_t count, uint32_t mode);
+  void set_query_mapping(uint32_t edge_lanes, uint32_t heavy, uint32_t tile);
+  void gather_query(uint32_t q, uint32_t *values, uint32_t *parents);
+  uint32_t queries() const { return nq_; }
   cudaStream_t stream() const { return st_; }
 
   std::string last_error;
@@ -70,6 +75,9 @@ class Engine {
   Adj adj(const Arena &A) const;
   void sync_check(const char *where);
   void fill_stats(dycg_batch_stats *s, float ms[4]);
+  void init_queries(u64 timeout);
+  void repair_queries(uint32_t nd, uint32_t na, u64 timeout);
+  MultiLaunch multi_launch(uint32_t phases, uint32_t n_add, u64 timeout);
   void *dmalloc(size_t bytes);
   void dfree_all();
 
@@ -101,6 +109,20 @@ class Engine {
   uint32_t *queued_ = nullptr;
   uint32_t pr_cur_ = 0, pr_count_ = 0;
   uint32_t epoch_ = 0, tag_base_ = 1, touch_epoch_ = 0;
+
+  // many-query forms: batched (one launch, vertex-major keys) or per query
+  // (one single-source launch per query, query-major keys)
+  uint32_t nq_ = 0, qmode_ = 0, qnb_ = 0;
+  uint32_t *d_sources_ = nullptr;
+  std::vector<uint32_t> sources_;
+  u64 *qkey_ = nullptr;
+  uint32_t *affm_ = nullptr, *inew_[2] = {}, *nmask_[2] = {}, *cmask_ = nullptr;
+  uint32_t *seq_ = nullptr, *h_seq_ = nullptr;  // device {epoch, next wave tag}
+  Ctl *qctl_ = nullptr, *h_qctl_ = nullptr;     // per-query control blocks
+  uint4 *mtiles_ = nullptr;
+  uint32_t mtile_cap_ = 0;
+  uint32_t edge_lanes_ = 4, heavy_ = 1024, tile_ = 4096;
+  u64 qbytes_ = 0;
 
   // batch buffers
   size_t bcap_ = 0;

@@ -209,4 +209,25 @@ __device__ __forceinline__ u64 ld_key(const u64 *p) {
   return *(const volatile u64 *)p;
 }
 
+// Lower key[v] to cand only when the value strictly decreases. With
+// zero-weight edges (CC labels; stored weights may be 0) an equal value must
+// not move the parent: a switch to a smaller-id parent of equal value can
+// close a cycle in the parent forest, and deletion repair follows parents.
+// Returns true when this call lowered the value.
+__device__ __forceinline__ bool strict_lower(u64 *addr, u64 cand) {
+  u64 old = ld_key(addr);
+  while (key_value(cand) < key_value(old)) {
+    const u64 prev = atomicCAS(addr, old, cand);
+    if (prev == old) return true;
+    old = prev;
+  }
+  return false;
+}
+
+// Zero-weight edges possible: strict value decrease only.
+template <uint32_t ALGO, bool STORED>
+struct Strict {
+  static constexpr bool value = ALGO == ALGO_CC || STORED;
+};
+
 }  // namespace dycg

@@ -31,6 +31,7 @@ struct RepairLaunch {
   uint32_t n, source, epoch, tag_base, phases, max_waves;
   uint32_t delta;  // ordered closure bucket width (0: unordered)
   uint32_t *q2;
+  uint32_t *tag_dev;  // optional device wave-tag counter (replaces tag_base)
   u64 timeout_ns;
   uint32_t algo;
   bool stored;
@@ -39,6 +40,41 @@ struct RepairLaunch {
 cudaError_t launch_repair(const RepairLaunch &L, cudaStream_t s);
 cudaError_t launch_init_state(uint32_t algo, u64 *key, uint32_t n, uint32_t source,
                               uint32_t *q0, Ctl *ctl, cudaStream_t s);
+
+// Batched repair of Q = 32*nb queries over one graph (multi.cu).
+constexpr uint32_t MULTI_MAX_BLOCKS = 8;   // up to 256 queries
+constexpr uint32_t MULTI_EDGE_LANES_MAX = 8;
+constexpr uint32_t MULTI_MIN_TILE = 1024;  // smallest tile/heavy threshold (sizes the tile queue)
+struct MultiLaunch {
+  Adj out, in;
+  u64 *key;                     // n * Q, vertex-major
+  uint32_t *affm, *inew0, *inew1, *nmask0, *nmask1, *cmask;  // n * nb each
+  uint32_t *mark, *wtag, *aff, *q0, *q1;
+  uint4 *tiles;
+  uint32_t tile_cap;
+  Ctl *ctl;
+  uint32_t *seq;                // device {epoch, next wave tag}, advanced by each launch
+  const uint2 *del_uv;
+  const uint32_t *del_found;
+  const uint32_t *n_del_ptr;
+  const uint3 *add_uvw;
+  uint32_t n_add;
+  uint32_t n, nb, phases, max_waves;
+  uint32_t edge_lanes;          // rows with <= edge_lanes active queries map lanes to edges
+  uint32_t heavy, tile;         // heavy-row threshold and tile size, in slots
+  u64 timeout_ns;
+  uint32_t algo;
+  bool stored;
+  int num_sms;
+};
+cudaError_t launch_multi(const MultiLaunch &L, cudaStream_t s);
+cudaError_t launch_multi_init(u64 *key, uint32_t n, uint32_t nb, const uint32_t *sources,
+                              uint32_t *nmask0, uint32_t *q0, uint32_t *wtag, const uint32_t *seq,
+                              Ctl *ctl, cudaStream_t s);
+// values/parents of query q out of the vertex-major (Q = 32*nb) or
+// query-major (Q = 0: key already offset to the query) key array
+cudaError_t launch_multi_gather(const u64 *key, uint32_t n, uint32_t Q, uint32_t q,
+                                uint32_t *values, uint32_t *parents, cudaStream_t s);
 
 struct PrLaunch {
   Adj out;

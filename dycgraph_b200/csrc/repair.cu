@@ -46,6 +46,8 @@ struct RepairParams {
   uint32_t max_waves;
   uint32_t delta;           // ordered closure: expand values < wave min + delta (0: unordered)
   uint32_t *q2;             // ordered closure: the wave's bucket
+  uint32_t *tag_dev;        // non-null: wave tags start at *tag_dev, which the
+                            // launch advances past the tags it used
   u64 timeout_ns;
 };
 
@@ -53,27 +55,6 @@ template <uint32_t ALGO>
 __device__ __forceinline__ u64 reset_key(uint32_t v) {
   return ALGO == ALGO_CC ? pack_key(v, 0) : KEY_INF;
 }
-
-// Lower key[v] to cand only when the value strictly decreases. With
-// zero-weight edges (CC labels; stored weights may be 0) an equal value must
-// not move the parent: a switch to a smaller-id parent of equal value can
-// close a cycle in the parent forest, and deletion repair follows parents.
-// Returns true when this call lowered the value.
-__device__ __forceinline__ bool strict_lower(u64 *addr, u64 cand) {
-  u64 old = ld_key(addr);
-  while (key_value(cand) < key_value(old)) {
-    const u64 prev = atomicCAS(addr, old, cand);
-    if (prev == old) return true;
-    old = prev;
-  }
-  return false;
-}
-
-// Zero-weight edges possible: strict value decrease only.
-template <uint32_t ALGO, bool STORED>
-struct Strict {
-  static constexpr bool value = ALGO == ALGO_CC || STORED;
-};
 
 // Children of an affected vertex become affected.
 template <uint32_t ALGO>
@@ -167,6 +148,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t gstride = gridDim.x * blockDim.x;
   const uint32_t lane = lane_id();
+  const uint32_t tag_base = P.tag_dev ? *(volatile uint32_t *)P.tag_dev : P.tag_base;
 
   if (P.phases & PH_DELETE) {
     // 1. deletion seeds (warp-uniform loop so appends can aggregate)
@@ -218,7 +200,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
         if (i < na) {
           v = P.aff[i];
           if (key_value(ld_key(P.key + v)) != INF32)
-            want = atomicExch(P.wtag + v, P.tag_base) != P.tag_base;
+            want = atomicExch(P.wtag + v, tag_base) != tag_base;
         }
         warp_append(P.q[0], &ctl->q_count[0], P.n, want, v, &ctl->err);
       }
@@ -244,7 +226,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
             } else if (cand < ld_key(P.key + v)) {
               lowered = key_value(atomicMin(P.key + v, cand)) > (uint32_t)c;
             }
-            if (lowered) want = atomicExch(P.wtag + v, P.tag_base) != P.tag_base;
+            if (lowered) want = atomicExch(P.wtag + v, tag_base) != tag_base;
           }
         }
       }
@@ -267,7 +249,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
         if (gtid == 0) atomicCAS(&ctl->err, 0u, ERR_WAVES);
         break;
       }
-      const uint32_t tag = P.tag_base + 1 + wave;
+      const uint32_t tag = tag_base + 1 + wave;
       uint32_t m = INF32;
       for (uint32_t i = gtid; i < cnt; i += gstride)
         m = min(m, key_value(ld_key(P.key + P.q[cur][i])));
@@ -309,7 +291,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
         if (gtid == 0) atomicCAS(&ctl->err, 0u, ERR_WAVES);
         break;
       }
-      RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], P.tag_base + 1 + wave};
+      RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag_base + 1 + wave};
       if (!expand_rows<STORED>(P.out, P.q[cur], cnt, op, acc, P.tiles, ctl,
                                cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.timeout_ns))
         goto done;
@@ -319,7 +301,11 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
   }
 done:
   acc.flush(ctl);
-  if (gtid == 0) atomicAdd(&ctl->stat[ST_AFFECTED], (u64)ctl->snap_aff);
+  if (gtid == 0) {
+    atomicAdd(&ctl->stat[ST_AFFECTED], (u64)ctl->snap_aff);
+    // every block read *tag_dev before the first barrier
+    if (P.tag_dev) *P.tag_dev = tag_base + ctl->waves + 2;
+  }
 }
 
 // Static solve set-up: every key reset, the initial frontier in q[0].
@@ -371,6 +357,7 @@ static cudaError_t launch_one(const RepairLaunch &L, cudaStream_t s) {
   P.max_waves = L.max_waves;
   P.delta = L.delta;
   P.q2 = L.q2;
+  P.tag_dev = L.tag_dev;
   P.timeout_ns = L.timeout_ns;
   static int blocks_per_sm = -1;
   if (blocks_per_sm < 0) {

@@ -291,6 +291,31 @@ int dycg_group_updates_noalloc(const dycg_edge *d_records, size_t n, uint32_t nu
                                uint32_t *d_out_uv, uint32_t *d_out_mult,
                                uint32_t *d_segment_counts, uint32_t *d_counts, void *stream);
 
+/* ---- many-query forms (SSSP/BFS) ---------------------------------------
+ * The reference engine holds one source per engine (Engine::InitGraph(src),
+ * include/framework/framework.cuh:1803); these calls let one engine keep the
+ * results of up to DYCG_MAX_QUERIES sources over one graph, repaired together
+ * after every snapshot by dycg_apply_batch / dycg_delete_edges /
+ * dycg_insert_edges. No reference counterpart.
+ *  BATCHED: one repair launch per snapshot for all queries; results stored
+ *           vertex-major, so a row read serves every query active on it.
+ *  PER_QUERY: the single-source repair launched once per query (the plain
+ *           per-query path, kept for comparison); results query-major.
+ * Call after loading and before dycg_init. sources: count ids < n. */
+#define DYCG_MAX_QUERIES 256u
+#define DYCG_QUERIES_BATCHED 0u
+#define DYCG_QUERIES_PER_QUERY 1u
+int dycg_set_queries(dycg_engine *e, const uint32_t *sources, uint32_t count, uint32_t mode);
+
+/* Batched form's warp mapping: rows active in <= edge_lanes queries (0..8)
+ * map lanes to edges, others map lanes to queries; rows longer than heavy
+ * slots are split into tile-slot tiles for whole CTAs (both >= 1024). */
+int dycg_set_query_mapping(dycg_engine *e, uint32_t edge_lanes, uint32_t heavy, uint32_t tile);
+
+/* Results of query q (values/parents as dycg_gather; n entries each, either
+ * may be NULL). With queries set, dycg_gather returns query 0. */
+int dycg_gather_query(dycg_engine *e, uint32_t q, uint32_t *values, uint32_t *parents);
+
 /* cudaStream_t the engine launches on (for CUDA-event timing by callers). */
 int dycg_stream(dycg_engine *e, void **stream);
 

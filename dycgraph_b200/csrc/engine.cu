@@ -839,7 +839,11 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     // repair kernels' vertex-state bytes (algorithmic): per expanded row its
     // 16-byte descriptor and 8-byte key, per scanned slot the neighbour's
     // 8-byte key, per improvement 8 B key atomic + 4 B tag + 4 B queue slot
-    stats->state_bytes = stats->expanded * 24 + stats->edges_scanned * 8 + stats->improvements * 16;
+    if (nq_ && qmode_ == DYCG_QUERIES_BATCHED)
+      // batched: the kernel counts 8 B per (edge, active query) key access
+      stats->state_bytes = c.stat[ST_STATE_BYTES] + stats->expanded * 16 + stats->improvements * 16;
+    else
+      stats->state_bytes = stats->expanded * 24 + stats->edges_scanned * 8 + stats->improvements * 16;
   }
 }
 

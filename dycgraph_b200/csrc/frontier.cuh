@@ -76,10 +76,12 @@ struct Acc {
   u64 scanned;
   u64 expanded;
   u64 improved;
+  u64 state;  // vertex-state bytes counted by the kernel itself (batched form)
   __device__ void flush(Ctl *c) {
     u64 a = warp_sum(link), b = warp_sum(hbm), s = warp_sum(scanned), e = warp_sum(expanded),
-        i = warp_sum(improved);
+        i = warp_sum(improved), k = warp_sum(state);
     if (lane_id() == 0) {
+      if (k) atomicAdd(&c->stat[ST_STATE_BYTES], k);
       if (a) atomicAdd(&c->stat[ST_LINK_BYTES], a);
       if (b) atomicAdd(&c->stat[ST_HBM_ADJ_BYTES], b);
       if (s) atomicAdd(&c->stat[ST_SCANNED], s);

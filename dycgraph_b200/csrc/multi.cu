@@ -274,18 +274,23 @@ struct InvalidatePh {
     }
   }
   __device__ void beginQ(uint32_t, int, uint32_t, u64 &) {}
-  __device__ void visitQ(uint32_t x, uint32_t y, uint32_t, int k, uint32_t mk, u64 &, Acc &) {
+  __device__ void visitQ(uint32_t x, uint32_t y, uint32_t, int k, uint32_t mk, u64 &, Acc &acc) {
     const uint32_t lane = lane_id();
     bool child = false;
-    if ((mk >> lane) & 1u)
+    if ((mk >> lane) & 1u) {
       child = key_parent1(ld_key(P->key + ((u64)y * NB + k) * 32 + lane)) == x + 1u;
+      acc.state += 8;
+    }
     const unsigned bits = __ballot_sync(0xffffffffu, child);
     if (bits && lane == 0) mark(y, k, bits);
   }
   __device__ void endQ(uint32_t, int, uint32_t, u64 &) {}
   __device__ void beginE(uint32_t, uint32_t, u64 &) {}
-  __device__ void visitE(uint32_t x, uint32_t y, uint32_t, bool valid, uint32_t q, u64 &, Acc &) {
-    if (valid && key_parent1(ld_key(P->key + (u64)y * NB * 32 + q)) == x + 1u)
+  __device__ void visitE(uint32_t x, uint32_t y, uint32_t, bool valid, uint32_t q, u64 &,
+                         Acc &acc) {
+    if (!valid) return;
+    acc.state += 8;
+    if (key_parent1(ld_key(P->key + (u64)y * NB * 32 + q)) == x + 1u)
       mark(y, q >> 5, 1u << (q & 31));
   }
   __device__ void endE(uint32_t, uint32_t, u64 &) {}
@@ -297,9 +302,11 @@ struct PullPh {
   const MultiParams *P;
   static constexpr bool STRICT = Strict<ALGO, STORED>::value;
   __device__ void beginQ(uint32_t, int, uint32_t, u64 &best) { best = KEY_INF; }
-  __device__ void visitQ(uint32_t v, uint32_t x, uint32_t w, int k, uint32_t mk, u64 &best, Acc &) {
+  __device__ void visitQ(uint32_t v, uint32_t x, uint32_t w, int k, uint32_t mk, u64 &best,
+                         Acc &acc) {
     const uint32_t lane = lane_id();
     if (!((mk >> lane) & 1u)) return;
+    acc.state += 8;
     const uint32_t vx = key_value(ld_key(P->key + ((u64)x * NB + k) * 32 + lane));
     if (vx == INF32) return;
     const u64 c = (u64)vx + mweight<ALGO, STORED>(x, v, w);
@@ -314,8 +321,9 @@ struct PullPh {
   }
   __device__ void beginE(uint32_t, uint32_t, u64 &best) { best = KEY_INF; }
   __device__ void visitE(uint32_t v, uint32_t x, uint32_t w, bool valid, uint32_t q, u64 &best,
-                         Acc &) {
+                         Acc &acc) {
     if (!valid) return;
+    acc.state += 8;
     const uint32_t vx = key_value(ld_key(P->key + (u64)x * NB * 32 + q));
     if (vx == INF32) return;
     const u64 c = (u64)vx + mweight<ALGO, STORED>(x, v, w);
@@ -345,6 +353,7 @@ struct RelaxPh {
     const uint32_t lane = lane_id();
     bool low = false;
     if (dx != INF32) {
+      acc.state += 8;
       const u64 c = dx + mweight<ALGO, STORED>(x, y, w);
       if (c < INF32)
         low = lower_key<STRICT>(P->key + ((u64)y * NB + k) * 32 + lane,
@@ -364,6 +373,7 @@ struct RelaxPh {
   __device__ void visitE(uint32_t x, uint32_t y, uint32_t w, bool valid, uint32_t q, u64 &dx,
                          Acc &acc) {
     if (!valid || dx == INF32) return;
+    acc.state += 8;
     const u64 c = dx + mweight<ALGO, STORED>(x, y, w);
     if (c >= INF32) return;
     if (lower_key<STRICT>(P->key + (u64)y * NB * 32 + q, pack_key((uint32_t)c, x + 1u))) {
@@ -398,7 +408,7 @@ __device__ __forceinline__ bool take_masks(uint32_t *src, uint32_t v, bool consu
 template <uint32_t ALGO, bool STORED, int NB>
 __global__ void __launch_bounds__(BLOCK) multi_repair_kernel(MultiParams P) {
   Ctl *ctl = P.ctl;
-  Acc acc = {0, 0, 0, 0, 0};
+  Acc acc = {0, 0, 0, 0, 0, 0};
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t lane = lane_id();
   const uint32_t gw = gtid >> 5, nw = (gridDim.x * blockDim.x) >> 5;

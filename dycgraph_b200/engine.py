@@ -121,6 +121,9 @@ def lib():
                                        ctypes.POINTER(ctypes.c_double)]),
         "dycg_group_updates": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
         "dycg_group_updates_noalloc": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
+        "dycg_set_queries": (I, [P, u32p, u32, u32]),
+        "dycg_set_query_mapping": (I, [P, u32, u32, u32]),
+        "dycg_gather_query": (I, [P, u32, u32p, u32p]),
         "dycg_last_error": (I, [P, ctypes.c_char_p, sz]),
         "dycg_version": (ctypes.c_char_p, []),
     }
@@ -336,6 +339,29 @@ class Engine:
 
     def GatherParent(self):
         return self.gather()[1]
+
+    # -- many-query forms --------------------------------------------------------
+    QUERY_MODES = {"batched": 0, "per_query": 1}
+
+    def set_queries(self, sources, mode="batched"):
+        """Keep the results of every source in `sources` (SSSP/BFS, up to 256):
+        "batched" repairs all of them in one launch per snapshot, "per_query"
+        launches the single-source repair once per query. Call before start()."""
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        self._check(lib().dycg_set_queries(self._h, _ptr(src, ctypes.c_uint32), len(src),
+                                           self.QUERY_MODES[mode]), "set_queries")
+        self.queries = len(src)
+
+    def set_query_mapping(self, edge_lanes=4, heavy=1024, tile=4096):
+        self._check(lib().dycg_set_query_mapping(self._h, edge_lanes, heavy, tile),
+                    "set_query_mapping")
+
+    def gather_query(self, q):
+        v = np.empty(self.n, np.uint32)
+        p = np.empty(self.n, np.uint32)
+        self._check(lib().dycg_gather_query(self._h, q, _ptr(v, ctypes.c_uint32),
+                                            _ptr(p, ctypes.c_uint32)), "gather_query")
+        return v, p
 
     def gather_ranks(self):
         x = np.empty(self.n, np.float32)

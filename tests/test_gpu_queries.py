@@ -1,0 +1,158 @@
+"""GPU parity of the many-query forms (dycg_set_queries): after the static
+solve and after every snapshot, each query's distances / levels must equal a
+from-scratch static recompute (Dijkstra / FIFO BFS from that query's source)
+on the oracle's copy of the graph, bit for bit, and every parent must be a
+live, tight in-edge. The batched form and the per-query form must agree."""
+import numpy as np
+import pytest
+
+import dycgraph_b200 as dg
+import oracle
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+INF = 0xFFFFFFFF
+ALGO = {"sssp": oracle.SSSP, "bfs": oracle.BFS}
+
+
+def static(algo, n, off, dst, w, stored, src):
+    if algo == "bfs":
+        return oracle.static_bfs(n, off, dst, src)
+    return oracle.static_sssp(n, off, dst, w if stored else None,
+                              oracle.WEIGHT_STORED if stored else oracle.WEIGHT_HASH128, src)
+
+
+def tight_parents(algo, stored, off, dst, w, vals, par, src):
+    """Count reachable non-source vertices whose parent is not a live tight in-edge."""
+    n = len(vals)
+    rows = np.repeat(np.arange(n), np.diff(off).astype(np.int64))
+    weight = {}
+    for u, v, x in zip(rows.tolist(), dst.tolist(), w.tolist()):
+        wt = x if stored else cases.rule_w(ALGO[algo], u, v)
+        weight.setdefault((u, v), set()).add(wt)
+    bad = 0
+    for v in range(n):
+        if vals[v] == INF:
+            bad += par[v] != INF
+            continue
+        if v == src:
+            continue
+        p = int(par[v])
+        ok = p < n and any(int(vals[p]) + x == int(vals[v]) for x in weight.get((p, v), ()))
+        bad += not ok
+    return bad
+
+
+def run_queries(algo, nq, mode, scale=10, batches=3, nd=300, na=300, seed=7, stored=False,
+                budget=0, edge_lanes=4, heavy=1024, tile=4096, split=False, ef=8,
+                parent_every=16):
+    n, off, dst, w = cases.small_rmat(scale, ef, seed)
+    rng = np.random.default_rng(seed)
+    # sources: distinct vertices with out-edges (plus vertex 0)
+    cand = np.nonzero(np.diff(off) > 0)[0]
+    sources = np.unique(np.concatenate([[0], rng.choice(cand, size=min(nq, len(cand)), replace=False)]))[:nq]
+    sources = rng.permutation(sources)
+    e = dg.Engine(algo, weight_mode="stored" if stored else "hash128",
+                  hbm_graph_budget_bytes=budget, page_shift=8)
+    e.load_csr(n, off, dst, w if stored else None)
+    e.set_queries(sources, mode)
+    if mode == "batched":
+        e.set_query_mapping(edge_lanes, heavy, tile)
+    e.start()
+    orc = oracle.Oracle(ALGO[algo], n, off, dst, w if stored else None,
+                        weight_mode=oracle.WEIGHT_STORED if stored else oracle.WEIGHT_HASH128)
+    cur = (off, dst, w)
+
+    def check(tag, parents):
+        o, d, ww = cur
+        for q, s in enumerate(sources):
+            vals, par = e.gather_query(q)
+            ref = static(algo, n, o, d, ww, stored, int(s))
+            assert (vals == ref).all(), (tag, q, int(s), int(np.sum(vals != ref)))
+            if parents and q % parent_every == 0:
+                assert tight_parents(algo, stored, o, d, ww, vals, par, int(s)) == 0, (tag, q)
+
+    check("init", True)
+    for bi in range(batches):
+        dels, adds = cases.random_batch(n, cur[0], cur[1], cur[2], nd, na, seed * 100 + bi)
+        if not stored:
+            dels = [(u, v, cases.rule_w(ALGO[algo], u, v)) for u, v, _ in dels]
+            adds = [(u, v, cases.rule_w(ALGO[algo], u, v)) for u, v, _ in adds]
+        if split:
+            e.delete_edges(dels)
+            orc.mutate(dels, [])
+            cur = orc.csr()
+            check(("delete", bi), False)
+            e.insert_edges(adds)
+            orc.mutate([], adds)
+        else:
+            e.apply_batch(dels, adds)
+            orc.mutate(dels, adds)
+        cur = orc.csr()
+        check(bi, bi == batches - 1)
+    return e, sources
+
+
+@pytest.mark.parametrize("mode", ["batched", "per_query"])
+@pytest.mark.parametrize("algo,stored", [("sssp", False), ("sssp", True), ("bfs", False)])
+def test_queries_match_static(algo, stored, mode):
+    run_queries(algo, 40, mode, stored=stored)
+
+
+@pytest.mark.parametrize("edge_lanes", [0, 1, 8])
+def test_batched_warp_mappings(edge_lanes):
+    # 0: every row on the query-lane mapping; 8: rows active in <= 8 queries on edge lanes
+    run_queries("sssp", 64, "batched", stored=True, edge_lanes=edge_lanes, seed=9)
+
+
+def test_batched_256_queries_split_phases():
+    run_queries("bfs", 256, "batched", scale=9, batches=2, split=True, seed=11, parent_every=64)
+
+
+def test_batched_few_queries_single_block():
+    run_queries("sssp", 3, "batched", batches=3, seed=13)
+
+
+def test_batched_heavy_rows_tiles_cached():
+    # scale 14 R-MAT hubs exceed the 1024-slot heavy threshold: tile phase, HBM cache on
+    n, off, dst, _ = cases.small_rmat(14, 16, 17)
+    assert int(np.max(np.diff(off))) > 2 * 1024
+    for lanes in (0, 8):
+        run_queries("sssp", 32, "batched", scale=14, ef=16, batches=2, nd=1500, na=1500,
+                    seed=17, stored=True, budget=1 << 20, edge_lanes=lanes, heavy=1024,
+                    tile=1024, parent_every=32)
+
+
+def test_batched_equals_per_query():
+    a, src = run_queries("sssp", 24, "batched", batches=2, seed=19, stored=True)
+    b, _ = run_queries("sssp", 24, "per_query", batches=2, seed=19, stored=True)
+    for q in range(len(src)):
+        assert (a.gather_query(q)[0] == b.gather_query(q)[0]).all()
+    # with queries set, dycg_gather returns query 0
+    assert (a.gather()[0] == a.gather_query(0)[0]).all()
+
+
+def test_query_argument_errors():
+    n, off, dst, w = cases.small_rmat(8, 4, 3)
+    e = dg.Engine("sssp")
+    e.load_csr(n, off, dst)
+    for bad in ([], list(range(257))):
+        with pytest.raises(dg.DycgError):
+            e.set_queries(np.array(bad, np.uint32))
+    with pytest.raises(dg.DycgError):
+        e.set_queries([n])
+    with pytest.raises(dg.DycgError):
+        e.set_query_mapping(9, 1024, 1024)
+    with pytest.raises(dg.DycgError):
+        e.set_query_mapping(4, 512, 4096)
+    e.set_queries([0, 1, 2])
+    with pytest.raises(dg.DycgError):
+        e.set_queries([0])
+    e.start()
+    with pytest.raises(dg.DycgError):
+        e.gather_query(3)
+    cc = dg.Engine("cc")
+    cc.load_csr(n, off, dst)
+    with pytest.raises(dg.DycgError):
+        cc.set_queries([0])

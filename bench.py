@@ -63,7 +63,8 @@ def parse():
     ap.add_argument("--plain-queries", type=int, default=None,
                     help="batched config: queries timed on the per-query path (default all)")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--edge-lanes", type=int, default=4)
+    ap.add_argument("--qratio", type=int, default=4)
+    ap.add_argument("--heavy", type=int, default=64)
     ap.add_argument("--tile", type=int, default=4096)
     ap.add_argument("--batch-min", type=int, default=1_000)
     ap.add_argument("--batch-max", type=int, default=1_000_000)
@@ -540,7 +541,10 @@ def run_batched(args):
                     torch.from_numpy(a.astype(np.int32)).cuda()) for d, a in batches[:W + K]]
     torch.cuda.synchronize()
 
+    max_records = int(max(max(len(d), len(a)) for d, a in batches))
+
     def timed(e, use_clocks):
+        e.reserve_batch(max_records)
         stream = torch.cuda.ExternalStream(e.stream())
         st = dg.BatchStats()
         for i in range(W):
@@ -571,7 +575,7 @@ def run_batched(args):
 
     # ---- batched form
     eng.set_queries(sources, "batched")
-    eng.set_query_mapping(args.edge_lanes, 1024, args.tile)
+    eng.set_query_mapping(args.qratio, args.heavy, args.tile)
     t0 = time.time()
     eng.start()
     t_init = time.time() - t0
@@ -662,7 +666,10 @@ def run_batched(args):
                          f"{P} of {Q} queries timed; repair time scaled by {Q}/{P}, "
                          "shared ingest/mutation/cache time counted once"),
                  "static_solve_s": round(p_init * (Q / P), 2),
-                 "gpu_launches": int(sum(p["kernel_launches"] for p in pper))}
+                 "gpu_launches": int(sum(p["kernel_launches"] for p in pper)),
+                 "per_step": {k: round(float(np.mean([p[k] for p in pper])), 4) for k in
+                              ("ms_ingest", "ms_mutate", "ms_repair", "ms_cache", "ms_total",
+                               "edges_scanned", "cache_pages_loaded")}}
 
     out = {
         "metric": METRIC + f", all {Q} queries repaired per snapshot", "value": round(value, 1),
@@ -676,7 +683,7 @@ def run_batched(args):
                    "updates_timed": timed_updates,
                    "snapshot_sizes": [int(x) for x in sizes[W:W + K]],
                    "weights": "uint32 uniform [1,64] stored" if algo == "sssp" else "rule",
-                   "mapping": {"edge_lanes": args.edge_lanes, "heavy": 1024, "tile": args.tile},
+                   "mapping": {"qratio": args.qratio, "heavy": args.heavy, "tile": args.tile},
                    "l2": "inputs larger than L2 (graph in pinned host memory, "
                          f"{info['nodes'] * Q * 8 / 1e9:.0f} GB of query state in HBM)",
                    "parallelism": f"replicas x{world}", "load_s": round(t_load, 2),

@@ -125,6 +125,10 @@ int dycg_cache_maintenance(dycg_engine *e, dycg_batch_stats *stats) {
   return guard(e, [&](Engine &g) { g.cache_maintenance(false, stats); });
 }
 
+int dycg_reserve_batch(dycg_engine *e, size_t max_records) {
+  return guard(e, [&](Engine &g) { g.reserve_batch(max_records); });
+}
+
 int dycg_apply_batch(dycg_engine *e, const dycg_edge *dels, size_t nd, const dycg_edge *adds,
                      size_t na, dycg_batch_stats *stats) {
   return guard(e, [&](Engine &g) { g.apply(dels, nd, adds, na, false, 0, true, stats); });
@@ -190,8 +194,8 @@ int dycg_set_queries(dycg_engine *e, const uint32_t *sources, uint32_t count, ui
   return guard(e, [&](Engine &g) { g.set_queries(sources, count, mode); });
 }
 
-int dycg_set_query_mapping(dycg_engine *e, uint32_t edge_lanes, uint32_t heavy, uint32_t tile) {
-  return guard(e, [&](Engine &g) { g.set_query_mapping(edge_lanes, heavy, tile); });
+int dycg_set_query_mapping(dycg_engine *e, uint32_t qratio, uint32_t heavy, uint32_t tile) {
+  return guard(e, [&](Engine &g) { g.set_query_mapping(qratio, heavy, tile); });
 }
 
 int dycg_gather_query(dycg_engine *e, uint32_t q, uint32_t *values, uint32_t *parents) {

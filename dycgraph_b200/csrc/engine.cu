@@ -541,6 +541,13 @@ void Engine::init() {
   cache_maintenance(true, nullptr);
 }
 
+void Engine::reserve_batch(size_t max_records) {
+  check_loaded();
+  if (max_records > 0x3FFFFFFFull) throw Error(DYCG_EINVAL, "batch too large");
+  ensure_batch(std::max<size_t>(max_records, 1));
+  sync_check("reserve batch");
+}
+
 void Engine::ensure_batch(size_t cnt) {
   if (cnt <= bcap_) return;
   for (void *p : batch_allocs_) cudaFree(p);
@@ -878,9 +885,9 @@ void Engine::set_queries(const uint32_t *sources, uint32_t count, uint32_t mode)
       *m = (uint32_t *)dmalloc(n * nb * 4);
       CK(cudaMemsetAsync(*m, 0, n * nb * 4, st_));
     }
-    // tiles for the smallest tile size the mapping accepts
+    // tiles of one wave: at most one per MULTI_MIN_TILE slots plus one per row
     const u64 maxslots = std::max(out_.slots, in_.slots);
-    mtile_cap_ = (uint32_t)std::min<u64>(2 * (maxslots / MULTI_MIN_TILE) + 4096, 0x7FFFFFFFull);
+    mtile_cap_ = (uint32_t)std::min<u64>(maxslots / MULTI_MIN_TILE + n + 4096, 0x7FFFFFFFull);
     mtiles_ = (uint4 *)dmalloc((u64)mtile_cap_ * sizeof(uint4));
     qnb_ = nb;
     qbytes_ = (u64)Q * 4 + n * Q * 8 + 6 * n * nb * 4 + (u64)mtile_cap_ * sizeof(uint4);
@@ -908,11 +915,10 @@ void Engine::set_queries(const uint32_t *sources, uint32_t count, uint32_t mode)
   sync_check("queries");
 }
 
-void Engine::set_query_mapping(uint32_t edge_lanes, uint32_t heavy, uint32_t tile) {
-  if (edge_lanes > MULTI_EDGE_LANES_MAX) throw Error(DYCG_EINVAL, "edge_lanes must be <= 8");
-  if (heavy < MULTI_MIN_TILE || tile < MULTI_MIN_TILE)
-    throw Error(DYCG_EINVAL, "heavy and tile must be >= 1024 slots");
-  edge_lanes_ = edge_lanes;
+void Engine::set_query_mapping(uint32_t qratio, uint32_t heavy, uint32_t tile) {
+  if (heavy == 0) throw Error(DYCG_EINVAL, "heavy must be >= 1");
+  if (tile < MULTI_MIN_TILE) throw Error(DYCG_EINVAL, "tile must be >= 1024 slots");
+  qratio_ = qratio;
   heavy_ = heavy;
   tile_ = tile;
 }
@@ -946,7 +952,7 @@ MultiLaunch Engine::multi_launch(uint32_t phases, uint32_t n_add, u64 timeout) {
   L.nb = qnb_;
   L.phases = phases;
   L.max_waves = (uint32_t)std::min<u64>(4ull * n_ + 1024, 0x7FFFFFFFull);
-  L.edge_lanes = edge_lanes_;
+  L.qratio = qratio_;
   L.heavy = heavy_;
   L.tile = tile_;
   L.timeout_ns = timeout;

@@ -48,6 +48,7 @@ class Engine {
   void apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na, bool device_ptrs,
              int mode, bool maintenance, dycg_batch_stats *stats);
   void cache_maintenance(bool initial, dycg_batch_stats *stats);
+  void reserve_batch(size_t max_records);
   void gather(uint32_t *values, uint32_t *parents);
   void gather_ranks(float *ranks, float *residuals);
   void get_row(uint32_t v, int incoming, uint32_t *dst, uint32_t *w, uint32_t cap, uint32_t *deg);
@@ -56,7 +57,7 @@ class Engine {
   void sample_edges(uint64_t count, uint64_t seed, dycg_edge *out);
   // many-query forms (SSSP/BFS): set after loading, before init
   void set_queries(const uint32_t *sources, uint32_t count, uint32_t mode);
-  void set_query_mapping(uint32_t edge_lanes, uint32_t heavy, uint32_t tile);
+  void set_query_mapping(uint32_t qratio, uint32_t heavy, uint32_t tile);
   void gather_query(uint32_t q, uint32_t *values, uint32_t *parents);
   uint32_t queries() const { return nq_; }
   cudaStream_t stream() const { return st_; }
@@ -121,7 +122,7 @@ class Engine {
   Ctl *qctl_ = nullptr, *h_qctl_ = nullptr;     // per-query control blocks
   uint4 *mtiles_ = nullptr;
   uint32_t mtile_cap_ = 0;
-  uint32_t edge_lanes_ = 4, heavy_ = 1024, tile_ = 4096;
+  uint32_t qratio_ = 4, heavy_ = 64, tile_ = 4096;
   u64 qbytes_ = 0;
 
   // batch buffers

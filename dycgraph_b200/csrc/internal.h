@@ -43,8 +43,7 @@ cudaError_t launch_init_state(uint32_t algo, u64 *key, uint32_t n, uint32_t sour
 
 // Batched repair of Q = 32*nb queries over one graph (multi.cu).
 constexpr uint32_t MULTI_MAX_BLOCKS = 8;   // up to 256 queries
-constexpr uint32_t MULTI_EDGE_LANES_MAX = 8;
-constexpr uint32_t MULTI_MIN_TILE = 1024;  // smallest tile/heavy threshold (sizes the tile queue)
+constexpr uint32_t MULTI_MIN_TILE = 1024;  // smallest tile (sizes the tile queue)
 struct MultiLaunch {
   Adj out, in;
   u64 *key;                     // n * Q, vertex-major
@@ -60,8 +59,9 @@ struct MultiLaunch {
   const uint3 *add_uvw;
   uint32_t n_add;
   uint32_t n, nb, phases, max_waves;
-  uint32_t edge_lanes;          // rows with <= edge_lanes active queries map lanes to edges
-  uint32_t heavy, tile;         // heavy-row threshold and tile size, in slots
+  uint32_t qratio;              // query lanes when 4*active >= qratio*min(len,32)
+  uint32_t heavy;               // rows with more work (warp iterations) are tiled
+  uint32_t tile;                // tile size, in slots
   u64 timeout_ns;
   uint32_t algo;
   bool stored;

@@ -10,13 +10,20 @@
 // buffer per invalidation-wave parity; nmask: improved, one buffer per
 // closure-wave parity; cmask: the masks of a heavy row, read by its tiles).
 //
-// Two warp mappings, chosen per vertex by the number of active queries
-// (edge_lanes, the tuned threshold):
-//   query lanes -- the warp loads 32 slots, then visits them one by one; for
-//                  each edge lane i works on query 32*b + i of every active
-//                  block b (one coalesced key line per edge and block);
-//   edge lanes  -- lane i works on slot i for each active query in turn (the
-//                  single-query mapping), for vertices active in few queries.
+// Two warp mappings, chosen per row by a cost model (qratio, tuned):
+//   edge lanes  -- lane i takes slot i of each 32-slot chunk and works through
+//                  the row's active queries four at a time (their key loads
+//                  issued together); per-query state (the row's own value, or
+//                  the best pull candidate) sits in the warp's shared memory.
+//                  Every lane does useful work whatever the query count.
+//   query lanes -- the warp visits the row's edges one by one and lane i works
+//                  on query 32*b + i of every active block b (one coalesced
+//                  key line per edge and block, all blocks' loads issued
+//                  together); for rows active in many queries.
+// Rows whose work (slot chunks x active queries, or edges) exceeds `heavy`
+// are cut into tiles processed by whole CTAs after a grid barrier: an
+// edge-lane tile is staged once in shared memory and the CTA's warps split
+// its (chunk, query group) pairs; a query-lane tile's warps split its chunks.
 // Per query the phases are the single-query repair's (repair.cu): deletion
 // seeds (parent == u), invalidation waves over out-rows, reset, pull over
 // in-rows, frontier + insertion seeds, push closure. The batched form has no
@@ -27,8 +34,7 @@
 
 namespace dycg {
 
-constexpr int ST = 8;  // per-vertex state slots: max(blocks, edge-lane queries)
-static_assert(MULTI_MAX_BLOCKS <= ST && MULTI_EDGE_LANES_MAX <= ST, "state slots");
+constexpr uint32_t WARPS = BLOCK / 32;
 
 struct MultiParams {
   Adj out, in;
@@ -49,7 +55,7 @@ struct MultiParams {
   const uint32_t *n_del_ptr;
   const uint3 *add_uvw;
   uint32_t n_add;
-  uint32_t n, phases, max_waves, edge_lanes, heavy, tile;
+  uint32_t n, phases, max_waves, qratio, heavy, tile;
   u64 timeout_ns;
 };
 
@@ -58,13 +64,32 @@ __device__ __forceinline__ uint32_t mweight(uint32_t u, uint32_t v, uint32_t w) 
   return STORED ? w : rule_weight<ALGO>(u, v);
 }
 
-// Lower *addr to cand; true when the value decreased (strict CAS form where
-// zero weights are possible, atomicMin with parent tie-break otherwise).
+// Key reads inside a phase go to L2 (no L1 copy): within a phase values only
+// decrease, so a read that misses a concurrent update only costs an atomic
+// that turns out to be a no-op; across phases the grid barrier orders them.
+__device__ __forceinline__ u64 ldk(const u64 *p) { return __ldcg(p); }
+
+// Lower *addr to cand given a recent read `seen`; true when the value
+// decreased (strict CAS form where zero weights are possible, atomicMin with
+// parent tie-break otherwise).
+template <bool STRICT>
+__device__ __forceinline__ bool lower_from(u64 *addr, u64 cand, u64 seen) {
+  if (cand >= seen) return false;
+  if (STRICT) {
+    u64 old = seen;
+    while (key_value(cand) < key_value(old)) {
+      const u64 prev = atomicCAS(addr, old, cand);
+      if (prev == old) return true;
+      old = prev;
+    }
+    return false;
+  }
+  return key_value(atomicMin(addr, cand)) > key_value(cand);
+}
+
 template <bool STRICT>
 __device__ __forceinline__ bool lower_key(u64 *addr, u64 cand) {
-  if (STRICT) return strict_lower(addr, cand);
-  if (cand < ld_key(addr)) return key_value(atomicMin(addr, cand)) > key_value(cand);
-  return false;
+  return lower_from<STRICT>(addr, cand, ldk(addr));
 }
 
 __device__ __forceinline__ void enqueue_once(const MultiParams &P, uint32_t *q, uint32_t *count,
@@ -145,50 +170,23 @@ __device__ __forceinline__ void walk(const Adj &A, u64 off, uint32_t b, uint32_t
   if (lane == 0 && hit_n) atomicAdd(A.page_hits + hit_pg, hit_n);
 }
 
-// Expand slots [b, e) of v's row for the queries in masks m (warp-uniform).
-// Ph supplies, for the query-lane mapping, beginQ/visitQ/endQ over blocks and,
-// for the edge-lane mapping, beginE/visitE/endE over single queries.
+// Mapping of a row of `len` slots active in `act` queries: query lanes when
+// 4*act >= qratio * min(len, 32) (qratio 0: always query lanes).
+__device__ __forceinline__ bool use_query_lanes(uint32_t act, uint32_t len, uint32_t qratio) {
+  return 4ull * act >= (u64)qratio * min(len, 32u);
+}
+
+// Expand slots [b, e) of v's row, `stride` apart per lane, for the queries
+// in masks m (warp-uniform); s is the warp's shared per-query state (Q
+// entries) for the edge-lane mapping.
 template <int NB, bool WITH_W, class Ph>
-__device__ __forceinline__ void expand_vertex(const MultiParams &P, const Adj &A, uint32_t v,
-                                              const uint32_t (&m)[NB], uint32_t b, uint32_t e,
-                                              uint32_t stride, Ph &ph, Acc &acc) {
-  const uint32_t lane = lane_id();
-  uint32_t tot = 0;
-#pragma unroll
-  for (int k = 0; k < NB; k++) tot += __popc(m[k]);
-  if (tot == 0) return;
-  if (lane == 0 && b == 0) acc.expanded++;
+__device__ __forceinline__ void expand_vertex(const Adj &A, uint32_t v, const uint32_t (&m)[NB],
+                                              uint32_t b, uint32_t e, uint32_t stride, bool qlanes,
+                                              Ph &ph, u64 *s, Acc &acc) {
+  if (lane_id() == 0 && b == 0) acc.expanded++;
   const u64 off = A.off[v];
-  u64 st[ST];
-  if (tot <= P.edge_lanes) {
-    // lane j < tot finds the j-th active query; broadcast into registers
-    uint32_t mine = INF32, seen = 0;
-#pragma unroll
-    for (int k = 0; k < NB; k++) {
-      const uint32_t c = __popc(m[k]);
-      if (mine == INF32 && lane >= seen && lane < seen + c) {
-        uint32_t mm = m[k];
-        for (uint32_t r = lane - seen; r; r--) mm &= mm - 1;
-        mine = k * 32 + __ffs(mm) - 1;
-      }
-      seen += c;
-    }
-    uint32_t qj[MULTI_EDGE_LANES_MAX];
-#pragma unroll
-    for (int j = 0; j < (int)MULTI_EDGE_LANES_MAX; j++) {
-      qj[j] = __shfl_sync(0xffffffffu, mine, j);
-      if (j < (int)tot) ph.beginE(v, qj[j], st[j]);
-    }
-    auto visit = [&](uint32_t y, uint32_t w, bool valid) {
-#pragma unroll
-      for (int j = 0; j < (int)MULTI_EDGE_LANES_MAX; j++)
-        if (j < (int)tot) ph.visitE(v, y, w, valid, qj[j], st[j], acc);
-    };
-    walk<WITH_W>(A, off, b, e, stride, visit, acc);
-#pragma unroll
-    for (int j = 0; j < (int)MULTI_EDGE_LANES_MAX; j++)
-      if (j < (int)tot) ph.endE(v, qj[j], st[j]);
-  } else {
+  if (qlanes) {
+    u64 st[NB];
 #pragma unroll
     for (int k = 0; k < NB; k++) ph.beginQ(v, k, m[k], st[k]);
     auto visit = [&](uint32_t y, uint32_t w, bool valid) {
@@ -196,27 +194,137 @@ __device__ __forceinline__ void expand_vertex(const MultiParams &P, const Adj &A
       while (vb) {
         const int src = __ffs(vb) - 1;
         vb &= vb - 1;
-        const uint32_t yy = __shfl_sync(0xffffffffu, y, src);
-        const uint32_t ww = __shfl_sync(0xffffffffu, w, src);
-#pragma unroll
-        for (int k = 0; k < NB; k++)
-          if (m[k]) ph.visitQ(v, yy, ww, k, m[k], st[k], acc);
+        ph.edgeQ(v, __shfl_sync(0xffffffffu, y, src), __shfl_sync(0xffffffffu, w, src), m, st,
+                 acc);
       }
     };
     walk<WITH_W>(A, off, b, e, stride, visit, acc);
 #pragma unroll
     for (int k = 0; k < NB; k++)
       if (m[k]) ph.endQ(v, k, m[k], st[k]);
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < NB; k++)
+    if (m[k]) ph.beginE(v, k, m[k], s);
+  __syncwarp();
+  auto visit = [&](uint32_t y, uint32_t w, bool valid) {
+    uint32_t qpk = 0, cnt = 0;
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+      uint32_t mm = m[k];
+      while (mm) {
+        const uint32_t bit = __ffs(mm) - 1;
+        mm &= mm - 1;
+        qpk |= (k * 32 + bit) << (8 * cnt);
+        if (++cnt == 4) {
+          ph.edgesE(v, y, w, valid, qpk, 4, s, acc);
+          qpk = 0;
+          cnt = 0;
+        }
+      }
+    }
+    if (cnt) ph.edgesE(v, y, w, valid, qpk, cnt, s, acc);
+  };
+  walk<WITH_W>(A, off, b, e, stride, visit, acc);
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < NB; k++)
+    if (m[k]) ph.endE(v, k, m[k], s);
+  __syncwarp();
+}
+
+// Stage slots [b, e) (e - b <= MULTI_MIN_TILE) of v's row into shared
+// memory, once per CTA: (id | TOMB when deleted, weight).
+template <bool WITH_W>
+__device__ __forceinline__ void stage_slots(const Adj &A, uint32_t v, uint32_t b, uint32_t e,
+                                            uint2 *st, Acc &acc) {
+  const uint32_t lane = lane_id();
+  const u64 off = A.off[v] + b;
+  const uint32_t len = e - b;
+  const uint32_t bytes = WITH_W ? 8u : 4u;
+  for (uint32_t i0 = threadIdx.x - lane; i0 < len; i0 += blockDim.x) {  // warp-uniform
+    const uint32_t i = i0 + lane;
+    const bool in = i < len;
+    uint32_t d = TOMB, w = 0, pg = PAGE_NONE;
+    bool cached = false;
+    if (in) {
+      const u64 p = off + i;
+      pg = page_of(A, p);
+      if (WITH_W) {
+        const uint2 pr = read_pair(A, p, cached);
+        d = pr.x;
+        w = pr.y;
+      } else {
+        d = read_dst(A, p, cached);
+      }
+      if (slot_deleted(A, p, d)) d |= TOMB;
+      const bool valid = !(d & TOMB);
+      if (cached) acc.hbm += valid ? bytes : 4u;
+      else acc.link += valid ? bytes : 4u;
+      acc.scanned++;
+      st[i] = make_uint2(d, w);
+    }
+    const uint32_t pg0 = __shfl_sync(0xffffffffu, pg, 0);
+    const unsigned same = __ballot_sync(0xffffffffu, in && pg == pg0);
+    if (lane == 0 && same) atomicAdd(A.page_hits + pg0, __popc(same));
+    if (in && pg != pg0) atomicAdd(A.page_hits + pg, 1u);
   }
 }
 
-// Expand items[0..cnt): prep(v, m) fills v's masks (false: skip). Rows longer
-// than P.heavy are cut into P.tile-slot tiles that whole CTAs process after a
-// grid barrier; their masks travel through cmask. Ends with a barrier that
-// applies reset_flags. Returns false when the launch has failed.
+// Edge-lane expansion of a staged tile of len slots: the CTA's warps split
+// the (32-slot chunk, group of four active queries) pairs.
+template <int NB, class Ph>
+__device__ __forceinline__ void staged_pairs(uint32_t v, const uint32_t (&m)[NB], uint32_t len,
+                                             const uint2 *st, Ph &ph, u64 *s, Acc &acc) {
+  const uint32_t lane = lane_id();
+  const uint32_t wib = threadIdx.x >> 5;
+  uint32_t act = 0;
+#pragma unroll
+  for (int k = 0; k < NB; k++) act += __popc(m[k]);
+  const uint32_t C = (len + 31) / 32, G = (act + 3) / 4;
+#pragma unroll
+  for (int k = 0; k < NB; k++)
+    if (m[k]) ph.beginE(v, k, m[k], s);
+  __syncwarp();
+  for (uint32_t p = wib; p < C * G; p += WARPS) {
+    const uint32_t c = p % C, lo = (p / C) * 4;
+    uint32_t j = 0, qpk = 0, cnt = 0;
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+      const uint32_t pc = __popc(m[k]);
+      if (j < lo + 4 && j + pc > lo) {
+        uint32_t mm = m[k];
+        while (mm) {
+          const uint32_t bit = __ffs(mm) - 1;
+          mm &= mm - 1;
+          if (j >= lo && j < lo + 4) qpk |= (k * 32 + bit) << (8 * cnt++);
+          j++;
+        }
+      } else {
+        j += pc;
+      }
+    }
+    const uint32_t slot = c * 32 + lane;
+    const uint2 sl = slot < len ? st[slot] : make_uint2(TOMB, 0u);
+    ph.edgesE(v, sl.x & VMASK, sl.y, !(sl.x & TOMB), qpk, cnt, s, acc);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < NB; k++)
+    if (m[k]) ph.endE(v, k, m[k], s);
+  __syncwarp();
+}
+
+// Expand items[0..cnt): prep(v, m) fills v's masks (false: skip). Rows whose
+// work exceeds P.heavy are cut into P.tile-slot tiles (x = row, y/z = slot
+// range, w = mapping) that whole CTAs process after a grid barrier; their
+// masks travel through cmask. Ends with a barrier that applies reset_flags.
+// Returns false when the launch has failed.
 template <int NB, bool WITH_W, class Prep, class Ph>
 __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t *items,
-                             uint32_t cnt, Prep &prep, Ph &ph, Acc &acc, uint32_t reset_flags) {
+                             uint32_t cnt, Prep &prep, Ph &ph, u64 *s, uint2 *stage, Acc &acc,
+                             uint32_t reset_flags) {
   Ctl *ctl = P.ctl;
   const uint32_t lane = lane_id();
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -226,23 +334,31 @@ __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t 
     uint32_t m[NB];
     if (!prep(v, m)) continue;
     const uint32_t len = A.len[v];
-    if (len > P.heavy) {
+    if (len == 0) continue;
+    uint32_t act = 0;
+#pragma unroll
+    for (int k = 0; k < NB; k++) act += __popc(m[k]);
+    const bool ql = use_query_lanes(act, len, P.qratio);
+    const u64 work = ql ? len : (u64)((len + 31) / 32) * act;
+    if (work > P.heavy) {
 #pragma unroll
       for (int k = 0; k < NB; k++)
         if (lane == (uint32_t)k) P.cmask[(u64)v * NB + k] = m[k];
       if (lane == 0) {
-        const uint32_t nt = (len + P.tile - 1) / P.tile;
+        // query-lane tiles: P.tile slots; edge-lane tiles: one staging buffer
+        const uint32_t ts = ql ? P.tile : MULTI_MIN_TILE;
+        const uint32_t nt = (len + ts - 1) / ts;
         const uint32_t base = atomicAdd(&ctl->tile_count, nt);
         if (base + nt > P.tiles.cap) {
           atomicCAS(&ctl->err, 0u, ERR_TILES);
         } else {
           for (uint32_t t = 0; t < nt; t++)
-            P.tiles.tiles[base + t] = make_uint4(v, t * P.tile, min(len, (t + 1) * P.tile), 0);
+            P.tiles.tiles[base + t] = make_uint4(v, t * ts, min(len, (t + 1) * ts), ql ? 1u : 0u);
         }
       }
       continue;
     }
-    expand_vertex<NB, WITH_W>(P, A, v, m, 0, len, 32, ph, acc);
+    expand_vertex<NB, WITH_W>(A, v, m, 0, len, 32, ql, ph, s, acc);
   }
   if (!grid_sync(ctl, reset_flags, P.timeout_ns)) return false;
   const uint32_t nt = min(*(volatile uint32_t *)&ctl->snap_tiles, P.tiles.cap);
@@ -253,7 +369,15 @@ __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t 
     uint32_t m[NB];
 #pragma unroll
     for (int k = 0; k < NB; k++) m[k] = P.cmask[(u64)tl.x * NB + k];
-    expand_vertex<NB, WITH_W>(P, A, tl.x, m, tl.y + wib * 32, tl.z, blockDim.x, ph, acc);
+    if (tl.w) {  // query lanes: the CTA's warps split the slot chunks
+      expand_vertex<NB, WITH_W>(A, tl.x, m, tl.y + wib * 32, tl.z, blockDim.x, true, ph, s, acc);
+    } else {     // edge lanes: slots staged once, warps split (chunk, query group) pairs
+      __syncthreads();
+      stage_slots<WITH_W>(A, tl.x, tl.y, tl.z, stage, acc);
+      __syncthreads();
+      if (threadIdx.x == 0 && tl.y == 0) acc.expanded++;
+      staged_pairs<NB>(tl.x, m, tl.z - tl.y, stage, ph, s, acc);
+    }
   }
   return grid_sync(ctl, SYNC_RESET_TILES, P.timeout_ns);
 }
@@ -274,26 +398,46 @@ struct InvalidatePh {
     }
   }
   __device__ void beginQ(uint32_t, int, uint32_t, u64 &) {}
-  __device__ void visitQ(uint32_t x, uint32_t y, uint32_t, int k, uint32_t mk, u64 &, Acc &acc) {
+  __device__ void edgeQ(uint32_t x, uint32_t y, uint32_t, const uint32_t (&m)[NB],
+                        u64 (&)[NB], Acc &acc) {
     const uint32_t lane = lane_id();
-    bool child = false;
-    if ((mk >> lane) & 1u) {
-      child = key_parent1(ld_key(P->key + ((u64)y * NB + k) * 32 + lane)) == x + 1u;
-      acc.state += 8;
+    u64 cur[NB];
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+      cur[k] = 0;
+      if ((m[k] >> lane) & 1u) {
+        cur[k] = ldk(P->key + ((u64)y * NB + k) * 32 + lane);
+        acc.state += 8;
+      }
     }
-    const unsigned bits = __ballot_sync(0xffffffffu, child);
-    if (bits && lane == 0) mark(y, k, bits);
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+      if (!m[k]) continue;
+      const bool child = ((m[k] >> lane) & 1u) && key_parent1(cur[k]) == x + 1u;
+      const unsigned bits = __ballot_sync(0xffffffffu, child);
+      if (bits && lane == 0) mark(y, k, bits);
+    }
   }
   __device__ void endQ(uint32_t, int, uint32_t, u64 &) {}
-  __device__ void beginE(uint32_t, uint32_t, u64 &) {}
-  __device__ void visitE(uint32_t x, uint32_t y, uint32_t, bool valid, uint32_t q, u64 &,
-                         Acc &acc) {
-    if (!valid) return;
-    acc.state += 8;
-    if (key_parent1(ld_key(P->key + (u64)y * NB * 32 + q)) == x + 1u)
-      mark(y, q >> 5, 1u << (q & 31));
+  __device__ void beginE(uint32_t, int, uint32_t, u64 *) {}
+  __device__ void edgesE(uint32_t x, uint32_t y, uint32_t, bool valid, uint32_t qpk,
+                         uint32_t cnt, u64 *, Acc &acc) {
+    u64 cur[4];
+#pragma unroll
+    for (uint32_t u = 0; u < 4; u++) {
+      cur[u] = 0;
+      if (u < cnt && valid) {
+        cur[u] = ldk(P->key + (u64)y * NB * 32 + ((qpk >> (8 * u)) & 255));
+        acc.state += 8;
+      }
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < 4; u++) {
+      const uint32_t q = (qpk >> (8 * u)) & 255;
+      if (u < cnt && valid && key_parent1(cur[u]) == x + 1u) mark(y, q >> 5, 1u << (q & 31));
+    }
   }
-  __device__ void endE(uint32_t, uint32_t, u64 &) {}
+  __device__ void endE(uint32_t, int, uint32_t, u64 *) {}
 };
 
 // Affected (v, q) takes the best (value(x) + w, parent x) over live in-edges.
@@ -301,39 +445,68 @@ template <uint32_t ALGO, bool STORED, int NB>
 struct PullPh {
   const MultiParams *P;
   static constexpr bool STRICT = Strict<ALGO, STORED>::value;
-  __device__ void beginQ(uint32_t, int, uint32_t, u64 &best) { best = KEY_INF; }
-  __device__ void visitQ(uint32_t v, uint32_t x, uint32_t w, int k, uint32_t mk, u64 &best,
-                         Acc &acc) {
-    const uint32_t lane = lane_id();
-    if (!((mk >> lane) & 1u)) return;
-    acc.state += 8;
-    const uint32_t vx = key_value(ld_key(P->key + ((u64)x * NB + k) * 32 + lane));
-    if (vx == INF32) return;
+  __device__ u64 cand(uint32_t v, uint32_t x, uint32_t w, u64 kx) const {
+    const uint32_t vx = key_value(kx);
+    if (vx == INF32) return KEY_INF;
     const u64 c = (u64)vx + mweight<ALGO, STORED>(x, v, w);
-    if (c >= INF32) return;
-    const u64 cand = pack_key((uint32_t)c, x + 1u);
-    best = cand < best ? cand : best;
+    return c >= INF32 ? KEY_INF : pack_key((uint32_t)c, x + 1u);
+  }
+  __device__ void beginQ(uint32_t, int, uint32_t, u64 &best) { best = KEY_INF; }
+  __device__ void edgeQ(uint32_t v, uint32_t x, uint32_t w, const uint32_t (&m)[NB],
+                        u64 (&best)[NB], Acc &acc) {
+    const uint32_t lane = lane_id();
+    u64 cur[NB];
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+      cur[k] = KEY_INF;
+      if ((m[k] >> lane) & 1u) {
+        cur[k] = ldk(P->key + ((u64)x * NB + k) * 32 + lane);
+        acc.state += 8;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+      const u64 c = cand(v, x, w, cur[k]);
+      best[k] = c < best[k] ? c : best[k];
+    }
   }
   __device__ void endQ(uint32_t v, int k, uint32_t mk, u64 &best) {
     const uint32_t lane = lane_id();
     if (((mk >> lane) & 1u) && best != KEY_INF)
       lower_key<STRICT>(P->key + ((u64)v * NB + k) * 32 + lane, best);
   }
-  __device__ void beginE(uint32_t, uint32_t, u64 &best) { best = KEY_INF; }
-  __device__ void visitE(uint32_t v, uint32_t x, uint32_t w, bool valid, uint32_t q, u64 &best,
-                         Acc &acc) {
-    if (!valid) return;
-    acc.state += 8;
-    const uint32_t vx = key_value(ld_key(P->key + (u64)x * NB * 32 + q));
-    if (vx == INF32) return;
-    const u64 c = (u64)vx + mweight<ALGO, STORED>(x, v, w);
-    if (c >= INF32) return;
-    const u64 cand = pack_key((uint32_t)c, x + 1u);
-    best = cand < best ? cand : best;
+  __device__ void beginE(uint32_t, int k, uint32_t mk, u64 *s) {
+    const uint32_t lane = lane_id();
+    if ((mk >> lane) & 1u) s[k * 32 + lane] = KEY_INF;
   }
-  __device__ void endE(uint32_t v, uint32_t q, u64 &best) {
-    const u64 mn = warp_min(best);
-    if (lane_id() == 0 && mn != KEY_INF) lower_key<STRICT>(P->key + (u64)v * NB * 32 + q, mn);
+  __device__ void edgesE(uint32_t v, uint32_t x, uint32_t w, bool valid, uint32_t qpk,
+                         uint32_t cnt, u64 *s, Acc &acc) {
+    u64 cur[4];
+#pragma unroll
+    for (uint32_t u = 0; u < 4; u++) {
+      cur[u] = KEY_INF;
+      if (u < cnt && valid) {
+        cur[u] = ldk(P->key + (u64)x * NB * 32 + ((qpk >> (8 * u)) & 255));
+        acc.state += 8;
+      }
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < 4; u++) {
+      if (u >= cnt) break;  // warp-uniform
+      const u64 c = cand(v, x, w, cur[u]);
+      if (__any_sync(0xffffffffu, c != KEY_INF)) {
+        const u64 mn = warp_min(c);
+        const uint32_t q = (qpk >> (8 * u)) & 255;
+        if (lane_id() == 0 && mn < s[q]) s[q] = mn;
+      }
+    }
+  }
+  __device__ void endE(uint32_t v, int k, uint32_t mk, u64 *s) {
+    const uint32_t lane = lane_id();
+    if ((mk >> lane) & 1u) {
+      const u64 best = s[k * 32 + lane];
+      if (best != KEY_INF) lower_key<STRICT>(P->key + ((u64)v * NB + k) * 32 + lane, best);
+    }
   }
 };
 
@@ -347,42 +520,75 @@ struct RelaxPh {
   __device__ void beginQ(uint32_t x, int k, uint32_t mk, u64 &dx) {
     const uint32_t lane = lane_id();
     dx = INF32;
-    if ((mk >> lane) & 1u) dx = key_value(ld_key(P->key + ((u64)x * NB + k) * 32 + lane));
+    if ((mk >> lane) & 1u) dx = key_value(ldk(P->key + ((u64)x * NB + k) * 32 + lane));
   }
-  __device__ void visitQ(uint32_t x, uint32_t y, uint32_t w, int k, uint32_t, u64 &dx, Acc &acc) {
+  __device__ void edgeQ(uint32_t x, uint32_t y, uint32_t w, const uint32_t (&m)[NB],
+                        u64 (&dx)[NB], Acc &acc) {
     const uint32_t lane = lane_id();
-    bool low = false;
-    if (dx != INF32) {
-      acc.state += 8;
-      const u64 c = dx + mweight<ALGO, STORED>(x, y, w);
-      if (c < INF32)
-        low = lower_key<STRICT>(P->key + ((u64)y * NB + k) * 32 + lane,
-                                pack_key((uint32_t)c, x + 1u));
+    const uint32_t wt = mweight<ALGO, STORED>(x, y, w);
+    u64 cur[NB];
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+      cur[k] = 0;
+      if (dx[k] != INF32 && dx[k] + wt < INF32) {
+        cur[k] = ldk(P->key + ((u64)y * NB + k) * 32 + lane);
+        acc.state += 8;
+      }
     }
-    const unsigned bits = __ballot_sync(0xffffffffu, low);
-    if (bits && lane == 0) {
-      atomicOr(nmask_next + (u64)y * NB + k, bits);
-      enqueue_once(*P, nq, nc, y, tag);
-      acc.improved += __popc(bits);
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+      if (!m[k]) continue;
+      bool low = false;
+      if (dx[k] != INF32 && dx[k] + wt < INF32)
+        low = lower_from<STRICT>(P->key + ((u64)y * NB + k) * 32 + lane,
+                                 pack_key((uint32_t)(dx[k] + wt), x + 1u), cur[k]);
+      const unsigned bits = __ballot_sync(0xffffffffu, low);
+      if (bits && lane == 0) {
+        atomicOr(nmask_next + (u64)y * NB + k, bits);
+        acc.improved += __popc(bits);
+        any = true;
+      }
     }
+    if (lane == 0 && any) enqueue_once(*P, nq, nc, y, tag);
   }
   __device__ void endQ(uint32_t, int, uint32_t, u64 &) {}
-  __device__ void beginE(uint32_t x, uint32_t q, u64 &dx) {
-    dx = key_value(ld_key(P->key + (u64)x * NB * 32 + q));
+  __device__ void beginE(uint32_t x, int k, uint32_t mk, u64 *s) {
+    const uint32_t lane = lane_id();
+    if ((mk >> lane) & 1u)
+      s[k * 32 + lane] = key_value(ldk(P->key + ((u64)x * NB + k) * 32 + lane));
   }
-  __device__ void visitE(uint32_t x, uint32_t y, uint32_t w, bool valid, uint32_t q, u64 &dx,
-                         Acc &acc) {
-    if (!valid || dx == INF32) return;
-    acc.state += 8;
-    const u64 c = dx + mweight<ALGO, STORED>(x, y, w);
-    if (c >= INF32) return;
-    if (lower_key<STRICT>(P->key + (u64)y * NB * 32 + q, pack_key((uint32_t)c, x + 1u))) {
-      atomicOr(nmask_next + (u64)y * NB + (q >> 5), 1u << (q & 31));
-      enqueue_once(*P, nq, nc, y, tag);
-      acc.improved++;
+  __device__ void edgesE(uint32_t x, uint32_t y, uint32_t w, bool valid, uint32_t qpk,
+                         uint32_t cnt, u64 *s, Acc &acc) {
+    const uint32_t wt = mweight<ALGO, STORED>(x, y, w);
+    u64 cur[4], c[4];
+#pragma unroll
+    for (uint32_t u = 0; u < 4; u++) {
+      cur[u] = 0;
+      c[u] = INF32;
+      if (u < cnt && valid) {
+        const uint32_t q = (qpk >> (8 * u)) & 255;
+        const uint32_t dx = (uint32_t)s[q];
+        if (dx != INF32 && (u64)dx + wt < INF32) {
+          c[u] = (u64)dx + wt;
+          cur[u] = ldk(P->key + (u64)y * NB * 32 + q);
+          acc.state += 8;
+        }
+      }
+    }
+#pragma unroll
+    for (uint32_t u = 0; u < 4; u++) {
+      if (c[u] == INF32) continue;
+      const uint32_t q = (qpk >> (8 * u)) & 255;
+      if (lower_from<STRICT>(P->key + (u64)y * NB * 32 + q, pack_key((uint32_t)c[u], x + 1u),
+                             cur[u])) {
+        atomicOr(nmask_next + (u64)y * NB + (q >> 5), 1u << (q & 31));
+        enqueue_once(*P, nq, nc, y, tag);
+        acc.improved++;
+      }
     }
   }
-  __device__ void endE(uint32_t, uint32_t, u64 &) {}
+  __device__ void endE(uint32_t, int, uint32_t, u64 *) {}
 };
 
 // Masks of v taken from src[v] (cleared when `consume`; nobody else writes
@@ -406,7 +612,7 @@ __device__ __forceinline__ bool take_masks(uint32_t *src, uint32_t v, bool consu
 }
 
 template <uint32_t ALGO, bool STORED, int NB>
-__global__ void __launch_bounds__(BLOCK) multi_repair_kernel(MultiParams P) {
+__global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(MultiParams P) {
   Ctl *ctl = P.ctl;
   Acc acc = {0, 0, 0, 0, 0, 0};
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -418,6 +624,9 @@ __global__ void __launch_bounds__(BLOCK) multi_repair_kernel(MultiParams P) {
   const uint32_t tag0 = *(volatile uint32_t *)&P.seq[1];
   uint32_t tag = tag0 + 1;  // next unused wave tag (uniform over the grid)
   uint32_t waves = 0;
+  __shared__ u64 s_state[WARPS][Q];  // edge-lane per-query state of each warp
+  __shared__ uint2 s_stage[MULTI_MIN_TILE];  // staged slots of an edge-lane tile
+  u64 *s = s_state[threadIdx.x >> 5];
 
   if (P.phases & PH_DELETE) {
     // 1. seeds: (v, q) with parent_q(v) == u for a deleted (u, v); one warp per record
@@ -458,7 +667,7 @@ __global__ void __launch_bounds__(BLOCK) multi_repair_kernel(MultiParams P) {
         InvalidatePh<NB> ph{&P, P.inew[par ^ 1], P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag++, epoch};
         uint32_t *src = P.inew[par];
         auto prep = [&](uint32_t v, uint32_t (&m)[NB]) { return take_masks<NB>(src, v, true, m); };
-        if (!multi_expand<NB, false>(P, P.out, P.q[cur], cnt, prep, ph, acc,
+        if (!multi_expand<NB, false>(P, P.out, P.q[cur], cnt, prep, ph, s, s_stage, acc,
                                      cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0))
           goto done;
         waves++;
@@ -480,7 +689,7 @@ __global__ void __launch_bounds__(BLOCK) multi_repair_kernel(MultiParams P) {
       // 4. pull over in-rows
       PullPh<ALGO, STORED, NB> ph{&P};
       auto prep = [&](uint32_t v, uint32_t (&m)[NB]) { return take_masks<NB>(P.affm, v, false, m); };
-      if (!multi_expand<NB, STORED>(P, P.in, P.aff, na, prep, ph, acc, 0)) goto done;
+      if (!multi_expand<NB, STORED>(P, P.in, P.aff, na, prep, ph, s, s_stage, acc, 0)) goto done;
     }
   }
   {
@@ -545,7 +754,7 @@ __global__ void __launch_bounds__(BLOCK) multi_repair_kernel(MultiParams P) {
       RelaxPh<ALGO, STORED, NB> ph{&P, P.nmask[par ^ 1], P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag++};
       uint32_t *src = P.nmask[par];
       auto prep = [&](uint32_t v, uint32_t (&m)[NB]) { return take_masks<NB>(src, v, true, m); };
-      if (!multi_expand<NB, STORED>(P, P.out, P.q[cur], cnt, prep, ph, acc,
+      if (!multi_expand<NB, STORED>(P, P.out, P.q[cur], cnt, prep, ph, s, s_stage, acc,
                                     cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0))
         goto done;
       waves++;
@@ -629,8 +838,8 @@ static cudaError_t launch_multi_t(const MultiLaunch &L, cudaStream_t s) {
   P.n = L.n;
   P.phases = L.phases;
   P.max_waves = L.max_waves;
-  P.edge_lanes = std::min(L.edge_lanes, MULTI_EDGE_LANES_MAX);
-  P.heavy = std::max(L.heavy, MULTI_MIN_TILE);
+  P.qratio = L.qratio;
+  P.heavy = std::max(L.heavy, 1u);
   P.tile = std::max(L.tile, MULTI_MIN_TILE);
   P.timeout_ns = L.timeout_ns;
   static int blocks_per_sm = -1;

@@ -106,6 +106,7 @@ def lib():
         "dycg_insert_edges": (I, [P, ep, sz, sp]),
         "dycg_cache_maintenance": (I, [P, sp]),
         "dycg_apply_batch": (I, [P, ep, sz, ep, sz, sp]),
+        "dycg_reserve_batch": (I, [P, sz]),
         "dycg_apply_batch_device": (I, [P, P, sz, P, sz, sp]),
         "dycg_gather": (I, [P, u32p, u32p]),
         "dycg_gather_ranks": (I, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
@@ -308,6 +309,11 @@ class Engine:
 
     UpdatePageRank = apply_batch
 
+    def reserve_batch(self, max_records):
+        """Size the per-batch buffers for up to max_records deletions (and as
+        many insertions) before timing or replay."""
+        self._check(lib().dycg_reserve_batch(self._h, int(max_records)), "reserve_batch")
+
     def apply_batch_device(self, d_dels_ptr, nd, d_adds_ptr, na, stats=None):
         """Records already in device memory (raw device addresses)."""
         st = stats if stats is not None else BatchStats()
@@ -352,8 +358,11 @@ class Engine:
                                            self.QUERY_MODES[mode]), "set_queries")
         self.queries = len(src)
 
-    def set_query_mapping(self, edge_lanes=4, heavy=1024, tile=4096):
-        self._check(lib().dycg_set_query_mapping(self._h, edge_lanes, heavy, tile),
+    def set_query_mapping(self, qratio=4, heavy=64, tile=4096):
+        """Batched form's work mapping (speed only): rows with
+        4*active >= qratio*min(len, 32) map lanes to queries, others lanes to
+        slots; rows above `heavy` warp iterations are tiled (tile slots)."""
+        self._check(lib().dycg_set_query_mapping(self._h, qratio, heavy, tile),
                     "set_query_mapping")
 
     def gather_query(self, q):

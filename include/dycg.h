@@ -214,6 +214,13 @@ int dycg_cache_maintenance(dycg_engine *e, dycg_batch_stats *stats);
 int dycg_apply_batch(dycg_engine *e, const dycg_edge *dels, size_t nd,
                      const dycg_edge *adds, size_t na, dycg_batch_stats *stats);
 
+/* Size the per-batch buffers for snapshots of up to max_records deletions
+ * (and as many insertions) ahead of time, the way the reference sizes its
+ * mapped update arrays from the update file before replay
+ * (include/framework/framework.cuh:2387-2412 get_update_file). Without it the
+ * buffers grow on the first larger batch, inside that call. */
+int dycg_reserve_batch(dycg_engine *e, size_t max_records);
+
 /* Same as dycg_apply_batch with the records already in device memory. */
 int dycg_apply_batch_device(dycg_engine *e, const dycg_edge *d_dels, size_t nd,
                             const dycg_edge *d_adds, size_t na,
@@ -307,10 +314,14 @@ int dycg_group_updates_noalloc(const dycg_edge *d_records, size_t n, uint32_t nu
 #define DYCG_QUERIES_PER_QUERY 1u
 int dycg_set_queries(dycg_engine *e, const uint32_t *sources, uint32_t count, uint32_t mode);
 
-/* Batched form's warp mapping: rows active in <= edge_lanes queries (0..8)
- * map lanes to edges, others map lanes to queries; rows longer than heavy
- * slots are split into tile-slot tiles for whole CTAs (both >= 1024). */
-int dycg_set_query_mapping(dycg_engine *e, uint32_t edge_lanes, uint32_t heavy, uint32_t tile);
+/* Batched form's work mapping. A row of len slots active in act queries is
+ * expanded with lanes over queries (one edge at a time) when
+ * 4*act >= qratio*min(len, 32), else with lanes over slots (the active queries
+ * in turn); qratio 0 always maps lanes to queries. Rows whose work exceeds
+ * `heavy` warp iterations are split into tile-slot pieces processed by whole
+ * CTAs (tile >= 1024). Defaults: qratio 4, heavy 64, tile 4096. The mapping
+ * changes speed only, never results. */
+int dycg_set_query_mapping(dycg_engine *e, uint32_t qratio, uint32_t heavy, uint32_t tile);
 
 /* Results of query q (values/parents as dycg_gather; n entries each, either
  * may be NULL). With queries set, dycg_gather returns query 0. */

@@ -45,7 +45,7 @@ def tight_parents(algo, stored, off, dst, w, vals, par, src):
 
 
 def run_queries(algo, nq, mode, scale=10, batches=3, nd=300, na=300, seed=7, stored=False,
-                budget=0, edge_lanes=4, heavy=1024, tile=4096, split=False, ef=8,
+                budget=0, qratio=4, heavy=64, tile=4096, split=False, ef=8,
                 parent_every=16):
     n, off, dst, w = cases.small_rmat(scale, ef, seed)
     rng = np.random.default_rng(seed)
@@ -58,7 +58,7 @@ def run_queries(algo, nq, mode, scale=10, batches=3, nd=300, na=300, seed=7, sto
     e.load_csr(n, off, dst, w if stored else None)
     e.set_queries(sources, mode)
     if mode == "batched":
-        e.set_query_mapping(edge_lanes, heavy, tile)
+        e.set_query_mapping(qratio, heavy, tile)
     e.start()
     orc = oracle.Oracle(ALGO[algo], n, off, dst, w if stored else None,
                         weight_mode=oracle.WEIGHT_STORED if stored else oracle.WEIGHT_HASH128)
@@ -100,10 +100,11 @@ def test_queries_match_static(algo, stored, mode):
     run_queries(algo, 40, mode, stored=stored)
 
 
-@pytest.mark.parametrize("edge_lanes", [0, 1, 8])
-def test_batched_warp_mappings(edge_lanes):
-    # 0: every row on the query-lane mapping; 8: rows active in <= 8 queries on edge lanes
-    run_queries("sssp", 64, "batched", stored=True, edge_lanes=edge_lanes, seed=9)
+@pytest.mark.parametrize("qratio,heavy", [(0, 64), (1 << 20, 64), (4, 1), (4, 1 << 30)])
+def test_batched_work_mappings(qratio, heavy):
+    # qratio 0: every row on query lanes; 2^20: every row on edge lanes;
+    # heavy 1: every row tiled (CTA splits); 2^30: no row tiled
+    run_queries("sssp", 64, "batched", stored=True, qratio=qratio, heavy=heavy, seed=9)
 
 
 def test_batched_256_queries_split_phases():
@@ -118,9 +119,9 @@ def test_batched_heavy_rows_tiles_cached():
     # scale 14 R-MAT hubs exceed the 1024-slot heavy threshold: tile phase, HBM cache on
     n, off, dst, _ = cases.small_rmat(14, 16, 17)
     assert int(np.max(np.diff(off))) > 2 * 1024
-    for lanes in (0, 8):
+    for qratio in (0, 1 << 20):
         run_queries("sssp", 32, "batched", scale=14, ef=16, batches=2, nd=1500, na=1500,
-                    seed=17, stored=True, budget=1 << 20, edge_lanes=lanes, heavy=1024,
+                    seed=17, stored=True, budget=1 << 20, qratio=qratio, heavy=64,
                     tile=1024, parent_every=32)
 
 
@@ -143,9 +144,9 @@ def test_query_argument_errors():
     with pytest.raises(dg.DycgError):
         e.set_queries([n])
     with pytest.raises(dg.DycgError):
-        e.set_query_mapping(9, 1024, 1024)
+        e.set_query_mapping(4, 0, 4096)
     with pytest.raises(dg.DycgError):
-        e.set_query_mapping(4, 512, 4096)
+        e.set_query_mapping(4, 64, 512)
     e.set_queries([0, 1, 2])
     with pytest.raises(dg.DycgError):
         e.set_queries([0])

@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--qratio", type=int, default=4)
     ap.add_argument("--heavy", type=int, default=64)
     ap.add_argument("--tile", type=int, default=4096)
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--no-replay", action="store_true")
+    ap.add_argument("--tune-batch", type=int, default=100_000)
     ap.add_argument("--batch-min", type=int, default=1_000)
     ap.add_argument("--batch-max", type=int, default=1_000_000)
     args = ap.parse_args()
@@ -522,6 +525,8 @@ def run_batched(args):
     rng = np.random.default_rng(args.seed + 41 + 1000 * rank)
     sizes = np.exp(rng.uniform(np.log(args.batch_min), np.log(args.batch_max), W + K + E))
     sizes = np.maximum(2, sizes.astype(np.int64))
+    # snapshot 0 tunes the mapping (untimed); all deletions are disjoint
+    sizes = np.concatenate([[args.tune_batch], sizes])
 
     def build():
         eng = dg.Engine(algo, weight_mode="stored" if algo == "sssp" else "hash128",
@@ -537,13 +542,22 @@ def run_batched(args):
     _, first = np.unique(smp[:, 0], return_index=True)
     sources = smp[np.sort(first), 0][:Q].astype(np.uint32)
     batches = query_snapshots(eng, args, sizes, args.seed + 17 + 1000 * rank)
+    tune_batch, batches, sizes = batches[0], batches[1:], sizes[1:]
     dev_batches = [(torch.from_numpy(d.astype(np.int32)).cuda(),
                     torch.from_numpy(a.astype(np.int32)).cuda()) for d, a in batches[:W + K]]
     torch.cuda.synchronize()
 
     max_records = int(max(max(len(d), len(a)) for d, a in batches))
+    # the timed snapshots' records, concatenated on the device for one replay call
+    t_nd = [len(d) for d, _ in batches[W:W + K]]
+    t_na = [len(a) for _, a in batches[W:W + K]]
+    t_dels = torch.from_numpy(np.concatenate([d for d, _ in batches[W:W + K]]).astype(np.int32)).cuda()
+    t_adds = torch.from_numpy(np.concatenate([a for _, a in batches[W:W + K]]).astype(np.int32)).cuda()
 
-    def timed(e, use_clocks):
+    def timed(e, use_clocks, replay):
+        """W warm-up snapshots, then K timed ones: with replay, the K
+        snapshots go through one dycg_apply_batches_device call (graph
+        replay); without, one dycg_apply_batch_device call each."""
         e.reserve_batch(max_records)
         stream = torch.cuda.ExternalStream(e.stream())
         st = dg.BatchStats()
@@ -561,10 +575,14 @@ def run_batched(args):
         per = []
         t_begin = time.time()
         ev0.record(stream)
-        for i in range(W, W + K):
-            d, a = dev_batches[i]
-            e.apply_batch_device(d.data_ptr(), d.shape[0], a.data_ptr(), a.shape[0], st)
-            per.append(st.as_dict())
+        if replay:
+            arr = e.apply_batches_device(t_dels.data_ptr(), t_nd, t_adds.data_ptr(), t_na)
+            per = [arr[i].as_dict() for i in range(K)]
+        else:
+            for i in range(W, W + K):
+                d, a = dev_batches[i]
+                e.apply_batch_device(d.data_ptr(), d.shape[0], a.data_ptr(), a.shape[0], st)
+                per.append(st.as_dict())
         ev1.record(stream)
         torch.cuda.synchronize()
         clk = None
@@ -579,7 +597,13 @@ def run_batched(args):
     t0 = time.time()
     eng.start()
     t_init = time.time() - t0
-    ms, per, clk = timed(eng, True)
+    tried = []
+    if not args.no_tune:
+        # autotune the work mapping on one extra snapshot (not timed)
+        tried = eng.tune_query_mapping(*tune_batch)
+    mapping = min(tried, key=lambda t: t["repair_ms"]) if tried else \
+        {"qratio": args.qratio, "heavy": args.heavy, "tile": args.tile}
+    ms, per, clk = timed(eng, True, replay=not args.no_replay)
     timed_updates = int(sum(len(d) + len(a) for d, a in batches[W:W + K]))
     # e2e: host records through dycg_apply_batch, copies inside the timed region
     e2e_ms, e2e_updates = 0.0, 0
@@ -589,8 +613,11 @@ def run_batched(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for d, a in batches[W + K:]:
-            eng.apply_batch(d, a)
+        if args.no_replay:
+            for d, a in batches[W + K:]:
+                eng.apply_batch(d, a)
+        else:
+            eng.apply_batches(batches[W + K:])
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1)
@@ -647,7 +674,9 @@ def run_batched(args):
         t0 = time.time()
         peng.start()
         p_init = time.time() - t0
-        pms, pper, _ = timed(peng, False)
+        if not args.no_tune:
+            peng.apply_batch(*tune_batch)  # same graph as the batched engine
+        pms, pper, _ = timed(peng, False, replay=False)
         peng.close()
         del peng
         p_rep = float(np.sum([p["ms_repair"] for p in pper]))
@@ -683,7 +712,12 @@ def run_batched(args):
                    "updates_timed": timed_updates,
                    "snapshot_sizes": [int(x) for x in sizes[W:W + K]],
                    "weights": "uint32 uniform [1,64] stored" if algo == "sssp" else "rule",
-                   "mapping": {"qratio": args.qratio, "heavy": args.heavy, "tile": args.tile},
+                   "mapping": {k: mapping[k] for k in ("qratio", "heavy", "tile")},
+                   "mapping_tuned_on": (f"one {args.tune_batch}-update snapshot, "
+                                        f"{len(tried)} candidates") if tried else "not tuned",
+                   "replay": "one dycg_apply_batches_device call for the timed snapshots "
+                             "(a CUDA graph per batch-size class)" if not args.no_replay
+                             else "one dycg_apply_batch_device call per snapshot",
                    "l2": "inputs larger than L2 (graph in pinned host memory, "
                          f"{info['nodes'] * Q * 8 / 1e9:.0f} GB of query state in HBM)",
                    "parallelism": f"replicas x{world}", "load_s": round(t_load, 2),
@@ -695,6 +729,7 @@ def run_batched(args):
         "gpu_launches": launches,
         "roofline": roofline,
         "per_step": per_step,
+        "mapping_candidates": [[t["qratio"], t["heavy"], round(t["repair_ms"], 3)] for t in tried],
         "plain_per_query": plain,
         "speedup_vs_plain": round(value / plain["value"], 2) if plain else None,
     }

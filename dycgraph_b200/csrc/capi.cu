@@ -202,6 +202,28 @@ int dycg_gather_query(dycg_engine *e, uint32_t q, uint32_t *values, uint32_t *pa
   return guard(e, [&](Engine &g) { g.gather_query(q, values, parents); });
 }
 
+int dycg_tune_query_mapping(dycg_engine *e, const dycg_edge *dels, size_t nd,
+                            const dycg_edge *adds, size_t na, dycg_query_mapping *tried,
+                            uint32_t cap, uint32_t *n_tried, dycg_batch_stats *stats) {
+  return guard(e, [&](Engine &g) { g.tune(dels, nd, adds, na, tried, cap, n_tried, stats); });
+}
+
+int dycg_apply_batches(dycg_engine *e, const dycg_edge *dels, const uint64_t *del_counts,
+                       const dycg_edge *adds, const uint64_t *add_counts, uint32_t snapshots,
+                       dycg_batch_stats *stats) {
+  return guard(e, [&](Engine &g) {
+    g.apply_batches(dels, del_counts, adds, add_counts, snapshots, false, stats);
+  });
+}
+
+int dycg_apply_batches_device(dycg_engine *e, const dycg_edge *d_dels, const uint64_t *del_counts,
+                              const dycg_edge *d_adds, const uint64_t *add_counts,
+                              uint32_t snapshots, dycg_batch_stats *stats) {
+  return guard(e, [&](Engine &g) {
+    g.apply_batches(d_dels, del_counts, d_adds, add_counts, snapshots, true, stats);
+  });
+}
+
 int dycg_stream(dycg_engine *e, void **stream) {
   if (!stream) return DYCG_EINVAL;
   return guard(e, [&](Engine &g) { *stream = (void *)g.stream(); });

@@ -131,7 +131,7 @@ struct Ctl {
   uint32_t wave_tag;     // running wave tag (never reused)
   uint32_t waves;        // waves run in this launch
   uint32_t pad[2];
-  u64 stat[16];
+  u64 stat[20];
 };
 
 enum StatIdx {
@@ -150,6 +150,8 @@ enum StatIdx {
   ST_PAGES_EVICTED,
   ST_MUT_LINK_BYTES,   // mutation kernels' adjacency bytes over the host link
   ST_MUT_HBM_BYTES,    // mutation kernels' adjacency bytes in the HBM cache
+  ST_T_START,          // batched repair: global timer at launch start (ns)
+  ST_T_END,            // batched repair: latest block exit (ns)
   ST_COUNT
 };
 

@@ -59,6 +59,11 @@ Engine::Engine(const dycg_options &opt) : opt_(opt) {
 
 Engine::~Engine() {
   if (st_) cudaStreamSynchronize(st_);
+  drop_graphs();
+  for (cudaEvent_t e : bev_) cudaEventDestroy(e);
+  if (h_rec_) cudaFreeHost(h_rec_);
+  if (d_rec_) cudaFree(d_rec_);
+  if (h_bctl_) cudaFreeHost(h_bctl_);
   dfree_all();
   for (void *p : hallocs_) cudaFreeHost(p);
   for (auto &e : ev_)
@@ -544,12 +549,22 @@ void Engine::init() {
 void Engine::reserve_batch(size_t max_records) {
   check_loaded();
   if (max_records > 0x3FFFFFFFull) throw Error(DYCG_EINVAL, "batch too large");
-  ensure_batch(std::max<size_t>(max_records, 1));
+  if (inited_ && nq_ && qmode_ == DYCG_QUERIES_BATCHED) {
+    // multi-snapshot replay: buffers for the largest padding class, and the
+    // graph of every class up to it captured now rather than on first use
+    uint32_t top = 1024;
+    while (top < max_records) top *= 2;
+    ensure_batch(top);
+    for (uint32_t c = 1024; c <= top; c *= 2) graph_for(c);
+  } else {
+    ensure_batch(std::max<size_t>(max_records, 1));
+  }
   sync_check("reserve batch");
 }
 
 void Engine::ensure_batch(size_t cnt) {
   if (cnt <= bcap_) return;
+  drop_graphs();  // captured graphs hold the old buffers
   for (void *p : batch_allocs_) cudaFree(p);
   batch_allocs_.clear();
   size_t c = std::max<size_t>(cnt, 1024);
@@ -609,29 +624,11 @@ void Engine::ensure_batch(size_t cnt) {
   bcap_ = c;
 }
 
-void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na,
-                   bool device_ptrs, int mode, bool maintenance, dycg_batch_stats *stats) {
-  check_loaded();
-  if (!inited_) throw Error(DYCG_ESTATE, "dycg_init must run before batches");
-  if (failed) throw Error(DYCG_ESTATE, "engine is in a failed state");
-  if ((nd && !dels) || (na && !adds)) throw Error(DYCG_EINVAL, "null update array");
-  if (nd > 0x3FFFFFFFull || na > 0x3FFFFFFFull) throw Error(DYCG_EINVAL, "batch too large");
-  if (mode == 1) na = 0;
-  if (mode == 2) nd = 0;
-  ensure_batch(std::max<size_t>(std::max(nd, na), 1));
-  const uint64_t l0 = launches_;
-  CK(cudaEventRecord(ev_[0], st_));
-  const dycg_edge_dev *d_dels = (const dycg_edge_dev *)dels;
-  const dycg_edge_dev *d_adds = (const dycg_edge_dev *)adds;
-  if (!device_ptrs) {
-    if (nd) std::memcpy(h_stage_, dels, nd * sizeof(dycg_edge));
-    if (na) std::memcpy(h_stage_ + nd, adds, na * sizeof(dycg_edge));
-    if (nd + na)
-      CK(cudaMemcpyAsync(d_edges_, h_stage_, (nd + na) * sizeof(dycg_edge),
-                         cudaMemcpyHostToDevice, st_));
-    d_dels = d_edges_;
-    d_adds = d_edges_ + nd;
-  }
+// Device half of a snapshot on st_: counters reset, ingest, mutation and
+// repair, no host synchronisation. capture: being recorded into a CUDA graph
+// (no stage events, no touched-source pass).
+void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg_edge_dev *d_adds,
+                              size_t na, bool capture) {
   CK(cudaMemsetAsync(ctl_, 0, sizeof(Ctl), st_));
   CK(cudaMemsetAsync(counts_, 0, 64, st_));
   if (opt_.algo == DYCG_ALGO_PR) {
@@ -674,13 +671,17 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
       launches_ += 2;
     }
   }
-  ++touch_epoch_;
-  if (nd) CK(launch_touched(k_del_out_, (uint32_t)nd, touch_, touch_epoch_, touched_, counts_ + 4,
-                            ctl_, st_));
-  if (na) CK(launch_touched(k_add_out_, (uint32_t)na, touch_, touch_epoch_, touched_, counts_ + 4,
-                            ctl_, st_));
-  launches_ += (nd ? 1 : 0) + (na ? 1 : 0);
-  CK(cudaEventRecord(ev_[1], st_));
+  // distinct touched sources (PR amends and the touched_sources counter);
+  // a captured graph would replay one epoch, so replays leave it out
+  if (!capture) {
+    ++touch_epoch_;
+    if (nd) CK(launch_touched(k_del_out_, (uint32_t)nd, touch_, touch_epoch_, touched_, counts_ + 4,
+                              ctl_, st_));
+    if (na) CK(launch_touched(k_add_out_, (uint32_t)na, touch_, touch_epoch_, touched_, counts_ + 4,
+                              ctl_, st_));
+    launches_ += (nd ? 1 : 0) + (na ? 1 : 0);
+  }
+  if (!capture) CK(cudaEventRecord(ev_[1], st_));
   const u64 timeout = 60ull * 1000000000ull;
   PrLaunch PL{};
   if (opt_.algo == DYCG_ALGO_PR) {
@@ -733,7 +734,7 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
       launches_ += 3;
     }
   }
-  CK(cudaEventRecord(ev_[2], st_));
+  if (!capture) CK(cudaEventRecord(ev_[2], st_));
   // ---- repair
   if (opt_.algo == DYCG_ALGO_PR) {
     PL.phases = (nd + na) ? (PR_AMEND | PR_CONVERGE) : PR_CONVERGE;
@@ -741,7 +742,8 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     CK(launch_pr(PL, st_));
     launches_++;
   } else if (nq_) {
-    repair_queries((uint32_t)nd, (uint32_t)na, timeout);
+    if (tune_) tune_repair((uint32_t)nd, (uint32_t)na, timeout);
+    else repair_queries((uint32_t)nd, (uint32_t)na, timeout);
   } else {
     RepairLaunch L{};
     L.out = A_out;
@@ -775,7 +777,33 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     CK(launch_repair(L, st_));
     launches_++;
   }
-  CK(cudaEventRecord(ev_[3], st_));
+  if (!capture) CK(cudaEventRecord(ev_[3], st_));
+}
+
+void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na,
+                   bool device_ptrs, int mode, bool maintenance, dycg_batch_stats *stats) {
+  check_loaded();
+  if (!inited_) throw Error(DYCG_ESTATE, "dycg_init must run before batches");
+  if (failed) throw Error(DYCG_ESTATE, "engine is in a failed state");
+  if ((nd && !dels) || (na && !adds)) throw Error(DYCG_EINVAL, "null update array");
+  if (nd > 0x3FFFFFFFull || na > 0x3FFFFFFFull) throw Error(DYCG_EINVAL, "batch too large");
+  if (mode == 1) na = 0;
+  if (mode == 2) nd = 0;
+  ensure_batch(std::max<size_t>(std::max(nd, na), 1));
+  const uint64_t l0 = launches_;
+  CK(cudaEventRecord(ev_[0], st_));
+  const dycg_edge_dev *d_dels = (const dycg_edge_dev *)dels;
+  const dycg_edge_dev *d_adds = (const dycg_edge_dev *)adds;
+  if (!device_ptrs) {
+    if (nd) std::memcpy(h_stage_, dels, nd * sizeof(dycg_edge));
+    if (na) std::memcpy(h_stage_ + nd, adds, na * sizeof(dycg_edge));
+    if (nd + na)
+      CK(cudaMemcpyAsync(d_edges_, h_stage_, (nd + na) * sizeof(dycg_edge),
+                         cudaMemcpyHostToDevice, st_));
+    d_dels = d_edges_;
+    d_adds = d_edges_ + nd;
+  }
+  enqueue_snapshot(d_dels, nd, d_adds, na, false);
   CK(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
   if (nq_) {
     if (qmode_ == DYCG_QUERIES_PER_QUERY)
@@ -921,6 +949,7 @@ void Engine::set_query_mapping(uint32_t qratio, uint32_t heavy, uint32_t tile) {
   qratio_ = qratio;
   heavy_ = heavy;
   tile_ = tile;
+  drop_graphs();  // captured graphs hold the old mapping
 }
 
 MultiLaunch Engine::multi_launch(uint32_t phases, uint32_t n_add, u64 timeout) {
@@ -1084,6 +1113,267 @@ void Engine::gather_query(uint32_t q, uint32_t *values, uint32_t *parents) {
   if (values) CK(cudaMemcpyAsync(values, q0_, (u64)n_ * 4, cudaMemcpyDeviceToHost, st_));
   if (parents) CK(cudaMemcpyAsync(parents, q1_, (u64)n_ * 4, cudaMemcpyDeviceToHost, st_));
   sync_check("gather query");
+}
+
+// ---- mapping autotuner and multi-snapshot replay ------------------------------
+
+// Repair of the current snapshot under every candidate mapping, each from the
+// same saved state (keys, page hotness, counters); keeps the fastest mapping
+// and ends with that mapping's run, so the engine state and the stage events
+// describe one ordinary repair.
+void Engine::tune_repair(uint32_t nd, uint32_t na, u64 timeout) {
+  if (qmode_ != DYCG_QUERIES_BATCHED) {
+    repair_queries(nd, na, timeout);
+    return;
+  }
+  const uint32_t phases = (nd ? PH_DELETE : 0) | (na ? PH_INSERT : 0) | PH_CLOSE;
+  const u64 kbytes = (u64)n_ * qnb_ * 32 * 8, hbytes = (u64)npages_ * 4;
+  struct Scratch {
+    void *p[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t a = nullptr, b = nullptr;
+    ~Scratch() {
+      for (void *x : p) cudaFree(x);
+      if (a) cudaEventDestroy(a);
+      if (b) cudaEventDestroy(b);
+    }
+  } sc;
+  CK(cudaMalloc(&sc.p[0], kbytes));
+  CK(cudaMalloc(&sc.p[1], std::max<u64>(hbytes, 4)));
+  CK(cudaMalloc(&sc.p[2], sizeof(Ctl)));
+  CK(cudaEventCreate(&sc.a));
+  CK(cudaEventCreate(&sc.b));
+  CK(cudaMemcpyAsync(sc.p[0], qkey_, kbytes, cudaMemcpyDeviceToDevice, st_));
+  CK(cudaMemcpyAsync(sc.p[1], page_hits_, hbytes, cudaMemcpyDeviceToDevice, st_));
+  CK(cudaMemcpyAsync(sc.p[2], ctl_, sizeof(Ctl), cudaMemcpyDeviceToDevice, st_));
+  auto restore = [&]() {
+    CK(cudaMemcpyAsync(qkey_, sc.p[0], kbytes, cudaMemcpyDeviceToDevice, st_));
+    CK(cudaMemcpyAsync(page_hits_, sc.p[1], hbytes, cudaMemcpyDeviceToDevice, st_));
+    CK(cudaMemcpyAsync(ctl_, sc.p[2], sizeof(Ctl), cudaMemcpyDeviceToDevice, st_));
+  };
+  static const uint32_t kRatio[] = {2, 4, 8, 1u << 20};
+  static const uint32_t kHeavy[] = {16, 64, 256};
+  tried_.clear();
+  dycg_query_mapping best{qratio_, heavy_, tile_, 1e30f};
+  for (uint32_t r : kRatio)
+    for (uint32_t h : kHeavy) {
+      if (!tried_.empty()) restore();
+      qratio_ = r;
+      heavy_ = h;
+      CK(cudaEventRecord(sc.a, st_));
+      CK(launch_multi(multi_launch(phases, na, timeout), st_));
+      CK(cudaEventRecord(sc.b, st_));
+      CK(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
+      sync_check("tune");
+      if (h_ctl_->err) {
+        failed = true;
+        throw Error(DYCG_ELIMIT, "mapping trial failed on the device (error code " +
+                                     std::to_string(h_ctl_->err) + ")");
+      }
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, sc.a, sc.b));
+      tried_.push_back({r, h, tile_, ms});
+      if (ms < best.repair_ms) best = tried_.back();
+      launches_++;
+    }
+  restore();
+  qratio_ = best.qratio;
+  heavy_ = best.heavy;
+  drop_graphs();
+  CK(cudaEventRecord(ev_[2], st_));  // the stage boundary of the kept run
+  CK(launch_multi(multi_launch(phases, na, timeout), st_));
+  launches_++;
+  sync_check("tune final");  // scratch is released on return
+}
+
+void Engine::tune(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na,
+                  dycg_query_mapping *tried, uint32_t cap, uint32_t *n_tried,
+                  dycg_batch_stats *stats) {
+  if (!nq_ || qmode_ != DYCG_QUERIES_BATCHED)
+    throw Error(DYCG_ESTATE, "mapping tuning needs the batched many-query form");
+  tune_ = true;
+  try {
+    apply(dels, nd, adds, na, false, 0, true, stats);
+  } catch (...) {
+    tune_ = false;
+    throw;
+  }
+  tune_ = false;
+  if (n_tried) *n_tried = (uint32_t)tried_.size();
+  for (uint32_t i = 0; tried && i < cap && i < tried_.size(); i++) tried[i] = tried_[i];
+}
+
+void Engine::drop_graphs() {
+  for (auto &g : graphs_) cudaGraphExecDestroy(g.second.exec);
+  graphs_.clear();
+}
+
+// Graph of one snapshot of padded size cls (records at d_edges_: deletions
+// [0, cls), insertions [cls, 2 cls)), captured on first use.
+const Engine::SnapshotGraph &Engine::graph_for(uint32_t cls) {
+  auto it = graphs_.find(cls);
+  if (it != graphs_.end()) return it->second;
+  cudaGraph_t g = nullptr;
+  const uint64_t l0 = launches_;
+  CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+  try {
+    enqueue_snapshot(d_edges_, cls, d_edges_ + cls, cls, true);
+  } catch (...) {
+    cudaStreamEndCapture(st_, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  CK(cudaStreamEndCapture(st_, &g));
+  SnapshotGraph sg{nullptr, launches_ - l0};
+  const cudaError_t e = cudaGraphInstantiate(&sg.exec, g, 0);
+  cudaGraphDestroy(g);
+  CK(e);
+  launches_ = l0;
+  return graphs_.emplace(cls, sg).first->second;
+}
+
+void Engine::apply_batches(const dycg_edge *dels, const uint64_t *nd, const dycg_edge *adds,
+                           const uint64_t *na, uint32_t count, bool device_ptrs,
+                           dycg_batch_stats *stats) {
+  check_loaded();
+  if (!inited_) throw Error(DYCG_ESTATE, "dycg_init must run before batches");
+  if (failed) throw Error(DYCG_ESTATE, "engine is in a failed state");
+  if (count && (!nd || !na)) throw Error(DYCG_EINVAL, "null count array");
+  u64 td = 0, ta = 0, mx = 1;
+  for (uint32_t i = 0; i < count; i++) {
+    if (nd[i] > 0x3FFFFFFFull || na[i] > 0x3FFFFFFFull) throw Error(DYCG_EINVAL, "batch too large");
+    td += nd[i];
+    ta += na[i];
+    mx = std::max<u64>(mx, std::max(nd[i], na[i]));
+  }
+  if ((td && !dels) || (ta && !adds)) throw Error(DYCG_EINVAL, "null update array");
+  if (!(nq_ && qmode_ == DYCG_QUERIES_BATCHED)) {
+    // other forms: one ordinary apply per snapshot
+    u64 od = 0, oa = 0;
+    for (uint32_t i = 0; i < count; i++) {
+      apply(dels + od, nd[i], adds + oa, na[i], device_ptrs, 0, true, stats ? stats + i : nullptr);
+      od += nd[i];
+      oa += na[i];
+    }
+    return;
+  }
+  auto cls_of = [](u64 x) {
+    uint32_t c = 1024;
+    while (c < x) c *= 2;
+    return c;
+  };
+  ensure_batch(cls_of(mx));
+  // records on the device: the caller's, or one staged copy of all snapshots
+  const dycg_edge_dev *d_dels = (const dycg_edge_dev *)dels, *d_adds = (const dycg_edge_dev *)adds;
+  if (!device_ptrs && td + ta) {
+    const u64 bytes = (td + ta) * sizeof(dycg_edge);
+    if (bytes > hrec_bytes_) {
+      if (h_rec_) cudaFreeHost(h_rec_);
+      if (d_rec_) cudaFree(d_rec_);
+      h_rec_ = nullptr;
+      d_rec_ = nullptr;
+      hrec_bytes_ = 0;
+      CK(cudaHostAlloc(&h_rec_, bytes, cudaHostAllocDefault));
+      CK(cudaMalloc(&d_rec_, bytes));
+      hrec_bytes_ = bytes;
+    }
+    if (td) std::memcpy(h_rec_, dels, td * sizeof(dycg_edge));
+    if (ta) std::memcpy((char *)h_rec_ + td * sizeof(dycg_edge), adds, ta * sizeof(dycg_edge));
+    CK(cudaMemcpyAsync(d_rec_, h_rec_, bytes, cudaMemcpyHostToDevice, st_));
+    d_dels = (const dycg_edge_dev *)d_rec_;
+    d_adds = d_dels + td;
+  }
+  if (count > bctl_cap_) {
+    if (h_bctl_) cudaFreeHost(h_bctl_);
+    h_bctl_ = nullptr;
+    bctl_cap_ = 0;
+    CK(cudaHostAlloc((void **)&h_bctl_, (u64)count * sizeof(Ctl), cudaHostAllocDefault));
+    bctl_cap_ = count;
+  }
+  while (bev_.size() < 2 * (size_t)count) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    bev_.push_back(e);
+  }
+  std::vector<uint32_t> cls(count);
+  u64 od = 0, oa = 0;
+  for (uint32_t i = 0; i < count; i++) {
+    cls[i] = cls_of(std::max<u64>(std::max(nd[i], na[i]), 1));
+    const SnapshotGraph &g = graph_for(cls[i]);
+    // padding records carry out-of-range ids: ingest drops them
+    CK(cudaMemsetAsync(d_edges_, 0xFF, 2ull * cls[i] * sizeof(dycg_edge), st_));
+    if (nd[i])
+      CK(cudaMemcpyAsync(d_edges_, d_dels + od, nd[i] * sizeof(dycg_edge),
+                         cudaMemcpyDeviceToDevice, st_));
+    if (na[i])
+      CK(cudaMemcpyAsync(d_edges_ + cls[i], d_adds + oa, na[i] * sizeof(dycg_edge),
+                         cudaMemcpyDeviceToDevice, st_));
+    CK(cudaEventRecord(bev_[2 * i], st_));
+    CK(cudaGraphLaunch(g.exec, st_));
+    CK(cudaEventRecord(bev_[2 * i + 1], st_));
+    CK(cudaMemcpyAsync(h_bctl_ + i, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
+    launches_ += g.kernels;
+    od += nd[i];
+    oa += na[i];
+  }
+  CK(cudaMemcpyAsync(h_seq_, seq_, 8, cudaMemcpyDeviceToHost, st_));
+  sync_check("batches");
+  for (uint32_t i = 0; i < count; i++)
+    if (h_bctl_[i].err) {
+      failed = true;
+      const uint32_t er = h_bctl_[i].err;
+      throw Error(er == ERR_WAVES || er == ERR_BARRIER ? DYCG_ELIMIT : DYCG_ECAPACITY,
+                  "snapshot " + std::to_string(i) + " failed on the device (error code " +
+                      std::to_string(er) + ")");
+    }
+  if (h_seq_[1] > 0xF0000000u) {
+    CK(cudaMemsetAsync(wtag_, 0, (n_ + 1ull) * 4, st_));
+    h_seq_[1] = 1;
+    CK(cudaMemcpyAsync(seq_ + 1, h_seq_ + 1, 4, cudaMemcpyHostToDevice, st_));
+    sync_check("tag reset");
+  }
+  if (stats) {
+    for (uint32_t i = 0; i < count; i++) {
+      const Ctl &c = h_bctl_[i];
+      dycg_batch_stats *s = stats + i;
+      std::memset(s, 0, sizeof(*s));
+      s->deletions = nd[i];
+      s->insertions = na[i];
+      s->missing_deletes = c.stat[ST_MISSING];
+      // padding records count as invalid in the device counter
+      s->invalid_updates = c.stat[ST_INVALID] - (2ull * cls[i] - nd[i] - na[i]);
+      s->relocated_rows = c.stat[ST_RELOCATED];
+      s->affected = c.stat[ST_AFFECTED];
+      s->expanded = c.stat[ST_EXPANDED];
+      s->edges_scanned = c.stat[ST_SCANNED];
+      s->improvements = c.stat[ST_IMPROVED];
+      s->waves = c.waves;
+      s->link_bytes = c.stat[ST_LINK_BYTES] + c.stat[ST_MUT_LINK_BYTES];
+      s->hbm_adj_bytes = c.stat[ST_HBM_ADJ_BYTES] + c.stat[ST_MUT_HBM_BYTES];
+      s->mutate_link_bytes = c.stat[ST_MUT_LINK_BYTES];
+      s->mutate_hbm_bytes = c.stat[ST_MUT_HBM_BYTES];
+      s->state_bytes = c.stat[ST_STATE_BYTES] + s->expanded * 16 + s->improvements * 16;
+      s->kernel_launches = graphs_.count(cls[i]) ? graphs_[cls[i]].kernels : 0;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, bev_[2 * i], bev_[2 * i + 1]);
+      s->ms_total = ms;
+      // the repair kernel's own start/end stamps (no stage events in a graph)
+      if (c.stat[ST_T_END] > c.stat[ST_T_START] && c.stat[ST_T_START])
+        s->ms_repair = (c.stat[ST_T_END] - c.stat[ST_T_START]) * 1e-6;
+    }
+  }
+  // cache maintenance once, after the last snapshot
+  dycg_batch_stats last{};
+  cache_maintenance(false, stats ? &last : nullptr);
+  if (stats && count) {
+    dycg_batch_stats *s = stats + count - 1;
+    s->ms_cache = last.ms_cache;
+    s->ms_total += last.ms_cache;
+    s->cache_pages_loaded = last.cache_pages_loaded;
+    s->cache_pages_evicted = last.cache_pages_evicted;
+    s->link_bytes += last.link_bytes;
+    s->hbm_adj_bytes += last.hbm_adj_bytes;
+    s->kernel_launches += 8;
+  }
 }
 
 void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {

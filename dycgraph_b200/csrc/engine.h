@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -59,6 +60,10 @@ class Engine {
   void set_queries(const uint32_t *sources, uint32_t count, uint32_t mode);
   void set_query_mapping(uint32_t qratio, uint32_t heavy, uint32_t tile);
   void gather_query(uint32_t q, uint32_t *values, uint32_t *parents);
+  void tune(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na,
+            dycg_query_mapping *tried, uint32_t cap, uint32_t *n_tried, dycg_batch_stats *stats);
+  void apply_batches(const dycg_edge *dels, const uint64_t *nd, const dycg_edge *adds,
+                     const uint64_t *na, uint32_t count, bool device_ptrs, dycg_batch_stats *stats);
   uint32_t queries() const { return nq_; }
   cudaStream_t stream() const { return st_; }
 
@@ -76,6 +81,15 @@ class Engine {
   Adj adj(const Arena &A) const;
   void sync_check(const char *where);
   void fill_stats(dycg_batch_stats *s, float ms[4]);
+  void enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg_edge_dev *d_adds,
+                        size_t na, bool capture);
+  void tune_repair(uint32_t nd, uint32_t na, u64 timeout);
+  struct SnapshotGraph {
+    cudaGraphExec_t exec;
+    uint64_t kernels;
+  };
+  const SnapshotGraph &graph_for(uint32_t cls);
+  void drop_graphs();
   void init_queries(u64 timeout);
   void repair_queries(uint32_t nd, uint32_t na, u64 timeout);
   MultiLaunch multi_launch(uint32_t phases, uint32_t n_add, u64 timeout);
@@ -124,6 +138,15 @@ class Engine {
   uint32_t mtile_cap_ = 0;
   uint32_t qratio_ = 4, heavy_ = 64, tile_ = 4096;
   u64 qbytes_ = 0;
+  bool tune_ = false;
+  std::vector<dycg_query_mapping> tried_;
+  // multi-snapshot replay: one graph per padded batch-size class
+  std::map<uint32_t, SnapshotGraph> graphs_;
+  std::vector<cudaEvent_t> bev_;
+  Ctl *h_bctl_ = nullptr;
+  uint32_t bctl_cap_ = 0;
+  void *h_rec_ = nullptr, *d_rec_ = nullptr;
+  u64 hrec_bytes_ = 0;
 
   // batch buffers
   size_t bcap_ = 0;

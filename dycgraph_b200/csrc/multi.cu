@@ -624,6 +624,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
   const uint32_t tag0 = *(volatile uint32_t *)&P.seq[1];
   uint32_t tag = tag0 + 1;  // next unused wave tag (uniform over the grid)
   uint32_t waves = 0;
+  if (gtid == 0) ctl->stat[ST_T_START] = globaltimer_ns();
   __shared__ u64 s_state[WARPS][Q];  // edge-lane per-query state of each warp
   __shared__ uint2 s_stage[MULTI_MIN_TILE];  // staged slots of an edge-lane tile
   u64 *s = s_state[threadIdx.x >> 5];
@@ -769,6 +770,8 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
   }
 done:
   acc.flush(ctl);
+  __syncthreads();
+  if (threadIdx.x == 0) atomicMax(&ctl->stat[ST_T_END], globaltimer_ns());
   if (gtid == 0) {
     atomicAdd(&ctl->stat[ST_AFFECTED], (u64)ctl->snap_aff);
     ctl->waves = waves;
@@ -849,9 +852,18 @@ static cudaError_t launch_multi_t(const MultiLaunch &L, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     if (blocks_per_sm < 1) return cudaErrorLaunchOutOfResources;
   }
-  void *args[] = {&P};
-  return cudaLaunchCooperativeKernel((const void *)multi_repair_kernel<ALGO, STORED, NB>,
-                                     blocks_per_sm * L.num_sms, BLOCK, args, 0, s);
+  // cooperative (co-resident blocks for the grid barrier); this launch form
+  // can also be recorded into a CUDA graph
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks_per_sm * L.num_sms);
+  cfg.blockDim = dim3(BLOCK);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, multi_repair_kernel<ALGO, STORED, NB>, P);
 }
 
 template <uint32_t ALGO, bool STORED>

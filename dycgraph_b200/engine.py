@@ -60,6 +60,14 @@ class BatchStats(ctypes.Structure):
         return {k: getattr(self, k) for k in _STAT_U64 + _STAT_F64 + _STAT_TAIL}
 
 
+class QueryMapping(ctypes.Structure):
+    _fields_ = [("qratio", ctypes.c_uint32), ("heavy", ctypes.c_uint32), ("tile", ctypes.c_uint32),
+                ("repair_ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class GraphInfo(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in (
         "nodes", "live_edges", "arena_slots", "arena_used", "pages", "cache_slots",
@@ -107,6 +115,10 @@ def lib():
         "dycg_cache_maintenance": (I, [P, sp]),
         "dycg_apply_batch": (I, [P, ep, sz, ep, sz, sp]),
         "dycg_reserve_batch": (I, [P, sz]),
+        "dycg_tune_query_mapping": (I, [P, ep, sz, ep, sz, ctypes.POINTER(QueryMapping), u32,
+                                        ctypes.POINTER(ctypes.c_uint32), sp]),
+        "dycg_apply_batches": (I, [P, ep, u64p, ep, u64p, u32, sp]),
+        "dycg_apply_batches_device": (I, [P, P, u64p, P, u64p, u32, sp]),
         "dycg_apply_batch_device": (I, [P, P, sz, P, sz, sp]),
         "dycg_gather": (I, [P, u32p, u32p]),
         "dycg_gather_ranks": (I, [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
@@ -320,6 +332,47 @@ class Engine:
         self._check(lib().dycg_apply_batch_device(self._h, ctypes.c_void_p(d_dels_ptr), nd,
                                                   ctypes.c_void_p(d_adds_ptr), na,
                                                   ctypes.byref(st)), "apply_batch_device")
+        return st
+
+    def tune_query_mapping(self, dels, adds):
+        """Apply one snapshot while timing the batched repair under each
+        candidate work mapping; keeps the fastest. Returns the candidates."""
+        d = edges_array(dels)
+        a = edges_array(adds)
+        tried = (QueryMapping * 64)()
+        nt = ctypes.c_uint32(0)
+        st = BatchStats()
+        self._check(lib().dycg_tune_query_mapping(
+            self._h, d.ctypes.data_as(ctypes.POINTER(Edge)), d.shape[0],
+            a.ctypes.data_as(ctypes.POINTER(Edge)), a.shape[0], tried, 64, ctypes.byref(nt),
+            ctypes.byref(st)), "tune_query_mapping")
+        self.last_stats = st.as_dict()
+        return [tried[i].as_dict() for i in range(nt.value)]
+
+    def apply_batches(self, snapshots):
+        """Many snapshots [(dels, adds), ...] in one call; one stats dict each."""
+        ds = [edges_array(d) for d, _ in snapshots]
+        as_ = [edges_array(a) for _, a in snapshots]
+        nd = np.asarray([x.shape[0] for x in ds], np.uint64)
+        na = np.asarray([x.shape[0] for x in as_], np.uint64)
+        d = np.ascontiguousarray(np.concatenate(ds) if ds else np.zeros((0, 3), np.uint32))
+        a = np.ascontiguousarray(np.concatenate(as_) if as_ else np.zeros((0, 3), np.uint32))
+        st = (BatchStats * max(len(snapshots), 1))()
+        self._check(lib().dycg_apply_batches(
+            self._h, d.ctypes.data_as(ctypes.POINTER(Edge)), _ptr(nd, ctypes.c_uint64),
+            a.ctypes.data_as(ctypes.POINTER(Edge)), _ptr(na, ctypes.c_uint64), len(snapshots), st),
+            "apply_batches")
+        return [st[i].as_dict() for i in range(len(snapshots))]
+
+    def apply_batches_device(self, d_dels_ptr, nd, d_adds_ptr, na, stats=None):
+        """Records already in device memory: nd/na per-snapshot counts."""
+        nd = np.ascontiguousarray(nd, np.uint64)
+        na = np.ascontiguousarray(na, np.uint64)
+        st = stats if stats is not None else (BatchStats * max(len(nd), 1))()
+        self._check(lib().dycg_apply_batches_device(
+            self._h, ctypes.c_void_p(d_dels_ptr), _ptr(nd, ctypes.c_uint64),
+            ctypes.c_void_p(d_adds_ptr), _ptr(na, ctypes.c_uint64), len(nd), st),
+            "apply_batches_device")
         return st
 
     def cache_maintenance(self):

@@ -218,7 +218,9 @@ int dycg_apply_batch(dycg_engine *e, const dycg_edge *dels, size_t nd,
  * (and as many insertions) ahead of time, the way the reference sizes its
  * mapped update arrays from the update file before replay
  * (include/framework/framework.cuh:2387-2412 get_update_file). Without it the
- * buffers grow on the first larger batch, inside that call. */
+ * buffers grow on the first larger batch, inside that call. After dycg_init
+ * in the batched many-query form it also captures the replay graphs of every
+ * batch-size class up to max_records (see dycg_apply_batches). */
 int dycg_reserve_batch(dycg_engine *e, size_t max_records);
 
 /* Same as dycg_apply_batch with the records already in device memory. */
@@ -322,6 +324,46 @@ int dycg_set_queries(dycg_engine *e, const uint32_t *sources, uint32_t count, ui
  * CTAs (tile >= 1024). Defaults: qratio 4, heavy 64, tile 4096. The mapping
  * changes speed only, never results. */
 int dycg_set_query_mapping(dycg_engine *e, uint32_t qratio, uint32_t heavy, uint32_t tile);
+
+/* One work mapping of the batched form and the repair time it took. */
+typedef struct dycg_query_mapping {
+  uint32_t qratio;
+  uint32_t heavy;
+  uint32_t tile;
+  float repair_ms;
+} dycg_query_mapping;
+
+/* Autotuner of the batched form's work mapping (no reference counterpart):
+ * applies one snapshot like dycg_apply_batch, but repairs it once per
+ * candidate mapping (qratio in {2,4,8,2^20} x heavy in {16,64,256}), each
+ * from the same saved state, keeps the fastest mapping for later snapshots
+ * and leaves the state of one ordinary repair. Needs HBM for one extra copy
+ * of the query results while it runs. tried (cap entries, may be NULL)
+ * receives the candidates with their repair times; *n_tried their count. */
+int dycg_tune_query_mapping(dycg_engine *e, const dycg_edge *dels, size_t nd,
+                            const dycg_edge *adds, size_t na, dycg_query_mapping *tried,
+                            uint32_t cap, uint32_t *n_tried, dycg_batch_stats *stats);
+
+/* Many snapshots in one call, in order (the reference's sample drivers loop
+ * over batches one call each, samples/hybrid_sssp/hybrid_sssp.cu:444-548).
+ * The records of snapshot i follow those of snapshot i-1: del_counts[i]
+ * deletions in dels, add_counts[i] insertions in adds. stats: one entry per
+ * snapshot, or NULL. In the batched many-query form each snapshot is one
+ * replay of a CUDA graph (ingest, mutation, repair) captured once per batch
+ * size class (powers of two >= 1024; records are padded with out-of-range
+ * entries that ingest drops), with no host synchronisation between
+ * snapshots, and cache maintenance runs once, after the last snapshot;
+ * per-stage times are then not split (ms_total per snapshot). Other forms
+ * apply the snapshots one by one. */
+int dycg_apply_batches(dycg_engine *e, const dycg_edge *dels, const uint64_t *del_counts,
+                       const dycg_edge *adds, const uint64_t *add_counts, uint32_t snapshots,
+                       dycg_batch_stats *stats);
+
+/* Same as dycg_apply_batches with the records already in device memory. */
+int dycg_apply_batches_device(dycg_engine *e, const dycg_edge *d_dels,
+                              const uint64_t *del_counts, const dycg_edge *d_adds,
+                              const uint64_t *add_counts, uint32_t snapshots,
+                              dycg_batch_stats *stats);
 
 /* Results of query q (values/parents as dycg_gather; n entries each, either
  * may be NULL). With queries set, dycg_gather returns query 0. */

@@ -157,3 +157,79 @@ def test_query_argument_errors():
     cc.load_csr(n, off, dst)
     with pytest.raises(dg.DycgError):
         cc.set_queries([0])
+
+
+def _engine_and_sources(scale, nq, seed, stored=True, mode="batched", budget=0):
+    n, off, dst, w = cases.small_rmat(scale, 8, seed)
+    rng = np.random.default_rng(seed)
+    cand = np.nonzero(np.diff(off) > 0)[0]
+    sources = rng.choice(cand, size=nq, replace=False).astype(np.uint32)
+    e = dg.Engine("sssp", weight_mode="stored" if stored else "hash128",
+                  hbm_graph_budget_bytes=budget, page_shift=8)
+    e.load_csr(n, off, dst, w if stored else None)
+    e.set_queries(sources, mode)
+    e.start()
+    return e, (n, off, dst, w), sources
+
+
+def _check_all(e, n, csr_, sources):
+    o, d, ww = csr_
+    for q, s in enumerate(sources):
+        ref = oracle.static_sssp(n, o, d, ww, oracle.WEIGHT_STORED, int(s))
+        assert (e.gather_query(q)[0] == ref).all(), q
+
+
+def test_tune_mapping_keeps_results():
+    e, (n, off, dst, w), src = _engine_and_sources(11, 48, 23)
+    orc = oracle.Oracle(oracle.SSSP, n, off, dst, w, weight_mode=oracle.WEIGHT_STORED)
+    cur = (off, dst, w)
+    dels, adds = cases.random_batch(n, *cur, 600, 600, 2301)
+    tried = e.tune_query_mapping(dels, adds)
+    orc.mutate(dels, adds)
+    cur = orc.csr()
+    assert len(tried) == 12 and all(t["repair_ms"] > 0 for t in tried)
+    _check_all(e, n, cur, src)
+    for bi in range(2):  # later snapshots under the kept mapping
+        dels, adds = cases.random_batch(n, *cur, 400, 400, 2310 + bi)
+        e.apply_batch(dels, adds)
+        orc.mutate(dels, adds)
+        cur = orc.csr()
+    _check_all(e, n, cur, src)
+
+
+@pytest.mark.parametrize("mode", ["batched", "per_query"])
+def test_apply_batches_replay_matches_one_by_one(mode):
+    # uneven snapshot sizes across three padding classes, classes replayed twice
+    a, (n, off, dst, w), src = _engine_and_sources(11, 40, 29, mode=mode)
+    b, _, _ = _engine_and_sources(11, 40, 29, mode=mode)
+    orc = oracle.Oracle(oracle.SSSP, n, off, dst, w, weight_mode=oracle.WEIGHT_STORED)
+    cur = (off, dst, w)
+    for rnd, sizes in enumerate([(5, 700, 1500), (3000, 1, 900)]):
+        snaps = []
+        for i, sz in enumerate(sizes):
+            dels, adds = cases.random_batch(n, *cur, sz // 2, sz - sz // 2, 2900 + 10 * rnd + i)
+            snaps.append((dels, adds))
+            orc.mutate(dels, adds)
+            cur = orc.csr()
+        stats = a.apply_batches(snaps)
+        one = [b.apply_batch(d, ad) for d, ad in snaps]
+        assert len(stats) == len(snaps)
+        for s, o, (d, ad) in zip(stats, one, snaps):
+            assert s["deletions"] == len(d) and s["insertions"] == len(ad)
+            assert s["invalid_updates"] == 0
+            assert s["missing_deletes"] == o["missing_deletes"]
+            assert s["ms_total"] > 0
+        _check_all(a, n, cur, src)
+        for q in range(len(src)):
+            assert (a.gather_query(q)[0] == b.gather_query(q)[0]).all()
+
+
+def test_apply_batches_invalid_records_and_empty_snapshots():
+    e, (n, off, dst, w), src = _engine_and_sources(10, 32, 31)
+    orc = oracle.Oracle(oracle.SSSP, n, off, dst, w, weight_mode=oracle.WEIGHT_STORED)
+    dels, adds = cases.random_batch(n, off, dst, w, 50, 50, 3101)
+    bad = [(n + 5, 1, 3), (2, n, 4)]
+    stats = e.apply_batches([([], []), (dels, adds + bad), ([], [])])
+    assert stats[1]["invalid_updates"] == 2 and stats[0]["invalid_updates"] == 0
+    orc.mutate(dels, adds)
+    _check_all(e, n, orc.csr(), src)

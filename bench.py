@@ -44,7 +44,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dycg", choices=["dycg", "reference"])
     ap.add_argument("--algo", default="sssp", choices=["sssp", "bfs", "cc", "pr"])
-    ap.add_argument("--config", default="rmat26", choices=["rmat26", "rmat16", "grid", "batched"],
+    ap.add_argument("--config", default="rmat26",
+                    choices=["rmat26", "rmat16", "grid", "batched", "learned"],
                     help="rmat26: headline out-of-memory R-MAT; rmat16: the small CPU-runnable "
                          "R-MAT; grid: 4096^2 road-like grid")
     ap.add_argument("--scale", type=int, default=None)
@@ -69,13 +70,18 @@ def parse():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--no-replay", action="store_true")
     ap.add_argument("--tune-batch", type=int, default=100_000)
+    ap.add_argument("--trace-snapshots", type=int, default=10)
+    ap.add_argument("--train-epochs", type=int, default=3)
+    ap.add_argument("--train-lr", type=float, default=2e-3)
+    ap.add_argument("--train-batch", type=int, default=8192)
     ap.add_argument("--batch-min", type=int, default=1_000)
     ap.add_argument("--batch-max", type=int, default=1_000_000)
     args = ap.parse_args()
     if args.ordered_delta is None:
         args.ordered_delta = 0 if args.config != "grid" else (256 if args.algo == "sssp" else 1)
     defaults = {"rmat26": (26, 100_000, 4.0), "rmat16": (16, 2_000, 0.0),
-                "grid": (12, 10_000, 0.25), "batched": (24, 0, 2.0)}[args.config]
+                "grid": (12, 10_000, 0.25), "batched": (24, 0, 2.0),
+                "learned": (27, 1_000_000, 8.0)}[args.config]
     if args.scale is None:
         args.scale = defaults[0]
     if args.batch is None:
@@ -769,12 +775,210 @@ def query_cpu_baseline(eng, args, algo, source, Q):
             "gpu_matches_oracle": parity}
 
 
+# ----------------------------------------------------------------------------
+def zipf_ids(n, count, rng, perm, s=1.1):
+    """Vertex ids with Zipf(s)-distributed ranks (rank 1 hottest), scattered by perm."""
+    out = np.empty(0, np.int64)
+    while len(out) < count:
+        k = rng.zipf(s, size=2 * (count - len(out)) + 16)
+        out = np.concatenate([out, k[k <= n] - 1])
+    return perm[out[:count]].astype(np.uint32)
+
+
+def zipf_snapshots(eng, count, size, seed, n, wmax=64):
+    """Snapshots of `size` updates (half deletions, half insertions) whose
+    endpoints are Zipf(1.1) over the vertices: insertions draw both endpoints,
+    deletions take a live out-edge of a drawn source (drawn on the initial
+    graph, so a later snapshot may name an edge deleted before: a missing
+    delete, counted as such)."""
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(n)
+    out = []
+    for _ in range(count):
+        nd = size // 2
+        d = eng.sample_row_edges(zipf_ids(n, nd, rng, perm), int(rng.integers(1 << 62)))
+        d = d[d[:, 0] != 0xFFFFFFFF]
+        u = zipf_ids(n, size - nd, rng, perm)
+        v = zipf_ids(n, size - nd, rng, perm)
+        keep = u != v
+        u, v = u[keep], v[keep]
+        # weight from the endpoints, so parallel copies of an edge agree
+        w = 1 + (u.astype(np.uint64) * np.uint64(0x9E3779B1) +
+                 v.astype(np.uint64) * np.uint64(0x85EBCA77)) % np.uint64(wmax)
+        out.append((d, np.stack([u, v, w.astype(np.uint32)], 1).astype(np.uint32)))
+    return out
+
+
+def run_learned(args):
+    """Learned cache admission against the hotness and no-cache policies on
+    the same snapshots: R-MAT 27 (134M vertices, ~2.1B edges), HBM graph budget
+    8 GB, snapshots of 1M Zipf(1.1)-skewed updates; the network is trained on
+    the traces of the first `trace` snapshots (hotness policy), then all
+    policies repair the same following snapshots."""
+    import torch
+    import dycgraph_b200 as dg
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    torch.cuda.set_device(local)
+    K, W = args.steps, max(args.warmup, 3)
+    E = args.e2e_steps if args.e2e_steps is not None else 3
+    T = args.trace_snapshots
+    algo = args.algo if args.algo in ("sssp", "pr") else "sssp"
+    budget = int(args.budget_gb * (1 << 30))
+    snaps = None
+    res = {}
+    report = None
+    for policy in ("learned", "hotness", "none"):
+        t0 = time.time()
+        eng = dg.Engine(algo, weight_mode="stored" if algo == "sssp" else "hash128",
+                        hbm_graph_budget_bytes=0 if policy == "none" else budget,
+                        cache_policy="none" if policy == "none" else "hotness", epsilon=1e-4,
+                        device=local)
+        eng.load_rmat(args.scale, args.edge_factor, seed=args.seed, wlo=1, whi=64)
+        t_load = time.time() - t0
+        t0 = time.time()
+        eng.start()
+        t_init = time.time() - t0
+        if snaps is None:
+            snaps = zipf_snapshots(eng, T + W + K + E, args.batch, args.seed + 77, eng.n)
+        eng.reserve_batch(max(max(len(d), len(a)) for d, a in snaps))
+        if policy == "learned":
+            eng.policy_trace(T)
+        for d, a in snaps[:T]:
+            eng.apply_batch(d, a)
+        if policy == "learned":
+            report = eng.policy_train(epochs=args.train_epochs, lr=args.train_lr,
+                                      batch=args.train_batch, seed=args.seed)
+            eng.set_cache_policy("learned")
+        for d, a in snaps[T:T + W]:
+            eng.apply_batch(d, a)
+        dev = [(torch.from_numpy(d.astype(np.int32)).cuda(), torch.from_numpy(a.astype(np.int32)).cuda())
+               for d, a in snaps[T + W:T + W + K]]
+        stream = torch.cuda.ExternalStream(eng.stream())
+        st = dg.BatchStats()
+        per = []
+        clocks = Clocks(local) if policy == "learned" else None
+        torch.cuda.synchronize()
+        if clocks:
+            clocks.start()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        t_begin = time.time()
+        ev0.record(stream)
+        for d, a in dev:
+            eng.apply_batch_device(d.data_ptr(), d.shape[0], a.data_ptr(), a.shape[0], st)
+            per.append(st.as_dict())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        clk = None
+        if clocks:
+            clocks.mark(t_begin, time.time())
+            clk = clocks.stop()
+        ms = ev0.elapsed_time(ev1)
+        e2e_ms, e2e_upd = 0.0, 0
+        if E:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for d, a in snaps[T + W + K:]:
+                eng.apply_batch(d, a)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms = e0.elapsed_time(e1)
+            e2e_upd = int(sum(len(d) + len(a) for d, a in snaps[T + W + K:]))
+        upd = int(sum(len(d) + len(a) for d, a in snaps[T + W:T + W + K]))
+        link = int(sum(p["link_bytes"] for p in per))
+        hbm = int(sum(p["hbm_adj_bytes"] for p in per))
+        vals = eng.gather()[0] if algo != "pr" else eng.gather_ranks()[0]
+        info = eng.info()
+        res[policy] = {
+            "value": round(upd / (ms / 1e3), 1), "ms_per_step": round(ms / K, 3),
+            "e2e": round(e2e_upd / (e2e_ms / 1e3), 1) if e2e_ms > 0 else None,
+            "link_bytes_per_step": link // K, "hbm_adj_bytes_per_step": hbm // K,
+            "hit_rate": round(hbm / max(1, hbm + link), 4),
+            "per_step": {k: round(float(np.mean([p[k] for p in per])), 4) for k in
+                         ("ms_ingest", "ms_mutate", "ms_repair", "ms_cache", "ms_total",
+                          "affected", "edges_scanned", "cache_pages_loaded", "missing_deletes")},
+            "cached_pages": info["cached_pages"], "cache_slots": info["cache_slots"],
+            "load_s": round(t_load, 1), "static_solve_s": round(t_init, 1),
+            "gpu_launches": int(sum(p["kernel_launches"] for p in per)),
+            "_vals": vals, "_clk": clk, "_per": per, "_info": info,
+        }
+        eng.close()
+        del eng, dev
+    L = res["learned"]
+    if algo == "pr":
+        parity = {p: float(np.max(np.abs(res[p]["_vals"].astype(np.float64) -
+                                         L["_vals"].astype(np.float64)))) for p in res}
+    else:
+        parity = {p: bool((res[p]["_vals"] == L["_vals"]).all()) for p in res}
+    per = L["_per"]
+    info = L["_info"]
+    page_bytes = (4 << 12) * (2 if algo == "sssp" else 1)
+    rep_ms = float(np.sum([p["ms_repair"] for p in per]))
+    rep_link = float(np.sum([p["link_bytes"] - p["mutate_link_bytes"] - p["cache_pages_loaded"] * page_bytes
+                             for p in per]))
+    rep_hbm = float(np.sum([p["hbm_adj_bytes"] - p["mutate_hbm_bytes"] - p["cache_pages_loaded"] * page_bytes
+                            + p["state_bytes"] for p in per]))
+    hbm_peak, peak_kind = peaks()
+    link_h2d, link_zc = dg.measure_host_link(local, 1 << 30)
+    roofline = {
+        "kernel": f"repair_kernel<{algo}>" if algo != "pr" else "pr_kernel",
+        "bound": "hbm", "achieved": round(rep_hbm / (rep_ms * 1e6), 2), "peak": hbm_peak,
+        "unit": "GB/s", "frac": round(rep_hbm / (rep_ms * 1e6) / hbm_peak, 5), "traffic": None,
+        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                       else "fallback 6650 GB/s",
+        "algorithmic_bytes_per_launch": {"hbm": int(rep_hbm / K), "host_link": int(rep_link / K)},
+        "launch_ms": round(rep_ms / K, 4),
+        "host_link": {"achieved": round(rep_link / (rep_ms * 1e6), 2),
+                      "peak_zero_copy": round(link_zc, 2), "peak_h2d_copy": round(link_h2d, 2),
+                      "unit": "GB/s", "frac": round(rep_link / (rep_ms * 1e6) / link_zc, 5)},
+    }
+    policies = {p: {k: v for k, v in r.items() if not k.startswith("_")} for p, r in res.items()}
+    H = res["hotness"]
+    return {
+        "metric": METRIC + ", learned admission vs hotness and no cache on the same snapshots",
+        "value": L["value"], "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": L["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32" if algo != "pr" else "f32",
+        "data": "synthetic (seeded R-MAT, Zipf(1.1) update endpoints; real graphs not available)",
+        "config": {"workload": f"rmat{args.scale}-ef{args.edge_factor} {algo}, "
+                               f"{args.batch // 1000}K Zipf(1.1) updates per snapshot, HBM graph "
+                               f"budget {args.budget_gb:g} GB, learned admission trained on the "
+                               f"first {T} snapshots",
+                   "vertices": info["nodes"], "edges": info["live_edges"],
+                   "graph_host_bytes": info["host_bytes"], "snapshots": T + W + K + E,
+                   "l2": "inputs larger than L2 (graph in pinned host memory)",
+                   "parallelism": "single GPU (replicas only)"},
+        "clocks": L["_clk"],
+        "e2e": {"value": L["e2e"], "unit": UNIT, "h2d_bytes_per_step": args.batch * 12,
+                "d2h_bytes_per_step": 256, "steps": E},
+        "gpu_launches": L["gpu_launches"],
+        "roofline": roofline,
+        "policies": policies,
+        "gain_vs_hotness": {"updates_per_s": round(L["value"] / H["value"], 3),
+                            "link_bytes": round(H["link_bytes_per_step"] /
+                                                max(1, L["link_bytes_per_step"]), 3),
+                            "hit_rate": [H["hit_rate"], L["hit_rate"]]},
+        "training": report,
+        "results_equal_across_policies": parity,
+        "cpu_baseline": {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                         "sample": "not run for this configuration (the CPU oracle at scale 27 "
+                                   "needs the whole graph in host memory twice); see the rmat26 "
+                                   "and batched configurations"},
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         out = run_reference(args)
     elif args.config == "batched":
         out = run_batched(args)
+    elif args.config == "learned":
+        out = run_learned(args)
     else:
         out = run_dycg(args)
     if out is not None:

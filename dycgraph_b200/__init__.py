@@ -10,7 +10,8 @@ a CUDA device is missing.
 """
 from .engine import (  # noqa: F401
     Engine, DycgError, BatchStats, GraphInfo, Edge, lib, library_path, edges_array,
-    gen_rmat_edges, hash_weight, measure_host_link, ALGOS, STATUS,
+    gen_rmat_edges, hash_weight, measure_host_link, mlp_infer, mlp_loss_grad, ALGOS, STATUS,
+    POLICY_F, POLICY_H, POLICY_PARAMS,
 )
 from . import operators  # noqa: F401
 

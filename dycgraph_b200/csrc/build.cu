@@ -283,6 +283,51 @@ __global__ void resolve_positions_kernel(const u64 *pos, u64 count, const u64 *p
   }
 }
 
+// One live out-edge of each given source, uniform over its live slots (up to
+// 16 random probes, then a scan); (INF32, INF32, 0) when the row is empty or
+// the source is out of range.
+__global__ void row_edges_kernel(Adj A, const uint32_t *sources, u64 count, u64 seed, uint32_t n,
+                                 uint32_t *out) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < count;
+       i += (u64)gridDim.x * blockDim.x) {
+    const uint32_t u = sources[i];
+    uint32_t v = INF32, w = 0, uu = INF32;
+    if (u < n && A.live[u] > 0) {
+      const u64 off = A.off[u];
+      const uint32_t len = A.len[u];
+      bool got = false;
+      for (int t = 0; t < 16 && !got; t++) {
+        const uint32_t k = (uint32_t)(mix64(seed ^ mix64(i * 16 + t + 1)) % len);
+        const uint2 pr = read_pair_rw(A, off + k);
+        if (!slot_deleted_rw(A, off + k, pr.x)) {
+          v = pr.x & VMASK;
+          w = pr.y;
+          got = true;
+        }
+      }
+      for (uint32_t k = 0; k < len && !got; k++) {
+        const uint2 pr = read_pair_rw(A, off + k);
+        if (!slot_deleted_rw(A, off + k, pr.x)) {
+          v = pr.x & VMASK;
+          w = pr.y;
+          got = true;
+        }
+      }
+      if (got) uu = u;
+    }
+    out[3 * i] = uu;
+    out[3 * i + 1] = v;
+    out[3 * i + 2] = w;
+  }
+}
+
+cudaError_t sample_row_edges(const Adj &A, const uint32_t *sources, u64 count, u64 seed,
+                             uint32_t n, uint32_t *out, cudaStream_t s) {
+  if (!count) return cudaSuccess;
+  row_edges_kernel<<<grid_for(count), BLOCK, 0, s>>>(A, sources, count, seed, n, out);
+  return cudaGetLastError();
+}
+
 cudaError_t sample_draw(u64 *pos, u64 count, u64 seed, u64 total, cudaStream_t s) {
   draw_positions_kernel<<<grid_for(count), BLOCK, 0, s>>>(pos, count, seed, total);
   return cudaGetLastError();

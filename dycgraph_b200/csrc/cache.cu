@@ -115,6 +115,27 @@ cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay, f
   return cudaGetLastError();
 }
 
+cudaError_t cache_rank_given(CacheWork &W, uint32_t npages, uint32_t K, float min_score,
+                             const uint32_t *page_slot, cudaStream_t s) {
+  size_t bytes = W.temp_bytes;
+  cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(
+      W.temp, bytes, W.score, W.score_sorted, W.ids, W.ids_sorted, (int)npages, 0, 32, s);
+  if (e != cudaSuccess) return e;
+  flag_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, W.score_sorted, npages, K,
+                                                 min_score, page_slot, W.fa, W.fe);
+  bytes = W.temp_bytes;
+  e = cub::DeviceScan::ExclusiveSum(W.temp, bytes, W.fa, W.sa, (int)npages, s);
+  if (e != cudaSuccess) return e;
+  bytes = W.temp_bytes;
+  e = cub::DeviceScan::ExclusiveSum(W.temp, bytes, W.fe, W.se, (int)npages, s);
+  if (e != cudaSuccess) return e;
+  cudaMemcpyAsync(W.h_counts + 0, W.sa + npages - 1, 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(W.h_counts + 1, W.fa + npages - 1, 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(W.h_counts + 2, W.se + npages - 1, 4, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(W.h_counts + 3, W.fe + npages - 1, 4, cudaMemcpyDeviceToHost, s);
+  return cudaGetLastError();
+}
+
 size_t cache_temp_bytes(uint32_t npages) {
   size_t a = 0, b = 0;
   cub::DeviceRadixSort::SortPairsDescending(nullptr, a, (const float *)nullptr, (float *)nullptr,

@@ -224,6 +224,57 @@ int dycg_apply_batches_device(dycg_engine *e, const dycg_edge *d_dels, const uin
   });
 }
 
+int dycg_set_cache_policy(dycg_engine *e, uint32_t policy) {
+  return guard(e, [&](Engine &g) { g.set_cache_policy(policy); });
+}
+
+int dycg_policy_trace(dycg_engine *e, uint32_t snapshots) {
+  return guard(e, [&](Engine &g) { g.policy_trace(snapshots); });
+}
+
+int dycg_policy_train(dycg_engine *e, uint32_t epochs, float lr, uint32_t batch, uint64_t seed,
+                      dycg_policy_report *report) {
+  return guard(e, [&](Engine &g) { g.policy_train(epochs, lr, batch, seed, report); });
+}
+
+int dycg_policy_params(dycg_engine *e, float *params) {
+  if (!params) return DYCG_EINVAL;
+  return guard(e, [&](Engine &g) { g.policy_params(params); });
+}
+
+int dycg_policy_set_params(dycg_engine *e, const float *params) {
+  if (!params) return DYCG_EINVAL;
+  return guard(e, [&](Engine &g) { g.policy_set_params(params); });
+}
+
+int dycg_mlp_infer(const void *d_x, uint32_t n, const float *d_params, float *d_out,
+                   void *stream) {
+  if ((!d_x || !d_out) && n) return DYCG_EINVAL;
+  if (!d_params) return DYCG_EINVAL;
+  if (!n) return DYCG_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dycg::launch_mlp_infer(d_x, n, d_params, d_out, nullptr, s) != cudaSuccess)
+    return DYCG_ECUDA;
+  return cudaStreamSynchronize(s) == cudaSuccess ? DYCG_OK : DYCG_ECUDA;
+}
+
+int dycg_mlp_loss_grad(const void *d_x, const float *d_y, uint32_t n, const float *d_params,
+                       float *d_grad, float *d_loss, void *stream) {
+  if ((!d_x || !d_y) && n) return DYCG_EINVAL;
+  if (!d_params || !d_grad || !d_loss) return DYCG_EINVAL;
+  if (!n) return DYCG_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dycg::launch_mlp_grad(d_x, d_y, n, n, 0, d_params, 2.f, d_grad, d_loss, s) != cudaSuccess)
+    return DYCG_ECUDA;
+  return cudaStreamSynchronize(s) == cudaSuccess ? DYCG_OK : DYCG_ECUDA;
+}
+
+int dycg_sample_row_edges(dycg_engine *e, const uint32_t *sources, uint64_t count, uint64_t seed,
+                          dycg_edge *out) {
+  if ((!sources || !out) && count) return DYCG_EINVAL;
+  return guard(e, [&](Engine &g) { g.sample_row_edges(sources, count, seed, out); });
+}
+
 int dycg_stream(dycg_engine *e, void **stream) {
   if (!stream) return DYCG_EINVAL;
   return guard(e, [&](Engine &g) { *stream = (void *)g.stream(); });

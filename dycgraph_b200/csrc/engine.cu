@@ -53,6 +53,8 @@ Engine::Engine(const dycg_options &opt) : opt_(opt) {
   if (!coop) throw Error(DYCG_ENOGPU, "device lacks cooperative launch");
   CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
   for (auto &e : ev_) CK(cudaEventCreate(&e));
+  if (opt_.cache_policy > DYCG_CACHE_LEARNED) throw Error(DYCG_EINVAL, "unknown cache policy");
+  policy_ = opt_.cache_policy;
   stored_ = opt_.algo == DYCG_ALGO_SSSP && opt_.weight_mode == DYCG_WEIGHT_STORED;
   has_in_ = !opt_.symmetric && opt_.algo != DYCG_ALGO_PR;
 }
@@ -64,6 +66,10 @@ Engine::~Engine() {
   if (h_rec_) cudaFreeHost(h_rec_);
   if (d_rec_) cudaFree(d_rec_);
   if (h_bctl_) cudaFreeHost(h_bctl_);
+  if (tx_) cudaFree(tx_);
+  if (ty_) cudaFree(ty_);
+  for (auto &e : pev_)
+    if (e) cudaEventDestroy(e);
   dfree_all();
   for (void *p : hallocs_) cudaFreeHost(p);
   for (auto &e : ev_)
@@ -148,7 +154,8 @@ void Engine::build_direction(Arena &A, const u64 *keys, const uint32_t *wv, u64 
   CK(cudaMemcpyAsync(&total, A.off + n, 8, cudaMemcpyDeviceToHost, st_));
   sync_check("layout");
   const u64 page = 1ull << page_shift_;
-  const u64 head = std::max<u64>(total / 8, 1ull << 20);
+  const u64 permille = opt_.arena_headroom_permille ? opt_.arena_headroom_permille : 125;
+  const u64 head = std::max<u64>(total / 1000 * permille, 1ull << 20);
   A.slots = round_up(total + head, page);
   A.pages = (uint32_t)(A.slots >> page_shift_);
   A.stride = stored_ ? 2 : 1;
@@ -469,6 +476,7 @@ void Engine::init() {
   if (inited_) throw Error(DYCG_ESTATE, "engine already initialised");
   CK(cudaMemsetAsync(ctl_, 0, sizeof(Ctl), st_));
   const u64 timeout = 120ull * 1000000000ull;
+  if (policy_ == DYCG_CACHE_LEARNED) policy_alloc();
   if (nq_) {
     init_queries(timeout);
     inited_ = true;
@@ -682,6 +690,9 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
     launches_ += (nd ? 1 : 0) + (na ? 1 : 0);
   }
   if (!capture) CK(cudaEventRecord(ev_[1], st_));
+  // learned admission / trace features, between ingest and mutation
+  if (!capture && feat_ && (policy_ == DYCG_CACHE_LEARNED || trace_n_ < trace_cap_))
+    policy_prefetch(nd, na);
   const u64 timeout = 60ull * 1000000000ull;
   PrLaunch PL{};
   if (opt_.algo == DYCG_ALGO_PR) {
@@ -863,6 +874,11 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     stats->mutate_hbm_bytes = c.stat[ST_MUT_HBM_BYTES];
     stats->ms_ingest = ms[0];
     stats->ms_mutate = ms[1];
+    if (prefetched_) {  // the learned admission ran inside the mutation stage's events
+      float pm = 0;
+      cudaEventElapsedTime(&pm, pev_[0], pev_[1]);
+      stats->ms_mutate -= pm;
+    }
     stats->ms_repair = ms[2];
   }
   if (maintenance) cache_maintenance(false, stats);
@@ -1246,8 +1262,10 @@ void Engine::apply_batches(const dycg_edge *dels, const uint64_t *nd, const dycg
     mx = std::max<u64>(mx, std::max(nd[i], na[i]));
   }
   if ((td && !dels) || (ta && !adds)) throw Error(DYCG_EINVAL, "null update array");
-  if (!(nq_ && qmode_ == DYCG_QUERIES_BATCHED)) {
-    // other forms: one ordinary apply per snapshot
+  if (!(nq_ && qmode_ == DYCG_QUERIES_BATCHED) || policy_ == DYCG_CACHE_LEARNED ||
+      trace_n_ < trace_cap_) {
+    // other forms, the learned policy (its admission synchronises with the
+    // host mid-snapshot) and trace recording: one ordinary apply per snapshot
     u64 od = 0, oa = 0;
     for (uint32_t i = 0; i < count; i++) {
       apply(dels + od, nd[i], adds + oa, na[i], device_ptrs, 0, true, stats ? stats + i : nullptr);
@@ -1376,8 +1394,245 @@ void Engine::apply_batches(const dycg_edge *dels, const uint64_t *nd, const dycg
   }
 }
 
+// ---- learned cache admission policy -------------------------------------------
+
+void Engine::policy_alloc() {
+  check_loaded();
+  if (feat_) return;
+  const u64 np = npages_;
+  feat_ = dmalloc(np * POLICY_F * 2);
+  hist_ = (float *)dmalloc(np * 4 * 4);
+  age_ = (uint8_t *)dmalloc(np);
+  prows_ = (uint32_t *)dmalloc(np * 4);
+  pmax_ = (uint32_t *)dmalloc(np * 4);
+  pdelta_ = (uint32_t *)dmalloc(np * 4);
+  CK(cudaMemsetAsync(hist_, 0, np * 16, st_));
+  CK(cudaMemsetAsync(age_, 0xFF, np, st_));
+  params_ = (float *)dmalloc(POLICY_PARAMS * 4);
+  grad_ = (float *)dmalloc(POLICY_PARAMS * 4);
+  adam_m_ = (float *)dmalloc(POLICY_PARAMS * 4);
+  adam_v_ = (float *)dmalloc(POLICY_PARAMS * 4);
+  ploss_ = (float *)dmalloc(16);
+  CK(cudaMemsetAsync(grad_, 0, POLICY_PARAMS * 4, st_));
+  CK(cudaMemsetAsync(adam_m_, 0, POLICY_PARAMS * 4, st_));
+  CK(cudaMemsetAsync(adam_v_, 0, POLICY_PARAMS * 4, st_));
+  // Glorot-uniform weights from a fixed seed, zero biases
+  std::vector<float> p(POLICY_PARAMS, 0.f);
+  auto fill = [&](int off, int fan_in, int fan_out, u64 tag) {
+    const float a = std::sqrt(6.f / (fan_in + fan_out));
+    for (int i = 0; i < fan_in * fan_out; i++) {
+      const double u = (double)(mix64(tag ^ mix64((u64)i + 1)) >> 11) / 9007199254740992.0;
+      p[off + i] = (float)((2.0 * u - 1.0) * a);
+    }
+  };
+  const int F = POLICY_F, H = POLICY_H;
+  fill(0, F, H, 0x5031);
+  fill(F * H + H, H, H, 0x5032);
+  fill(F * H + H + H * H + H, H, 1, 0x5033);
+  CK(cudaMemcpyAsync(params_, p.data(), POLICY_PARAMS * 4, cudaMemcpyHostToDevice, st_));
+  CK(cudaEventCreate(&pev_[0]));
+  CK(cudaEventCreate(&pev_[1]));
+  sync_check("policy alloc");
+  policy_bytes_ = np * (POLICY_F * 2 + 16 + 1 + 12) + 4ull * POLICY_PARAMS * 4;
+}
+
+void Engine::set_cache_policy(uint32_t policy) {
+  check_loaded();
+  if (policy != DYCG_CACHE_HOTNESS && policy != DYCG_CACHE_LEARNED)
+    throw Error(DYCG_EINVAL, "switchable policies: DYCG_CACHE_HOTNESS, DYCG_CACHE_LEARNED");
+  if (!cache_slots_) throw Error(DYCG_ESTATE, "no HBM page cache (budget or policy NONE at create)");
+  if (policy == DYCG_CACHE_LEARNED) policy_alloc();
+  policy_ = policy;
+  drop_graphs();
+}
+
+void Engine::policy_trace(uint32_t snapshots) {
+  check_loaded();
+  policy_alloc();
+  if (tx_) cudaFree(tx_);
+  if (ty_) cudaFree(ty_);
+  tx_ = nullptr;
+  ty_ = nullptr;
+  trace_cap_ = trace_n_ = 0;
+  if (!snapshots) return;
+  CK(cudaMalloc(&tx_, (u64)snapshots * npages_ * POLICY_F * 2));
+  CK(cudaMalloc((void **)&ty_, (u64)snapshots * npages_ * 4));
+  trace_cap_ = snapshots;
+  drop_graphs();
+}
+
+// Features of the snapshot being applied (after ingest, before mutation);
+// under the learned policy, admit the pages the network ranks highest.
+void Engine::policy_prefetch(size_t nd, size_t na) {
+  const u64 np = npages_;
+  CK(cudaEventRecord(pev_[0], st_));
+  CK(cudaMemsetAsync(prows_, 0, np * 4, st_));
+  CK(cudaMemsetAsync(pmax_, 0, np * 4, st_));
+  CK(cudaMemsetAsync(pdelta_, 0, np * 4, st_));
+  CK(launch_page_rows(out_.off, out_.len, n_, out_.page_base, page_shift_, prows_, pmax_, st_));
+  if (has_in_)
+    CK(launch_page_rows(in_.off, in_.len, n_, in_.page_base, page_shift_, prows_, pmax_, st_));
+  if (nd) {
+    CK(launch_page_delta(k_del_out_, (uint32_t)nd, out_.off, out_.page_base, page_shift_, pdelta_,
+                         st_));
+    if (has_in_)
+      CK(launch_page_delta(k_del_in_, (uint32_t)nd, in_.off, in_.page_base, page_shift_, pdelta_,
+                           st_));
+  }
+  if (na) {
+    CK(launch_page_delta(k_add_out_, (uint32_t)na, out_.off, out_.page_base, page_shift_, pdelta_,
+                         st_));
+    if (has_in_)
+      CK(launch_page_delta(k_add_in_, (uint32_t)na, in_.off, in_.page_base, page_shift_, pdelta_,
+                           st_));
+  }
+  CK(launch_features(hist_, age_, pdelta_, prows_, pmax_, npages_, feat_, st_));
+  launches_ += 3 + (has_in_ ? 1 : 0) + (nd ? 1 : 0) * (has_in_ ? 2 : 1) +
+               (na ? 1 : 0) * (has_in_ ? 2 : 1);
+  trace_pending_ = trace_n_ < trace_cap_;
+  if (trace_pending_)
+    CK(cudaMemcpyAsync((char *)tx_ + (u64)trace_n_ * np * POLICY_F * 2, feat_,
+                       np * POLICY_F * 2, cudaMemcpyDeviceToDevice, st_));
+  prefetch_loaded_ = prefetch_evicted_ = 0;
+  if (policy_ == DYCG_CACHE_LEARNED && cache_slots_) {
+    CK(launch_mlp_infer(feat_, npages_, params_, cwk_.score, cwk_.ids, st_));
+    // admit pages predicted to be read at least ~64 times in this snapshot
+    CK(cache_rank_given(cwk_, npages_, cache_slots_, std::log1p(64.f), page_slot_, st_));
+    launches_ += 6;
+    sync_check("learned rank");
+    const uint32_t n_admit = cwk_.h_counts[0] + cwk_.h_counts[1];
+    const uint32_t n_evict_cand = cwk_.h_counts[2] + cwk_.h_counts[3];
+    const uint32_t cap = std::max<uint32_t>(cache_slots_ / learned_cap_div_, 256u);
+    uint32_t admit = std::min(n_admit, cap);
+    const uint32_t need = admit > free_count_ ? admit - free_count_ : 0u;
+    const uint32_t evict = std::min(n_evict_cand, need);
+    admit = std::min(admit, free_count_ + evict);
+    if (admit) {
+      CachePages pg{out_.d_dst, has_in_ ? in_.d_dst : nullptr, out_.pages, page_shift_,
+                    out_.stride, cdst_};
+      CK(cache_apply(cwk_, npages_, n_evict_cand, evict, admit, page_slot_, free_list_,
+                     free_count_, pg, st_));
+      free_count_ = free_count_ + evict - admit;
+      pages_loaded_ += admit;
+      pages_evicted_ += evict;
+      launches_ += 3;
+    }
+    prefetch_loaded_ = admit;
+    prefetch_evicted_ = evict;
+  }
+  CK(cudaEventRecord(pev_[1], st_));
+  prefetched_ = true;
+}
+
+void Engine::policy_train(uint32_t epochs, float lr, uint32_t batch, uint64_t seed,
+                          dycg_policy_report *rep) {
+  check_loaded();
+  if (!trace_n_) throw Error(DYCG_ESTATE, "no access traces recorded (dycg_policy_trace)");
+  if (batch == 0 || !(lr > 0.f)) throw Error(DYCG_EINVAL, "batch and lr must be positive");
+  const u64 total = (u64)trace_n_ * npages_;
+  auto eval = [&]() {
+    CK(cudaMemsetAsync(ploss_, 0, 4, st_));
+    for (u64 o = 0; o < total; o += (1ull << 30)) {
+      const uint32_t c = (uint32_t)std::min<u64>(1ull << 30, total - o);
+      CK(launch_mlp_grad((const char *)tx_ + o * POLICY_F * 2, ty_ + o, c, c, 0, params_, 0.f,
+                         grad_, ploss_, st_));
+    }
+    CK(cudaMemsetAsync(grad_, 0, POLICY_PARAMS * 4, st_));
+    float l = 0;
+    CK(cudaMemcpyAsync(&l, ploss_, 4, cudaMemcpyDeviceToHost, st_));
+    sync_check("policy eval");
+    return l / (float)total;
+  };
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, st_));
+  const float l0 = eval();
+  const u64 steps = std::max<u64>(1, (u64)epochs * total / batch);
+  for (u64 s = 0; s < steps; s++) {
+    CK(launch_mlp_grad(tx_, ty_, total, batch, mix64(seed + s + 1) | 1, params_, 2.f / batch,
+                       grad_, ploss_, st_));
+    CK(launch_adam(params_, grad_, adam_m_, adam_v_, lr, ++adam_step_, st_));
+  }
+  const float l1 = eval();
+  CK(cudaEventRecord(b, st_));
+  sync_check("policy train");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (rep) {
+    std::memset(rep, 0, sizeof(*rep));
+    rep->samples = total;
+    rep->steps = steps;
+    rep->loss_before = l0;
+    rep->loss_after = l1;
+    rep->ms = ms;
+  }
+}
+
+void Engine::policy_params(float *out) {
+  policy_alloc();
+  CK(cudaMemcpyAsync(out, params_, POLICY_PARAMS * 4, cudaMemcpyDeviceToHost, st_));
+  sync_check("policy params");
+}
+
+void Engine::policy_set_params(const float *in) {
+  policy_alloc();
+  CK(cudaMemcpyAsync(params_, in, POLICY_PARAMS * 4, cudaMemcpyHostToDevice, st_));
+  sync_check("policy set params");
+}
+
+void Engine::sample_row_edges(const uint32_t *sources, uint64_t count, uint64_t seed,
+                              dycg_edge *out) {
+  check_loaded();
+  if (!count) return;
+  uint32_t *d_src = nullptr, *d_out = nullptr;
+  CK(cudaMalloc(&d_src, count * 4));
+  const cudaError_t e0 = cudaMalloc(&d_out, count * 12);
+  if (e0 != cudaSuccess) {
+    cudaFree(d_src);
+    CK(e0);
+  }
+  cudaError_t e = cudaMemcpyAsync(d_src, sources, count * 4, cudaMemcpyHostToDevice, st_);
+  if (e == cudaSuccess) e = dycg::sample_row_edges(adj(out_), d_src, count, seed, n_, d_out, st_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, count * 12, cudaMemcpyDeviceToHost, st_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+  cudaFree(d_src);
+  cudaFree(d_out);
+  CK(e);
+}
+
 void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
   check_loaded();
+  if (feat_ && !initial) {
+    // page-read history for the learned policy, and the training target of
+    // the features taken at this snapshot's start when traces are recorded
+    float *target = trace_pending_ ? ty_ + (u64)trace_n_ * npages_ : nullptr;
+    const bool clear = policy_ != DYCG_CACHE_HOTNESS || !cache_slots_;
+    CK(launch_history(page_hits_, hist_, age_, npages_, target, clear, st_));
+    launches_++;
+    if (trace_pending_) trace_n_++;
+    trace_pending_ = false;
+  }
+  if (policy_ == DYCG_CACHE_LEARNED && !initial) {
+    // admission ran before the repair (policy_prefetch); the call ends here
+    CK(cudaEventRecord(ev_[5], st_));
+    if (prefetched_ && stats) {
+      sync_check("learned maintenance");
+      float ms = 0;
+      cudaEventElapsedTime(&ms, pev_[0], pev_[1]);
+      stats->ms_cache = ms;
+      stats->cache_pages_loaded = prefetch_loaded_;
+      stats->cache_pages_evicted = prefetch_evicted_;
+      const u64 page_bytes = (4ull << page_shift_) * out_.stride;
+      stats->link_bytes += (u64)prefetch_loaded_ * page_bytes;
+      stats->hbm_adj_bytes += (u64)prefetch_loaded_ * page_bytes;
+    }
+    prefetched_ = false;
+    return;
+  }
+  prefetched_ = false;
   if (!cache_slots_) {
     CK(cudaMemsetAsync(page_hits_, 0, (u64)npages_ * 4, st_));
     return;
@@ -1528,7 +1783,7 @@ void Engine::info(dycg_graph_info *out) {
   out->host_bytes = out->arena_slots * 4 * out_.stride;
   out->device_bytes = (u64)n_ * (8 + 4 * 6) + (u64)n_ * (has_in_ ? 48 : 24) +
                       ((u64)cache_slots_ << page_shift_) * 4 * out_.stride + index_bytes_ +
-                      qbytes_;
+                      qbytes_ + policy_bytes_;
   out->reserved[0] = index_bytes_;  // fence index + deletion bitmap (part of the budget)
   out->page_shift = page_shift_;
   out->has_incoming = has_in_ ? 1 : 0;

@@ -65,6 +65,14 @@ class Engine {
   void apply_batches(const dycg_edge *dels, const uint64_t *nd, const dycg_edge *adds,
                      const uint64_t *na, uint32_t count, bool device_ptrs, dycg_batch_stats *stats);
   uint32_t queries() const { return nq_; }
+  // learned cache admission
+  void set_cache_policy(uint32_t policy);
+  void policy_trace(uint32_t snapshots);
+  void policy_train(uint32_t epochs, float lr, uint32_t batch, uint64_t seed,
+                    dycg_policy_report *rep);
+  void policy_params(float *out);
+  void policy_set_params(const float *in);
+  void sample_row_edges(const uint32_t *sources, uint64_t count, uint64_t seed, dycg_edge *out);
   cudaStream_t stream() const { return st_; }
 
   std::string last_error;
@@ -90,6 +98,8 @@ class Engine {
   };
   const SnapshotGraph &graph_for(uint32_t cls);
   void drop_graphs();
+  void policy_alloc();
+  void policy_prefetch(size_t nd, size_t na);
   void init_queries(u64 timeout);
   void repair_queries(uint32_t nd, uint32_t na, u64 timeout);
   MultiLaunch multi_launch(uint32_t phases, uint32_t n_add, u64 timeout);
@@ -147,6 +157,23 @@ class Engine {
   uint32_t bctl_cap_ = 0;
   void *h_rec_ = nullptr, *d_rec_ = nullptr;
   u64 hrec_bytes_ = 0;
+
+  // learned cache admission (policy.cu): features, history, network, traces
+  uint32_t policy_ = 0;
+  void *feat_ = nullptr;
+  float *hist_ = nullptr;
+  uint8_t *age_ = nullptr;
+  uint32_t *prows_ = nullptr, *pmax_ = nullptr, *pdelta_ = nullptr;
+  float *params_ = nullptr, *grad_ = nullptr, *adam_m_ = nullptr, *adam_v_ = nullptr,
+        *ploss_ = nullptr;
+  uint32_t adam_step_ = 0;
+  void *tx_ = nullptr;
+  float *ty_ = nullptr;
+  uint32_t trace_cap_ = 0, trace_n_ = 0;
+  bool trace_pending_ = false, prefetched_ = false;
+  uint32_t prefetch_loaded_ = 0, prefetch_evicted_ = 0, learned_cap_div_ = 64;
+  cudaEvent_t pev_[2] = {};
+  u64 policy_bytes_ = 0;
 
   // batch buffers
   size_t bcap_ = 0;

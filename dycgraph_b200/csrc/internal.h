@@ -155,6 +155,35 @@ cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t n_evict_cand, ui
                         uint32_t admit, uint32_t *page_slot, uint32_t *free_list,
                         uint32_t free_count, const CachePages &pg, cudaStream_t s);
 
+// cache given precomputed scores (W.score, W.ids filled): sort, flags, counts
+cudaError_t cache_rank_given(CacheWork &W, uint32_t npages, uint32_t K, float min_score,
+                             const uint32_t *page_slot, cudaStream_t s);
+
+// learned admission policy (policy.cu)
+constexpr int POLICY_F = 8, POLICY_H = 64;
+constexpr int POLICY_PARAMS = POLICY_F * POLICY_H + POLICY_H + POLICY_H * POLICY_H + POLICY_H +
+                              POLICY_H + 1;
+size_t mlp_grad_smem();
+cudaError_t launch_page_rows(const u64 *off, const uint32_t *len, uint32_t n, uint32_t page_base,
+                             uint32_t page_shift, uint32_t *rows, uint32_t *maxlen,
+                             cudaStream_t s);
+cudaError_t launch_page_delta(const u64 *keys, uint32_t cnt, const u64 *off, uint32_t page_base,
+                              uint32_t page_shift, uint32_t *delta, cudaStream_t s);
+cudaError_t launch_features(const float *hist, const uint8_t *age, const uint32_t *delta,
+                            const uint32_t *rows, const uint32_t *maxlen, uint32_t npages,
+                            void *x, cudaStream_t s);
+cudaError_t launch_history(uint32_t *hits, float *hist, uint8_t *age, uint32_t npages,
+                           float *target, bool clear, cudaStream_t s);
+cudaError_t launch_mlp_infer(const void *x, uint32_t n, const float *params, float *score,
+                             uint32_t *ids, cudaStream_t s);
+cudaError_t launch_mlp_grad(const void *x, const float *y, uint64_t total, uint32_t count,
+                            uint64_t sample_seed, const float *params, float scale, float *grad,
+                            float *loss, cudaStream_t s);
+cudaError_t launch_adam(float *p, float *g, float *m, float *v, float lr, uint32_t step,
+                        cudaStream_t s);
+cudaError_t sample_row_edges(const Adj &A, const uint32_t *sources, u64 count, u64 seed,
+                             uint32_t n, uint32_t *out, cudaStream_t s);
+
 // build
 cudaError_t build_gen_rmat(u64 *keys, u64 draws, u64 seed, uint32_t scale, double a, double b,
                            double c, int symmetrize, cudaStream_t s);

@@ -1,0 +1,366 @@
+// policy.cu -- learned cache admission: per-page features, a BF16 MLP served
+// and trained by the kernels below, and the per-snapshot bookkeeping that
+// records access traces.
+//
+// No reference counterpart: the reference admits rows by a decayed activity
+// count (include/framework/variants/driver.cuh:486-515, comp_hotness_sssp),
+// which stays here as the hotness policy (cache.cu) and as the yardstick.
+//
+// Unit: one cache page (2^page_shift adjacency slots). Features per page
+// (POLICY_F = 8, BF16):
+//   0-3  log1p(slot reads of the page in each of the last four snapshots)
+//   4    log1p(update records of the current batch whose row starts in the page)
+//   5    min(snapshots since the page was last read, 16) / 16
+//   6    log1p(rows starting in the page) / 8
+//   7    log1p(longest row starting in the page) / 16
+// Target: log1p(slot reads of the page during the current snapshot). The
+// network is POLICY_F -> 64 -> 64 -> 1, ReLU, BF16 weights and inputs, FP32
+// accumulation and FP32 master weights; loss = mean squared error.
+//
+// The MLP is 4.7K multiply-adds per page (~5 GMAC for a million pages, well
+// under a millisecond on the CUDA cores); it is not worth tensor-core tiles.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace dycg {
+
+namespace {
+
+constexpr int F = POLICY_F, H = POLICY_H;
+constexpr int OFF_W1 = 0, OFF_B1 = F * H, OFF_W2 = OFF_B1 + H, OFF_B2 = OFF_W2 + H * H,
+              OFF_W3 = OFF_B2 + H, OFF_B3 = OFF_W3 + H;
+static_assert(OFF_B3 + 1 == POLICY_PARAMS, "parameter layout");
+
+__device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// Parameters into shared memory, BF16-rounded (the precision the MLP runs at).
+__device__ __forceinline__ void load_params(const float *p, float *s) {
+  for (int i = threadIdx.x; i < POLICY_PARAMS; i += blockDim.x) s[i] = bf(p[i]);
+  __syncthreads();
+}
+
+int grid_for(u64 threads) {
+  u64 b = (threads + BLOCK - 1) / BLOCK;
+  if (b < 1) b = 1;
+  if (b > 148ull * 32) b = 148ull * 32;
+  return (int)b;
+}
+
+}  // namespace
+
+// ---- features ----------------------------------------------------------------
+
+// Rows starting in each page and the longest of them (one arena).
+__global__ void page_rows_kernel(const u64 *off, const uint32_t *len, uint32_t n,
+                                 uint32_t page_base, uint32_t page_shift, uint32_t *rows,
+                                 uint32_t *maxlen) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t l = len[v];
+    if (!l) continue;
+    const uint32_t p = page_base + (uint32_t)(off[v] >> page_shift);
+    atomicAdd(rows + p, 1u);
+    atomicMax(maxlen + p, l);
+  }
+}
+
+// Update records per page: each sorted batch key (row << 32 | neighbour) names
+// the row it touches in this arena.
+__global__ void page_delta_kernel(const u64 *keys, uint32_t cnt, const u64 *off,
+                                  uint32_t page_base, uint32_t page_shift, uint32_t *delta) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    const u64 k = keys[i];
+    if (k == KEY_INF) continue;
+    atomicAdd(delta + page_base + (uint32_t)(off[(uint32_t)(k >> 32)] >> page_shift), 1u);
+  }
+}
+
+__global__ void features_kernel(const float *hist, const uint8_t *age, const uint32_t *delta,
+                                const uint32_t *rows, const uint32_t *maxlen, uint32_t npages,
+                                __nv_bfloat16 *x) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npages;
+       p += gridDim.x * blockDim.x) {
+    float f[F];
+    for (int k = 0; k < 4; k++) f[k] = hist[(u64)k * npages + p];
+    f[4] = log1pf((float)delta[p]);
+    f[5] = fminf((float)age[p], 16.f) / 16.f;
+    f[6] = log1pf((float)rows[p]) / 8.f;
+    f[7] = log1pf((float)maxlen[p]) / 16.f;
+    __align__(16) __nv_bfloat16 o[F];
+    for (int k = 0; k < F; k++) o[k] = __float2bfloat16_rn(f[k]);
+    *reinterpret_cast<uint4 *>(x + (u64)p * F) = *reinterpret_cast<const uint4 *>(o);
+  }
+}
+
+// End of a snapshot: shift this snapshot's page reads into the history,
+// update ages, optionally write the training target for the features taken
+// at the snapshot's start, and clear the counters (unless the hotness policy
+// still has to read them).
+__global__ void history_kernel(uint32_t *hits, float *hist, uint8_t *age, uint32_t npages,
+                               float *target, bool clear) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npages;
+       p += gridDim.x * blockDim.x) {
+    const float y = log1pf((float)hits[p]);
+    hist[3ull * npages + p] = hist[2ull * npages + p];
+    hist[2ull * npages + p] = hist[1ull * npages + p];
+    hist[1ull * npages + p] = hist[p];
+    hist[p] = y;
+    age[p] = hits[p] ? 0 : (uint8_t)min(255, age[p] + 1);
+    if (target) target[p] = y;
+    if (clear) hits[p] = 0;
+  }
+}
+
+// ---- inference -----------------------------------------------------------------
+
+// score[p] = MLP(x[p]); ids[p] = p (for the admission sort).
+__global__ void __launch_bounds__(BLOCK) mlp_infer_kernel(const __nv_bfloat16 *x, uint32_t n,
+                                                          const float *params, float *score,
+                                                          uint32_t *ids) {
+  __shared__ float w[POLICY_PARAMS];
+  load_params(params, w);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    float in[F];
+    const uint4 raw = *reinterpret_cast<const uint4 *>(x + (u64)p * F);
+    const __nv_bfloat16 *xb = reinterpret_cast<const __nv_bfloat16 *>(&raw);
+#pragma unroll
+    for (int k = 0; k < F; k++) in[k] = __bfloat162float(xb[k]);
+    // layer 2 accumulated hidden unit by hidden unit: 64 accumulators, no
+    // stored first layer
+    float acc[H];
+#pragma unroll
+    for (int j = 0; j < H; j++) acc[j] = w[OFF_B2 + j];
+#pragma unroll 1
+    for (int i = 0; i < H; i++) {
+      float a = w[OFF_B1 + i];
+#pragma unroll
+      for (int k = 0; k < F; k++) a = fmaf(in[k], w[OFF_W1 + k * H + i], a);
+      const float h = fmaxf(a, 0.f);
+#pragma unroll
+      for (int j = 0; j < H; j++) acc[j] = fmaf(h, w[OFF_W2 + i * H + j], acc[j]);
+    }
+    float y = w[OFF_B3];
+#pragma unroll
+    for (int j = 0; j < H; j++) y = fmaf(fmaxf(acc[j], 0.f), w[OFF_W3 + j], y);
+    score[p] = y;
+    if (ids) ids[p] = p;
+  }
+}
+
+// ---- training ------------------------------------------------------------------
+
+constexpr int TS = 128;     // samples per tile
+constexpr int HP = H + 1;   // padded activation row (bank-conflict free)
+
+// Loss and gradient over samples: sample s of the pass is row idx(s) of x
+// (idx = identity, or a seeded draw when sample_seed != 0 and total > 0).
+// Gradients (FP32, w.r.t. the BF16-rounded parameters) and the summed squared
+// error are added into grad[] and *loss. scale multiplies the gradient
+// (2/batch for a mean).
+__global__ void __launch_bounds__(BLOCK) mlp_grad_kernel(const __nv_bfloat16 *x, const float *y,
+                                                         uint64_t total, uint32_t count,
+                                                         uint64_t sample_seed, const float *params,
+                                                         float scale, float *grad, float *loss) {
+  extern __shared__ float sm[];
+  float *w = sm;                          // POLICY_PARAMS
+  float *X = w + POLICY_PARAMS;           // TS x F
+  float *A1 = X + TS * F;                 // TS x HP: H1, then dH1
+  float *A2 = A1 + TS * HP;               // TS x HP: H2, then dH2
+  float *T = A2 + TS * HP;                // TS: target, then dy
+  load_params(params, w);
+  const int t = threadIdx.x;
+  float gW2[H * H / BLOCK] = {}, gW1[F * H / BLOCK] = {};
+  float gb1 = 0, gb2 = 0, gW3 = 0, gb3 = 0, lsum = 0;
+  const uint32_t tiles = (count + TS - 1) / TS;
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const uint32_t s0 = tile * TS;
+    const int ns = (int)min((uint32_t)TS, count - s0);
+    // load inputs and targets
+    for (int e = t; e < TS * F; e += BLOCK) {
+      const int s = e / F, k = e % F;
+      float v = 0.f;
+      if (s < ns) {
+        u64 r = s0 + s;
+        if (sample_seed) r = mix64(sample_seed ^ mix64(r)) % total;
+        v = __bfloat162float(x[r * F + k]);
+        if (k == 0) T[s] = y[r];
+      }
+      X[s * F + k] = v;
+    }
+    __syncthreads();
+    // H1 = relu(X W1 + b1)
+    for (int e = t; e < TS * H; e += BLOCK) {
+      const int s = e / H, i = e % H;
+      float a = w[OFF_B1 + i];
+#pragma unroll
+      for (int k = 0; k < F; k++) a = fmaf(X[s * F + k], w[OFF_W1 + k * H + i], a);
+      A1[s * HP + i] = fmaxf(a, 0.f);
+    }
+    __syncthreads();
+    // H2 = relu(H1 W2 + b2)
+    for (int e = t; e < TS * H; e += BLOCK) {
+      const int s = e / H, j = e % H;
+      float a = w[OFF_B2 + j];
+      for (int i = 0; i < H; i++) a = fmaf(A1[s * HP + i], w[OFF_W2 + i * H + j], a);
+      A2[s * HP + j] = fmaxf(a, 0.f);
+    }
+    __syncthreads();
+    // y = H2 W3 + b3; dy = scale * (y - target)
+    if (t < TS) {
+      float d = 0.f;
+      if (t < ns) {
+        float a = w[OFF_B3];
+        for (int j = 0; j < H; j++) a = fmaf(A2[t * HP + j], w[OFF_W3 + j], a);
+        d = a - T[t];
+        lsum += d * d;
+      }
+      T[t] = scale * d;
+    }
+    __syncthreads();
+    // gW3, gb3 (need H2), then dH2 in place
+    if (t < H) {
+      float a = 0.f;
+      for (int s = 0; s < ns; s++) a = fmaf(A2[s * HP + t], T[s], a);
+      gW3 += a;
+    }
+    if (t == 0)
+      for (int s = 0; s < ns; s++) gb3 += T[s];
+    __syncthreads();
+    for (int e = t; e < TS * H; e += BLOCK) {
+      const int s = e / H, j = e % H;
+      A2[s * HP + j] = A2[s * HP + j] > 0.f ? T[s] * w[OFF_W3 + j] : 0.f;
+    }
+    __syncthreads();
+    // gW2[i][j] += sum_s H1[s][i] dH2[s][j]; gb2[j] += sum_s dH2[s][j]
+#pragma unroll
+    for (int r = 0; r < H * H / BLOCK; r++) {
+      const int e = t + r * BLOCK, i = e / H, j = e % H;
+      float a = 0.f;
+      for (int s = 0; s < ns; s++) a = fmaf(A1[s * HP + i], A2[s * HP + j], a);
+      gW2[r] += a;
+    }
+    if (t < H) {
+      float a = 0.f;
+      for (int s = 0; s < ns; s++) a += A2[s * HP + t];
+      gb2 += a;
+    }
+    __syncthreads();
+    // dH1 = mask(H1) * (dH2 W2^T), in place
+    for (int e = t; e < TS * H; e += BLOCK) {
+      const int s = e / H, i = e % H;
+      float a = 0.f;
+      if (A1[s * HP + i] > 0.f)
+        for (int j = 0; j < H; j++) a = fmaf(A2[s * HP + j], w[OFF_W2 + i * H + j], a);
+      A1[s * HP + i] = a;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < F * H / BLOCK; r++) {
+      const int e = t + r * BLOCK, k = e / H, i = e % H;
+      float a = 0.f;
+      for (int s = 0; s < ns; s++) a = fmaf(X[s * F + k], A1[s * HP + i], a);
+      gW1[r] += a;
+    }
+    if (t < H) {
+      float a = 0.f;
+      for (int s = 0; s < ns; s++) a += A1[s * HP + t];
+      gb1 += a;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < H * H / BLOCK; r++) atomicAdd(grad + OFF_W2 + t + r * BLOCK, gW2[r]);
+#pragma unroll
+  for (int r = 0; r < F * H / BLOCK; r++) atomicAdd(grad + OFF_W1 + t + r * BLOCK, gW1[r]);
+  if (t < H) {
+    atomicAdd(grad + OFF_B1 + t, gb1);
+    atomicAdd(grad + OFF_B2 + t, gb2);
+    atomicAdd(grad + OFF_W3 + t, gW3);
+  }
+  if (t == 0) atomicAdd(grad + OFF_B3, gb3);
+  for (int o = 16; o; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
+  if ((t & 31) == 0 && lsum != 0.f) atomicAdd(loss, lsum);
+}
+
+// Adam on the FP32 master parameters; clears the gradient.
+__global__ void adam_kernel(float *p, float *g, float *m, float *v, float lr, float b1, float b2,
+                            float eps, float c1, float c2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < POLICY_PARAMS;
+       i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    m[i] = b1 * m[i] + (1.f - b1) * gi;
+    v[i] = b2 * v[i] + (1.f - b2) * gi * gi;
+    p[i] -= lr * (m[i] / c1) / (sqrtf(v[i] / c2) + eps);
+    g[i] = 0.f;
+  }
+}
+
+// ---- launchers -----------------------------------------------------------------
+
+size_t mlp_grad_smem() {
+  return sizeof(float) * (POLICY_PARAMS + TS * F + 2 * TS * HP + TS);
+}
+
+cudaError_t launch_page_rows(const u64 *off, const uint32_t *len, uint32_t n, uint32_t page_base,
+                             uint32_t page_shift, uint32_t *rows, uint32_t *maxlen,
+                             cudaStream_t s) {
+  page_rows_kernel<<<grid_for(n), BLOCK, 0, s>>>(off, len, n, page_base, page_shift, rows, maxlen);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_page_delta(const u64 *keys, uint32_t cnt, const u64 *off, uint32_t page_base,
+                              uint32_t page_shift, uint32_t *delta, cudaStream_t s) {
+  if (!cnt) return cudaSuccess;
+  page_delta_kernel<<<grid_for(cnt), BLOCK, 0, s>>>(keys, cnt, off, page_base, page_shift, delta);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_features(const float *hist, const uint8_t *age, const uint32_t *delta,
+                            const uint32_t *rows, const uint32_t *maxlen, uint32_t npages,
+                            void *x, cudaStream_t s) {
+  features_kernel<<<grid_for(npages), BLOCK, 0, s>>>(hist, age, delta, rows, maxlen, npages,
+                                                     (__nv_bfloat16 *)x);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_history(uint32_t *hits, float *hist, uint8_t *age, uint32_t npages,
+                           float *target, bool clear, cudaStream_t s) {
+  history_kernel<<<grid_for(npages), BLOCK, 0, s>>>(hits, hist, age, npages, target, clear);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_infer(const void *x, uint32_t n, const float *params, float *score,
+                             uint32_t *ids, cudaStream_t s) {
+  mlp_infer_kernel<<<grid_for(n), BLOCK, 0, s>>>((const __nv_bfloat16 *)x, n, params, score, ids);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_grad(const void *x, const float *y, uint64_t total, uint32_t count,
+                            uint64_t sample_seed, const float *params, float scale, float *grad,
+                            float *loss, cudaStream_t s) {
+  static bool attr = false;
+  const size_t smem = mlp_grad_smem();
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const uint32_t tiles = (count + TS - 1) / TS;
+  const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(tiles, 148 * 2));
+  mlp_grad_kernel<<<grid, BLOCK, smem, s>>>((const __nv_bfloat16 *)x, y, total, count,
+                                            sample_seed, params, scale, grad, loss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adam(float *p, float *g, float *m, float *v, float lr, uint32_t step,
+                        cudaStream_t s) {
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  adam_kernel<<<(POLICY_PARAMS + BLOCK - 1) / BLOCK, BLOCK, 0, s>>>(p, g, m, v, lr, b1, b2, 1e-8f,
+                                                                    c1, c2);
+  return cudaGetLastError();
+}
+
+}  // namespace dycg

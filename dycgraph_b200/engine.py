@@ -17,7 +17,8 @@ _LIB = None
 
 ALGOS = {"sssp": 0, "bfs": 1, "cc": 2, "pr": 3}
 WEIGHTS = {"hash128": 0, "stored": 1}
-CACHE = {"none": 0, "hotness": 1}
+CACHE = {"none": 0, "hotness": 1, "learned": 2}
+POLICY_F, POLICY_H, POLICY_PARAMS = 8, 64, 4801
 STATUS = {0: "DYCG_OK", -1: "DYCG_EINVAL", -2: "DYCG_ECUDA", -3: "DYCG_ENOMEM",
           -4: "DYCG_ESTATE", -5: "DYCG_ECAPACITY", -6: "DYCG_ELIMIT", -7: "DYCG_EIO",
           -8: "DYCG_ENOGPU"}
@@ -41,7 +42,8 @@ class Options(ctypes.Structure):
                 ("symmetric", ctypes.c_uint32), ("epsilon", ctypes.c_float),
                 ("alpha", ctypes.c_float), ("max_rounds", ctypes.c_uint32),
                 ("device", ctypes.c_int32), ("page_shift", ctypes.c_uint32),
-                ("ordered_delta", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
+                ("ordered_delta", ctypes.c_uint32), ("arena_headroom_permille", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 5)]
 
 
 _STAT_U64 = ["deletions", "insertions", "missing_deletes", "invalid_updates", "touched_sources",
@@ -68,6 +70,15 @@ class QueryMapping(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class PolicyReport(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_uint64), ("steps", ctypes.c_uint64),
+                ("loss_before", ctypes.c_float), ("loss_after", ctypes.c_float),
+                ("ms", ctypes.c_float), ("reserved", ctypes.c_uint32 * 5)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k in ("samples", "steps", "loss_before", "loss_after", "ms")}
+
+
 class GraphInfo(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in (
         "nodes", "live_edges", "arena_slots", "arena_used", "pages", "cache_slots",
@@ -76,7 +87,9 @@ class GraphInfo(ctypes.Structure):
         ("reserved", ctypes.c_uint64 * 6)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d["index_bytes"] = self.reserved[0]  # fence index + deletion bitmaps (in the budget)
+        return d
 
 
 def library_path():
@@ -137,6 +150,14 @@ def lib():
         "dycg_set_queries": (I, [P, u32p, u32, u32]),
         "dycg_set_query_mapping": (I, [P, u32, u32, u32]),
         "dycg_gather_query": (I, [P, u32, u32p, u32p]),
+        "dycg_set_cache_policy": (I, [P, u32]),
+        "dycg_policy_trace": (I, [P, u32]),
+        "dycg_policy_train": (I, [P, u32, ctypes.c_float, u32, u64, ctypes.POINTER(PolicyReport)]),
+        "dycg_policy_params": (I, [P, ctypes.POINTER(ctypes.c_float)]),
+        "dycg_policy_set_params": (I, [P, ctypes.POINTER(ctypes.c_float)]),
+        "dycg_mlp_infer": (I, [P, u32, P, P, P]),
+        "dycg_mlp_loss_grad": (I, [P, P, u32, P, P, P, P]),
+        "dycg_sample_row_edges": (I, [P, u32p, u64, u64, ep]),
         "dycg_last_error": (I, [P, ctypes.c_char_p, sz]),
         "dycg_version": (ctypes.c_char_p, []),
     }
@@ -174,6 +195,23 @@ def gen_rmat_edges(scale, count, seed, first=0, a=0.57, b=0.19, c=0.19, wlo=1, w
     return out
 
 
+def mlp_infer(d_x, n, d_params, d_out, stream=None):
+    """Policy network on device buffers (raw addresses): n bf16 feature rows."""
+    rc = lib().dycg_mlp_infer(ctypes.c_void_p(d_x), n, ctypes.c_void_p(d_params),
+                              ctypes.c_void_p(d_out), ctypes.c_void_p(stream))
+    if rc:
+        raise DycgError(rc, "dycg_mlp_infer")
+
+
+def mlp_loss_grad(d_x, d_y, n, d_params, d_grad, d_loss, stream=None):
+    """Adds sum((mlp(x) - y)^2) into *d_loss and its parameter gradient into d_grad."""
+    rc = lib().dycg_mlp_loss_grad(ctypes.c_void_p(d_x), ctypes.c_void_p(d_y), n,
+                                  ctypes.c_void_p(d_params), ctypes.c_void_p(d_grad),
+                                  ctypes.c_void_p(d_loss), ctypes.c_void_p(stream))
+    if rc:
+        raise DycgError(rc, "dycg_mlp_loss_grad")
+
+
 def measure_host_link(device=0, nbytes=1 << 30):
     """(h2d copy GB/s, zero-copy read GB/s) over the host link of `device`."""
     a, b = ctypes.c_double(0), ctypes.c_double(0)
@@ -192,7 +230,8 @@ class Engine:
 
     def __init__(self, algo="sssp", weight_mode="hash128", source=0, segments=1,
                  hbm_graph_budget_bytes=0, cache_policy=None, symmetric=False, epsilon=1e-6,
-                 alpha=0.85, max_rounds=100, device=0, page_shift=12, ordered_delta=0):
+                 alpha=0.85, max_rounds=100, device=0, page_shift=12, ordered_delta=0,
+                 arena_headroom_permille=0):
         L = lib()
         opt = Options()
         L.dycg_options_default(ctypes.byref(opt))
@@ -211,6 +250,7 @@ class Engine:
         opt.device = device
         opt.page_shift = page_shift
         opt.ordered_delta = ordered_delta
+        opt.arena_headroom_permille = arena_headroom_permille
         self.algo = opt.algo
         self.options = opt
         self._h = ctypes.c_void_p()
@@ -333,6 +373,41 @@ class Engine:
                                                   ctypes.c_void_p(d_adds_ptr), na,
                                                   ctypes.byref(st)), "apply_batch_device")
         return st
+
+    # -- learned cache admission -------------------------------------------------
+    def set_cache_policy(self, policy):
+        self._check(lib().dycg_set_cache_policy(self._h, CACHE[policy] if isinstance(policy, str)
+                                                else int(policy)), "set_cache_policy")
+
+    def policy_trace(self, snapshots):
+        """Record features and page reads of the next `snapshots` snapshot calls."""
+        self._check(lib().dycg_policy_trace(self._h, snapshots), "policy_trace")
+
+    def policy_train(self, epochs=2, lr=1e-3, batch=4096, seed=1):
+        rep = PolicyReport()
+        self._check(lib().dycg_policy_train(self._h, epochs, lr, batch, seed, ctypes.byref(rep)),
+                    "policy_train")
+        return rep.as_dict()
+
+    def policy_params(self):
+        p = np.empty(POLICY_PARAMS, np.float32)
+        self._check(lib().dycg_policy_params(self._h, _ptr(p, ctypes.c_float)), "policy_params")
+        return p
+
+    def policy_set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.shape == (POLICY_PARAMS,)
+        self._check(lib().dycg_policy_set_params(self._h, _ptr(p, ctypes.c_float)),
+                    "policy_set_params")
+
+    def sample_row_edges(self, sources, seed):
+        """One live out-edge per source; rows (INF, INF, 0) for empty rows."""
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        out = np.empty((len(src), 3), np.uint32)
+        self._check(lib().dycg_sample_row_edges(self._h, _ptr(src, ctypes.c_uint32), len(src), seed,
+                                                out.ctypes.data_as(ctypes.POINTER(Edge))),
+                    "sample_row_edges")
+        return out
 
     def tune_query_mapping(self, dels, adds):
         """Apply one snapshot while timing the batched repair under each

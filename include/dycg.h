@@ -57,6 +57,7 @@ extern "C" {
 /* ---- cache admission policy -------------------------------------------- */
 #define DYCG_CACHE_NONE 0     /* no page is staged in HBM (reference -cache=0) */
 #define DYCG_CACHE_HOTNESS 1  /* decayed per-page access counts, top-K pages   */
+#define DYCG_CACHE_LEARNED 2  /* BF16 MLP ranks pages before each repair        */
 
 #define DYCG_INFINITY 0xFFFFFFFFu /* unreachable distance / no parent        */
 
@@ -87,7 +88,10 @@ typedef struct dycg_options {
                           /* wave expands only values < wave min + d (the    */
                           /* reference's ordered schedule, for high-diameter */
                           /* graphs; 1 is exact-min order for BFS and CC)    */
-  uint32_t reserved[6];
+  uint32_t arena_headroom_permille; /* spare arena slots for row growth, per   */
+                          /* mille of the loaded slots (0: 125, the reference's */
+                          /* 1/8; at least 2^20 slots either way)              */
+  uint32_t reserved[5];
 } dycg_options;
 
 /* Per-call counters. Byte counts are algorithmic: every adjacency slot read
@@ -368,6 +372,66 @@ int dycg_apply_batches_device(dycg_engine *e, const dycg_edge *d_dels,
 /* Results of query q (values/parents as dycg_gather; n entries each, either
  * may be NULL). With queries set, dycg_gather returns query 0. */
 int dycg_gather_query(dycg_engine *e, uint32_t q, uint32_t *values, uint32_t *parents);
+
+/* ---- learned cache admission (no reference counterpart) -------------------
+ * The reference admits rows by a decayed activity count
+ * (include/framework/variants/driver.cuh:486-515); that is DYCG_CACHE_HOTNESS
+ * here. DYCG_CACHE_LEARNED ranks every cache page with a small MLP
+ * (DYCG_POLICY_FEATURES -> 64 -> 64 -> 1, ReLU, BF16 weights and inputs, FP32
+ * accumulation) right after a snapshot's ingest, from per-page features (page
+ * reads in each of the last four snapshots, update records of this batch
+ * whose row starts in the page, snapshots since the last read, rows starting
+ * in the page and the longest of them), and stages the pages it predicts to
+ * be read most (predicted reads >= 64) before the mutation and repair, up to
+ * cache pages/64 per snapshot. Which pages are cached never changes results.
+ * The network predicts log1p(page reads in this snapshot) and is trained on
+ * traces the engine records, by the library's own forward/backward and Adam
+ * kernels on the GPU. */
+#define DYCG_POLICY_FEATURES 8
+#define DYCG_POLICY_HIDDEN 64
+#define DYCG_POLICY_PARAMS 4801 /* W1[8x64] b1[64] W2[64x64] b2[64] W3[64] b3, FP32 */
+
+typedef struct dycg_policy_report {
+  uint64_t samples;      /* trace samples (pages x snapshots)                  */
+  uint64_t steps;        /* optimizer steps                                    */
+  float loss_before;     /* mean squared error over all samples, before/after   */
+  float loss_after;
+  float ms;              /* device time of the training call                    */
+  uint32_t reserved[5];
+} dycg_policy_report;
+
+/* Switch between DYCG_CACHE_HOTNESS and DYCG_CACHE_LEARNED (needs a page
+ * cache: a non-zero budget and a policy other than NONE at create). */
+int dycg_set_cache_policy(dycg_engine *e, uint32_t policy);
+
+/* Record (features, page reads) of the next `snapshots` snapshot calls, under
+ * whatever policy is active, as the training set; 0 drops the traces. */
+int dycg_policy_trace(dycg_engine *e, uint32_t snapshots);
+
+/* Train the network on the recorded traces with Adam (lr), minibatches of
+ * `batch` samples drawn with a seed, epochs x samples / batch steps. */
+int dycg_policy_train(dycg_engine *e, uint32_t epochs, float lr, uint32_t batch,
+                      uint64_t seed, dycg_policy_report *report);
+
+/* Read / replace the FP32 master parameters (DYCG_POLICY_PARAMS floats). */
+int dycg_policy_params(dycg_engine *e, float *params);
+int dycg_policy_set_params(dycg_engine *e, const float *params);
+
+/* Standalone network kernels on device buffers (stream = cudaStream_t or
+ * NULL): x = n rows of DYCG_POLICY_FEATURES bf16 values, params FP32 (used
+ * rounded to bf16). dycg_mlp_infer writes n predictions; dycg_mlp_loss_grad
+ * adds the summed squared error over n rows against y into *d_loss and its
+ * gradient w.r.t. the parameters into d_grad (both must start at zero). */
+int dycg_mlp_infer(const void *d_x, uint32_t n, const float *d_params, float *d_out,
+                   void *stream);
+int dycg_mlp_loss_grad(const void *d_x, const float *d_y, uint32_t n, const float *d_params,
+                       float *d_grad, float *d_loss, void *stream);
+
+/* For each source, one live out-edge drawn uniformly (deterministic in seed);
+ * {DYCG_INFINITY, DYCG_INFINITY, 0} for a source without live edges. Used to
+ * draw deletions with skewed endpoints. */
+int dycg_sample_row_edges(dycg_engine *e, const uint32_t *sources, uint64_t count,
+                          uint64_t seed, dycg_edge *out);
 
 /* cudaStream_t the engine launches on (for CUDA-event timing by callers). */
 int dycg_stream(dycg_engine *e, void **stream);

@@ -100,3 +100,28 @@ def random_batch(n, off, dst, w, nd, na, seed, wlo=1, whi=64, stored=True):
     aw = hw(au, av, wlo, whi)
     adds = [(int(x), int(y), int(z)) for x, y, z in zip(au, av, aw)]
     return dels, adds
+
+
+def zipf_vertices(n, count, rng, s=1.1, perm=None):
+    """count vertex ids whose ranks follow Zipf(s) over n vertices (rank 1 most
+    frequent), mapped through a permutation so the hot ids are scattered."""
+    out = np.empty(0, np.int64)
+    while len(out) < count:
+        k = rng.zipf(s, size=2 * (count - len(out)) + 16)
+        out = np.concatenate([out, k[k <= n] - 1])
+    out = out[:count]
+    return (perm[out] if perm is not None else out).astype(np.uint32)
+
+
+def zipf_snapshot(eng, n, nd, na, rng, perm, s=1.1, wlo=1, whi=64):
+    """nd deletions of live edges out of Zipf-chosen sources and na insertions
+    with both endpoints Zipf-chosen (weights hashed from the endpoints)."""
+    src = zipf_vertices(n, nd, rng, s, perm)
+    d = eng.sample_row_edges(src, int(rng.integers(1 << 62)))
+    d = d[d[:, 0] != 0xFFFFFFFF]
+    u = zipf_vertices(n, na, rng, s, perm)
+    v = zipf_vertices(n, na, rng, s, perm)
+    keep = u != v
+    u, v = u[keep], v[keep]
+    a = np.stack([u, v, hw(u, v, wlo, whi)], 1).astype(np.uint32)
+    return d, a

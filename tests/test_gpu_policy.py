@@ -1,0 +1,122 @@
+"""GPU checks of the learned cache-admission policy: the network's forward and
+gradient kernels against the float64 oracle (same BF16 rounding), training on
+recorded traces, and bit-exact results whichever pages the policy caches."""
+import numpy as np
+import pytest
+import torch
+
+import dycgraph_b200 as dg
+import oracle
+from oracle import mlp
+from tests import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _device_inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0, 1.5, (n, mlp.F)).astype(np.float32)
+    y = rng.uniform(0, 5, n).astype(np.float32)
+    xd = torch.from_numpy(x).cuda().to(torch.bfloat16).contiguous()
+    return x, y, xd, torch.from_numpy(y).cuda()
+
+
+@pytest.mark.parametrize("n", [1, 127, 1000, 5000])
+def test_mlp_gradient_matches_oracle(n):
+    x, y, xd, yd = _device_inputs(n, n)
+    p = mlp.glorot_params(n)
+    pd = torch.from_numpy(p).cuda()
+    g = torch.zeros(mlp.PARAMS, dtype=torch.float32, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    dg.mlp_loss_grad(xd.data_ptr(), yd.data_ptr(), n, pd.data_ptr(), g.data_ptr(), loss.data_ptr())
+    lo, go = mlp.loss_grad(x, y, p)
+    # FP32 accumulation against float64 with identical BF16-rounded operands
+    assert abs(float(loss.item()) - lo) <= 1e-4 * lo + 1e-6
+    gg = g.cpu().numpy().astype(np.float64)
+    tol = 2e-4 * np.max(np.abs(go)) + 1e-6
+    assert np.max(np.abs(gg - go)) <= tol, (np.max(np.abs(gg - go)), tol)
+
+
+def test_mlp_inference_matches_oracle():
+    n = 3001
+    x, _, xd, _ = _device_inputs(n, 7)
+    p = mlp.glorot_params(7)
+    out = torch.empty(n, dtype=torch.float32, device="cuda")
+    dg.mlp_infer(xd.data_ptr(), n, torch.from_numpy(p).cuda().data_ptr(), out.data_ptr())
+    ref = mlp.forward(x, p)
+    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=1e-4, atol=1e-5)
+
+
+def _zipf_engine(policy, scale, cache_frac, seed):
+    """Engine whose HBM budget holds its index plus cache_frac of the used pages."""
+    n, off, dst, w = cases.small_rmat(scale, 8, seed)
+    budget = 0
+    if cache_frac:
+        probe = dg.Engine("sssp", weight_mode="stored", page_shift=8, cache_policy="none")
+        probe.load_csr(n, off, dst, w)
+        gi = probe.info()
+        probe.close()
+        used_pages = (gi["arena_used"] >> gi["page_shift"]) + 2
+        budget = gi["index_bytes"] + int(cache_frac * used_pages * (8 << gi["page_shift"]))
+    e = dg.Engine("sssp", weight_mode="stored", hbm_graph_budget_bytes=budget, page_shift=8,
+                  cache_policy=policy)
+    e.load_csr(n, off, dst, w)
+    e.start()
+    return e, n, (off, dst, w)
+
+
+def test_learned_policy_trains_and_keeps_results_exact():
+    scale, seed = 12, 41
+    e, n, (off, dst, w) = _zipf_engine("hotness", scale, 0.3, seed)
+    info = e.info()
+    assert 0 < info["cache_slots"] < info["pages"]
+    orc = oracle.Oracle(oracle.SSSP, n, off, dst, w, weight_mode=oracle.WEIGHT_STORED)
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(n)
+    e.policy_trace(4)
+    for _ in range(5):  # 4 traced, then one more (tracing stops by itself)
+        d, a = cases.zipf_snapshot(e, n, 300, 300, rng, perm)
+        e.apply_batch(d, a)
+        orc.mutate(d, a)
+    rep = e.policy_train(epochs=4, lr=2e-3, batch=1024, seed=3)
+    assert rep["samples"] == 4 * e.info()["pages"] and rep["steps"] > 0
+    assert rep["loss_after"] < rep["loss_before"]
+    e.set_cache_policy("learned")
+    for _ in range(4):
+        d, a = cases.zipf_snapshot(e, n, 300, 300, rng, perm)
+        st = e.apply_batch(d, a)
+        orc.mutate(d, a)
+        o, dd, ww = orc.csr()
+        ref = oracle.static_sssp(n, o, dd, ww, oracle.WEIGHT_STORED, 0)
+        assert (e.gather()[0] == ref).all()
+        assert st["ms_cache"] >= 0
+
+
+def test_policy_params_round_trip_and_switching():
+    e, n, _ = _zipf_engine("hotness", 10, 0.3, 5)
+    p = mlp.glorot_params(9)
+    e.policy_set_params(p)
+    np.testing.assert_array_equal(e.policy_params(), p)
+    e.set_cache_policy("learned")
+    e.set_cache_policy("hotness")
+    with pytest.raises(dg.DycgError):
+        e.set_cache_policy(0)
+    with pytest.raises(dg.DycgError):
+        e.policy_train()  # no traces recorded
+    nc, _, _ = _zipf_engine("none", 10, 0.0, 5)
+    with pytest.raises(dg.DycgError):
+        nc.set_cache_policy("learned")
+
+
+def test_row_edge_sampler_returns_live_edges():
+    e, n, (off, dst, w) = _zipf_engine("none", 10, 0.0, 3)
+    src = np.arange(n, dtype=np.uint32)
+    out = e.sample_row_edges(src, 17)
+    deg = np.diff(off)
+    for u in range(n):
+        if deg[u] == 0:
+            assert out[u, 0] == 0xFFFFFFFF
+        else:
+            row = dst[int(off[u]):int(off[u + 1])]
+            k = np.nonzero(row == out[u, 1])[0]
+            assert out[u, 0] == u and len(k) and out[u, 2] == w[int(off[u]) + k[0]]

@@ -785,19 +785,26 @@ def zipf_ids(n, count, rng, perm, s=1.1):
     return perm[out[:count]].astype(np.uint32)
 
 
-def zipf_snapshots(eng, count, size, seed, n, wmax=64):
-    """Snapshots of `size` updates (half deletions, half insertions) whose
-    endpoints are Zipf(1.1) over the vertices: insertions draw both endpoints,
-    deletions take a live out-edge of a drawn source (drawn on the initial
-    graph, so a later snapshot may name an edge deleted before: a missing
-    delete, counted as such)."""
-    rng = np.random.default_rng(seed)
-    perm = rng.permutation(n)
-    out = []
+def zipf_snapshots(eng, count, size, rng, perm, wmax=64):
+    """`count` snapshots of `size` updates (half deletions, half insertions)
+    whose endpoints are Zipf(1.1) over the vertices, drawn from the engine's
+    current graph: insertions draw both endpoints; deletions take a live
+    out-edge of a drawn source, each edge at most once across the snapshots
+    drawn together."""
+    n = eng.n
+    nd = size // 2
+    cands = []
     for _ in range(count):
-        nd = size // 2
-        d = eng.sample_row_edges(zipf_ids(n, nd, rng, perm), int(rng.integers(1 << 62)))
-        d = d[d[:, 0] != 0xFFFFFFFF]
+        d = eng.sample_row_edges(zipf_ids(n, nd + nd // 2, rng, perm), int(rng.integers(1 << 62)))
+        cands.append(d[d[:, 0] != 0xFFFFFFFF])
+    keys = np.concatenate([c[:, 0].astype(np.uint64) << np.uint64(32) | c[:, 1].astype(np.uint64)
+                           for c in cands])
+    first = np.zeros(len(keys), bool)
+    first[np.unique(keys, return_index=True)[1]] = True
+    out, o = [], 0
+    for c in cands:
+        d = c[first[o:o + len(c)]][:nd]
+        o += len(c)
         u = zipf_ids(n, size - nd, rng, perm)
         v = zipf_ids(n, size - nd, rng, perm)
         keep = u != v
@@ -841,9 +848,14 @@ def run_learned(args):
         t0 = time.time()
         eng.start()
         t_init = time.time() - t0
-        if snaps is None:
-            snaps = zipf_snapshots(eng, T + W + K + E, args.batch, args.seed + 77, eng.n)
-        eng.reserve_batch(max(max(len(d), len(a)) for d, a in snaps))
+        first = snaps is None
+        if first:
+            # the first engine draws each phase's snapshots from its graph at
+            # that point; the other engines replay the same records
+            rng = np.random.default_rng(args.seed + 77)
+            perm = rng.permutation(eng.n)
+            snaps = zipf_snapshots(eng, T, args.batch, rng, perm)
+        eng.reserve_batch(args.batch)
         if policy == "learned":
             eng.policy_trace(T)
         for d, a in snaps[:T]:
@@ -852,8 +864,12 @@ def run_learned(args):
             report = eng.policy_train(epochs=args.train_epochs, lr=args.train_lr,
                                       batch=args.train_batch, seed=args.seed)
             eng.set_cache_policy("learned")
+        if first:
+            snaps += zipf_snapshots(eng, W, args.batch, rng, perm)
         for d, a in snaps[T:T + W]:
             eng.apply_batch(d, a)
+        if first:
+            snaps += zipf_snapshots(eng, K, args.batch, rng, perm)
         dev = [(torch.from_numpy(d.astype(np.int32)).cuda(), torch.from_numpy(a.astype(np.int32)).cuda())
                for d, a in snaps[T + W:T + W + K]]
         stream = torch.cuda.ExternalStream(eng.stream())
@@ -878,6 +894,8 @@ def run_learned(args):
             clk = clocks.stop()
         ms = ev0.elapsed_time(ev1)
         e2e_ms, e2e_upd = 0.0, 0
+        if first and E:
+            snaps += zipf_snapshots(eng, E, args.batch, rng, perm)
         if E:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)

@@ -66,6 +66,9 @@ Engine::~Engine() {
   if (h_rec_) cudaFreeHost(h_rec_);
   if (d_rec_) cudaFree(d_rec_);
   if (h_bctl_) cudaFreeHost(h_bctl_);
+  for (void *p : {(void *)dbufs_.k_in, (void *)dbufs_.k_out, (void *)dbufs_.v_in,
+                  (void *)dbufs_.v_out, dbufs_.temp})
+    cudaFree(p);
   if (tx_) cudaFree(tx_);
   if (ty_) cudaFree(ty_);
   for (auto &e : pev_)
@@ -270,6 +273,10 @@ void Engine::finish_load() {
   CK(cudaHostAlloc(&hc, sizeof(Ctl), cudaHostAllocDefault));
   hallocs_.push_back(hc);
   h_ctl_ = (Ctl *)hc;
+  void *hdp = nullptr;
+  CK(cudaHostAlloc(&hdp, 8, cudaHostAllocDefault));
+  hallocs_.push_back(hdp);
+  h_dpacked_ = (u64 *)hdp;
   if (opt_.algo == DYCG_ALGO_PR) {
     x_ = (float *)dmalloc((n + 1ull) * 4);
     r_ = (float *)dmalloc((n + 1ull) * 4);
@@ -615,11 +622,19 @@ void Engine::ensure_batch(size_t cnt) {
   tombs_.pos = (u64 *)al(c * 8);
   tombs_.count = counts_ + 10;
   tombs_.cap = (uint32_t)c;
+  defer_.on = true;
+  defer_.rem = (uint32_t *)al(c * 4);
+  defer_.row_u = (uint32_t *)al(c * 4);
+  defer_.row_base = (u64 *)al(c * 8);
+  defer_.packed = (u64 *)(counts_ + 12);  // 8-byte aligned slot of the counters
+  defer_.cap_rows = (uint32_t)c;
   d_edges_ = (dycg_edge_dev *)al(c * 2 * sizeof(dycg_edge_dev));
+  run_flags_ = (uint32_t *)al(c * 4);
+  run_pos_ = (uint32_t *)al(c * 4);
   size_t a = 0, b = 0;
   CK(sort_keys(nullptr, a, k_tmp_out_, k_del_out_, (uint32_t)c, st_));
   CK(sort_pairs(nullptr, b, k_tmp_out_, k_add_out_, w_tmp_, w_add_out_, (uint32_t)c, st_));
-  cub_bytes_ = std::max(a, b);
+  cub_bytes_ = std::max(std::max(a, b), unique_runs_temp_bytes((uint32_t)c));
   cub_temp_ = al(cub_bytes_);
   if (h_stage_) {
     cudaFreeHost(h_stage_);
@@ -630,6 +645,44 @@ void Engine::ensure_batch(size_t cnt) {
   hallocs_.push_back(hs);
   h_stage_ = (dycg_edge *)hs;
   bcap_ = c;
+}
+
+// Deletions of one adjacency direction. Rows with a long unsorted suffix are
+// matched by sort-merge; that needs the gathered size on the host (one
+// synchronisation), so a captured graph keeps the per-record scan.
+void Engine::delete_direction(const Adj &A, const uint2 *uv, const uint32_t *mult,
+                              const uint32_t *n_ptr, uint32_t nd, uint32_t *found,
+                              int count_missing, bool capture) {
+  if (capture) {
+    CK(launch_delete_rows(A, uv, mult, n_ptr, nd, found, ctl_, count_missing, tombs_, st_));
+    launches_ += 2;
+    return;
+  }
+  CK(launch_delete_prefix(A, uv, mult, n_ptr, nd, found, ctl_, count_missing, tombs_, defer_,
+                          st_));
+  CK(cudaMemcpyAsync(h_dpacked_, defer_.packed, 8, cudaMemcpyDeviceToHost, st_));
+  sync_check("deferred deletions");
+  const u64 pk = *h_dpacked_;
+  const uint32_t nrows = (uint32_t)(pk >> 40);
+  const u64 total = pk & ((1ull << 40) - 1);
+  if (total > dbuf_cap_) {
+    for (void *p : {(void *)dbufs_.k_in, (void *)dbufs_.k_out, (void *)dbufs_.v_in,
+                    (void *)dbufs_.v_out, dbufs_.temp})
+      cudaFree(p);
+    dbufs_ = DeferBufs{};
+    dbuf_cap_ = 0;
+    const u64 c = total + total / 2;
+    CK(cudaMalloc((void **)&dbufs_.k_in, c * 8));
+    CK(cudaMalloc((void **)&dbufs_.k_out, c * 8));
+    CK(cudaMalloc((void **)&dbufs_.v_in, c * 4));
+    CK(cudaMalloc((void **)&dbufs_.v_out, c * 4));
+    dbufs_.temp_bytes = delete_sort_temp_bytes(c);
+    CK(cudaMalloc(&dbufs_.temp, std::max<size_t>(dbufs_.temp_bytes, 16)));
+    dbuf_cap_ = c;
+  }
+  CK(launch_delete_suffix(A, uv, n_ptr, nd, found, ctl_, count_missing, tombs_, defer_, nrows,
+                          total, dbufs_, st_));
+  launches_ += 2 + (nrows ? 7 : 0);
 }
 
 // Device half of a snapshot on st_: counters reset, ingest, mutation and
@@ -654,14 +707,16 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
                         nullptr, invalid, st_));
     CK(sort_keys(cub_temp_, tb, k_tmp_out_, k_del_out_, (uint32_t)nd, st_));
     CK(launch_unique_runs(k_del_out_, (uint32_t)nd, uv_out_, mult_out_, counts_ + 0,
-                          (uint32_t)bcap_, &ctl_->err, st_));
-    launches_ += 3;
+                          (uint32_t)bcap_, &ctl_->err, run_flags_, run_pos_, cub_temp_,
+                          cub_bytes_, st_));
+    launches_ += 5;
     if (has_in_) {
       tb = cub_bytes_;
       CK(sort_keys(cub_temp_, tb, k_tmp_in_, k_del_in_, (uint32_t)nd, st_));
       CK(launch_unique_runs(k_del_in_, (uint32_t)nd, uv_in_, mult_in_, counts_ + 1,
-                            (uint32_t)bcap_, &ctl_->err, st_));
-      launches_ += 2;
+                            (uint32_t)bcap_, &ctl_->err, run_flags_, run_pos_, cub_temp_,
+                            cub_bytes_, st_));
+      launches_ += 4;
     }
   }
   if (na) {
@@ -726,14 +781,9 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
   const Adj A_out = adj(out_);
   const Adj A_in = has_in_ ? adj(in_) : A_out;
   if (nd) {
-    CK(launch_delete_rows(A_out, uv_out_, mult_out_, counts_ + 0, (uint32_t)nd, found_out_, ctl_,
-                          1, tombs_, st_));
-    launches_ += 2;
-    if (has_in_) {
-      CK(launch_delete_rows(A_in, uv_in_, mult_in_, counts_ + 1, (uint32_t)nd, nullptr, ctl_, 0,
-                            tombs_, st_));
-      launches_ += 2;
-    }
+    delete_direction(A_out, uv_out_, mult_out_, counts_ + 0, (uint32_t)nd, found_out_, 1, capture);
+    if (has_in_)
+      delete_direction(A_in, uv_in_, mult_in_, counts_ + 1, (uint32_t)nd, nullptr, 0, capture);
   }
   if (na) {
     CK(launch_add_rows(A_out, k_add_out_, w_add_out_, seg_out_, counts_ + 2, (uint32_t)na,

@@ -99,6 +99,9 @@ class Engine {
   const SnapshotGraph &graph_for(uint32_t cls);
   void drop_graphs();
   void policy_alloc();
+  void delete_direction(const Adj &A, const uint2 *uv, const uint32_t *mult,
+                        const uint32_t *n_ptr, uint32_t nd, uint32_t *found, int count_missing,
+                        bool capture);
   void policy_prefetch(size_t nd, size_t na);
   void init_queries(u64 timeout);
   void repair_queries(uint32_t nd, uint32_t na, u64 timeout);
@@ -184,8 +187,13 @@ class Engine {
   uint32_t *mult_out_ = nullptr, *mult_in_ = nullptr, *found_out_ = nullptr;
   uint3 *seg_out_ = nullptr, *seg_in_ = nullptr, *add_uvw_ = nullptr;
   uint32_t *touched_ = nullptr, *counts_ = nullptr;
+  uint32_t *run_flags_ = nullptr, *run_pos_ = nullptr;  // unique-run scan scratch
   Reloc reloc_{};
   Tombs tombs_{};
+  DeferDel defer_{};
+  DeferBufs dbufs_{};
+  u64 dbuf_cap_ = 0;
+  u64 *h_dpacked_ = nullptr;  // pinned
   dycg_edge_dev *d_edges_ = nullptr;
   dycg_edge *h_stage_ = nullptr;
   void *cub_temp_ = nullptr;

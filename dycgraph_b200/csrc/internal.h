@@ -101,8 +101,10 @@ cudaError_t sort_keys(void *temp, size_t &temp_bytes, const u64 *in, u64 *out, u
                       cudaStream_t s);
 cudaError_t sort_pairs(void *temp, size_t &temp_bytes, const u64 *kin, u64 *kout,
                        const uint32_t *vin, uint32_t *vout, uint32_t cnt, cudaStream_t s);
+size_t unique_runs_temp_bytes(uint32_t cnt);
 cudaError_t launch_unique_runs(const u64 *k, uint32_t cnt, uint2 *uv, uint32_t *mult,
-                               uint32_t *n_out, uint32_t cap, uint32_t *err, cudaStream_t s);
+                               uint32_t *n_out, uint32_t cap, uint32_t *err, uint32_t *flags,
+                               uint32_t *pos, void *temp, size_t temp_bytes, cudaStream_t s);
 cudaError_t launch_row_segments(const u64 *k, uint32_t cnt, uint3 *seg, uint32_t *n_out,
                                 cudaStream_t s);
 // Deleted occurrences found by the read-only search, written afterwards.
@@ -114,6 +116,38 @@ struct Tombs {
 cudaError_t launch_delete_rows(const Adj &A, const uint2 *uv, const uint32_t *mult,
                                const uint32_t *n_ptr, uint32_t max_n, uint32_t *found, Ctl *ctl,
                                int count_missing, const Tombs &T, cudaStream_t s);
+// Deletions in rows whose unsorted suffix exceeds DEFER_SUFFIX slots are
+// matched by sort-merge (gather the live suffix slots once, stable sort by
+// (row, neighbour), binary search per record) instead of a suffix scan per
+// record, whose cost grows with (records in the row) x (suffix length).
+constexpr uint32_t DEFER_SUFFIX = 1024;
+struct DeferDel {
+  bool on;
+  uint32_t *rem;       // per record: occurrences left after the sorted-prefix pass
+  u64 *packed;         // (deferred rows << 40) | suffix slots reserved
+  uint32_t *row_u;     // deferred rows, in reservation order
+  u64 *row_base;       // first gather index of each deferred row
+  uint32_t cap_rows;
+};
+struct DeferBufs {
+  u64 *k_in, *k_out;
+  uint32_t *v_in, *v_out;
+  void *temp;
+  size_t temp_bytes;
+};
+// pass over the sorted prefixes (and short suffixes); long suffixes deferred
+cudaError_t launch_delete_prefix(const Adj &A, const uint2 *uv, const uint32_t *mult,
+                                 const uint32_t *n_ptr, uint32_t max_n, uint32_t *found, Ctl *ctl,
+                                 int count_missing, const Tombs &T, const DeferDel &D,
+                                 cudaStream_t s);
+size_t delete_sort_temp_bytes(u64 total);
+// sort-merge of the deferred suffixes (total gathered slots, nrows rows), then
+// the tombstones of all found occurrences
+cudaError_t launch_delete_suffix(const Adj &A, const uint2 *uv, const uint32_t *n_ptr,
+                                 uint32_t max_n, uint32_t *found, Ctl *ctl, int count_missing,
+                                 const Tombs &T, const DeferDel &D, uint32_t nrows, u64 total,
+                                 const DeferBufs &B, cudaStream_t s);
+
 // Relocation bookkeeping for rows that outgrow their block.
 constexpr uint32_t RELOC_CHUNK = 1024;
 struct RelocRec {

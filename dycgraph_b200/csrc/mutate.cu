@@ -37,37 +37,32 @@ __global__ void prep_keys_kernel(const dycg_edge_dev *e, uint32_t cnt, uint32_t 
   if (lane_id() == 0 && b) atomicAdd(invalid, b);
 }
 
-// Unique (row, neighbour) runs of a sorted key array with their multiplicity.
-__global__ void unique_runs_kernel(const u64 *k, uint32_t cnt, uint2 *uv, uint32_t *mult,
-                                   uint32_t *n_out, uint32_t cap, uint32_t *err) {
-  const uint32_t lane = lane_id();
-  const uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) - lane;
-  for (uint32_t i0 = base; i0 < cnt; i0 += gridDim.x * blockDim.x) {
-    const uint32_t i = i0 + lane;
-    bool head = false;
-    u64 key = KEY_INF;
-    if (i < cnt) {
-      key = k[i];
-      head = key != KEY_INF && (i == 0 || k[i - 1] != key);
-    }
-    uint32_t m = 0;
-    if (head) {
-      uint32_t j = i + 1;
-      while (j < cnt && k[j] == key) j++;
-      m = j - i;
-    }
-    const unsigned hm = __ballot_sync(0xffffffffu, head);
-    if (!hm) continue;
-    uint32_t slot = 0;
-    if (lane == (uint32_t)(__ffs(hm) - 1)) slot = atomicAdd(n_out, (uint32_t)__popc(hm));
-    slot = __shfl_sync(0xffffffffu, slot, __ffs(hm) - 1) + __popc(hm & ((1u << lane) - 1));
-    if (head) {
-      if (slot < cap) {
-        uv[slot] = make_uint2((uint32_t)(key >> 32), (uint32_t)key);
-        mult[slot] = m;
-      } else {
-        atomicCAS(err, 0u, ERR_QUEUE);
-      }
+// Unique (row, neighbour) runs of a sorted key array with their
+// multiplicity, written in ascending key order: head flags, an exclusive sum
+// for the output slots, then one write per head. Records of one row are
+// therefore contiguous (the deletion pass relies on it).
+__global__ void run_heads_kernel(const u64 *k, uint32_t cnt, uint32_t *flags) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    const u64 key = k[i];
+    flags[i] = key != KEY_INF && (i == 0 || k[i - 1] != key);
+  }
+}
+
+__global__ void run_emit_kernel(const u64 *k, uint32_t cnt, const uint32_t *flags,
+                                const uint32_t *pos, uint2 *uv, uint32_t *mult, uint32_t *n_out,
+                                uint32_t cap, uint32_t *err) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    if (i == cnt - 1) *n_out = min(pos[i] + flags[i], cap);
+    if (!flags[i]) continue;
+    const u64 key = k[i];
+    uint32_t j = i + 1;
+    while (j < cnt && k[j] == key) j++;
+    const uint32_t slot = pos[i];
+    if (slot < cap) {
+      uv[slot] = make_uint2((uint32_t)(key >> 32), (uint32_t)key);
+      mult[slot] = j - i;
+    } else {
+      atomicCAS(err, 0u, ERR_QUEUE);
     }
   }
 }
@@ -149,7 +144,7 @@ __device__ uint32_t warp_lower_bound(const Adj &A, u64 off, uint32_t srt, uint32
 // HBM deletion bitmap, so a deletion costs no host-link write.
 __global__ void delete_rows_kernel(Adj A, const uint2 *uv, const uint32_t *mult,
                                    const uint32_t *n_ptr, uint32_t *found_out, Ctl *ctl,
-                                   int count_missing, Tombs T) {
+                                   int count_missing, Tombs T, DeferDel D) {
   const uint32_t lane = lane_id();
   const uint32_t nrec = *n_ptr;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -162,7 +157,8 @@ __global__ void delete_rows_kernel(Adj A, const uint2 *uv, const uint32_t *mult,
     const u64 off = A.off[row];
     const uint32_t len = A.len[row], srt = A.srt[row];
     const uint32_t pos = warp_lower_bound(A, off, srt, target, reads);
-    for (uint32_t pass = 0; pass < 2; pass++) {
+    const bool defer = D.on && len - srt > DEFER_SUFFIX;
+    for (uint32_t pass = 0; pass < (defer ? 1u : 2u); pass++) {
       // pass 0: the run of target in the sorted prefix; pass 1: the unsorted suffix
       const uint32_t b = pass ? srt : pos, e2 = pass ? len : srt;
       for (uint32_t s0 = b; s0 < e2 && remaining; s0 += 32) {
@@ -190,7 +186,23 @@ __global__ void delete_rows_kernel(Adj A, const uint2 *uv, const uint32_t *mult,
     if (lane == 0) {
       if (found) atomicSub(A.live + row, found);
       if (found_out) found_out[i] = found;
-      missing += mult[i] - found;
+      if (defer) {
+        // the row's suffix is matched later, once for all its records
+        D.rem[i] = remaining;
+        if (i == 0 || uv[i - 1].x != row) {
+          const u64 old = atomicAdd(D.packed, (1ull << 40) | (u64)(len - srt));
+          const uint32_t k = (uint32_t)(old >> 40);
+          if (k < D.cap_rows) {
+            D.row_u[k] = row;
+            D.row_base[k] = old & ((1ull << 40) - 1);
+          } else {
+            atomicCAS(&ctl->err, 0u, ERR_QUEUE);
+          }
+        }
+      } else {
+        if (D.on) D.rem[i] = 0;
+        missing += mult[i] - found;
+      }
       if (total_reads) atomicAdd(A.page_hits + page_of(A, off + pos), (uint32_t)total_reads);
     }
   }
@@ -214,6 +226,83 @@ __global__ void tombstone_kernel(Adj A, Tombs T, Ctl *ctl) {
   }
   hbm = warp_sum(hbm);
   if (lane_id() == 0 && hbm) atomicAdd(&ctl->stat[ST_MUT_HBM_BYTES], hbm);
+}
+
+// Gather the live suffix slots of the deferred rows: thread per slot j,
+// key (row << 32 | neighbour) (KEY_INF for a deleted slot), value = the
+// slot's index in its suffix. Gathered in slot order, so a stable sort keeps
+// equal keys in slot order.
+__global__ void suffix_gather_kernel(Adj A, DeferDel D, uint32_t nrows, u64 total, u64 *keys,
+                                     uint32_t *vals, Ctl *ctl) {
+  const uint32_t lane = lane_id();
+  const uint32_t bytes = 4u * A.stride;
+  u64 link = 0, hbm = 0;
+  for (u64 j0 = (u64)blockIdx.x * blockDim.x + threadIdx.x - lane; j0 < total;
+       j0 += (u64)gridDim.x * blockDim.x) {  // warp-uniform
+    const u64 j = j0 + lane;
+    const bool in = j < total;
+    uint32_t pg = PAGE_NONE;
+    if (in) {
+      uint32_t lo = 0, hi = nrows;  // largest k with row_base[k] <= j
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (D.row_base[mid] <= j) lo = mid; else hi = mid;
+      }
+      const uint32_t u = D.row_u[lo];
+      const uint32_t si = (uint32_t)(j - D.row_base[lo]);
+      const u64 p = A.off[u] + A.srt[u] + si;
+      const uint32_t d = read_dst_rw(A, p);
+      pg = page_of(A, p);
+      if (A.page_slot[pg] != PAGE_NONE) hbm += bytes; else link += bytes;
+      keys[j] = slot_deleted_rw(A, p, d) ? KEY_INF : (((u64)u << 32) | (d & VMASK));
+      vals[j] = si;
+    }
+    const uint32_t pg0 = __shfl_sync(0xffffffffu, pg, 0);
+    const unsigned same = __ballot_sync(0xffffffffu, in && pg == pg0);
+    if (lane == 0 && same) atomicAdd(A.page_hits + pg0, __popc(same));
+    if (in && pg != pg0) atomicAdd(A.page_hits + pg, 1u);
+  }
+  link = warp_sum(link);
+  hbm = warp_sum(hbm);
+  if (lane == 0) {
+    if (link) atomicAdd(&ctl->stat[ST_MUT_LINK_BYTES], link);
+    if (hbm) atomicAdd(&ctl->stat[ST_MUT_HBM_BYTES], hbm);
+  }
+}
+
+// Records left unmatched by the prefix pass take the first `rem` entries of
+// their (row, neighbour) run in the sorted gather: the earliest live suffix
+// occurrences, as the scan would have found them.
+__global__ void suffix_match_kernel(Adj A, const uint2 *uv, const uint32_t *n_ptr, DeferDel D,
+                                    const u64 *keys, const uint32_t *vals, u64 total,
+                                    uint32_t *found_out, Ctl *ctl, int count_missing, Tombs T) {
+  const uint32_t nrec = *n_ptr;
+  u64 missing = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nrec;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t rem = D.rem[i];
+    if (!rem) continue;
+    const uint2 e = uv[i];
+    const u64 key = ((u64)e.x << 32) | e.y;
+    u64 lo = 0, hi = total;  // first index with keys[idx] >= key
+    while (lo < hi) {
+      const u64 mid = (lo + hi) / 2;
+      if (keys[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    const u64 base = A.off[e.x] + A.srt[e.x];
+    uint32_t taken = 0;
+    for (u64 j = lo; j < total && keys[j] == key && taken < rem; j++, taken++) {
+      const uint32_t slot = atomicAdd(T.count, 1u);
+      if (slot < T.cap) T.pos[slot] = base + vals[j];
+    }
+    if (taken) {
+      atomicSub(A.live + e.x, taken);
+      if (found_out) found_out[i] += taken;
+    }
+    missing += rem - taken;
+  }
+  missing = warp_sum(missing);
+  if (lane_id() == 0 && count_missing && missing) atomicAdd(&ctl->stat[ST_MISSING], missing);
 }
 
 __device__ __forceinline__ uint32_t next_pow2_u32(uint32_t x) {
@@ -404,10 +493,22 @@ cudaError_t sort_pairs(void *temp, size_t &temp_bytes, const u64 *kin, u64 *kout
                                          64, s);
 }
 
+size_t unique_runs_temp_bytes(uint32_t cnt) {
+  size_t b = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                (int)cnt);
+  return b;
+}
+
 cudaError_t launch_unique_runs(const u64 *k, uint32_t cnt, uint2 *uv, uint32_t *mult,
-                               uint32_t *n_out, uint32_t cap, uint32_t *err, cudaStream_t s) {
+                               uint32_t *n_out, uint32_t cap, uint32_t *err, uint32_t *flags,
+                               uint32_t *pos, void *temp, size_t temp_bytes, cudaStream_t s) {
   if (!cnt) return cudaSuccess;
-  unique_runs_kernel<<<grid_for(cnt), BLOCK, 0, s>>>(k, cnt, uv, mult, n_out, cap, err);
+  run_heads_kernel<<<grid_for(cnt), BLOCK, 0, s>>>(k, cnt, flags);
+  size_t tb = temp_bytes;
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, tb, flags, pos, (int)cnt, s);
+  if (e != cudaSuccess) return e;
+  run_emit_kernel<<<grid_for(cnt), BLOCK, 0, s>>>(k, cnt, flags, pos, uv, mult, n_out, cap, err);
   return cudaGetLastError();
 }
 
@@ -423,8 +524,50 @@ cudaError_t launch_delete_rows(const Adj &A, const uint2 *uv, const uint32_t *mu
                                int count_missing, const Tombs &T, cudaStream_t s) {
   if (!max_n) return cudaSuccess;
   cudaMemsetAsync(T.count, 0, 4, s);
+  DeferDel off{};
   delete_rows_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, uv, mult, n_ptr, found, ctl,
-                                                                 count_missing, T);
+                                                                 count_missing, T, off);
+  tombstone_kernel<<<grid_for(max_n), BLOCK, 0, s>>>(A, T, ctl);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_delete_prefix(const Adj &A, const uint2 *uv, const uint32_t *mult,
+                                 const uint32_t *n_ptr, uint32_t max_n, uint32_t *found, Ctl *ctl,
+                                 int count_missing, const Tombs &T, const DeferDel &D,
+                                 cudaStream_t s) {
+  if (!max_n) return cudaSuccess;
+  cudaMemsetAsync(T.count, 0, 4, s);
+  cudaMemsetAsync(D.packed, 0, 8, s);
+  delete_rows_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, uv, mult, n_ptr, found, ctl,
+                                                                 count_missing, T, D);
+  return cudaGetLastError();
+}
+
+size_t delete_sort_temp_bytes(u64 total) {
+  size_t b = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, b, (const u64 *)nullptr, (u64 *)nullptr,
+                                  (const uint32_t *)nullptr, (uint32_t *)nullptr, (int64_t)total,
+                                  0, 64);
+  return b;
+}
+
+cudaError_t launch_delete_suffix(const Adj &A, const uint2 *uv, const uint32_t *n_ptr,
+                                 uint32_t max_n, uint32_t *found, Ctl *ctl, int count_missing,
+                                 const Tombs &T, const DeferDel &D, uint32_t nrows, u64 total,
+                                 const DeferBufs &B, cudaStream_t s) {
+  if (!max_n) return cudaSuccess;
+  if (nrows && total) {
+    suffix_gather_kernel<<<grid_for(total), BLOCK, 0, s>>>(A, D, nrows, total, B.k_in, B.v_in, ctl);
+    size_t tb = B.temp_bytes;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(B.temp, tb, B.k_in, B.k_out, B.v_in, B.v_out,
+                                                    (int64_t)total, 0, 64, s);
+    if (e != cudaSuccess) return e;
+    suffix_match_kernel<<<grid_for(max_n), BLOCK, 0, s>>>(A, uv, n_ptr, D, B.k_out, B.v_out, total,
+                                                          found, ctl, count_missing, T);
+  } else if (nrows) {
+    suffix_match_kernel<<<grid_for(max_n), BLOCK, 0, s>>>(A, uv, n_ptr, D, B.k_out, B.v_out, 0,
+                                                          found, ctl, count_missing, T);
+  }
   tombstone_kernel<<<grid_for(max_n), BLOCK, 0, s>>>(A, T, ctl);
   return cudaGetLastError();
 }

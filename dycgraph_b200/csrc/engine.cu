@@ -629,13 +629,17 @@ void Engine::ensure_batch(size_t cnt) {
   defer_.packed = (u64 *)(counts_ + 12);  // 8-byte aligned slot of the counters
   defer_.cap_rows = (uint32_t)c;
   d_edges_ = (dycg_edge_dev *)al(c * 2 * sizeof(dycg_edge_dev));
-  run_flags_ = (uint32_t *)al(c * 4);
-  run_pos_ = (uint32_t *)al(c * 4);
+  runs_.flags = (uint32_t *)al(c * 4);
+  runs_.pos = (uint32_t *)al(c * 4);
+  runs_.start = (uint32_t *)al(c * 4);
+  runs_.valid = counts_ + 14;
   size_t a = 0, b = 0;
   CK(sort_keys(nullptr, a, k_tmp_out_, k_del_out_, (uint32_t)c, st_));
   CK(sort_pairs(nullptr, b, k_tmp_out_, k_add_out_, w_tmp_, w_add_out_, (uint32_t)c, st_));
   cub_bytes_ = std::max(std::max(a, b), unique_runs_temp_bytes((uint32_t)c));
   cub_temp_ = al(cub_bytes_);
+  runs_.temp = cub_temp_;  // used between the sorts, on the same stream
+  runs_.temp_bytes = cub_bytes_;
   if (h_stage_) {
     cudaFreeHost(h_stage_);
     hallocs_.erase(std::find(hallocs_.begin(), hallocs_.end(), (void *)h_stage_));
@@ -707,15 +711,13 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
                         nullptr, invalid, st_));
     CK(sort_keys(cub_temp_, tb, k_tmp_out_, k_del_out_, (uint32_t)nd, st_));
     CK(launch_unique_runs(k_del_out_, (uint32_t)nd, uv_out_, mult_out_, counts_ + 0,
-                          (uint32_t)bcap_, &ctl_->err, run_flags_, run_pos_, cub_temp_,
-                          cub_bytes_, st_));
+                          (uint32_t)bcap_, &ctl_->err, runs_, st_));
     launches_ += 5;
     if (has_in_) {
       tb = cub_bytes_;
       CK(sort_keys(cub_temp_, tb, k_tmp_in_, k_del_in_, (uint32_t)nd, st_));
       CK(launch_unique_runs(k_del_in_, (uint32_t)nd, uv_in_, mult_in_, counts_ + 1,
-                            (uint32_t)bcap_, &ctl_->err, run_flags_, run_pos_, cub_temp_,
-                            cub_bytes_, st_));
+                            (uint32_t)bcap_, &ctl_->err, runs_, st_));
       launches_ += 4;
     }
   }
@@ -724,13 +726,15 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
     CK(launch_prep_keys(d_adds, (uint32_t)na, n_, k_tmp_out_, has_in_ ? k_tmp_in_ : nullptr,
                         w_tmp_, invalid, st_));
     CK(sort_pairs(cub_temp_, tb, k_tmp_out_, k_add_out_, w_tmp_, w_add_out_, (uint32_t)na, st_));
-    CK(launch_row_segments(k_add_out_, (uint32_t)na, seg_out_, counts_ + 2, st_));
+    CK(launch_row_segments(k_add_out_, (uint32_t)na, seg_out_, counts_ + 2, (uint32_t)bcap_,
+                           &ctl_->err, runs_, st_));
     CK(launch_keys_to_uvw(k_add_out_, w_add_out_, (uint32_t)na, add_uvw_, st_));
     launches_ += 4;
     if (has_in_) {
       tb = cub_bytes_;
       CK(sort_pairs(cub_temp_, tb, k_tmp_in_, k_add_in_, w_tmp_, w_add_in_, (uint32_t)na, st_));
-      CK(launch_row_segments(k_add_in_, (uint32_t)na, seg_in_, counts_ + 3, st_));
+      CK(launch_row_segments(k_add_in_, (uint32_t)na, seg_in_, counts_ + 3, (uint32_t)bcap_,
+                             &ctl_->err, runs_, st_));
       launches_ += 2;
     }
   }
@@ -1516,12 +1520,16 @@ void Engine::policy_trace(uint32_t snapshots) {
 void Engine::policy_prefetch(size_t nd, size_t na) {
   const u64 np = npages_;
   CK(cudaEventRecord(pev_[0], st_));
-  CK(cudaMemsetAsync(prows_, 0, np * 4, st_));
-  CK(cudaMemsetAsync(pmax_, 0, np * 4, st_));
   CK(cudaMemsetAsync(pdelta_, 0, np * 4, st_));
-  CK(launch_page_rows(out_.off, out_.len, n_, out_.page_base, page_shift_, prows_, pmax_, st_));
-  if (has_in_)
-    CK(launch_page_rows(in_.off, in_.len, n_, in_.page_base, page_shift_, prows_, pmax_, st_));
+  if (prefetch_count_++ % 8 == 0) {
+    // the row-layout features (rows per page, longest row) drift slowly with
+    // relocations: refreshed every 8 snapshots
+    CK(cudaMemsetAsync(prows_, 0, np * 4, st_));
+    CK(cudaMemsetAsync(pmax_, 0, np * 4, st_));
+    CK(launch_page_rows(out_.off, out_.len, n_, out_.page_base, page_shift_, prows_, pmax_, st_));
+    if (has_in_)
+      CK(launch_page_rows(in_.off, in_.len, n_, in_.page_base, page_shift_, prows_, pmax_, st_));
+  }
   if (nd) {
     CK(launch_page_delta(k_del_out_, (uint32_t)nd, out_.off, out_.page_base, page_shift_, pdelta_,
                          st_));

@@ -175,6 +175,7 @@ class Engine {
   uint32_t trace_cap_ = 0, trace_n_ = 0;
   bool trace_pending_ = false, prefetched_ = false;
   uint32_t prefetch_loaded_ = 0, prefetch_evicted_ = 0, learned_cap_div_ = 64;
+  uint64_t prefetch_count_ = 0;
   cudaEvent_t pev_[2] = {};
   u64 policy_bytes_ = 0;
 
@@ -187,7 +188,7 @@ class Engine {
   uint32_t *mult_out_ = nullptr, *mult_in_ = nullptr, *found_out_ = nullptr;
   uint3 *seg_out_ = nullptr, *seg_in_ = nullptr, *add_uvw_ = nullptr;
   uint32_t *touched_ = nullptr, *counts_ = nullptr;
-  uint32_t *run_flags_ = nullptr, *run_pos_ = nullptr;  // unique-run scan scratch
+  RunScratch runs_{};  // run finder scratch (unique deletions, row segments)
   Reloc reloc_{};
   Tombs tombs_{};
   DeferDel defer_{};

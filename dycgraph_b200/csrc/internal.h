@@ -101,12 +101,18 @@ cudaError_t sort_keys(void *temp, size_t &temp_bytes, const u64 *in, u64 *out, u
                       cudaStream_t s);
 cudaError_t sort_pairs(void *temp, size_t &temp_bytes, const u64 *kin, u64 *kout,
                        const uint32_t *vin, uint32_t *vout, uint32_t cnt, cudaStream_t s);
+// Scratch of the run finder (per batch capacity; temp = CUB scan storage).
+struct RunScratch {
+  uint32_t *flags, *pos, *start, *valid;
+  void *temp;
+  size_t temp_bytes;
+};
 size_t unique_runs_temp_bytes(uint32_t cnt);
 cudaError_t launch_unique_runs(const u64 *k, uint32_t cnt, uint2 *uv, uint32_t *mult,
-                               uint32_t *n_out, uint32_t cap, uint32_t *err, uint32_t *flags,
-                               uint32_t *pos, void *temp, size_t temp_bytes, cudaStream_t s);
+                               uint32_t *n_out, uint32_t cap, uint32_t *err, const RunScratch &S,
+                               cudaStream_t s);
 cudaError_t launch_row_segments(const u64 *k, uint32_t cnt, uint3 *seg, uint32_t *n_out,
-                                cudaStream_t s);
+                                uint32_t cap, uint32_t *err, const RunScratch &S, cudaStream_t s);
 // Deleted occurrences found by the read-only search, written afterwards.
 struct Tombs {
   u64 *pos;

@@ -37,48 +37,57 @@ __global__ void prep_keys_kernel(const dycg_edge_dev *e, uint32_t cnt, uint32_t 
   if (lane_id() == 0 && b) atomicAdd(invalid, b);
 }
 
-// Unique (row, neighbour) runs of a sorted key array with their
-// multiplicity, written in ascending key order: head flags, an exclusive sum
-// for the output slots, then one write per head. Records of one row are
-// therefore contiguous (the deletion pass relies on it).
-__global__ void run_heads_kernel(const u64 *k, uint32_t cnt, uint32_t *flags) {
+// Runs of a sorted key array, found without any serial walk (a hub row or a
+// heavily repeated edge can span tens of thousands of keys): head flags, an
+// exclusive sum for the output slots, one start index per run, and the run
+// lengths as differences of consecutive starts. ROWS: runs of equal row
+// (key >> 32); otherwise runs of equal key. Sentinel keys (KEY_INF, the
+// invalid records, sorted last) belong to no run. Runs come out in ascending
+// key order, so the records of one row are contiguous.
+template <bool ROWS>
+__device__ __forceinline__ bool same_run(u64 a, u64 b) {
+  return ROWS ? (a >> 32) == (b >> 32) : a == b;
+}
+
+template <bool ROWS>
+__global__ void run_heads_kernel(const u64 *k, uint32_t cnt, uint32_t *flags, uint32_t *valid) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
     const u64 key = k[i];
-    flags[i] = key != KEY_INF && (i == 0 || k[i - 1] != key);
+    flags[i] = key != KEY_INF && (i == 0 || !same_run<ROWS>(k[i - 1], key));
+    // end of the non-sentinel keys
+    if (key != KEY_INF && (i + 1 == cnt || k[i + 1] == KEY_INF)) *valid = i + 1;
   }
 }
 
-__global__ void run_emit_kernel(const u64 *k, uint32_t cnt, const uint32_t *flags,
-                                const uint32_t *pos, uint2 *uv, uint32_t *mult, uint32_t *n_out,
-                                uint32_t cap, uint32_t *err) {
+__global__ void run_starts_kernel(uint32_t cnt, const uint32_t *flags, const uint32_t *pos,
+                                  uint32_t *start, uint32_t *n_out, uint32_t cap, uint32_t *err) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
     if (i == cnt - 1) *n_out = min(pos[i] + flags[i], cap);
     if (!flags[i]) continue;
-    const u64 key = k[i];
-    uint32_t j = i + 1;
-    while (j < cnt && k[j] == key) j++;
-    const uint32_t slot = pos[i];
-    if (slot < cap) {
-      uv[slot] = make_uint2((uint32_t)(key >> 32), (uint32_t)key);
-      mult[slot] = j - i;
-    } else {
-      atomicCAS(err, 0u, ERR_QUEUE);
-    }
+    if (pos[i] < cap) start[pos[i]] = i;
+    else atomicCAS(err, 0u, ERR_QUEUE);
   }
 }
 
-// Row segments (row, first index, count) of a sorted key array.
-__global__ void row_segments_kernel(const u64 *k, uint32_t cnt, uint3 *seg, uint32_t *n_out) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
-       i += gridDim.x * blockDim.x) {
-    const u64 key = k[i];
-    if (key == KEY_INF) continue;
-    const uint32_t row = (uint32_t)(key >> 32);
-    if (i > 0 && (uint32_t)(k[i - 1] >> 32) == row) continue;
-    uint32_t j = i + 1;
-    while (j < cnt && k[j] != KEY_INF && (uint32_t)(k[j] >> 32) == row) j++;
-    const uint32_t slot = atomicAdd(n_out, 1u);
-    seg[slot] = make_uint3(row, i, j - i);
+// unique (u, v) records with their multiplicity
+__global__ void runs_emit_kernel(const u64 *k, const uint32_t *start, const uint32_t *n_ptr,
+                                 const uint32_t *valid, uint2 *uv, uint32_t *mult) {
+  const uint32_t n = *n_ptr;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const uint32_t b = start[r], e = r + 1 < n ? start[r + 1] : *valid;
+    const u64 key = k[b];
+    uv[r] = make_uint2((uint32_t)(key >> 32), (uint32_t)key);
+    mult[r] = e - b;
+  }
+}
+
+// row segments (row, first index, count)
+__global__ void segs_emit_kernel(const u64 *k, const uint32_t *start, const uint32_t *n_ptr,
+                                 const uint32_t *valid, uint3 *seg) {
+  const uint32_t n = *n_ptr;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const uint32_t b = start[r], e = r + 1 < n ? start[r + 1] : *valid;
+    seg[r] = make_uint3((uint32_t)(k[b] >> 32), b, e - b);
   }
 }
 
@@ -500,22 +509,34 @@ size_t unique_runs_temp_bytes(uint32_t cnt) {
   return b;
 }
 
-cudaError_t launch_unique_runs(const u64 *k, uint32_t cnt, uint2 *uv, uint32_t *mult,
-                               uint32_t *n_out, uint32_t cap, uint32_t *err, uint32_t *flags,
-                               uint32_t *pos, void *temp, size_t temp_bytes, cudaStream_t s) {
-  if (!cnt) return cudaSuccess;
-  run_heads_kernel<<<grid_for(cnt), BLOCK, 0, s>>>(k, cnt, flags);
-  size_t tb = temp_bytes;
-  cudaError_t e = cub::DeviceScan::ExclusiveSum(temp, tb, flags, pos, (int)cnt, s);
+template <bool ROWS>
+static cudaError_t run_starts(const u64 *k, uint32_t cnt, uint32_t *n_out, uint32_t cap,
+                              uint32_t *err, const RunScratch &S, cudaStream_t s) {
+  cudaMemsetAsync(S.valid, 0, 4, s);
+  run_heads_kernel<ROWS><<<grid_for(cnt), BLOCK, 0, s>>>(k, cnt, S.flags, S.valid);
+  size_t tb = S.temp_bytes;
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(S.temp, tb, S.flags, S.pos, (int)cnt, s);
   if (e != cudaSuccess) return e;
-  run_emit_kernel<<<grid_for(cnt), BLOCK, 0, s>>>(k, cnt, flags, pos, uv, mult, n_out, cap, err);
+  run_starts_kernel<<<grid_for(cnt), BLOCK, 0, s>>>(cnt, S.flags, S.pos, S.start, n_out, cap, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unique_runs(const u64 *k, uint32_t cnt, uint2 *uv, uint32_t *mult,
+                               uint32_t *n_out, uint32_t cap, uint32_t *err, const RunScratch &S,
+                               cudaStream_t s) {
+  if (!cnt) return cudaSuccess;
+  cudaError_t e = run_starts<false>(k, cnt, n_out, cap, err, S, s);
+  if (e != cudaSuccess) return e;
+  runs_emit_kernel<<<grid_for(cnt), BLOCK, 0, s>>>(k, S.start, n_out, S.valid, uv, mult);
   return cudaGetLastError();
 }
 
 cudaError_t launch_row_segments(const u64 *k, uint32_t cnt, uint3 *seg, uint32_t *n_out,
-                                cudaStream_t s) {
+                                uint32_t cap, uint32_t *err, const RunScratch &S, cudaStream_t s) {
   if (!cnt) return cudaSuccess;
-  row_segments_kernel<<<grid_for(cnt), BLOCK, 0, s>>>(k, cnt, seg, n_out);
+  cudaError_t e = run_starts<true>(k, cnt, n_out, cap, err, S, s);
+  if (e != cudaSuccess) return e;
+  segs_emit_kernel<<<grid_for(cnt), BLOCK, 0, s>>>(k, S.start, n_out, S.valid, seg);
   return cudaGetLastError();
 }
 

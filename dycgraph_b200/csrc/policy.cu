@@ -52,16 +52,32 @@ int grid_for(u64 threads) {
 
 // ---- features ----------------------------------------------------------------
 
-// Rows starting in each page and the longest of them (one arena).
+// Rows starting in each page and the longest of them (one arena). Rows laid
+// out in vertex order share pages, so a warp whose lanes all land in one page
+// adds once.
 __global__ void page_rows_kernel(const u64 *off, const uint32_t *len, uint32_t n,
                                  uint32_t page_base, uint32_t page_shift, uint32_t *rows,
                                  uint32_t *maxlen) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    const uint32_t l = len[v];
-    if (!l) continue;
-    const uint32_t p = page_base + (uint32_t)(off[v] >> page_shift);
-    atomicAdd(rows + p, 1u);
-    atomicMax(maxlen + p, l);
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t v0 = blockIdx.x * blockDim.x + threadIdx.x - lane; v0 < n;
+       v0 += gridDim.x * blockDim.x) {  // warp-uniform
+    const uint32_t v = v0 + lane;
+    const uint32_t l = v < n ? len[v] : 0;
+    const uint32_t p = l ? page_base + (uint32_t)(off[v] >> page_shift) : 0xFFFFFFFFu;
+    const uint32_t p0 = __shfl_sync(0xffffffffu, p, 0);
+    const bool uni = __all_sync(0xffffffffu, p == p0 || p == 0xFFFFFFFFu) && p0 != 0xFFFFFFFFu;
+    if (uni) {
+      const unsigned has = __ballot_sync(0xffffffffu, l != 0);
+      uint32_t m = l;
+      for (int o = 16; o; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+      if (lane == 0) {
+        atomicAdd(rows + p0, (uint32_t)__popc(has));
+        atomicMax(maxlen + p0, m);
+      }
+    } else if (l) {
+      atomicAdd(rows + p, 1u);
+      atomicMax(maxlen + p, l);
+    }
   }
 }
 

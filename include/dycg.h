@@ -381,7 +381,8 @@ int dycg_gather_query(dycg_engine *e, uint32_t q, uint32_t *values, uint32_t *pa
  * accumulation) right after a snapshot's ingest, from per-page features (page
  * reads in each of the last four snapshots, update records of this batch
  * whose row starts in the page, snapshots since the last read, rows starting
- * in the page and the longest of them), and stages the pages it predicts to
+ * in the page and the longest of them -- these two refreshed every 8
+ * snapshots), and stages the pages it predicts to
  * be read most (predicted reads >= 64) before the mutation and repair, up to
  * cache pages/64 per snapshot. Which pages are cached never changes results.
  * The network predicts log1p(page reads in this snapshot) and is trained on

@@ -918,7 +918,8 @@ def run_learned(args):
             "hit_rate": round(hbm / max(1, hbm + link), 4),
             "per_step": {k: round(float(np.mean([p[k] for p in per])), 4) for k in
                          ("ms_ingest", "ms_mutate", "ms_repair", "ms_cache", "ms_total",
-                          "affected", "edges_scanned", "cache_pages_loaded", "missing_deletes")},
+                          "affected", "edges_scanned", "cache_pages_loaded", "missing_deletes",
+                          "mutate_link_bytes", "mutate_hbm_bytes")},
             "cached_pages": info["cached_pages"], "cache_slots": info["cache_slots"],
             "load_s": round(t_load, 1), "static_solve_s": round(t_init, 1),
             "gpu_launches": int(sum(p["kernel_launches"] for p in per)),

@@ -749,9 +749,6 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
     launches_ += (nd ? 1 : 0) + (na ? 1 : 0);
   }
   if (!capture) CK(cudaEventRecord(ev_[1], st_));
-  // learned admission / trace features, between ingest and mutation
-  if (!capture && feat_ && (policy_ == DYCG_CACHE_LEARNED || trace_n_ < trace_cap_))
-    policy_prefetch(nd, na);
   const u64 timeout = 60ull * 1000000000ull;
   PrLaunch PL{};
   if (opt_.algo == DYCG_ALGO_PR) {
@@ -800,6 +797,10 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
     }
   }
   if (!capture) CK(cudaEventRecord(ev_[2], st_));
+  // learned admission / trace features, between mutation and repair: rows
+  // that moved to new blocks in this snapshot are seen at their new pages
+  if (!capture && feat_ && (policy_ == DYCG_CACHE_LEARNED || trace_n_ < trace_cap_))
+    policy_prefetch(nd, na);
   // ---- repair
   if (opt_.algo == DYCG_ALGO_PR) {
     PL.phases = (nd + na) ? (PR_AMEND | PR_CONVERGE) : PR_CONVERGE;
@@ -928,12 +929,12 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     stats->mutate_hbm_bytes = c.stat[ST_MUT_HBM_BYTES];
     stats->ms_ingest = ms[0];
     stats->ms_mutate = ms[1];
-    if (prefetched_) {  // the learned admission ran inside the mutation stage's events
+    stats->ms_repair = ms[2];
+    if (prefetched_) {  // the learned admission ran inside the repair stage's events
       float pm = 0;
       cudaEventElapsedTime(&pm, pev_[0], pev_[1]);
-      stats->ms_mutate -= pm;
+      stats->ms_repair -= pm;
     }
-    stats->ms_repair = ms[2];
   }
   if (maintenance) cache_maintenance(false, stats);
   if (stats) {
@@ -1507,7 +1508,7 @@ void Engine::policy_trace(uint32_t snapshots) {
   if (ty_) cudaFree(ty_);
   tx_ = nullptr;
   ty_ = nullptr;
-  trace_cap_ = trace_n_ = 0;
+  trace_cap_ = trace_n_ = trace_post_ = 0;
   if (!snapshots) return;
   CK(cudaMalloc(&tx_, (u64)snapshots * npages_ * POLICY_F * 2));
   CK(cudaMalloc((void **)&ty_, (u64)snapshots * npages_ * 4));
@@ -1544,13 +1545,15 @@ void Engine::policy_prefetch(size_t nd, size_t na) {
       CK(launch_page_delta(k_add_in_, (uint32_t)na, in_.off, in_.page_base, page_shift_, pdelta_,
                            st_));
   }
-  CK(launch_features(hist_, age_, pdelta_, prows_, pmax_, npages_, feat_, st_));
+  CK(launch_features(page_hits_, hist_, age_, pdelta_, prows_, pmax_, npages_, feat_, st_));
   launches_ += 3 + (has_in_ ? 1 : 0) + (nd ? 1 : 0) * (has_in_ ? 2 : 1) +
                (na ? 1 : 0) * (has_in_ ? 2 : 1);
   trace_pending_ = trace_n_ < trace_cap_;
-  if (trace_pending_)
+  if (trace_pending_) {
     CK(cudaMemcpyAsync((char *)tx_ + (u64)trace_n_ * np * POLICY_F * 2, feat_,
                        np * POLICY_F * 2, cudaMemcpyDeviceToDevice, st_));
+    CK(cudaMemsetAsync(ty_ + (u64)trace_n_ * np, 0, np * 4, st_));
+  }
   prefetch_loaded_ = prefetch_evicted_ = 0;
   if (policy_ == DYCG_CACHE_LEARNED && cache_slots_) {
     CK(launch_mlp_infer(feat_, npages_, params_, cwk_.score, cwk_.ids, st_));
@@ -1587,12 +1590,22 @@ void Engine::policy_train(uint32_t epochs, float lr, uint32_t batch, uint64_t se
   check_loaded();
   if (!trace_n_) throw Error(DYCG_ESTATE, "no access traces recorded (dycg_policy_trace)");
   if (batch == 0 || !(lr > 0.f)) throw Error(DYCG_EINVAL, "batch and lr must be positive");
-  const u64 total = (u64)trace_n_ * npages_;
+  // traced snapshots whose target horizon is complete (at least one)
+  const int64_t complete = (int64_t)trace_n_ + trace_post_ - POLICY_HORIZON + 1;
+  const uint32_t usable = (uint32_t)std::max<int64_t>(1, std::min<int64_t>(trace_n_, complete));
+  const u64 total = (u64)usable * npages_;
+  float *ylog = nullptr;
+  CK(cudaMalloc((void **)&ylog, total * 4));
+  struct Free {
+    float *p;
+    ~Free() { cudaFree(p); }
+  } fy{ylog};
+  CK(launch_log1p(ty_, ylog, total, st_));
   auto eval = [&]() {
     CK(cudaMemsetAsync(ploss_, 0, 4, st_));
     for (u64 o = 0; o < total; o += (1ull << 30)) {
       const uint32_t c = (uint32_t)std::min<u64>(1ull << 30, total - o);
-      CK(launch_mlp_grad((const char *)tx_ + o * POLICY_F * 2, ty_ + o, c, c, 0, params_, 0.f,
+      CK(launch_mlp_grad((const char *)tx_ + o * POLICY_F * 2, ylog + o, c, c, 0, params_, 0.f,
                          grad_, ploss_, st_));
     }
     CK(cudaMemsetAsync(grad_, 0, POLICY_PARAMS * 4, st_));
@@ -1608,7 +1621,7 @@ void Engine::policy_train(uint32_t epochs, float lr, uint32_t batch, uint64_t se
   const float l0 = eval();
   const u64 steps = std::max<u64>(1, (u64)epochs * total / batch);
   for (u64 s = 0; s < steps; s++) {
-    CK(launch_mlp_grad(tx_, ty_, total, batch, mix64(seed + s + 1) | 1, params_, 2.f / batch,
+    CK(launch_mlp_grad(tx_, ylog, total, batch, mix64(seed + s + 1) | 1, params_, 2.f / batch,
                        grad_, ploss_, st_));
     CK(launch_adam(params_, grad_, adam_m_, adam_v_, lr, ++adam_step_, st_));
   }
@@ -1664,13 +1677,25 @@ void Engine::sample_row_edges(const uint32_t *sources, uint64_t count, uint64_t 
 void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
   check_loaded();
   if (feat_ && !initial) {
-    // page-read history for the learned policy, and the training target of
-    // the features taken at this snapshot's start when traces are recorded
-    float *target = trace_pending_ ? ty_ + (u64)trace_n_ * npages_ : nullptr;
+    // page-read history for the learned policy; this snapshot's reads go into
+    // the raw targets of the traced snapshots whose horizon covers it: the
+    // current snapshot is number c in trace order (traced or not)
+    TargetRefs tg{};
+    const int64_t traced = (int64_t)trace_n_ + (trace_pending_ ? 1 : 0);
+    const int64_t c = trace_pending_ ? (int64_t)trace_n_ : (int64_t)trace_n_ + trace_post_;
+    for (int j = 0; j < POLICY_HORIZON; j++) {
+      const int64_t k = c - j;
+      if (k >= 0 && k < traced) tg.t[j] = ty_ + (u64)k * npages_;
+    }
     const bool clear = policy_ != DYCG_CACHE_HOTNESS || !cache_slots_;
-    CK(launch_history(page_hits_, hist_, age_, npages_, target, clear, st_));
+    CK(launch_history(page_hits_, hist_, age_, npages_, tg, clear, st_));
     launches_++;
-    if (trace_pending_) trace_n_++;
+    if (trace_pending_) {
+      trace_n_++;
+      trace_post_ = 0;
+    } else if (trace_post_ < POLICY_HORIZON) {
+      trace_post_++;
+    }
     trace_pending_ = false;
   }
   if (policy_ == DYCG_CACHE_LEARNED && !initial) {

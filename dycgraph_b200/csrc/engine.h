@@ -172,9 +172,9 @@ class Engine {
   uint32_t adam_step_ = 0;
   void *tx_ = nullptr;
   float *ty_ = nullptr;
-  uint32_t trace_cap_ = 0, trace_n_ = 0;
+  uint32_t trace_cap_ = 0, trace_n_ = 0, trace_post_ = 0;
   bool trace_pending_ = false, prefetched_ = false;
-  uint32_t prefetch_loaded_ = 0, prefetch_evicted_ = 0, learned_cap_div_ = 64;
+  uint32_t prefetch_loaded_ = 0, prefetch_evicted_ = 0, learned_cap_div_ = 256;
   uint64_t prefetch_count_ = 0;
   cudaEvent_t pev_[2] = {};
   u64 policy_bytes_ = 0;

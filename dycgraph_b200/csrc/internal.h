@@ -209,11 +209,16 @@ cudaError_t launch_page_rows(const u64 *off, const uint32_t *len, uint32_t n, ui
                              cudaStream_t s);
 cudaError_t launch_page_delta(const u64 *keys, uint32_t cnt, const u64 *off, uint32_t page_base,
                               uint32_t page_shift, uint32_t *delta, cudaStream_t s);
-cudaError_t launch_features(const float *hist, const uint8_t *age, const uint32_t *delta,
-                            const uint32_t *rows, const uint32_t *maxlen, uint32_t npages,
-                            void *x, cudaStream_t s);
+cudaError_t launch_features(const uint32_t *hits, const float *hist, const uint8_t *age,
+                            const uint32_t *delta, const uint32_t *rows, const uint32_t *maxlen,
+                            uint32_t npages, void *x, cudaStream_t s);
+constexpr int POLICY_HORIZON = 3;  // training target: reads over this many snapshots
+struct TargetRefs {
+  float *t[POLICY_HORIZON];  // raw targets receiving this snapshot's reads (or null)
+};
 cudaError_t launch_history(uint32_t *hits, float *hist, uint8_t *age, uint32_t npages,
-                           float *target, bool clear, cudaStream_t s);
+                           const TargetRefs &tg, bool clear, cudaStream_t s);
+cudaError_t launch_log1p(const float *in, float *out, u64 n, cudaStream_t s);
 cudaError_t launch_mlp_infer(const void *x, uint32_t n, const float *params, float *score,
                              uint32_t *ids, cudaStream_t s);
 cudaError_t launch_mlp_grad(const void *x, const float *y, uint64_t total, uint32_t count,

@@ -8,12 +8,17 @@
 //
 // Unit: one cache page (2^page_shift adjacency slots). Features per page
 // (POLICY_F = 8, BF16):
-//   0-3  log1p(slot reads of the page in each of the last four snapshots)
-//   4    log1p(update records of the current batch whose row starts in the page)
+//   0    log1p(slot reads of the page so far in this snapshot: its mutation)
+//   1-2  log1p(slot reads of the page in each of the last two snapshots)
+//   3    log1p(decayed read score: score * 0.75 + reads, per snapshot -- the
+//        hotness policy's ranking signal)
+//   4    log1p(update records of the current batch whose row starts in the
+//        page, at the row's place after the mutation)
 //   5    min(snapshots since the page was last read, 16) / 16
 //   6    log1p(rows starting in the page) / 8
 //   7    log1p(longest row starting in the page) / 16
-// Target: log1p(slot reads of the page during the current snapshot). The
+// Target: log1p(slot reads of the page during the current snapshot and the
+// next POLICY_HORIZON - 1 ones), so pages rank by near-future value. The
 // network is POLICY_F -> 64 -> 64 -> 1, ReLU, BF16 weights and inputs, FP32
 // accumulation and FP32 master weights; loss = mean squared error.
 //
@@ -92,13 +97,16 @@ __global__ void page_delta_kernel(const u64 *keys, uint32_t cnt, const u64 *off,
   }
 }
 
-__global__ void features_kernel(const float *hist, const uint8_t *age, const uint32_t *delta,
-                                const uint32_t *rows, const uint32_t *maxlen, uint32_t npages,
-                                __nv_bfloat16 *x) {
+__global__ void features_kernel(const uint32_t *hits, const float *hist, const uint8_t *age,
+                                const uint32_t *delta, const uint32_t *rows,
+                                const uint32_t *maxlen, uint32_t npages, __nv_bfloat16 *x) {
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npages;
        p += gridDim.x * blockDim.x) {
     float f[F];
-    for (int k = 0; k < 4; k++) f[k] = hist[(u64)k * npages + p];
+    f[0] = log1pf((float)hits[p]);
+    f[1] = hist[p];
+    f[2] = hist[1ull * npages + p];
+    f[3] = log1pf(hist[3ull * npages + p]);
     f[4] = log1pf((float)delta[p]);
     f[5] = fminf((float)age[p], 16.f) / 16.f;
     f[6] = log1pf((float)rows[p]) / 8.f;
@@ -110,22 +118,29 @@ __global__ void features_kernel(const float *hist, const uint8_t *age, const uin
 }
 
 // End of a snapshot: shift this snapshot's page reads into the history,
-// update ages, optionally write the training target for the features taken
-// at the snapshot's start, and clear the counters (unless the hotness policy
-// still has to read them).
+// decay the read score, update ages, add the reads to the raw training
+// targets of the traced snapshots whose horizon covers this one (target[j],
+// up to POLICY_HORIZON of them), and clear the counters (unless the hotness
+// policy still has to read them).
 __global__ void history_kernel(uint32_t *hits, float *hist, uint8_t *age, uint32_t npages,
-                               float *target, bool clear) {
+                               TargetRefs tg, bool clear) {
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npages;
        p += gridDim.x * blockDim.x) {
-    const float y = log1pf((float)hits[p]);
-    hist[3ull * npages + p] = hist[2ull * npages + p];
+    const uint32_t h = hits[p];
     hist[2ull * npages + p] = hist[1ull * npages + p];
     hist[1ull * npages + p] = hist[p];
-    hist[p] = y;
-    age[p] = hits[p] ? 0 : (uint8_t)min(255, age[p] + 1);
-    if (target) target[p] = y;
+    hist[p] = log1pf((float)h);
+    hist[3ull * npages + p] = hist[3ull * npages + p] * 0.75f + (float)h;
+    age[p] = h ? 0 : (uint8_t)min(255, age[p] + 1);
+    for (int j = 0; j < POLICY_HORIZON; j++)
+      if (tg.t[j]) tg.t[j][p] += (float)h;
     if (clear) hits[p] = 0;
   }
+}
+
+__global__ void log1p_kernel(const float *in, float *out, u64 n) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n; i += (u64)gridDim.x * blockDim.x)
+    out[i] = log1pf(in[i]);
 }
 
 // ---- inference -----------------------------------------------------------------
@@ -332,17 +347,22 @@ cudaError_t launch_page_delta(const u64 *keys, uint32_t cnt, const u64 *off, uin
   return cudaGetLastError();
 }
 
-cudaError_t launch_features(const float *hist, const uint8_t *age, const uint32_t *delta,
-                            const uint32_t *rows, const uint32_t *maxlen, uint32_t npages,
-                            void *x, cudaStream_t s) {
-  features_kernel<<<grid_for(npages), BLOCK, 0, s>>>(hist, age, delta, rows, maxlen, npages,
+cudaError_t launch_features(const uint32_t *hits, const float *hist, const uint8_t *age,
+                            const uint32_t *delta, const uint32_t *rows, const uint32_t *maxlen,
+                            uint32_t npages, void *x, cudaStream_t s) {
+  features_kernel<<<grid_for(npages), BLOCK, 0, s>>>(hits, hist, age, delta, rows, maxlen, npages,
                                                      (__nv_bfloat16 *)x);
   return cudaGetLastError();
 }
 
 cudaError_t launch_history(uint32_t *hits, float *hist, uint8_t *age, uint32_t npages,
-                           float *target, bool clear, cudaStream_t s) {
-  history_kernel<<<grid_for(npages), BLOCK, 0, s>>>(hits, hist, age, npages, target, clear);
+                           const TargetRefs &tg, bool clear, cudaStream_t s) {
+  history_kernel<<<grid_for(npages), BLOCK, 0, s>>>(hits, hist, age, npages, tg, clear);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_log1p(const float *in, float *out, u64 n, cudaStream_t s) {
+  log1p_kernel<<<grid_for(n), BLOCK, 0, s>>>(in, out, n);
   return cudaGetLastError();
 }
 

@@ -378,22 +378,23 @@ int dycg_gather_query(dycg_engine *e, uint32_t q, uint32_t *values, uint32_t *pa
  * (include/framework/variants/driver.cuh:486-515); that is DYCG_CACHE_HOTNESS
  * here. DYCG_CACHE_LEARNED ranks every cache page with a small MLP
  * (DYCG_POLICY_FEATURES -> 64 -> 64 -> 1, ReLU, BF16 weights and inputs, FP32
- * accumulation) right after a snapshot's ingest, from per-page features (page
- * reads in each of the last four snapshots, update records of this batch
- * whose row starts in the page, snapshots since the last read, rows starting
- * in the page and the longest of them -- these two refreshed every 8
- * snapshots), and stages the pages it predicts to
- * be read most (predicted reads >= 64) before the mutation and repair, up to
- * cache pages/64 per snapshot. Which pages are cached never changes results.
- * The network predicts log1p(page reads in this snapshot) and is trained on
- * traces the engine records, by the library's own forward/backward and Adam
- * kernels on the GPU. */
+ * accumulation) after a snapshot's mutation, from per-page features (page
+ * reads of the mutation just done and of the last two snapshots, the decayed
+ * read score, update records of this batch whose row starts in the page,
+ * snapshots since the last read, rows starting in the page and the longest of
+ * them -- these two refreshed every 8 snapshots), and stages the pages it
+ * predicts to be read most (predicted reads >= 64) before the repair, up to
+ * cache pages/256 per snapshot. Which pages are cached never changes results.
+ * The network predicts log1p(page reads over this snapshot and the next
+ * two) and is trained on traces the engine records, by the library's own
+ * forward/backward and Adam kernels on the GPU; one of its history features
+ * is the hotness policy's decayed read score. */
 #define DYCG_POLICY_FEATURES 8
 #define DYCG_POLICY_HIDDEN 64
 #define DYCG_POLICY_PARAMS 4801 /* W1[8x64] b1[64] W2[64x64] b2[64] W3[64] b3, FP32 */
 
 typedef struct dycg_policy_report {
-  uint64_t samples;      /* trace samples (pages x snapshots)                  */
+  uint64_t samples;      /* trace samples used (pages x complete snapshots)    */
   uint64_t steps;        /* optimizer steps                                    */
   float loss_before;     /* mean squared error over all samples, before/after   */
   float loss_after;
@@ -405,8 +406,10 @@ typedef struct dycg_policy_report {
  * cache: a non-zero budget and a policy other than NONE at create). */
 int dycg_set_cache_policy(dycg_engine *e, uint32_t policy);
 
-/* Record (features, page reads) of the next `snapshots` snapshot calls, under
- * whatever policy is active, as the training set; 0 drops the traces. */
+/* Record the features of the next `snapshots` snapshot calls and their page
+ * reads (over each snapshot and the two after it), under whatever policy is
+ * active, as the training set; 0 drops the traces. Training uses the traced
+ * snapshots whose two following snapshots have also run. */
 int dycg_policy_trace(dycg_engine *e, uint32_t snapshots);
 
 /* Train the network on the recorded traces with Adam (lr), minibatches of

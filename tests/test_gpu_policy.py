@@ -79,7 +79,9 @@ def test_learned_policy_trains_and_keeps_results_exact():
         e.apply_batch(d, a)
         orc.mutate(d, a)
     rep = e.policy_train(epochs=4, lr=2e-3, batch=1024, seed=3)
-    assert rep["samples"] == 4 * e.info()["pages"] and rep["steps"] > 0
+    # 4 traced snapshots, one more applied: targets span 3 snapshots, so the
+    # first 3 traced snapshots have complete targets
+    assert rep["samples"] == 3 * e.info()["pages"] and rep["steps"] > 0
     assert rep["loss_after"] < rep["loss_before"]
     e.set_cache_policy("learned")
     for _ in range(4):

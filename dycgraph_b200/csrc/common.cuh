@@ -113,6 +113,8 @@ struct Adj {
   uint32_t *tbits;       // HBM deletion bitmap, one bit per arena slot
 };
 
+constexpr uint32_t BAR_GROUPS = 16;
+
 // Per-launch control block in device memory: barrier, queues, counters.
 struct Ctl {
   uint32_t bar_count;
@@ -132,6 +134,8 @@ struct Ctl {
   uint32_t waves;        // waves run in this launch
   uint32_t pad[2];
   u64 stat[20];
+  // grid-barrier arrival groups, one 128-byte line each (frontier.cuh)
+  uint32_t bar_sub[BAR_GROUPS * 32];
 };
 
 enum StatIdx {

@@ -18,10 +18,19 @@ constexpr uint32_t SYNC_RESET_Q1 = 4;
 constexpr uint32_t SYNC_RESET_Q2 = 8;
 constexpr uint32_t SYNC_RESET_VMIN = 16;
 
-// Grid-wide barrier for cooperative launches. Every wait is bounded: past
-// timeout_ns the waiting block records ERR_BARRIER and all blocks leave at
-// their next barrier. The last block to arrive snapshots the queue counters
-// and applies the requested resets while every other block is waiting.
+// Back-off of a block waiting at the grid barrier between polls (ns).
+#ifndef DYCG_SPIN_NS
+#define DYCG_SPIN_NS 100
+#endif
+
+// Grid-wide barrier for cooperative launches. Arrival is two-level: a block
+// arrives at one of BAR_GROUPS group counters (separate 128-byte lines) and
+// only the last arriver of each group arrives at the top counter, so the
+// serialised atomics per barrier drop from one per block to about
+// blocks / BAR_GROUPS + BAR_GROUPS. Every wait is bounded: past timeout_ns
+// the waiting block records ERR_BARRIER and all blocks leave at their next
+// barrier. The last block to arrive snapshots the queue counters and applies
+// the requested resets while every other block is waiting.
 __device__ __forceinline__ bool grid_sync(Ctl *c, uint32_t flags, u64 timeout_ns) {
   __shared__ int s_ok;
   __syncthreads();
@@ -30,9 +39,16 @@ __device__ __forceinline__ bool grid_sync(Ctl *c, uint32_t flags, u64 timeout_ns
     volatile uint32_t *verr = &c->err;
     uint32_t g = *vgen;
     __threadfence();
-    uint32_t arrived = atomicAdd(&c->bar_count, 1u) + 1;
+    const uint32_t groups = min(gridDim.x, BAR_GROUPS);
+    const uint32_t grp = blockIdx.x % groups;
+    const uint32_t members = (gridDim.x - grp + groups - 1) / groups;
+    bool last = false;
+    if (atomicAdd(&c->bar_sub[grp * 32], 1u) + 1 == members) {
+      atomicExch(&c->bar_sub[grp * 32], 0u);  // every member has arrived
+      last = atomicAdd(&c->bar_count, 1u) + 1 == groups;
+    }
     int ok = 1;
-    if (arrived == gridDim.x) {
+    if (last) {
       if (flags & SYNC_RESET_TILES) c->tile_count = 0;
       if (flags & SYNC_RESET_Q0) c->q_count[0] = 0;
       if (flags & SYNC_RESET_Q1) c->q_count[1] = 0;
@@ -59,7 +75,7 @@ __device__ __forceinline__ bool grid_sync(Ctl *c, uint32_t flags, u64 timeout_ns
           ok = 0;
           break;
         }
-        __nanosleep(100);
+        if (DYCG_SPIN_NS) __nanosleep(DYCG_SPIN_NS);
       }
     }
     __threadfence();

@@ -434,6 +434,11 @@ def run_reference(args):
     if algo == "pr" or args.config == "grid":
         return {"impl": "reference",
                 "unavailable": "the CPU reference arm is wired for SSSP/BFS/CC on R-MAT configs"}
+    if args.config in ("batched", "learned"):
+        return {"impl": "reference",
+                "unavailable": "the reference engine has no many-query form or learned admission; "
+                               "these configurations report the CPU oracle in their cpu_baseline "
+                               "and compare against this build's plain path"}
     threads = os.cpu_count() or 1
     t0 = time.time()
     n, off, dst, w = oracle.rmat_csr(args.scale, args.edge_factor, args.seed, wlo=1, whi=64,
@@ -664,7 +669,8 @@ def run_batched(args):
     per_step = {k: round(float(np.mean([p[k] for p in per])), 4) for k in
                 ("ms_ingest", "ms_mutate", "ms_repair", "ms_cache", "ms_total", "affected",
                  "expanded", "edges_scanned", "improvements", "waves", "missing_deletes",
-                 "cache_pages_loaded")}
+                 "cache_pages_loaded", "ms_phase_invalidate", "ms_phase_pull", "ms_phase_seed",
+                 "ms_phase_closure")}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = query_cpu_baseline(eng, args, algo, int(sources[0]), Q)

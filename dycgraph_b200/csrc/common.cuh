@@ -134,6 +134,7 @@ struct Ctl {
   uint32_t waves;        // waves run in this launch
   uint32_t pad[2];
   u64 stat[20];
+  u64 tphase[8];         // batched repair: global timer at phase boundaries (ns)
   // grid-barrier arrival groups, one 128-byte line each (frontier.cuh)
   uint32_t bar_sub[BAR_GROUPS * 32];
 };

@@ -33,6 +33,7 @@ namespace dycg {
   } while (0)
 
 static u64 round_up(u64 x, u64 m) { return (x + m - 1) / m * m; }
+static void fill_phases(dycg_batch_stats *s, const Ctl &c);
 
 Engine::Engine(const dycg_options &opt) : opt_(opt) {
   if (opt_.algo > DYCG_ALGO_PR) throw Error(DYCG_EINVAL, "unknown algorithm");
@@ -945,11 +946,29 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
     // repair kernels' vertex-state bytes (algorithmic): per expanded row its
     // 16-byte descriptor and 8-byte key, per scanned slot the neighbour's
     // 8-byte key, per improvement 8 B key atomic + 4 B tag + 4 B queue slot
-    if (nq_ && qmode_ == DYCG_QUERIES_BATCHED)
+    if (nq_ && qmode_ == DYCG_QUERIES_BATCHED) {
       // batched: the kernel counts 8 B per (edge, active query) key access
       stats->state_bytes = c.stat[ST_STATE_BYTES] + stats->expanded * 16 + stats->improvements * 16;
+      fill_phases(stats, c);
+    }
     else
       stats->state_bytes = stats->expanded * 24 + stats->edges_scanned * 8 + stats->improvements * 16;
+  }
+}
+
+// Phase times of a batched repair from the kernel's own timer stamps
+// (phases a launch skipped have no stamp and count zero).
+static void fill_phases(dycg_batch_stats *s, const Ctl &c) {
+  const u64 t[4] = {c.tphase[0], c.tphase[1], c.tphase[2], c.tphase[3]};
+  double *out[4] = {&s->ms_phase_invalidate, &s->ms_phase_pull, &s->ms_phase_seed,
+                    &s->ms_phase_closure};
+  u64 prev = c.stat[ST_T_START];
+  for (int i = 0; i < 4; i++) {
+    *out[i] = 0;
+    if (t[i] && prev && t[i] >= prev) {
+      *out[i] = (t[i] - prev) * 1e-6;
+      prev = t[i];
+    }
   }
 }
 
@@ -1432,6 +1451,7 @@ void Engine::apply_batches(const dycg_edge *dels, const uint64_t *nd, const dycg
       // the repair kernel's own start/end stamps (no stage events in a graph)
       if (c.stat[ST_T_END] > c.stat[ST_T_START] && c.stat[ST_T_START])
         s->ms_repair = (c.stat[ST_T_END] - c.stat[ST_T_START]) * 1e-6;
+      fill_phases(s, c);
     }
   }
   // cache maintenance once, after the last snapshot

@@ -675,6 +675,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
         cur ^= 1;
       }
     }
+    if (gtid == 0) ctl->tphase[0] = globaltimer_ns();  // seeds + invalidation done
     // 3. reset the affected (v, q)
     {
       const uint32_t na = *(volatile uint32_t *)&ctl->snap_aff;
@@ -691,6 +692,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
       PullPh<ALGO, STORED, NB> ph{&P};
       auto prep = [&](uint32_t v, uint32_t (&m)[NB]) { return take_masks<NB>(P.affm, v, false, m); };
       if (!multi_expand<NB, STORED>(P, P.in, P.aff, na, prep, ph, s, s_stage, acc, 0)) goto done;
+      if (gtid == 0) ctl->tphase[1] = globaltimer_ns();  // reset + pull done
     }
   }
   {
@@ -741,6 +743,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
     }
   }
   if (!grid_sync(ctl, 0, P.timeout_ns)) goto done;
+  if (gtid == 0) ctl->tphase[2] = globaltimer_ns();  // frontier + insertion seeds done
   // 6. closure waves
   if (P.phases & PH_CLOSE) {
     uint32_t cur = 0;
@@ -762,6 +765,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
       cur ^= 1;
     }
   }
+  if (gtid == 0) ctl->tphase[3] = globaltimer_ns();  // closure done
   // 7. clear the snapshot's affected masks
   if (P.phases & PH_DELETE) {
     const uint32_t na = *(volatile uint32_t *)&ctl->snap_aff;

@@ -52,14 +52,16 @@ _STAT_U64 = ["deletions", "insertions", "missing_deletes", "invalid_updates", "t
              "cache_pages_evicted", "kernel_launches"]
 _STAT_F64 = ["ms_ingest", "ms_mutate", "ms_repair", "ms_cache", "ms_total"]
 _STAT_TAIL = ["mutate_link_bytes", "mutate_hbm_bytes"]
+_STAT_PHASE = ["ms_phase_invalidate", "ms_phase_pull", "ms_phase_seed", "ms_phase_closure"]
 
 
 class BatchStats(ctypes.Structure):
     _fields_ = ([(k, ctypes.c_uint64) for k in _STAT_U64] + [(k, ctypes.c_double) for k in _STAT_F64]
-                + [(k, ctypes.c_uint64) for k in _STAT_TAIL] + [("reserved", ctypes.c_uint64 * 6)])
+                + [(k, ctypes.c_uint64) for k in _STAT_TAIL]
+                + [(k, ctypes.c_double) for k in _STAT_PHASE] + [("reserved", ctypes.c_uint64 * 2)])
 
     def as_dict(self):
-        return {k: getattr(self, k) for k in _STAT_U64 + _STAT_F64 + _STAT_TAIL}
+        return {k: getattr(self, k) for k in _STAT_U64 + _STAT_F64 + _STAT_TAIL + _STAT_PHASE}
 
 
 class QueryMapping(ctypes.Structure):

@@ -122,7 +122,12 @@ typedef struct dycg_batch_stats {
   double ms_total;
   uint64_t mutate_link_bytes;  /* mutation kernels' share of link_bytes      */
   uint64_t mutate_hbm_bytes;   /* mutation kernels' share of hbm_adj_bytes    */
-  uint64_t reserved[6];
+  /* batched many-query form: time inside the repair kernel per phase */
+  double ms_phase_invalidate;  /* deletion seeds + invalidation waves        */
+  double ms_phase_pull;        /* reset + pull over in-rows                  */
+  double ms_phase_seed;        /* frontier + insertion seeds                 */
+  double ms_phase_closure;     /* push closure waves                         */
+  uint64_t reserved[2];
 } dycg_batch_stats;
 
 typedef struct dycg_graph_info {

@@ -724,7 +724,7 @@ def run_batched(args):
                    "updates_timed": timed_updates,
                    "snapshot_sizes": [int(x) for x in sizes[W:W + K]],
                    "weights": "uint32 uniform [1,64] stored" if algo == "sssp" else "rule",
-                   "mapping": {k: mapping[k] for k in ("qratio", "heavy", "tile")},
+                   "mapping": {k: mapping.get(k) for k in ("qratio", "heavy", "tile", "pull_qratio")},
                    "mapping_tuned_on": (f"one {args.tune_batch}-update snapshot, "
                                         f"{len(tried)} candidates") if tried else "not tuned",
                    "replay": "one dycg_apply_batches_device call for the timed snapshots "
@@ -741,7 +741,8 @@ def run_batched(args):
         "gpu_launches": launches,
         "roofline": roofline,
         "per_step": per_step,
-        "mapping_candidates": [[t["qratio"], t["heavy"], round(t["repair_ms"], 3)] for t in tried],
+        "mapping_candidates": [[t["qratio"], t["heavy"], t["pull_qratio"], round(t["repair_ms"], 3)]
+                               for t in tried],
         "plain_per_query": plain,
         "speedup_vs_plain": round(value / plain["value"], 2) if plain else None,
     }

@@ -1036,7 +1036,7 @@ void Engine::set_queries(const uint32_t *sources, uint32_t count, uint32_t mode)
 void Engine::set_query_mapping(uint32_t qratio, uint32_t heavy, uint32_t tile) {
   if (heavy == 0) throw Error(DYCG_EINVAL, "heavy must be >= 1");
   if (tile < MULTI_MIN_TILE) throw Error(DYCG_EINVAL, "tile must be >= 1024 slots");
-  qratio_ = qratio;
+  qratio_ = pull_qratio_ = qratio;
   heavy_ = heavy;
   tile_ = tile;
   drop_graphs();  // captured graphs hold the old mapping
@@ -1072,6 +1072,7 @@ MultiLaunch Engine::multi_launch(uint32_t phases, uint32_t n_add, u64 timeout) {
   L.phases = phases;
   L.max_waves = (uint32_t)std::min<u64>(4ull * n_ + 1024, 0x7FFFFFFFull);
   L.qratio = qratio_;
+  L.pull_qratio = pull_qratio_;
   L.heavy = heavy_;
   L.tile = tile_;
   L.timeout_ns = timeout;
@@ -1242,32 +1243,41 @@ void Engine::tune_repair(uint32_t nd, uint32_t na, u64 timeout) {
   };
   static const uint32_t kRatio[] = {2, 4, 8, 1u << 20};
   static const uint32_t kHeavy[] = {16, 64, 256};
+  static const uint32_t kPull[] = {0, 1, 2, 8};
   tried_.clear();
-  dycg_query_mapping best{qratio_, heavy_, tile_, 1e30f};
-  for (uint32_t r : kRatio)
-    for (uint32_t h : kHeavy) {
-      if (!tried_.empty()) restore();
-      qratio_ = r;
-      heavy_ = h;
-      CK(cudaEventRecord(sc.a, st_));
-      CK(launch_multi(multi_launch(phases, na, timeout), st_));
-      CK(cudaEventRecord(sc.b, st_));
-      CK(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
-      sync_check("tune");
-      if (h_ctl_->err) {
-        failed = true;
-        throw Error(DYCG_ELIMIT, "mapping trial failed on the device (error code " +
-                                     std::to_string(h_ctl_->err) + ")");
-      }
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, sc.a, sc.b));
-      tried_.push_back({r, h, tile_, ms});
-      if (ms < best.repair_ms) best = tried_.back();
-      launches_++;
+  dycg_query_mapping best{qratio_, heavy_, tile_, pull_qratio_, 1e30f};
+  auto trial = [&](uint32_t r, uint32_t h, uint32_t pr) {
+    if (!tried_.empty()) restore();
+    qratio_ = r;
+    heavy_ = h;
+    pull_qratio_ = pr;
+    CK(cudaEventRecord(sc.a, st_));
+    CK(launch_multi(multi_launch(phases, na, timeout), st_));
+    CK(cudaEventRecord(sc.b, st_));
+    CK(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
+    sync_check("tune");
+    if (h_ctl_->err) {
+      failed = true;
+      throw Error(DYCG_ELIMIT, "mapping trial failed on the device (error code " +
+                                   std::to_string(h_ctl_->err) + ")");
     }
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, sc.a, sc.b));
+    tried_.push_back({r, h, tile_, pr, ms});
+    if (ms < best.repair_ms) best = tried_.back();
+    launches_++;
+  };
+  // coordinate search: (qratio, heavy) with the pull phase on the same rule,
+  // then the pull phase's own ratio
+  for (uint32_t r : kRatio)
+    for (uint32_t h : kHeavy) trial(r, h, r);
+  const dycg_query_mapping first = best;
+  for (uint32_t pr : kPull)
+    if (pr != first.qratio) trial(first.qratio, first.heavy, pr);
   restore();
   qratio_ = best.qratio;
   heavy_ = best.heavy;
+  pull_qratio_ = best.pull_qratio;
   drop_graphs();
   CK(cudaEventRecord(ev_[2], st_));  // the stage boundary of the kept run
   CK(launch_multi(multi_launch(phases, na, timeout), st_));

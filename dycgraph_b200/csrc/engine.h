@@ -149,7 +149,7 @@ class Engine {
   Ctl *qctl_ = nullptr, *h_qctl_ = nullptr;     // per-query control blocks
   uint4 *mtiles_ = nullptr;
   uint32_t mtile_cap_ = 0;
-  uint32_t qratio_ = 4, heavy_ = 64, tile_ = 4096;
+  uint32_t qratio_ = 4, heavy_ = 64, tile_ = 4096, pull_qratio_ = 4;
   u64 qbytes_ = 0;
   bool tune_ = false;
   std::vector<dycg_query_mapping> tried_;

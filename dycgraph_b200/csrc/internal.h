@@ -60,6 +60,7 @@ struct MultiLaunch {
   uint32_t n_add;
   uint32_t n, nb, phases, max_waves;
   uint32_t qratio;              // query lanes when 4*active >= qratio*min(len,32)
+  uint32_t pull_qratio;         // the same rule for the pull phase
   uint32_t heavy;               // rows with more work (warp iterations) are tiled
   uint32_t tile;                // tile size, in slots
   u64 timeout_ns;

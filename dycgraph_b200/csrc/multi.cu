@@ -55,7 +55,7 @@ struct MultiParams {
   const uint32_t *n_del_ptr;
   const uint3 *add_uvw;
   uint32_t n_add;
-  uint32_t n, phases, max_waves, qratio, heavy, tile;
+  uint32_t n, phases, max_waves, qratio, pull_qratio, heavy, tile;
   u64 timeout_ns;
 };
 
@@ -324,7 +324,7 @@ __device__ __forceinline__ void staged_pairs(uint32_t v, const uint32_t (&m)[NB]
 template <int NB, bool WITH_W, class Prep, class Ph>
 __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t *items,
                              uint32_t cnt, Prep &prep, Ph &ph, u64 *s, uint2 *stage, Acc &acc,
-                             uint32_t reset_flags) {
+                             uint32_t reset_flags, uint32_t qratio) {
   Ctl *ctl = P.ctl;
   const uint32_t lane = lane_id();
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -338,7 +338,7 @@ __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t 
     uint32_t act = 0;
 #pragma unroll
     for (int k = 0; k < NB; k++) act += __popc(m[k]);
-    const bool ql = use_query_lanes(act, len, P.qratio);
+    const bool ql = use_query_lanes(act, len, qratio);
     const u64 work = ql ? len : (u64)((len + 31) / 32) * act;
     if (work > P.heavy) {
 #pragma unroll
@@ -669,7 +669,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
         uint32_t *src = P.inew[par];
         auto prep = [&](uint32_t v, uint32_t (&m)[NB]) { return take_masks<NB>(src, v, true, m); };
         if (!multi_expand<NB, false>(P, P.out, P.q[cur], cnt, prep, ph, s, s_stage, acc,
-                                     cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0))
+                                     cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.qratio))
           goto done;
         waves++;
         cur ^= 1;
@@ -691,7 +691,9 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
       // 4. pull over in-rows
       PullPh<ALGO, STORED, NB> ph{&P};
       auto prep = [&](uint32_t v, uint32_t (&m)[NB]) { return take_masks<NB>(P.affm, v, false, m); };
-      if (!multi_expand<NB, STORED>(P, P.in, P.aff, na, prep, ph, s, s_stage, acc, 0)) goto done;
+      if (!multi_expand<NB, STORED>(P, P.in, P.aff, na, prep, ph, s, s_stage, acc, 0,
+                                    P.pull_qratio))
+        goto done;
       if (gtid == 0) ctl->tphase[1] = globaltimer_ns();  // reset + pull done
     }
   }
@@ -759,7 +761,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
       uint32_t *src = P.nmask[par];
       auto prep = [&](uint32_t v, uint32_t (&m)[NB]) { return take_masks<NB>(src, v, true, m); };
       if (!multi_expand<NB, STORED>(P, P.out, P.q[cur], cnt, prep, ph, s, s_stage, acc,
-                                    cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0))
+                                    cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.qratio))
         goto done;
       waves++;
       cur ^= 1;
@@ -846,6 +848,7 @@ static cudaError_t launch_multi_t(const MultiLaunch &L, cudaStream_t s) {
   P.phases = L.phases;
   P.max_waves = L.max_waves;
   P.qratio = L.qratio;
+  P.pull_qratio = L.pull_qratio;
   P.heavy = std::max(L.heavy, 1u);
   P.tile = std::max(L.tile, MULTI_MIN_TILE);
   P.timeout_ns = L.timeout_ns;

@@ -66,7 +66,7 @@ class BatchStats(ctypes.Structure):
 
 class QueryMapping(ctypes.Structure):
     _fields_ = [("qratio", ctypes.c_uint32), ("heavy", ctypes.c_uint32), ("tile", ctypes.c_uint32),
-                ("repair_ms", ctypes.c_float)]
+                ("pull_qratio", ctypes.c_uint32), ("repair_ms", ctypes.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

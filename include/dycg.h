@@ -339,13 +339,16 @@ typedef struct dycg_query_mapping {
   uint32_t qratio;
   uint32_t heavy;
   uint32_t tile;
+  uint32_t pull_qratio;  /* the mapping rule's ratio for the pull phase       */
   float repair_ms;
 } dycg_query_mapping;
 
 /* Autotuner of the batched form's work mapping (no reference counterpart):
  * applies one snapshot like dycg_apply_batch, but repairs it once per
- * candidate mapping (qratio in {2,4,8,2^20} x heavy in {16,64,256}), each
- * from the same saved state, keeps the fastest mapping for later snapshots
+ * candidate mapping (qratio in {2,4,8,2^20} x heavy in {16,64,256} with the
+ * pull phase on the same ratio, then the best of those with the pull phase's
+ * ratio in {0,1,2,8}), each from the same saved state, keeps the fastest
+ * mapping for later snapshots
  * and leaves the state of one ordinary repair. Needs HBM for one extra copy
  * of the query results while it runs. tried (cap entries, may be NULL)
  * receives the candidates with their repair times; *n_tried their count. */

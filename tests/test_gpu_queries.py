@@ -187,7 +187,7 @@ def test_tune_mapping_keeps_results():
     tried = e.tune_query_mapping(dels, adds)
     orc.mutate(dels, adds)
     cur = orc.csr()
-    assert len(tried) == 12 and all(t["repair_ms"] > 0 for t in tried)
+    assert 12 < len(tried) <= 16 and all(t["repair_ms"] > 0 for t in tried)
     _check_all(e, n, cur, src)
     for bi in range(2):  # later snapshots under the kept mapping
         dels, adds = cases.random_batch(n, *cur, 400, 400, 2310 + bi)

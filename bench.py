@@ -156,6 +156,12 @@ class Clocks:
                 "samples_inside_timed_region": len(inside)}
 
 
+# DRAM bytes (read + write) per launch of the dominant kernel, from one ncu
+# capture of the same workload (the capture command and its reading are in
+# profiles/dram_traffic_repair_rmat26.md); None where no capture was taken.
+NCU_TRAFFIC = {("rmat26", "sssp"): 48_340_000}
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -333,7 +339,8 @@ def run_dycg(args):
     roofline = {
         "kernel": f"repair_kernel<{algo}>",
         "bound": "hbm", "achieved": round(ach_hbm, 2), "peak": hbm_peak, "unit": "GB/s",
-        "frac": round(ach_hbm / hbm_peak, 5), "traffic": None,
+        "frac": round(ach_hbm / hbm_peak, 5),
+        "traffic": NCU_TRAFFIC.get((args.config, algo)) if args.scale == 26 else None,
         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6650 GB/s",
         "algorithmic_bytes_per_launch": {"hbm": int(rep_hbm), "host_link": int(rep_link)},
         "launch_ms": round(float(rep_ms), 4),

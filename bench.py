@@ -157,8 +157,10 @@ class Clocks:
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel, from one ncu
-# capture of the same workload (the capture command and its reading are in
-# profiles/dram_traffic_repair_rmat26.md); None where no capture was taken.
+# capture of the same workload: `ncu --metrics dram__bytes_read.sum,
+# dram__bytes_write.sum -k regex:repair_kernel -s 5 -c 1` on
+# `bench.py --steps 3 --warmup 3 --e2e-steps 0 --no-cpu-baseline`; None where
+# no capture was taken.
 NCU_TRAFFIC = {("rmat26", "sssp"): 48_340_000}
 
 

@@ -447,7 +447,7 @@ def run_reference(args):
         return {"impl": "reference",
                 "unavailable": "the reference engine has no many-query form or learned admission; "
                                "these configurations report the CPU oracle in their cpu_baseline "
-                               "and compare against this build's plain path"}
+                               "and compare against the library's plain per-query path"}
     threads = os.cpu_count() or 1
     t0 = time.time()
     n, off, dst, w = oracle.rmat_csr(args.scale, args.edge_factor, args.seed, wlo=1, whi=64,

@@ -122,3 +122,45 @@ def test_row_edge_sampler_returns_live_edges():
             row = dst[int(off[u]):int(off[u + 1])]
             k = np.nonzero(row == out[u, 1])[0]
             assert out[u, 0] == u and len(k) and out[u, 2] == w[int(off[u]) + k[0]]
+
+
+def test_trained_network_beats_hotness_hit_rate():
+    """What the trained network gains over the method without it: on the same
+    Zipf snapshots with the same HBM budget, the share of adjacency reads
+    served from HBM (page fills excluded) is higher under the learned policy
+    than under the hotness policy, and the results are identical."""
+    scale, seed, nb, T, C = 16, 1, 20000, 8, 8
+    n, off, dst, w = cases.small_rmat(scale, 8, seed)
+    probe = dg.Engine("sssp", weight_mode="stored", page_shift=8, cache_policy="none")
+    probe.load_csr(n, off, dst, w)
+    gi = probe.info()
+    probe.close()
+    budget = gi["index_bytes"] + int(0.25 * gi["arena_used"] * 8)
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(n)
+    snaps, rates, vals = [], {}, {}
+    for pol in ("hotness", "learned"):
+        e = dg.Engine("sssp", weight_mode="stored", page_shift=8, hbm_graph_budget_bytes=budget,
+                      cache_policy="hotness")
+        e.load_csr(n, off, dst, w)
+        e.start()
+        if pol == "learned":
+            e.policy_trace(T)
+        served = [0, 0]
+        for i in range(T + C):
+            if len(snaps) <= i:  # drawn by the first engine, replayed by the second
+                snaps.append(cases.zipf_snapshot(e, n, nb // 2, nb // 2, rng, perm))
+            if pol == "learned" and i == T:
+                e.policy_train(epochs=3, lr=2e-3, batch=4096, seed=1)
+                e.set_cache_policy("learned")
+            st = e.apply_batch(*snaps[i])
+            if i >= T:
+                fill = st["cache_pages_loaded"] * (8 << 8)
+                served[0] += st["hbm_adj_bytes"] - fill
+                served[1] += st["link_bytes"] - fill
+        rates[pol] = served[0] / (served[0] + served[1])
+        vals[pol] = e.gather()[0]
+        e.close()
+    assert (vals["learned"] == vals["hotness"]).all()
+    # measured on B200: ~0.80 vs ~0.60 across seeds and scales 16/18
+    assert rates["learned"] > rates["hotness"] + 0.08, rates

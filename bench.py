@@ -943,6 +943,11 @@ def run_learned(args):
             "cached_pages": info["cached_pages"], "cache_slots": info["cache_slots"],
             "load_s": round(t_load, 1), "static_solve_s": round(t_init, 1),
             "gpu_launches": int(sum(p["kernel_launches"] for p in per)),
+            # per snapshot, so slow snapshots can be matched across policies
+            "steps_ms_total": [round(p["ms_total"], 2) for p in per],
+            "steps_ms_mutate": [round(p["ms_mutate"], 2) for p in per],
+            "steps_link_mb": [round(p["link_bytes"] / 1e6, 1) for p in per],
+            "steps_relocated_rows": [int(p["relocated_rows"]) for p in per],
             "_vals": vals, "_clk": clk, "_per": per, "_info": info,
         }
         eng.close()

@@ -164,3 +164,42 @@ def test_trained_network_beats_hotness_hit_rate():
     assert (vals["learned"] == vals["hotness"]).all()
     # measured on B200: ~0.80 vs ~0.60 across seeds and scales 16/18
     assert rates["learned"] > rates["hotness"] + 0.08, rates
+
+
+def test_learned_policy_pagerank_within_tolerance():
+    """PageRank under the learned policy: traces recorded under the hotness
+    policy train the network, and with the network deciding which pages sit in
+    HBM the FP32 ranks after every snapshot stay within the tolerance of the
+    FP64 oracle on the mutated graph."""
+    from tests.test_gpu_parity import _assert_pr_close
+    scale, seed = 11, 23
+    n, off, dst, _ = cases.small_rmat(scale, 8, seed)
+    probe = dg.Engine("pr", page_shift=8, cache_policy="none")
+    probe.load_csr(n, off, dst)
+    gi = probe.info()
+    probe.close()
+    budget = gi["index_bytes"] + int(0.3 * gi["arena_used"] * 4)
+    e = dg.Engine("pr", page_shift=8, hbm_graph_budget_bytes=budget, cache_policy="hotness",
+                  epsilon=1e-7, max_rounds=100000)
+    e.load_csr(n, off, dst)
+    e.start()
+    info = e.info()
+    assert 0 < info["cache_slots"] < info["pages"]
+    orc = oracle.Oracle(oracle.PR, n, off, dst)
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(n)
+    e.policy_trace(4)
+    for _ in range(5):
+        d, a = cases.zipf_snapshot(e, n, 200, 200, rng, perm)
+        e.apply_batch(d, a)
+        orc.mutate(d, a)
+    rep = e.policy_train(epochs=4, lr=2e-3, batch=1024, seed=5)
+    assert rep["steps"] > 0 and rep["loss_after"] < rep["loss_before"]
+    e.set_cache_policy("learned")
+    for _ in range(3):
+        d, a = cases.zipf_snapshot(e, n, 200, 200, rng, perm)
+        e.apply_batch(d, a)
+        orc.mutate(d, a)
+        o, dd, _ = orc.csr()
+        x, r = e.gather_ranks()
+        _assert_pr_close(x, r, oracle.static_pr(n, o, dd))

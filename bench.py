@@ -954,8 +954,17 @@ def run_learned(args):
         del eng, dev
     L = res["learned"]
     if algo == "pr":
-        parity = {p: float(np.max(np.abs(res[p]["_vals"].astype(np.float64) -
-                                         L["_vals"].astype(np.float64)))) for p in res}
+        # FP32 ranks: accumulation order differs between runs, so the policies
+        # are compared by their largest rank difference, absolute and on the
+        # normalised scale (ranks / their sum)
+        ref = L["_vals"].astype(np.float64)
+        tot = float(np.sum(ref))
+        parity = {}
+        for p in res:
+            d = float(np.max(np.abs(res[p]["_vals"].astype(np.float64) - ref)))
+            parity[p] = {"max_abs": d, "max_abs_normalized": d / tot,
+                         "max_rel": float(np.max(np.abs(res[p]["_vals"].astype(np.float64) - ref) /
+                                                 np.maximum(np.abs(ref), 1.0)))}
     else:
         parity = {p: bool((res[p]["_vals"] == L["_vals"]).all()) for p in res}
     per = L["_per"]

@@ -22,8 +22,10 @@
 // network is POLICY_F -> 64 -> 64 -> 1, ReLU, BF16 weights and inputs, FP32
 // accumulation and FP32 master weights; loss = mean squared error.
 //
-// The MLP is 4.7K multiply-adds per page (~5 GMAC for a million pages, well
-// under a millisecond on the CUDA cores); it is not worth tensor-core tiles.
+// The MLP is 4.7K multiply-adds per page. Inference runs every snapshot over
+// every page (1.85M pages at R-MAT 27, ~9 GMAC): it runs on the tensor cores
+// (mma.sync BF16 tiles of 16 pages), where the FP32-FMA version took ~1.2 ms
+// per snapshot. Training runs once per trained network on FP32 FMA tiles.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -145,37 +147,126 @@ __global__ void log1p_kernel(const float *in, float *out, u64 n) {
 
 // ---- inference -----------------------------------------------------------------
 
-// score[p] = MLP(x[p]); ids[p] = p (for the admission sort).
-__global__ void __launch_bounds__(BLOCK) mlp_infer_kernel(const __nv_bfloat16 *x, uint32_t n,
+// Tensor-core fragments (mma.sync, BF16 operands, FP32 accumulation). In a
+// warp, g = lane / 4 and t = lane % 4; a 16 x K A fragment holds rows g and
+// g + 8, columns 2t, 2t + 1 (and 2t + 8, 2t + 9 for K = 16); a K x 8 B
+// fragment holds rows 2t, 2t + 1 (and 2t + 8, 2t + 9) of column g; the 16 x 8
+// FP32 accumulator holds rows g and g + 8, columns 2t and 2t + 1.
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // lo in the low half
+  return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void mma_k8(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(b0));
+}
+
+__device__ __forceinline__ void mma_k16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                        uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+constexpr int IB = 128;  // inference block: 4 warps
+
+// score[p] = MLP(x[p]); ids[p] = p (for the admission sort). A warp runs 16
+// pages per tile: layer 1 as eight m16n8k8 products (K = the 8 features),
+// layer 2 as m16n8k16 products over the 64 hidden units, layer 3 as an FP32
+// dot product reduced over each lane quad. The first layer's FP32 outputs are
+// split into BF16 hi + lo parts (h = hi + lo to ~2^-17 relative) and both parts
+// go through layer 2, so activations keep FP32-level precision while the
+// operands stay BF16; the weight fragments live in registers for the whole
+// kernel.
+__global__ void __launch_bounds__(IB, 3) mlp_infer_kernel(const __nv_bfloat16 *x, uint32_t n,
                                                           const float *params, float *score,
                                                           uint32_t *ids) {
-  __shared__ float w[POLICY_PARAMS];
+  __shared__ __align__(16) float w[POLICY_PARAMS];
   load_params(params, w);
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    float in[F];
-    const uint4 raw = *reinterpret_cast<const uint4 *>(x + (u64)p * F);
-    const __nv_bfloat16 *xb = reinterpret_cast<const __nv_bfloat16 *>(&raw);
+  const uint32_t lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  uint32_t b1f[8];
 #pragma unroll
-    for (int k = 0; k < F; k++) in[k] = __bfloat162float(xb[k]);
-    // layer 2 accumulated hidden unit by hidden unit: 64 accumulators, no
-    // stored first layer
-    float acc[H];
+  for (int j = 0; j < 8; j++)
+    b1f[j] = pack2(w[OFF_W1 + (2 * t) * H + 8 * j + g], w[OFF_W1 + (2 * t + 1) * H + 8 * j + g]);
+  uint32_t b2f[4][8][2];
 #pragma unroll
-    for (int j = 0; j < H; j++) acc[j] = w[OFF_B2 + j];
-#pragma unroll 1
-    for (int i = 0; i < H; i++) {
-      float a = w[OFF_B1 + i];
+  for (int kk = 0; kk < 4; kk++)
 #pragma unroll
-      for (int k = 0; k < F; k++) a = fmaf(in[k], w[OFF_W1 + k * H + i], a);
-      const float h = fmaxf(a, 0.f);
-#pragma unroll
-      for (int j = 0; j < H; j++) acc[j] = fmaf(h, w[OFF_W2 + i * H + j], acc[j]);
+    for (int j = 0; j < 8; j++) {
+      const int k0 = 16 * kk + 2 * t, c = OFF_W2 + 8 * j + g;
+      b2f[kk][j][0] = pack2(w[c + k0 * H], w[c + (k0 + 1) * H]);
+      b2f[kk][j][1] = pack2(w[c + (k0 + 8) * H], w[c + (k0 + 9) * H]);
     }
-    float y = w[OFF_B3];
+  const float b3 = w[OFF_B3];
+  const uint32_t *xw = reinterpret_cast<const uint32_t *>(x);  // F = 8 BF16 = 4 words per page
+  const uint32_t tiles = (n + 15) / 16;
+  const uint32_t nwarps = gridDim.x * (IB / 32);
+  uint32_t tile = (blockIdx.x * IB + threadIdx.x) >> 5;
+  auto load_row = [&](uint32_t r) { return r < n ? __ldg(xw + (u64)r * 4 + t) : 0u; };
+  uint32_t na0 = load_row(tile * 16 + g), na1 = load_row(tile * 16 + g + 8);
+  for (; tile < tiles; tile += nwarps) {
+    const uint32_t a0 = na0, a1 = na1;
+    const uint32_t r0 = tile * 16 + g, r1 = r0 + 8;
+    if (tile + nwarps < tiles) {  // next tile's inputs in flight during this one
+      na0 = load_row(r0 + nwarps * 16);
+      na1 = load_row(r1 + nwarps * 16);
+    }
+    float c2[8][4];
 #pragma unroll
-    for (int j = 0; j < H; j++) y = fmaf(fmaxf(acc[j], 0.f), w[OFF_W3 + j], y);
-    score[p] = y;
-    if (ids) ids[p] = p;
+    for (int j = 0; j < 8; j++) {
+      const float2 b = *reinterpret_cast<const float2 *>(&w[OFF_B2 + 8 * j + 2 * t]);
+      c2[j][0] = b.x, c2[j][1] = b.y, c2[j][2] = b.x, c2[j][3] = b.y;
+    }
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+      // hidden units 16kk .. 16kk+15 of layer 1 = the A fragment of layer 2
+      uint32_t hi[4], lo[4];
+#pragma unroll
+      for (int half = 0; half < 2; half++) {
+        const int j1 = 2 * kk + half;
+        const float2 b = *reinterpret_cast<const float2 *>(&w[OFF_B1 + 8 * j1 + 2 * t]);
+        float c[4] = {b.x, b.y, b.x, b.y};
+        mma_k8(c, a0, a1, b1f[j1]);
+        float h[4], r[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const float v = fmaxf(c[e], 0.f);
+          h[e] = bf(v);
+          r[e] = v - h[e];  // exact in FP32
+        }
+        hi[2 * half] = pack2(h[0], h[1]);
+        hi[2 * half + 1] = pack2(h[2], h[3]);
+        lo[2 * half] = pack2(r[0], r[1]);
+        lo[2 * half + 1] = pack2(r[2], r[3]);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        mma_k16(c2[j], hi, b2f[kk][j][0], b2f[kk][j][1]);
+        mma_k16(c2[j], lo, b2f[kk][j][0], b2f[kk][j][1]);
+      }
+    }
+    float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const float2 w3 = *reinterpret_cast<const float2 *>(&w[OFF_W3 + 8 * j + 2 * t]);
+      y0 = fmaf(fmaxf(c2[j][0], 0.f), w3.x, y0);
+      y0 = fmaf(fmaxf(c2[j][1], 0.f), w3.y, y0);
+      y1 = fmaf(fmaxf(c2[j][2], 0.f), w3.x, y1);
+      y1 = fmaf(fmaxf(c2[j][3], 0.f), w3.y, y1);
+    }
+    y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+    y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+    if (t == 0) {
+      if (r0 < n) score[r0] = y0 + b3;
+      if (r1 < n) score[r1] = y1 + b3;
+    }
+    if (ids && lane < 16 && tile * 16 + lane < n) ids[tile * 16 + lane] = tile * 16 + lane;
   }
 }
 
@@ -368,7 +459,9 @@ cudaError_t launch_log1p(const float *in, float *out, u64 n, cudaStream_t s) {
 
 cudaError_t launch_mlp_infer(const void *x, uint32_t n, const float *params, float *score,
                              uint32_t *ids, cudaStream_t s) {
-  mlp_infer_kernel<<<grid_for(n), BLOCK, 0, s>>>((const __nv_bfloat16 *)x, n, params, score, ids);
+  const u64 warps = ((u64)n + 15) / 16;
+  const int grid = (int)std::max<u64>(1, std::min<u64>((warps + 3) / 4, 148ull * 3));
+  mlp_infer_kernel<<<grid, IB, 0, s>>>((const __nv_bfloat16 *)x, n, params, score, ids);
   return cudaGetLastError();
 }
 

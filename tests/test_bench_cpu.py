@@ -1,0 +1,53 @@
+"""bench.py's reference arm on the CPU (no GPU): the JSON line it prints keeps
+the benchmark contract, and under a multi-rank launch only rank 0 works and
+prints."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _run(args, **env):
+    e = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    e.update(env)
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], cwd=ROOT,
+                          env=e, capture_output=True, text=True, timeout=300)
+
+
+def test_reference_arm_line_keeps_the_contract(tmp_path):
+    out = tmp_path / "ref.json"
+    p = _run(["--impl", "reference", "--config", "rmat16", "--steps", "2", "--warmup", "3",
+              "--json-out", str(out)])
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert json.loads(out.read_text()) == d
+    assert d["impl"] == "reference" and d["unit"] == "updates/s" and d["value"] > 0
+    assert d["steps"] == 2 and d["warmup"] >= 3 and d["n_gpus"] == 1
+    assert d["higher_is_better"] is True and d["scaling"] == "weak" and d["vs_baseline"] is None
+    assert d["ms_per_step"] > 0 and "workload" in d["config"]
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
+    e2e = d["e2e"]
+    assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+    # same metric as the library's own arm
+    import bench
+    assert d["metric"] == bench.METRIC
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    p = _run(["--impl", "reference", "--config", "rmat16", "--steps", "2", "--warmup", "3"],
+             RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert not [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_reference_arm_declines_forms_without_a_reference_counterpart():
+    p = _run(["--impl", "reference", "--config", "batched", "--steps", "2", "--warmup", "3"])
+    assert p.returncode == 0, p.stderr[-2000:]
+    d = json.loads([ln for ln in p.stdout.splitlines() if ln.startswith("{")][-1])
+    assert d["impl"] == "reference" and d["unavailable"]

@@ -385,8 +385,11 @@ def run_dycg(args):
                       "expanded", "edges_scanned", "improvements", "waves", "relocated_rows",
                       "missing_deletes", "cache_pages_loaded")},
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and algo in ("sssp", "bfs", "cc"):
-        out["cpu_baseline"] = cpu_baseline(eng, args, algo, nd, na)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        if algo == "pr":
+            out["cpu_baseline"] = cpu_baseline_pr(eng, args, nd, na)
+        else:
+            out["cpu_baseline"] = cpu_baseline(eng, args, algo, nd, na)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -427,6 +430,48 @@ def cpu_baseline(eng, args, algo, nd, na):
                       f"and state as the GPU run ({cpu_s:.1f} s CPU; mutation parallel over "
                       f"sources, closures serial as in the reference's CPU-owner mode)",
             "setup_s": round(setup_s, 1), "gpu_matches_oracle": parity}
+
+
+def cpu_baseline_pr(eng, args, nd, na):
+    """PageRank: the CPU restatement of the reference's residual push (FP64)
+    takes the engine's ranks and residuals, both repair the next snapshot(s),
+    and the GPU's FP32 ranks are compared with the oracle's. Both stop pushing
+    at the same per-vertex threshold, so each is within |r|_1 / (1 - alpha) of
+    the exact ranks and the two within the sum of their bounds (plus FP32
+    rounding, 1e-4 relative)."""
+    import oracle
+    t0 = time.time()
+    off, dst, _ = eng.csr()
+    x, r = eng.gather_ranks()
+    threads = os.cpu_count() or 1
+    orc = oracle.Oracle(oracle.PR, eng.n, off, dst, None, epsilon=1e-4, alpha=0.85,
+                        max_rounds=100, threads=threads)
+    orc.set_state(ranks=x.astype(np.float64), residuals=r.astype(np.float64))
+    del off, dst
+    setup_s = time.time() - t0
+    nb = max(1, args.cpu_baseline_batches)
+    batches = make_batches(args.scale, nb, nd, na, args.seed + 999, eng.sample_edges, args.config)
+    cpu_s, err, within, tot = 0.0, 0.0, True, 1.0
+    for d, a in batches:
+        t = time.perf_counter()
+        orc.apply_batch(d, a)
+        cpu_s += time.perf_counter() - t
+        eng.apply_batch(d, a)
+        xg, rg = eng.gather_ranks()
+        xo, ro = orc.ranks()
+        diff = np.abs(xg.astype(np.float64) - xo)
+        bound = (float(np.sum(np.abs(rg.astype(np.float64)))) + float(np.sum(np.abs(ro)))) / 0.15 \
+            + 1e-4 * np.abs(xo)
+        within &= bool((diff <= bound).all())
+        err = max(err, float(diff.max()))
+        tot = float(np.sum(xo))
+    upd = sum(len(d) + len(a) for d, a in batches)
+    return {"value": round(upd / cpu_s, 1), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{nb} snapshot(s) of {upd // nb} updates on the same rmat{args.scale} graph "
+                      f"and PageRank state as the GPU run ({cpu_s:.1f} s CPU; FP64 residual push, "
+                      f"epsilon 1e-4, at most 100 rounds)",
+            "setup_s": round(setup_s, 1), "gpu_within_bound_of_oracle": within,
+            "gpu_vs_oracle_max_abs": err, "gpu_vs_oracle_max_abs_normalized": err / tot}
 
 
 # ----------------------------------------------------------------------------

@@ -51,3 +51,45 @@ def test_reference_arm_declines_forms_without_a_reference_counterpart():
     assert p.returncode == 0, p.stderr[-2000:]
     d = json.loads([ln for ln in p.stdout.splitlines() if ln.startswith("{")][-1])
     assert d["impl"] == "reference" and d["unavailable"]
+
+
+class _OracleEngine:
+    """Stands in for the GPU engine in the bench's PageRank CPU leg: the
+    interface the leg calls (csr, gather_ranks, apply_batch, sample_edges),
+    backed by a second oracle whose ranks are handed out in FP32."""
+
+    def __init__(self, n, off, dst):
+        import oracle
+        self.n = n
+        self.o = oracle.Oracle(oracle.PR, n, off, dst, epsilon=1e-4, max_rounds=100)
+        self.o.init()
+
+    def csr(self):
+        return self.o.csr()
+
+    def gather_ranks(self):
+        x, r = self.o.ranks()
+        return x.astype("float32"), r.astype("float32")
+
+    def apply_batch(self, d, a):
+        self.o.apply_batch(d, a)
+
+    def sample_edges(self, count, seed):
+        import numpy as np
+        off, dst, _ = self.o.csr()
+        pick = np.random.default_rng(seed).choice(len(dst), size=count, replace=False)
+        src = np.searchsorted(off, pick, side="right") - 1
+        return np.stack([src.astype(np.uint32), dst[pick], np.ones(count, np.uint32)], 1)
+
+
+def test_pagerank_cpu_leg_reports_the_oracle_comparison():
+    import argparse
+    import bench
+    import oracle
+    n, off, dst, _ = oracle.rmat_csr(12, 8, 3, with_w=False)
+    eng = _OracleEngine(n, off, dst)
+    args = argparse.Namespace(scale=12, seed=5, cpu_baseline_batches=2, config="rmat26")
+    out = bench.cpu_baseline_pr(eng, args, 500, 500)
+    assert out["value"] > 0 and out["kind"] == "port" and out["cores"] >= 1
+    assert out["gpu_within_bound_of_oracle"] is True
+    assert out["gpu_vs_oracle_max_abs_normalized"] < 1e-4

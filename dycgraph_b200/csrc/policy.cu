@@ -28,6 +28,8 @@
 // per snapshot. Training runs once per trained network on FP32 FMA tiles.
 #include <cuda_bf16.h>
 
+#include <atomic>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -468,13 +470,18 @@ cudaError_t launch_mlp_infer(const void *x, uint32_t n, const float *params, flo
 cudaError_t launch_mlp_grad(const void *x, const float *y, uint64_t total, uint32_t count,
                             uint64_t sample_seed, const float *params, float scale, float *grad,
                             float *loss, cudaStream_t s) {
-  static bool attr = false;
+  // the shared-memory opt-in is a per-device setting: once per device used
+  constexpr int kMaxDevices = 64;
+  static std::atomic<bool> attr[kMaxDevices];
   const size_t smem = mlp_grad_smem();
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices || !attr[dev].load(std::memory_order_acquire)) {
+    e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
     if (e != cudaSuccess) return e;
-    attr = true;
+    if (dev >= 0 && dev < kMaxDevices) attr[dev].store(true, std::memory_order_release);
   }
   const uint32_t tiles = (count + TS - 1) / TS;
   const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(tiles, 148 * 2));

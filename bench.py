@@ -173,15 +173,19 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def make_batches(scale, total_batches, nd, na, seed, sample_fn, config="rmat26", wmax=64):
+def make_batches(scale, total_batches, nd, na, seed, sample_fn, config="rmat26", wmax=64,
+                 rmat_fn=None):
     """Deletions: nd distinct live edges per snapshot, disjoint across snapshots
-    (sampled once from the initial graph); insertions: R-MAT draws. On the grid:
-    70% of the deletions are 4-neighbour grid edges and 30% shortcuts, and the
-    insertions are new shortcuts within radius 8."""
-    import dycgraph_b200 as dg
+    (sampled once from the initial graph); insertions: R-MAT draws (rmat_fn,
+    the library's generator unless given). On the grid: 70% of the deletions
+    are 4-neighbour grid edges and 30% shortcuts, and the insertions are new
+    shortcuts within radius 8."""
     if config != "grid":
+        if rmat_fn is None:
+            import dycgraph_b200 as dg
+            rmat_fn = dg.gen_rmat_edges
         dels = sample_fn(total_batches * nd, seed)
-        adds = dg.gen_rmat_edges(scale, total_batches * na, seed + 1, first=0)
+        adds = rmat_fn(scale, total_batches * na, seed + 1, first=0)
         return [(dels[i * nd:(i + 1) * nd], adds[i * na:(i + 1) * na])
                 for i in range(total_batches)]
     side = 1 << scale
@@ -475,8 +479,28 @@ def cpu_baseline_pr(eng, args, nd, na):
 
 
 # ----------------------------------------------------------------------------
+# PageRank's CPU initial solve costs ~0.45 us per edge on 8 host cores (7.2 s
+# at R-MAT 20): above R-MAT 24 it alone would exceed the run's few minutes
+REF_PR_MAX_SCALE = 24
+
+
+def _cpu_sampler(off, dst, w):
+    """Distinct live edges of a host CSR drawn uniformly (the reference arm's
+    stand-in for the engine's edge sampler)."""
+    def sample(count, seed):
+        pick = np.random.default_rng(seed).choice(len(dst), size=min(count, len(dst)),
+                                                  replace=False)
+        src = np.searchsorted(off, pick, side="right") - 1
+        ww = w[pick] if w is not None else np.ones(len(pick), np.uint32)
+        return np.stack([src.astype(np.uint32), dst[pick], ww], 1)
+    return sample
+
+
 def run_reference(args):
-    """The reference's repair algorithm (CPU oracle restatement) on host cores."""
+    """The reference's repair algorithm (CPU oracle restatement) on host cores,
+    on the same workload as the library's arm: the same generated graph
+    (R-MAT, symmetrised for CC, or the road-like grid), snapshots of the same
+    shape, and the same algorithm settings."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
@@ -485,64 +509,88 @@ def run_reference(args):
     nd = args.batch // 2
     na = args.batch - nd
     algo = args.algo
-    if algo == "pr" or args.config == "grid":
-        return {"impl": "reference",
-                "unavailable": "the CPU reference arm is wired for SSSP/BFS/CC on R-MAT configs"}
     if args.config in ("batched", "learned"):
         return {"impl": "reference",
                 "unavailable": "the reference engine has no many-query form or learned admission; "
                                "these configurations report the CPU oracle in their cpu_baseline "
                                "and compare against the library's plain per-query path"}
+    if algo == "pr" and (args.config == "grid" or args.scale > REF_PR_MAX_SCALE):
+        return {"impl": "reference",
+                "unavailable": f"PageRank's CPU initial solve above R-MAT {REF_PR_MAX_SCALE} takes "
+                               "longer than this run's time bound (~0.45 us per edge on 8 host "
+                               "cores); the library's line carries a PageRank cpu_baseline "
+                               "started from the engine's ranks instead"}
     threads = os.cpu_count() or 1
     t0 = time.time()
-    n, off, dst, w = oracle.rmat_csr(args.scale, args.edge_factor, args.seed, wlo=1, whi=64,
-                                     with_w=(algo == "sssp"))
-    code = {"sssp": oracle.SSSP, "bfs": oracle.BFS, "cc": oracle.CC}[algo]
+    grid = args.config == "grid"
+    wmax = 1000 if grid else 64
+    sym = algo == "cc" and not grid
+    if grid:
+        n, off, dst, w = oracle.grid_csr(1 << args.scale, 10, 8, args.seed, 1, wmax,
+                                         with_w=(algo == "sssp"))
+    else:
+        n, off, dst, w = oracle.rmat_csr(args.scale, args.edge_factor, args.seed, wlo=1, whi=wmax,
+                                         with_w=(algo == "sssp"), symmetrize=sym)
+    code = {"sssp": oracle.SSSP, "bfs": oracle.BFS, "cc": oracle.CC, "pr": oracle.PR}[algo]
     wmode = oracle.WEIGHT_STORED if algo == "sssp" else oracle.WEIGHT_HASH128
-    orc = oracle.Oracle(code, n, off, dst, w, weight_mode=wmode, threads=threads)
-    if algo == "cc":
+    orc = oracle.Oracle(code, n, off, dst, w, weight_mode=wmode, symmetric=sym, epsilon=1e-4,
+                        alpha=0.85, max_rounds=100, threads=threads)
+    if algo in ("cc", "pr"):
         orc.init()
+    elif grid:
+        # high diameter: one Dijkstra / BFS pass beats frontier waves by ~50x
+        vals = (oracle.static_sssp(n, off, dst, w, wmode, 0) if algo == "sssp"
+                else oracle.static_bfs(n, off, dst, 0))
+        orc.set_state(vals, oracle.tight_parents(n, off, dst, w, code, wmode, 0, vals))
     else:
         vals, par = oracle.parallel_sssp(n, off, dst, w, code, wmode, 0)
         orc.set_state(vals, par)
-    setup_s = time.time() - t0
-    rng = np.random.default_rng(args.seed + 17)
-    m = len(dst)
-    pick = rng.choice(m, size=(W + K) * nd, replace=False)
-    src = np.searchsorted(off, pick, side="right") - 1
-    dels = np.stack([src.astype(np.uint32), dst[pick], w[pick] if w is not None else np.ones(len(pick), np.uint32)], 1)
-    adds = oracle.gen_rmat_edges(args.scale, (W + K) * na, args.seed + 18)
+    batches = make_batches(args.scale, W + K, nd, na, args.seed + 17, _cpu_sampler(off, dst, w),
+                           args.config, wmax, rmat_fn=oracle.gen_rmat_edges)
+    if sym:  # symmetric updates on the symmetrised graph
+        batches = [(np.concatenate([d, d[:, [1, 0, 2]]]), np.concatenate([a, a[:, [1, 0, 2]]]))
+                   for d, a in batches]
     del off, dst, w
-    # a step is a bounded sample: a full snapshot, or a fixed slice of it when
-    # one snapshot would take too long on these cores
+    setup_s = time.time() - t0
+    # a step is a bounded sample: a full snapshot, or a fixed leading slice of
+    # its deletions and insertions when a whole one would not fit the run's
+    # time bound (~150 s of steps)
+    budget = min(20.0, max(1.0, 150.0 / (W + K)))
     frac = 1.0
-    d0, a0 = dels[:nd], adds[:na]
     t = time.perf_counter()
-    orc.apply_batch(d0, a0)
+    orc.apply_batch(*batches[0])
     first = time.perf_counter() - t
-    if first > 20.0:
-        frac = max(0.05, 20.0 / first)
-    sub_d, sub_a = int(nd * frac), int(na * frac)
+    if first > budget:
+        frac = max(0.01, budget / first)
+
+    def sample(i):
+        d, a = batches[i]
+        return d[:max(1, int(len(d) * frac))], a[:max(1, int(len(a) * frac))]
     for i in range(1, W):
-        orc.apply_batch(dels[i * nd:i * nd + sub_d], adds[i * na:i * na + sub_a])
+        orc.apply_batch(*sample(i))
+    steps = [sample(i) for i in range(W, W + K)]
     t = time.perf_counter()
-    for i in range(W, W + K):
-        orc.apply_batch(dels[i * nd:i * nd + sub_d], adds[i * na:i * na + sub_a])
+    for d, a in steps:
+        orc.apply_batch(d, a)
     el = time.perf_counter() - t
-    upd = (sub_d + sub_a) * K
+    upd = sum(len(d) + len(a) for d, a in steps)
     value = upd / el
-    sample = (f"{K} steps of {sub_d + sub_a} updates ({frac:.0%} of a {args.batch}-update snapshot) "
-              f"on rmat{args.scale}-ef{args.edge_factor}; CPU restatement of the reference's repair "
-              f"(reference engine itself not buildable without its CMake deps)")
+    workload = (f"grid{1 << args.scale}x{1 << args.scale}+1%shortcuts {algo}" if grid else
+                f"rmat{args.scale}-ef{args.edge_factor}{' symmetrised' if sym else ''} {algo}")
+    per = len(batches[0][0]) + len(batches[0][1])
+    sample_desc = (f"{K} steps of {upd // K} updates ({frac:.0%} of a {per}-update snapshot) "
+                   f"on {workload}; CPU restatement of the reference's repair (reference "
+                   f"engine itself not buildable without its CMake deps)")
     return {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": UNIT,
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": K, "warmup": W,
             "ms_per_step": round(el * 1e3 / K, 3), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded R-MAT)",
-            "config": {"workload": f"rmat{args.scale}-ef{args.edge_factor} {algo} "
-                                   f"{args.batch // 1000}K-update snapshots",
+            "vs_baseline": None, "dtype": "f64" if algo == "pr" else "u32",
+            "data": "synthetic (seeded " + ("grid)" if grid else "R-MAT)"),
+            "config": {"workload": f"{workload} " + (f"{args.batch // 1000}K" if args.batch % 1000 == 0
+                                                     else f"{args.batch}") + "-update snapshots",
                        "setup_s": round(setup_s, 1), "first_snapshot_s": round(first, 2)},
             "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads,
-                             "kind": "port", "sample": sample},
+                             "kind": "port", "sample": sample_desc},
             "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 

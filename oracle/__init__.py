@@ -87,7 +87,7 @@ def lib():
                                          ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ep]
         L.orc_rmat_csr.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
-                                   ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                   ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
                                    ctypes.POINTER(u64p), ctypes.POINTER(u32p),
                                    ctypes.POINTER(u32p), u64p]
         L.orc_free.argtypes = [P]
@@ -279,15 +279,18 @@ def gen_rmat_edges(scale, count, seed, first=0, a=0.57, b=0.19, c=0.19, wlo=1, w
     return out
 
 
-def rmat_csr(scale, ef, seed, a=0.57, b=0.19, c=0.19, wlo=1, whi=64, with_w=True):
+def rmat_csr(scale, ef, seed, a=0.57, b=0.19, c=0.19, wlo=1, whi=64, with_w=True,
+             symmetrize=False):
     """De-duplicated R-MAT CSR built on the host cores (numpy views over C arrays,
-    copied so the C allocations can be released)."""
+    copied so the C allocations can be released); symmetrize adds the reverse
+    of every draw."""
     L = lib()
     po = ctypes.POINTER(ctypes.c_uint64)()
     pd = ctypes.POINTER(ctypes.c_uint32)()
     pw = ctypes.POINTER(ctypes.c_uint32)()
     m = ctypes.c_uint64(0)
-    if L.orc_rmat_csr(scale, ef, a, b, c, seed, wlo, whi, int(with_w), ctypes.byref(po),
+    if L.orc_rmat_csr(scale, ef, a, b, c, seed, wlo, whi, int(with_w), int(symmetrize),
+                      ctypes.byref(po),
                       ctypes.byref(pd), ctypes.byref(pw), ctypes.byref(m)):
         raise MemoryError("rmat_csr failed")
     n = 1 << scale
@@ -298,6 +301,83 @@ def rmat_csr(scale, ef, seed, a=0.57, b=0.19, c=0.19, wlo=1, whi=64, with_w=True
         if p:
             L.orc_free(ctypes.cast(p, ctypes.c_void_p))
     return n, off, dst, w
+
+
+_U64 = np.uint64
+
+
+def _mix64(z):
+    """64-bit finaliser over uint64 arrays (wrapping arithmetic); the same
+    mixing function the library's generators use."""
+    z = (z + _U64(0x9E3779B97F4A7C15)) & _U64(0xFFFFFFFFFFFFFFFF)
+    z = (z ^ (z >> _U64(30))) * _U64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> _U64(27))) * _U64(0x94D049BB133111EB)
+    return z ^ (z >> _U64(31))
+
+
+def hash_weights(seed, u, v, wlo, whi):
+    """Stored weight of each directed edge (u, v) of a generated graph: the
+    library's hash of (seed, u, v) folded into [wlo, whi]."""
+    s = _U64(seed) ^ _U64(0x5745494748545321)
+    k = (np.asarray(u, _U64) << _U64(32)) | np.asarray(v, _U64)
+    r = _mix64(s ^ _mix64(k))
+    return (_U64(wlo) + r % _U64(whi - wlo + 1)).astype(np.uint32)
+
+
+def grid_csr(side, permille, radius, seed, wlo=1, whi=1000, with_w=True):
+    """The road-like grid graph of the library's generator, built on the host
+    cores: side x side vertices, 4-neighbour edges in both directions, plus
+    side^2 * permille / 1000 shortcut draws (each a vertex and an offset within
+    the Chebyshev radius, kept when the target is another vertex inside the
+    grid) in both directions; duplicates removed, rows sorted by target
+    (dycgraph_b200/csrc/build.cu grid_keys_kernel). Returns n, off, dst, w."""
+    with np.errstate(over="ignore"):
+        n = side * side
+        u = np.arange(n, dtype=_U64)
+        r, c = u // _U64(side), u % _U64(side)
+        right, down = u[c + _U64(1) < _U64(side)], u[r + _U64(1) < _U64(side)]
+        parts = [(right << _U64(32)) | (right + _U64(1)), ((right + _U64(1)) << _U64(32)) | right,
+                 (down << _U64(32)) | (down + _U64(side)), ((down + _U64(side)) << _U64(32)) | down]
+        j = np.arange(n * permille // 1000, dtype=_U64)
+        h = _mix64(_U64(seed) ^ _mix64(j + _U64(0x51ED270B)))
+        su = h % _U64(n)
+        span = _U64(2 * radius + 1)
+        dr = ((h >> _U64(32)) % span).astype(np.int64) - radius
+        dc = ((h >> _U64(48)) % span).astype(np.int64) - radius
+        rr = (su // _U64(side)).astype(np.int64) + dr
+        cc = (su % _U64(side)).astype(np.int64) + dc
+        ok = ((dr != 0) | (dc != 0)) & (rr >= 0) & (cc >= 0) & (rr < side) & (cc < side)
+        sv = (rr * side + cc)[ok].astype(_U64)
+        su = su[ok]
+        parts += [(su << _U64(32)) | sv, (sv << _U64(32)) | su]
+        keys = np.unique(np.concatenate(parts))
+        src = (keys >> _U64(32)).astype(np.uint32)
+        dst = (keys & _U64(0xFFFFFFFF)).astype(np.uint32)
+        off = np.zeros(n + 1, np.uint64)
+        off[1:] = np.cumsum(np.bincount(src, minlength=n)).astype(np.uint64)
+        w = hash_weights(seed, src, dst, wlo, whi) if with_w else None
+    return n, off, dst, w
+
+
+def tight_parents(n, off, dst, w, algo, weight_mode, source, dist):
+    """Parents for static distances: the smallest in-neighbour x with
+    dist[x] + w(x, y) == dist[y] (the tie rule of the repair), INF for the
+    source and for unreachable vertices."""
+    deg = np.diff(np.asarray(off, np.int64))
+    src = np.repeat(np.arange(n, dtype=np.uint32), deg)
+    dst = np.asarray(dst, np.uint32)
+    if algo == BFS:
+        wt = np.ones(len(dst), np.uint64)
+    elif weight_mode == WEIGHT_STORED:
+        wt = np.asarray(w, np.uint64)
+    else:
+        wt = (src.astype(np.uint64) + dst) % np.uint64(128) + np.uint64(1)
+    d = np.asarray(dist, np.uint64)
+    ok = (d[src] != np.uint64(INF)) & (d[src] + wt == d[dst])
+    par = np.full(n, INF, np.uint32)
+    np.minimum.at(par, dst[ok], src[ok])
+    par[source] = INF
+    return par
 
 
 def parallel_sssp(n, off, dst, w, algo, weight_mode, source=0):

@@ -68,10 +68,11 @@ static int cmp_u32(const void *x, const void *y) {
   return a < b ? -1 : a > b;
 }
 
-/* De-duplicated R-MAT CSR without self-loops, rows sorted. Arrays are
- * malloc'd; release with orc_free. Returns 0 on success. */
+/* De-duplicated R-MAT CSR without self-loops, rows sorted; with symmetrize,
+ * every draw (u, v) also yields (v, u) (the library's symmetrised R-MAT).
+ * Arrays are malloc'd; release with orc_free. Returns 0 on success. */
 int orc_rmat_csr(uint32_t scale, uint32_t ef, double a, double b, double c, uint64_t seed,
-                 uint32_t wlo, uint32_t whi, int with_w, uint64_t **off_out,
+                 uint32_t wlo, uint32_t whi, int with_w, int symmetrize, uint64_t **off_out,
                  uint32_t **dst_out, uint32_t **w_out, uint64_t *m_out) {
   const uint32_t n = 1u << scale;
   const u64 draws = (u64)ef << scale;
@@ -85,7 +86,10 @@ int orc_rmat_csr(uint32_t scale, uint32_t ef, double a, double b, double c, uint
   for (int64_t i = 0; i < (int64_t)draws; i++) {
     uint32_t u, v;
     rmat_draw(seed, (u64)i, scale, ta, tab, tabc, &u, &v);
-    if (u != v) __atomic_fetch_add(&deg[u], 1u, __ATOMIC_RELAXED);
+    if (u != v) {
+      __atomic_fetch_add(&deg[u], 1u, __ATOMIC_RELAXED);
+      if (symmetrize) __atomic_fetch_add(&deg[v], 1u, __ATOMIC_RELAXED);
+    }
   }
   u64 s = 0;
   for (uint32_t v = 0; v < n; v++) {
@@ -101,7 +105,10 @@ int orc_rmat_csr(uint32_t scale, uint32_t ef, double a, double b, double c, uint
   for (int64_t i = 0; i < (int64_t)draws; i++) {
     uint32_t u, v;
     rmat_draw(seed, (u64)i, scale, ta, tab, tabc, &u, &v);
-    if (u != v) dst[__atomic_fetch_add(&cur[u], 1ull, __ATOMIC_RELAXED)] = v;
+    if (u != v) {
+      dst[__atomic_fetch_add(&cur[u], 1ull, __ATOMIC_RELAXED)] = v;
+      if (symmetrize) dst[__atomic_fetch_add(&cur[v], 1ull, __ATOMIC_RELAXED)] = u;
+    }
   }
   free(cur);
   /* sort + unique each row in place */

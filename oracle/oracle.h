@@ -108,7 +108,8 @@ void orc_gen_rmat_edges(uint32_t scale, double a, double b, double c, uint64_t s
                         uint64_t first, uint64_t count, uint32_t wlo, uint32_t whi,
                         orc_edge *out);
 int orc_rmat_csr(uint32_t scale, uint32_t ef, double a, double b, double c, uint64_t seed,
-                 uint32_t wlo, uint32_t whi, int with_w, uint64_t **off, uint32_t **dst,
+                 uint32_t wlo, uint32_t whi, int with_w, int symmetrize, uint64_t **off,
+                 uint32_t **dst,
                  uint32_t **w, uint64_t *m);
 void orc_free(void *p);
 int orc_parallel_sssp(uint32_t n, const uint64_t *off, const uint32_t *dst, const uint32_t *w,

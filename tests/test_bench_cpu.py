@@ -93,3 +93,30 @@ def test_pagerank_cpu_leg_reports_the_oracle_comparison():
     assert out["value"] > 0 and out["kind"] == "port" and out["cores"] >= 1
     assert out["gpu_within_bound_of_oracle"] is True
     assert out["gpu_vs_oracle_max_abs_normalized"] < 1e-4
+
+
+def _line(args):
+    p = _run(args)
+    assert p.returncode == 0, p.stderr[-2000:]
+    return json.loads([ln for ln in p.stdout.splitlines() if ln.startswith("{")][-1])
+
+
+def test_reference_arm_covers_every_algorithm_and_the_grid():
+    for algo in ("bfs", "cc", "pr"):
+        d = _line(["--impl", "reference", "--config", "rmat16", "--algo", algo, "--steps", "2",
+                   "--warmup", "3"])
+        assert d["value"] > 0 and algo in d["config"]["workload"], d
+    # CC runs on the symmetrised graph with symmetric updates, as the library's arm does
+    d = _line(["--impl", "reference", "--config", "rmat16", "--algo", "cc", "--steps", "2",
+               "--warmup", "3"])
+    assert "symmetrised" in d["config"]["workload"]
+    for algo in ("sssp", "bfs", "cc"):
+        d = _line(["--impl", "reference", "--config", "grid", "--scale", "6", "--batch", "200",
+                   "--algo", algo, "--steps", "2", "--warmup", "3"])
+        assert d["value"] > 0 and d["config"]["workload"].startswith("grid64x64"), d
+
+
+def test_reference_arm_declines_pagerank_beyond_its_time_bound():
+    d = _line(["--impl", "reference", "--config", "rmat26", "--algo", "pr", "--steps", "2",
+               "--warmup", "3"])
+    assert d["impl"] == "reference" and "PageRank" in d["unavailable"]

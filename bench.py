@@ -390,7 +390,10 @@ def run_dycg(args):
                       "missing_deletes", "cache_pages_loaded")},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        if algo == "pr":
+        if algo == "cc" and args.config == "grid":
+            out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(),
+                                   "kind": "port", "sample": "not run: " + GRID_CC_CPU_REASON}
+        elif algo == "pr":
             out["cpu_baseline"] = cpu_baseline_pr(eng, args, nd, na)
         else:
             out["cpu_baseline"] = cpu_baseline(eng, args, algo, nd, na)
@@ -482,6 +485,12 @@ def cpu_baseline_pr(eng, args, nd, na):
 # PageRank's CPU initial solve costs ~0.45 us per edge on 8 host cores (7.2 s
 # at R-MAT 20): above R-MAT 24 it alone would exceed the run's few minutes
 REF_PR_MAX_SCALE = 24
+# CC on the grid: one deletion near a label root invalidates the whole
+# component, and the CPU restatement's unordered label propagation re-walks it
+GRID_CC_CPU_REASON = ("the CPU restatement's CC repair re-propagates labels over the whole "
+                      "component after a deletion near a label root (45.8 s for one 10K-update "
+                      "snapshot of a 1024x1024 grid, all 1.05M vertices affected, 8 host cores); "
+                      "a 4096x4096 snapshot exceeds this run's time bound")
 
 
 def _cpu_sampler(off, dst, w):
@@ -520,6 +529,8 @@ def run_reference(args):
                                "longer than this run's time bound (~0.45 us per edge on 8 host "
                                "cores); the library's line carries a PageRank cpu_baseline "
                                "started from the engine's ranks instead"}
+    if algo == "cc" and args.config == "grid":
+        return {"impl": "reference", "unavailable": GRID_CC_CPU_REASON}
     threads = os.cpu_count() or 1
     t0 = time.time()
     grid = args.config == "grid"

@@ -110,10 +110,13 @@ def test_reference_arm_covers_every_algorithm_and_the_grid():
     d = _line(["--impl", "reference", "--config", "rmat16", "--algo", "cc", "--steps", "2",
                "--warmup", "3"])
     assert "symmetrised" in d["config"]["workload"]
-    for algo in ("sssp", "bfs", "cc"):
+    for algo in ("sssp", "bfs"):
         d = _line(["--impl", "reference", "--config", "grid", "--scale", "6", "--batch", "200",
                    "--algo", algo, "--steps", "2", "--warmup", "3"])
         assert d["value"] > 0 and d["config"]["workload"].startswith("grid64x64"), d
+    d = _line(["--impl", "reference", "--config", "grid", "--scale", "6", "--algo", "cc",
+               "--steps", "2", "--warmup", "3"])
+    assert "component" in d["unavailable"]
 
 
 def test_reference_arm_declines_pagerank_beyond_its_time_bound():

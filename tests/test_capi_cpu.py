@@ -84,3 +84,8 @@ def test_binary_formats_round_trip(tmp_path):
     for (d, a), (d2_, a2) in zip(batches, back):
         assert (np.asarray(d, np.uint32).reshape(-1, 3) == d2_).all()
         assert (np.asarray(a, np.uint32).reshape(-1, 3) == a2).all()
+
+
+def test_integration_guide_indexes_every_entry_point():
+    guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    assert [n for n in header_functions() if n not in guide] == []

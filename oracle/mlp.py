@@ -5,8 +5,12 @@ never imports it).
 The network is POLICY_F -> 64 -> 64 -> 1 with ReLU, parameters laid out as
 W1[F x H] b1[H] W2[H x H] b2[H] W3[H] b3 (FP32 master copy). The GPU kernels
 round inputs and parameters to bfloat16 (round to nearest even) and
-accumulate in FP32; this restatement applies the same rounding and computes in
-float64, so the two agree to FP32 accumulation error. It has no counterpart in
+accumulate in FP32; the tensor-core inference also carries the first layer's
+activations as two bfloat16 parts (hi + lo, ~2^-17 relative). This
+restatement applies the same input and parameter rounding and computes in
+float64 with exact activations, so the two agree to within that activation
+split and FP32 accumulation error (the tests' tolerance: 1e-4 relative +
+1e-5 absolute for inference). It has no counterpart in
 the reference, whose admission is a decayed activity count
 (include/framework/variants/driver.cuh:486-515).
 """

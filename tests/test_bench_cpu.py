@@ -123,3 +123,28 @@ def test_reference_arm_declines_pagerank_beyond_its_time_bound():
     d = _line(["--impl", "reference", "--config", "rmat26", "--algo", "pr", "--steps", "2",
                "--warmup", "3"])
     assert d["impl"] == "reference" and "PageRank" in d["unavailable"]
+
+
+def test_grid_snapshots_mix_grid_edges_and_shortcuts():
+    import numpy as np
+    import bench
+    import oracle
+    side = 256
+    n, off, dst, w = oracle.grid_csr(side, 10, 8, 11, 1, 1000)
+    nd, na, nb = 100, 100, 3
+    batches = bench.make_batches(8, nb, nd, na, 5, bench._cpu_sampler(off, dst, w), "grid", 1000)
+    live = set((np.repeat(np.arange(n), np.diff(off.astype(np.int64))) * n + dst).tolist())
+    seen = set()
+    for d, a in batches:
+        assert len(d) == nd and len(a) == na
+        du, dv = d[:, 0].astype(np.int64), d[:, 1].astype(np.int64)
+        is_grid = (np.abs(du - dv) == 1) | (np.abs(du - dv) == side)
+        assert is_grid.sum() == 70
+        keys = (du * n + dv).tolist()
+        assert set(keys) <= live and not (set(keys) & seen) and len(set(keys)) == nd
+        seen |= set(keys)
+        au, av = a[:, 0].astype(np.int64), a[:, 1].astype(np.int64)
+        assert (au != av).all() and (a[:, 2] >= 1).all() and (a[:, 2] <= 1000).all()
+        cheb = np.maximum(np.abs(au // side - av // side), np.abs(au % side - av % side))
+        # within radius 8, except a draw that landed on u itself and was moved to u + 1
+        assert ((cheb <= 8) | (av == (au + 1) % n)).all()

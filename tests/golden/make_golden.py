@@ -20,6 +20,11 @@ What it records (all small JSON, committed):
   topology_replay.json -- tests/fixtures/topology_replay_* with the output of
                           the reference's topology_replay tool (built from the
                           reference sources by oracle/Makefile).
+  group_updates.json   -- seeded update batches grouped by the reference's own
+                          GroupedUpdateBatch (effective_update_batch.h, driven
+                          by oracle/ref_group_updates.cpp, built by
+                          oracle/Makefile): per source, its deletions and
+                          additions in the class's order.
 The reference is only read here; nothing at test time touches it.
 """
 import argparse
@@ -196,16 +201,55 @@ def topology_case(ref):
                       "src/topology_replay.cpp"}
 
 
+def group_case(ref):
+    """Seeded batches with skewed sources, repeated (u, v) pairs and both
+    phases; one batch above 4096 records takes the class's radix-sort path."""
+    subprocess.run(["make", "-s", "-C", str(REPO / "oracle"), f"REF={ref}"], check=True)
+    tool = REPO / "oracle/_ref/group_updates"
+    rng = random.Random(20261203)
+    out = []
+    for nd, na, nv in ((0, 0, 8), (1, 0, 8), (0, 3, 8), (40, 25, 16), (300, 200, 64),
+                       (2600, 1600, 1 << 12)):
+        def draw(k):
+            # squared uniform: low ids are hot, so sources repeat
+            return [[int(nv * rng.random() ** 2), rng.randrange(nv)] for _ in range(k)]
+        dels, adds = draw(nd), draw(na)
+        dels += dels[:nd // 10]  # repeated deletion requests
+        adds += adds[:na // 10]  # parallel insertions
+        text = f"{len(dels)} {len(adds)}\n" + "".join(f"{u} {v}\n" for u, v in dels + adds)
+        res = subprocess.run([str(tool)], input=text, check=True, capture_output=True,
+                             text=True).stdout.splitlines()
+        groups, phases = [], None
+        for line in res:
+            f = line.split()
+            if f[0] == "S":
+                groups.append([int(f[1]), [], []])
+            elif f[0] == "D":
+                groups[-1][1] = [int(x) for x in f[1:]]
+            elif f[0] == "A":
+                groups[-1][2] = [int(x) for x in f[1:]]
+            else:
+                phases = [int(f[1]), int(f[2])]
+        out.append({"num_vertices": nv, "dels": dels, "adds": adds, "groups": groups,
+                    "phases": phases})
+    return {"batches": out,
+            "origin": "include/framework/effective_update_batch.h:36-207 GroupedUpdateBatch "
+                      "(Mixed view per source; PhaseSize(Delete/Add))"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("DYCG_REFERENCE", "/root/reference"))
+    ap.add_argument("--only", nargs="*", default=None, help="regenerate only these fixtures")
     args = ap.parse_args()
     ref = Path(args.ref)
     if not (ref / "tests/bfs_dynamic_smoke.py").exists():
         sys.exit(f"reference checkout not found at {ref}")
-    cases = {"smoke_bfs_sssp.json": bfs_sssp_case(ref), "smoke_cc.json": cc_case(ref),
-             "smoke_pr.json": pr_case(ref), "pr_probe.json": pr_probe_case(ref),
-             "topology_replay.json": topology_case(ref)}
+    makers = {"smoke_bfs_sssp.json": bfs_sssp_case, "smoke_cc.json": cc_case,
+              "smoke_pr.json": pr_case, "pr_probe.json": pr_probe_case,
+              "topology_replay.json": topology_case, "group_updates.json": group_case}
+    cases = {name: make(ref) for name, make in makers.items()
+             if args.only is None or name in args.only}
     for name, data in cases.items():
         (HERE / name).write_text(json.dumps(data, separators=(",", ":")) + "\n")
         print(name, (HERE / name).stat().st_size, "bytes")

@@ -114,3 +114,37 @@ def test_topology_replay_fixture():
             if s["batch"] == bi:
                 assert orc.row_degree(s["source"]) == s["after_degree"]
                 assert orc.row_multiset_hash(s["source"]) == s["multiset_hash"]
+
+
+def test_grouping_checker_matches_the_reference_grouping():
+    """group_ref, the restatement tests/test_gpu_group.py checks
+    dycg_group_updates against, groups every batch exactly as the reference's
+    GroupedUpdateBatch does: per source (ascending), the same multiset of
+    deletion and of addition destinations, and the same number of sources per
+    phase. (The reference also keeps arrival order inside a source; the
+    device grouping sorts by destination, which changes no repair result.)"""
+    import collections
+    from tests.test_gpu_group import group_ref
+    case = cases.load("group_updates.json")
+    assert len(case["batches"]) == 6
+    for b in case["batches"]:
+        nv = b["num_vertices"]
+        ends = np.array([nv], np.uint32)
+        want = {s: (collections.Counter(d), collections.Counter(a)) for s, d, a in b["groups"]}
+        assert [g[0] for g in b["groups"]] == sorted(want)
+        got = {}
+        for phase, recs in ((0, b["dels"]), (1, b["adds"])):
+            rec = np.asarray(recs, np.uint32).reshape(-1, 2)
+            rec = np.concatenate([rec, np.ones((len(rec), 1), np.uint32)], 1)
+            keys, mult, invalid, _ = group_ref(rec, nv, ends)
+            assert invalid == 0
+            for k, m in zip(keys.tolist(), mult.tolist()):
+                got.setdefault(k >> 32, (collections.Counter(), collections.Counter()))[phase][
+                    k & 0xFFFFFFFF] += m
+        assert got == want
+        assert b["phases"] == [sum(1 for d, _ in want.values() if d),
+                               sum(1 for _, a in want.values() if a)]
+        # the reference keeps arrival order inside a source (stable grouping)
+        for s, d, a in b["groups"]:
+            assert d == [v for u, v in b["dels"] if u == s]
+            assert a == [v for u, v in b["adds"] if u == s]

@@ -20,6 +20,12 @@ What it records (all small JSON, committed):
   topology_replay.json -- tests/fixtures/topology_replay_* with the output of
                           the reference's topology_replay tool (built from the
                           reference sources by oracle/Makefile).
+  i16_repair.json      -- seeded SSSP deletion phases repaired by the oracle and
+                          checked by the reference's own CPU verifier
+                          (src/i16_repair_oracle.cpp, built by oracle/Makefile):
+                          graph, deletions, affected set, repaired distances and
+                          the verifier's report, plus one planted mistake that
+                          it must catch.
   group_updates.json   -- seeded update batches grouped by the reference's own
                           GroupedUpdateBatch (effective_update_batch.h, driven
                           by oracle/ref_group_updates.cpp, built by
@@ -237,6 +243,109 @@ def group_case(ref):
                       "(Mixed view per source; PhaseSize(Delete/Add))"}
 
 
+I16_INF = 0xFFFFFFFF
+
+
+def i16_affected(n, par, dels, source):
+    """The deletion-dependency closure: heads of deleted tree edges (parent ==
+    tail) and every vertex below them in the parent forest."""
+    children = {}
+    for x in range(n):
+        if par[x] != I16_INF:
+            children.setdefault(int(par[x]), []).append(x)
+    aff = {v for u, v, _ in dels if v != source and par[v] == u}
+    stack = list(aff)
+    while stack:
+        for c in children.get(stack.pop(), ()):
+            if c not in aff:
+                aff.add(c)
+                stack.append(c)
+    return sorted(aff)
+
+
+def i16_snapshot(path, batch, source, n, affected, inc_off, inc, before, after):
+    """The verifier's binary snapshot (include/framework/i16_repair_snapshot.h:
+    magic, version 1, infinity, weight rule 1 = (u+v)%128+1, then the
+    vectors)."""
+    import struct
+    import numpy as np
+    with open(path, "wb") as f:
+        f.write(struct.pack("<QIII", 0x4931365354415445, 1, I16_INF, 1))
+        f.write(struct.pack("<III", batch, source, n))
+        for arr, dt in ((affected, np.uint32), (inc_off, np.uint64), (inc, np.uint32)):
+            a = np.ascontiguousarray(arr, dt)
+            f.write(struct.pack("<Q", len(a)) + a.tobytes())
+        for st in (before, after):
+            a = np.ascontiguousarray(st, np.uint32).reshape(-1, 4)
+            f.write(struct.pack("<Q", len(a)) + a.tobytes())
+
+
+def i16_case(ref):
+    import tempfile
+    import numpy as np
+    sys.path.insert(0, str(REPO))
+    import oracle
+    subprocess.run(["make", "-s", "-C", str(REPO / "oracle"), f"REF={ref}"], check=True)
+    tool = REPO / "oracle/_ref/i16_repair_oracle"
+    cases_out = []
+    with tempfile.TemporaryDirectory() as td:
+        def verify(*snap):
+            i16_snapshot(f"{td}/s.bin", *snap)
+            r = subprocess.run([str(tool), f"{td}/s.bin", f"{td}/r.json"], capture_output=True,
+                               text=True)
+            rep = json.loads(r.stdout)
+            return {k: rep[k] for k in ("state", "affected", "incoming", "boundary",
+                                        "seed_vertices", "improvements", "distance_mismatches",
+                                        "external_state_changes")}
+        for seed in (1, 2):
+            rng = np.random.default_rng(seed)
+            n, m = 300, 2400
+            u, v = rng.integers(0, n, m), rng.integers(0, n, m)
+            edges = [[int(a), int(b)] for a, b in zip(u, v) if a != b]
+            off, dst, _ = oracle.csr_from_edges(n, [(a, b, 1) for a, b in edges])
+            orc = oracle.Oracle(oracle.SSSP, n, off, dst, source=0)
+            orc.init()
+            snaps = []
+            for b in range(4):
+                vals0, par0 = orc.values()
+                o, d, _ = orc.csr()
+                src = np.repeat(np.arange(n), np.diff(o.astype(np.int64)))
+                pick = rng.choice(len(d), size=40, replace=False)
+                dels = [(int(src[i]), int(d[i]), 1) for i in pick]
+                aff = i16_affected(n, par0, dels, 0)
+                orc.delete_edges(dels)
+                vals1, par1 = orc.values()
+                o, d, _ = orc.csr()
+                src = np.repeat(np.arange(n), np.diff(o.astype(np.int64)))
+                idx = {x: i for i, x in enumerate(aff)}
+                inc = [[] for _ in aff]
+                for s_, t_ in zip(src.tolist(), d.tolist()):
+                    if t_ in idx:
+                        inc[idx[t_]].append(s_)
+                inc_off = np.zeros(len(aff) + 1, np.uint64)
+                inc_off[1:] = np.cumsum([len(x) for x in inc])
+                flat = [s_ for row in inc for s_ in row]
+                listed = sorted(set(aff) | set(flat))
+                before = [(x, I16_INF, I16_INF, I16_INF) if x in idx else
+                          (x, int(vals0[x]), int(vals0[x]), int(par0[x])) for x in listed]
+                after = [(x, int(vals1[x]), int(vals1[x]), int(par1[x])) for x in listed]
+                snap = {"dels": [[a, b_] for a, b_, _ in dels], "affected": aff,
+                        "oracle_affected": int(orc.stats()["affected"]),
+                        "after": [int(vals1[x]) for x in aff],
+                        "report": verify(b, 0, n, aff, inc_off, flat, before, after)}
+                if seed == 1 and b == 0:
+                    # planted mistake (in the oracle's output, on the CPU): one
+                    # finite affected distance raised by one
+                    k = next(i for i, x in enumerate(listed) if x in idx and after[i][1] != I16_INF)
+                    bad = list(after)
+                    bad[k] = (bad[k][0], bad[k][1] + 1, bad[k][2] + 1, bad[k][3])
+                    snap["planted_report"] = verify(b, 0, n, aff, inc_off, flat, before, bad)
+                snaps.append(snap)
+            cases_out.append({"n": n, "source": 0, "graph": edges, "snapshots": snaps})
+    return {"cases": cases_out, "weight_rule": "(u+v)%128+1",
+            "origin": "src/i16_repair_oracle.cpp + include/framework/i16_repair_snapshot.h"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("DYCG_REFERENCE", "/root/reference"))
@@ -247,7 +356,8 @@ def main():
         sys.exit(f"reference checkout not found at {ref}")
     makers = {"smoke_bfs_sssp.json": bfs_sssp_case, "smoke_cc.json": cc_case,
               "smoke_pr.json": pr_case, "pr_probe.json": pr_probe_case,
-              "topology_replay.json": topology_case, "group_updates.json": group_case}
+              "topology_replay.json": topology_case, "group_updates.json": group_case,
+              "i16_repair.json": i16_case}
     cases = {name: make(ref) for name, make in makers.items()
              if args.only is None or name in args.only}
     for name, data in cases.items():

@@ -148,3 +148,43 @@ def test_grouping_checker_matches_the_reference_grouping():
         for s, d, a in b["groups"]:
             assert d == [v for u, v in b["dels"] if u == s]
             assert a == [v for u, v in b["adds"] if u == s]
+
+
+def test_deletion_repair_matches_the_reference_verifier():
+    """SSSP deletion phases (rule weights) whose repaired distances the
+    reference's own CPU verifier (src/i16_repair_oracle.cpp: Dijkstra over the
+    affected subgraph seeded from its boundary) accepted when the fixture was
+    made: the oracle invalidates the same dependency closure and repairs it to
+    the same distances, and the verifier caught the planted wrong distance."""
+    case_file = cases.load("i16_repair.json")
+    inf = oracle.INF
+    for c in case_file["cases"]:
+        n = c["n"]
+        off, dst, _ = oracle.csr_from_edges(n, [(a, b, 1) for a, b in c["graph"]])
+        orc = oracle.Oracle(oracle.SSSP, n, off, dst, source=c["source"])
+        orc.init()
+        for s in c["snapshots"]:
+            rep = s["report"]
+            assert rep["state"] == "passed" and rep["distance_mismatches"] == 0
+            assert rep["external_state_changes"] == 0 and rep["affected"] == len(s["affected"])
+            _, par = orc.values()
+            dels = [(u, v, 1) for u, v in s["dels"]]
+            # the dependency closure under the deleted tree edges
+            children = {}
+            for x in range(n):
+                if par[x] != inf:
+                    children.setdefault(int(par[x]), []).append(x)
+            aff = {v for u, v, _ in dels if v != c["source"] and par[v] == u}
+            stack = list(aff)
+            while stack:
+                for ch in children.get(stack.pop(), ()):
+                    if ch not in aff:
+                        aff.add(ch)
+                        stack.append(ch)
+            assert sorted(aff) == s["affected"]
+            orc.delete_edges(dels)
+            assert orc.stats()["affected"] == len(aff)
+            vals, _ = orc.values()
+            assert [int(vals[x]) for x in s["affected"]] == s["after"]
+            if "planted_report" in s:
+                assert s["planted_report"]["distance_mismatches"] == 1

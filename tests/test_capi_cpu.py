@@ -89,3 +89,23 @@ def test_binary_formats_round_trip(tmp_path):
 def test_integration_guide_indexes_every_entry_point():
     guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
     assert [n for n in header_functions() if n not in guide] == []
+
+
+def test_cli_usage_and_loud_failure_without_a_gpu(tmp_path):
+    import subprocess
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is visible")
+    except ImportError:
+        pass
+    for name in ("hybrid_sssp", "hybrid_bfs", "hybrid_cc", "hybrid_pr"):
+        exe = os.path.join(ROOT, "dycgraph_b200", name)
+        p = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+        assert p.returncode == 2 and "usage: " + name in p.stderr
+        g = tmp_path / "g.txt"
+        g.write_text("0 1\n1 2\n")
+        # the reference's flag spellings are accepted; no device means a clear error, no fallback
+        p = subprocess.run([exe, f"-graphfile={g}", "-format", "market_big", "--source_node=0",
+                            "-check"], capture_output=True, text=True, timeout=60)
+        assert p.returncode == 1 and "no CUDA device" in p.stderr

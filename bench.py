@@ -163,6 +163,22 @@ class Clocks:
 # no capture was taken.
 NCU_TRAFFIC = {("rmat26", "sssp"): 48_340_000}
 
+# Random host-link transactions: a probe of random GPU reads and writes of 4
+# to 128 bytes over an 8 GB pinned buffer on the B200 box took ~14 ns each
+# whatever the size, so a kernel whose host-link bytes move in transactions of
+# at most 128 bytes cannot finish faster than that.
+HOST_TX_NS = 14.0
+
+
+def link_transaction_bound(link_bytes, launch_ms, ns_per_tx=HOST_TX_NS):
+    """Lower bound on a launch's time from its host-link bytes: at least one
+    transaction per 128 bytes, each ns_per_tx; frac = bound / measured time."""
+    tx = int(np.ceil(max(0.0, float(link_bytes)) / 128.0))
+    bound_ms = tx * ns_per_tx / 1e6
+    return {"ns_per_transaction": ns_per_tx, "min_transactions": tx,
+            "bound_ms": round(bound_ms, 4),
+            "frac": round(bound_ms / launch_ms, 4) if launch_ms > 0 else None}
+
 
 def peaks():
     try:
@@ -352,7 +368,8 @@ def run_dycg(args):
         "launch_ms": round(float(rep_ms), 4),
         "host_link": {"achieved": round(ach_link, 2), "peak_zero_copy": round(link_zc, 2),
                       "peak_h2d_copy": round(link_h2d, 2), "unit": "GB/s",
-                      "frac": round(ach_link / link_zc, 5)},
+                      "frac": round(ach_link / link_zc, 5),
+                      "transaction_bound": link_transaction_bound(rep_link, float(rep_ms))},
         "roofline_time_frac": round(t_bound / (rep_ms / 1e3), 5),
         "mutation_kernels": {"ms": round(float(mut_ms), 4), "link_bytes": int(mut_bytes_link),
                              "hbm_bytes": int(mut_bytes_hbm)},
@@ -775,7 +792,8 @@ def run_batched(args):
         "launch_ms": round(rep_ms / K, 4),
         "host_link": {"achieved": round(ach_link, 2), "peak_zero_copy": round(link_zc, 2),
                       "peak_h2d_copy": round(link_h2d, 2), "unit": "GB/s",
-                      "frac": round(ach_link / link_zc, 5)},
+                      "frac": round(ach_link / link_zc, 5),
+                      "transaction_bound": link_transaction_bound(rep_link / K, rep_ms / K)},
         "roofline_time_frac": round(t_bound / (rep_ms / 1e3), 5),
     }
     launches = int(sum(p["kernel_launches"] for p in per))
@@ -1091,7 +1109,8 @@ def run_learned(args):
         "launch_ms": round(rep_ms / K, 4),
         "host_link": {"achieved": round(rep_link / (rep_ms * 1e6), 2),
                       "peak_zero_copy": round(link_zc, 2), "peak_h2d_copy": round(link_h2d, 2),
-                      "unit": "GB/s", "frac": round(rep_link / (rep_ms * 1e6) / link_zc, 5)},
+                      "unit": "GB/s", "frac": round(rep_link / (rep_ms * 1e6) / link_zc, 5),
+                      "transaction_bound": link_transaction_bound(rep_link / K, rep_ms / K)},
     }
     policies = {p: {k: v for k, v in r.items() if not k.startswith("_")} for p, r in res.items()}
     H = res["hotness"]

@@ -148,3 +148,13 @@ def test_grid_snapshots_mix_grid_edges_and_shortcuts():
         cheb = np.maximum(np.abs(au // side - av // side), np.abs(au % side - av % side))
         # within radius 8, except a draw that landed on u itself and was moved to u + 1
         assert ((cheb <= 8) | (av == (au + 1) % n)).all()
+
+
+def test_link_transaction_bound():
+    import bench
+    b = bench.link_transaction_bound(4_150_000, 0.98)
+    assert b["min_transactions"] == 32_422  # ceil(4.15 MB / 128 B)
+    assert abs(b["bound_ms"] - 32_422 * 14e-6) < 1e-3 and 0 < b["frac"] < 1
+    assert bench.link_transaction_bound(0, 1.0)["min_transactions"] == 0
+    assert bench.link_transaction_bound(-5.0, 1.0)["bound_ms"] == 0
+    assert bench.link_transaction_bound(1000, 0)["frac"] is None

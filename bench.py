@@ -872,8 +872,9 @@ def run_batched(args):
         "gpu_launches": launches,
         "roofline": roofline,
         "per_step": per_step,
-        "mapping_candidates": [[t["qratio"], t["heavy"], t["pull_qratio"], round(t["repair_ms"], 3)]
-                               for t in tried],
+        # [qratio, heavy, pull ratio, query-lane tile slots, repair ms] per trial
+        "mapping_candidates": [[t["qratio"], t["heavy"], t["pull_qratio"], t["tile"],
+                                round(t["repair_ms"], 3)] for t in tried],
         "plain_per_query": plain,
         "speedup_vs_plain": round(value / plain["value"], 2) if plain else None,
     }

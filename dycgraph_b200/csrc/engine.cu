@@ -1244,13 +1244,16 @@ void Engine::tune_repair(uint32_t nd, uint32_t na, u64 timeout) {
   static const uint32_t kRatio[] = {2, 4, 8, 1u << 20};
   static const uint32_t kHeavy[] = {16, 64, 256};
   static const uint32_t kPull[] = {0, 1, 2, 8};
+  static const uint32_t kTile[] = {1024, 4096, 16384};
   tried_.clear();
+  const uint32_t tile0 = tile_;
   dycg_query_mapping best{qratio_, heavy_, tile_, pull_qratio_, 1e30f};
-  auto trial = [&](uint32_t r, uint32_t h, uint32_t pr) {
+  auto trial = [&](uint32_t r, uint32_t h, uint32_t pr, uint32_t t) {
     if (!tried_.empty()) restore();
     qratio_ = r;
     heavy_ = h;
     pull_qratio_ = pr;
+    tile_ = t;
     CK(cudaEventRecord(sc.a, st_));
     CK(launch_multi(multi_launch(phases, na, timeout), st_));
     CK(cudaEventRecord(sc.b, st_));
@@ -1263,21 +1266,25 @@ void Engine::tune_repair(uint32_t nd, uint32_t na, u64 timeout) {
     }
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, sc.a, sc.b));
-    tried_.push_back({r, h, tile_, pr, ms});
+    tried_.push_back({r, h, t, pr, ms});
     if (ms < best.repair_ms) best = tried_.back();
     launches_++;
   };
   // coordinate search: (qratio, heavy) with the pull phase on the same rule,
-  // then the pull phase's own ratio
+  // then the pull phase's own ratio, then the slots per query-lane tile
   for (uint32_t r : kRatio)
-    for (uint32_t h : kHeavy) trial(r, h, r);
+    for (uint32_t h : kHeavy) trial(r, h, r, tile0);
   const dycg_query_mapping first = best;
   for (uint32_t pr : kPull)
-    if (pr != first.qratio) trial(first.qratio, first.heavy, pr);
+    if (pr != first.qratio) trial(first.qratio, first.heavy, pr, tile0);
+  const dycg_query_mapping second = best;
+  for (uint32_t t : kTile)
+    if (t != second.tile) trial(second.qratio, second.heavy, second.pull_qratio, t);
   restore();
   qratio_ = best.qratio;
   heavy_ = best.heavy;
   pull_qratio_ = best.pull_qratio;
+  tile_ = best.tile;
   drop_graphs();
   CK(cudaEventRecord(ev_[2], st_));  // the stage boundary of the kept run
   CK(launch_multi(multi_launch(phases, na, timeout), st_));

@@ -347,7 +347,8 @@ typedef struct dycg_query_mapping {
  * applies one snapshot like dycg_apply_batch, but repairs it once per
  * candidate mapping (qratio in {2,4,8,2^20} x heavy in {16,64,256} with the
  * pull phase on the same ratio, then the best of those with the pull phase's
- * ratio in {0,1,2,8}), each from the same saved state, keeps the fastest
+ * ratio in {0,1,2,8}, then the best so far with query-lane tiles of
+ * {1024,4096,16384} slots), each from the same saved state, keeps the fastest
  * mapping for later snapshots
  * and leaves the state of one ordinary repair. Needs HBM for one extra copy
  * of the query results while it runs. tried (cap entries, may be NULL)

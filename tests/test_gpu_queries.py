@@ -187,7 +187,9 @@ def test_tune_mapping_keeps_results():
     tried = e.tune_query_mapping(dels, adds)
     orc.mutate(dels, adds)
     cur = orc.csr()
-    assert 12 < len(tried) <= 16 and all(t["repair_ms"] > 0 for t in tried)
+    # 12 (qratio x heavy) + 3-4 pull ratios + 2-3 tile sizes
+    assert 12 < len(tried) <= 19 and all(t["repair_ms"] > 0 for t in tried)
+    assert {t["tile"] for t in tried} == {1024, 4096, 16384}
     _check_all(e, n, cur, src)
     for bi in range(2):  # later snapshots under the kept mapping
         dels, adds = cases.random_batch(n, *cur, 400, 400, 2310 + bi)

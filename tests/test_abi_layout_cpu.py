@@ -50,3 +50,28 @@ def test_ctypes_mirrors_match_the_c_header(tmp_path):
         for f, _ in cls._fields_:
             d = getattr(cls, f)
             assert got[(cname, f)] == (d.offset, d.size), (cname, f)
+
+
+def _code_blocks(path, lang):
+    import re
+    text = open(os.path.join(ROOT, path)).read()
+    return re.findall(r"```" + lang + r"\n(.*?)```", text, re.S)
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None or shutil.which("g++") is None,
+                    reason="no C/C++ compiler")
+def test_documented_examples_compile_against_the_header(tmp_path):
+    """The README's C example and INTEGRATION.md's C++ shim use only names and
+    signatures that include/dycg.h declares (syntax and type check, no link)."""
+    (c_example,) = _code_blocks("README.md", "c")
+    src = tmp_path / "readme.c"
+    src.write_text('#include "dycg.h"\n'
+                   "int example(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na,\n"
+                   "            uint32_t *dist, uint32_t *parent) {\n" + c_example + "  return 0;\n}\n")
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-fsyntax-only", "-I",
+                    os.path.join(ROOT, "include"), str(src)], check=True, capture_output=True)
+    (shim,) = _code_blocks("INTEGRATION.md", "cpp")
+    src = tmp_path / "shim.cpp"
+    src.write_text(shim)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I",
+                    os.path.join(ROOT, "include"), str(src)], check=True, capture_output=True)

@@ -184,6 +184,29 @@ int dycg_gen_rmat_edges(uint32_t scale, double a, double b, double c, uint64_t s
   return DYCG_OK;
 }
 
+int dycg_convert_graph_text(const char *text_path, const char *binary_path, uint32_t min_nodes,
+                            int weighted) {
+  if (!text_path || !binary_path) return DYCG_EINVAL;
+  try {
+    const dycg::TextGraph g = dycg::parse_text_graph(text_path, min_nodes, weighted);
+    std::FILE *f = std::fopen(binary_path, "wb");
+    if (!f) return DYCG_EIO;
+    const uint64_t hdr[3] = {g.n, g.m, weighted ? 1ull : 0ull};
+    bool ok = std::fwrite("DYCGCSR1", 1, 8, f) == 8 && std::fwrite(hdr, 8, 3, f) == 3 &&
+              std::fwrite(g.off.data(), 8, g.n + 1ull, f) == g.n + 1ull &&
+              std::fwrite(g.dst.data(), 4, g.m, f) == g.m &&
+              (!weighted || std::fwrite(g.w.data(), 4, g.m, f) == g.m);
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? DYCG_OK : DYCG_EIO;
+  } catch (const Error &x) {
+    return x.code;
+  } catch (const std::bad_alloc &) {
+    return DYCG_ENOMEM;
+  } catch (const std::exception &) {
+    return DYCG_EINVAL;
+  }
+}
+
 uint32_t dycg_hash_weight(uint64_t seed, uint32_t u, uint32_t v, uint32_t wlo, uint32_t whi) {
   if (whi < wlo) return wlo;
   return dycg::hash_weight(seed ^ 0x5745494748545321ull, u, v, wlo, whi);

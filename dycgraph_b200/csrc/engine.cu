@@ -336,7 +336,9 @@ void Engine::load_csr(uint32_t n, const uint64_t *off, const uint32_t *dst, cons
   if (d_w2) cudaFree(d_w2);
 }
 
-void Engine::load_file(const char *path, uint32_t min_nodes, int weighted) {
+// Text edge list ("u v [w]" lines; empty, '#' and '%' lines skipped; the
+// weight defaults to 1) -> CSR with each row's edges in file order.
+TextGraph parse_text_graph(const char *path, uint32_t min_nodes, int weighted) {
   std::ifstream in(path);
   if (!in) throw Error(DYCG_EIO, std::string("cannot open graph file ") + path);
   std::vector<uint32_t> us, vs, ws;
@@ -354,18 +356,26 @@ void Engine::load_file(const char *path, uint32_t min_nodes, int weighted) {
     ws.push_back((uint32_t)w);
     maxid = std::max(maxid, std::max(u, v));
   }
-  const uint32_t n = std::max<uint32_t>(us.empty() ? 1u : (uint32_t)(maxid + 1), min_nodes);
-  std::vector<uint64_t> off(n + 1ull, 0);
-  for (uint32_t u : us) off[u + 1]++;
-  for (uint32_t v = 0; v < n; v++) off[v + 1] += off[v];
-  std::vector<uint32_t> dst(us.size() + 1), wt(us.size() + 1);
-  std::vector<uint64_t> fill(off.begin(), off.end() - 1);
+  TextGraph g;
+  g.n = std::max<uint32_t>(us.empty() ? 1u : (uint32_t)(maxid + 1), min_nodes);
+  g.off.assign(g.n + 1ull, 0);
+  for (uint32_t u : us) g.off[u + 1]++;
+  for (uint32_t v = 0; v < g.n; v++) g.off[v + 1] += g.off[v];
+  g.dst.resize(us.size() + 1);
+  g.w.resize(us.size() + 1);
+  std::vector<uint64_t> fill(g.off.begin(), g.off.end() - 1);
   for (size_t i = 0; i < us.size(); i++) {
     const uint64_t p = fill[us[i]]++;
-    dst[p] = vs[i];
-    wt[p] = ws[i];
+    g.dst[p] = vs[i];
+    g.w[p] = ws[i];
   }
-  load_csr(n, off.data(), dst.data(), weighted ? wt.data() : nullptr);
+  g.m = us.size();
+  return g;
+}
+
+void Engine::load_file(const char *path, uint32_t min_nodes, int weighted) {
+  const TextGraph g = parse_text_graph(path, min_nodes, weighted);
+  load_csr(g.n, g.off.data(), g.dst.data(), weighted ? g.w.data() : nullptr);
 }
 
 // Binary CSR: header "DYCGCSR1", n, m, flags; offsets[n+1] (u64); dst[m] (u32);

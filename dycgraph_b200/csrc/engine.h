@@ -17,6 +17,16 @@ struct Error : std::runtime_error {
   Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
 };
 
+// A text edge list parsed on the host (shared by Engine::load_file and the
+// text-to-binary converter).
+struct TextGraph {
+  uint32_t n = 0;
+  uint64_t m = 0;
+  std::vector<uint64_t> off;
+  std::vector<uint32_t> dst, w;
+};
+TextGraph parse_text_graph(const char *path, uint32_t min_nodes, int weighted);
+
 // One adjacency direction: a pinned, mapped host arena plus its descriptors.
 struct Arena {
   uint32_t *h_dst = nullptr;  // host address of the slot words

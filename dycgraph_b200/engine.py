@@ -121,6 +121,7 @@ def lib():
         "dycg_load_graph_csr": (I, [P, u32, u64p, u32p, u32p]),
         "dycg_load_graph_file": (I, [P, ctypes.c_char_p, u32, I]),
         "dycg_load_graph_binary": (I, [P, ctypes.c_char_p]),
+        "dycg_convert_graph_text": (I, [ctypes.c_char_p, ctypes.c_char_p, u32, I]),
         "dycg_load_graph_rmat": (I, [P, u32, u32, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double, u64, u32, u32, I]),
         "dycg_load_graph_grid": (I, [P, u32, u32, u32, u64, u32, u32]),
@@ -225,6 +226,14 @@ def measure_host_link(device=0, nbytes=1 << 30):
 
 def hash_weight(seed, u, v, wlo=1, whi=64):
     return lib().dycg_hash_weight(seed, u, v, wlo, whi)
+
+
+def convert_graph_text(text_path, binary_path, min_nodes=0, weighted=False):
+    """Text edge list -> binary CSR file (as load_file reads the text; no GPU)."""
+    rc = lib().dycg_convert_graph_text(str(text_path).encode(), str(binary_path).encode(),
+                                       min_nodes, int(weighted))
+    if rc:
+        raise DycgError(rc, f"dycg_convert_graph_text({text_path})")
 
 
 class Engine:

@@ -67,3 +67,26 @@ def read_updates(path):
         out.append((recs[p:p + nd], recs[p + nd:p + nd + na]))
         p += nd + na
     return out
+
+
+def main(argv=None):
+    """python -m dycgraph_b200.formats graph TEXT OUT [--weighted] [--min-nodes N]
+    converts a text edge list (the reference's market_big lines) to the binary
+    graph file, parsed by the library exactly as its text loader does."""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m dycgraph_b200.formats")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    g = sub.add_parser("graph", help="text edge list -> DYCGCSR1")
+    g.add_argument("text")
+    g.add_argument("out")
+    g.add_argument("--weighted", action="store_true", help="read a third column as weights")
+    g.add_argument("--min-nodes", type=int, default=0)
+    args = ap.parse_args(argv)
+    from .engine import convert_graph_text
+    convert_graph_text(args.text, args.out, args.min_nodes, args.weighted)
+    n, off, dst, w = read_graph(args.out)
+    print(f"{args.out}: {n} vertices, {len(dst)} edges{', weighted' if w is not None else ''}")
+
+
+if __name__ == "__main__":
+    main()

@@ -177,6 +177,13 @@ int dycg_load_graph_file(dycg_engine *e, const char *path, uint32_t min_nodes,
  * read with one pass over a memory map. */
 int dycg_load_graph_binary(dycg_engine *e, const char *path);
 
+/* Converts a text edge list, read exactly as dycg_load_graph_file reads it
+ * (the market_big parse it replaces, src/utils/parser.cpp:296-406), into the
+ * binary CSR file above, so that large graphs are parsed once and later load
+ * from a memory map. Host only (no GPU needed). */
+int dycg_convert_graph_text(const char *text_path, const char *binary_path, uint32_t min_nodes,
+                            int weighted);
+
 /* Synthetic workloads built on the GPU straight into the engine. R-MAT:
  * 2^scale vertices, edge_factor*2^scale draws with quadrant probabilities
  * (a,b,c,1-a-b-c), self-loops and duplicates removed; weights uniform in

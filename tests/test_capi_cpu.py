@@ -109,3 +109,31 @@ def test_cli_usage_and_loud_failure_without_a_gpu(tmp_path):
         p = subprocess.run([exe, f"-graphfile={g}", "-format", "market_big", "--source_node=0",
                             "-check"], capture_output=True, text=True, timeout=60)
         assert p.returncode == 1 and "no CUDA device" in p.stderr
+
+
+def test_text_graph_converts_to_the_binary_format(tmp_path):
+    """dycg_convert_graph_text reads a text edge list the way the text loader
+    does (comment, blank and malformed lines skipped, a missing weight is 1,
+    rows in file order, duplicates and self-loops kept for the loader's rules)
+    and writes the binary graph file."""
+    from dycgraph_b200 import formats
+    lines = ["%%MatrixMarket matrix coordinate pattern general", "# comment", "3 1 7", "0 2 5",
+             "3 1 2", "", "0 4", "4 4 9", "not an edge", "1 0 3"]
+    txt = tmp_path / "g.txt"
+    txt.write_text("\n".join(lines) + "\n")
+    edges = [tuple(int(x) for x in ln.split()) for ln in lines
+             if ln and ln[0] not in "#%" and ln.split()[0].isdigit()]
+    for weighted, min_nodes in ((True, 0), (False, 9)):
+        out = tmp_path / f"g{int(weighted)}.bin"
+        dg.engine.convert_graph_text(txt, out, min_nodes, weighted)
+        n, off, dst, w = formats.read_graph(out)
+        assert n == max(5, min_nodes)
+        want_rows = [[(e[1], e[2] if len(e) > 2 else 1) for e in edges if e[0] == u]
+                     for u in range(n)]
+        assert list(np.diff(off.astype(np.int64))) == [len(r) for r in want_rows]
+        assert list(dst) == [v for r in want_rows for v, _ in r]
+        assert (w is not None) == weighted
+        if weighted:
+            assert list(w) == [x for r in want_rows for _, x in r]
+    with pytest.raises(dg.DycgError):
+        dg.engine.convert_graph_text(tmp_path / "missing.txt", tmp_path / "x.bin")

@@ -69,10 +69,42 @@ def read_updates(path):
     return out
 
 
+def text_updates_to_binary(update_path, sizes_path, out_path):
+    """Text update stream -> DYCGUPD1, split as the reference's Loader splits it
+    (include/framework/Loader.h:30-101): each sizes line "adds dels" takes the
+    next adds 'a' records and the next dels 'd' records in file order; an update
+    line is "t u v [w]" (t in {a, d}; w defaults to 1, other lines are skipped).
+    Returns the number of snapshots written."""
+    sizes = []
+    with open(sizes_path) as f:
+        for line in f:
+            p = line.split()
+            if len(p) >= 2 and p[0].isdigit() and p[1].isdigit():
+                sizes.append((int(p[0]), int(p[1])))
+    recs = {"a": [], "d": []}
+    with open(update_path) as f:
+        for line in f:
+            p = line.split()
+            if len(p) < 3 or p[0] not in recs or not (p[1].isdigit() and p[2].isdigit()):
+                continue
+            w = int(p[3]) if len(p) > 3 and p[3].isdigit() else 1
+            recs[p[0]].append((int(p[1]), int(p[2]), w))
+    batches, ia, idl = [], 0, 0
+    for na, nd in sizes:
+        batches.append((np.asarray(recs["d"][idl:idl + nd], np.uint32).reshape(-1, 3),
+                        np.asarray(recs["a"][ia:ia + na], np.uint32).reshape(-1, 3)))
+        ia += na
+        idl += nd
+    write_updates(out_path, batches)
+    return len(batches)
+
+
 def main(argv=None):
     """python -m dycgraph_b200.formats graph TEXT OUT [--weighted] [--min-nodes N]
     converts a text edge list (the reference's market_big lines) to the binary
-    graph file, parsed by the library exactly as its text loader does."""
+    graph file, parsed by the library exactly as its text loader does;
+    python -m dycgraph_b200.formats updates UPDATES SIZES OUT converts a text
+    update stream and its sizes file to the binary update stream."""
     import argparse
     ap = argparse.ArgumentParser(prog="python -m dycgraph_b200.formats")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -81,7 +113,15 @@ def main(argv=None):
     g.add_argument("out")
     g.add_argument("--weighted", action="store_true", help="read a third column as weights")
     g.add_argument("--min-nodes", type=int, default=0)
+    u = sub.add_parser("updates", help="text update stream + sizes file -> DYCGUPD1")
+    u.add_argument("updates")
+    u.add_argument("sizes")
+    u.add_argument("out")
     args = ap.parse_args(argv)
+    if args.cmd == "updates":
+        nb = text_updates_to_binary(args.updates, args.sizes, args.out)
+        print(f"{args.out}: {nb} snapshots")
+        return
     from .engine import convert_graph_text
     convert_graph_text(args.text, args.out, args.min_nodes, args.weighted)
     n, off, dst, w = read_graph(args.out)

@@ -137,3 +137,26 @@ def test_text_graph_converts_to_the_binary_format(tmp_path):
             assert list(w) == [x for r in want_rows for _, x in r]
     with pytest.raises(dg.DycgError):
         dg.engine.convert_graph_text(tmp_path / "missing.txt", tmp_path / "x.bin")
+
+
+def test_text_updates_convert_to_the_binary_stream(tmp_path):
+    """The update converter splits a text stream per the reference's Loader
+    (tests/cases.replay_batches restates it) and the binary stream reads back
+    the same snapshots, weights included (default 1)."""
+    from dycgraph_b200 import formats
+    from tests import cases
+    lines = ["# header", "a 1 2 5", "d 3 4", "a 5 6", "x 1 1", "d 7 8 9", "a 9 10 2",
+             "d 11 12", "bad", "a 13 14 1"]
+    (tmp_path / "u.txt").write_text("\n".join(lines) + "\n")
+    (tmp_path / "s.txt").write_text("2 1\n\n1 2\n1 0\n")
+    nb = formats.text_updates_to_binary(tmp_path / "u.txt", tmp_path / "s.txt", tmp_path / "u.bin")
+    assert nb == 3
+    back = formats.read_updates(tmp_path / "u.bin")
+    recs = [ln.split() for ln in lines if ln[:1] in ("a", "d") and len(ln.split()) >= 3]
+    weight = {(int(p[1]), int(p[2])): int(p[3]) if len(p) > 3 else 1 for p in recs}
+    want = cases.replay_batches([(p[0], int(p[1]), int(p[2])) for p in recs],
+                                [(2, 1), (1, 2), (1, 0)])
+    assert len(back) == len(want)
+    for (d, a), (wd, wa) in zip(back, want):
+        assert [tuple(r) for r in d.tolist()] == [(u, v, weight[(u, v)]) for u, v in wd]
+        assert [tuple(r) for r in a.tolist()] == [(u, v, weight[(u, v)]) for u, v in wa]

@@ -73,8 +73,10 @@ typedef struct dycg_options {
   uint32_t algo;          /* DYCG_ALGO_*                                      */
   uint32_t weight_mode;   /* DYCG_WEIGHT_* (SSSP only)                        */
   uint32_t source;        /* SSSP/BFS root (reference -source_node)           */
-  uint32_t segments;      /* reference -SEGMENT: edge-balanced vertex ranges  */
-                          /* used to bin each update batch                    */
+  uint32_t segments;      /* reference -SEGMENT, accepted for compatibility:   */
+                          /* the engine's unit of storage, caching and update */
+                          /* binning is the page (2^page_shift slots); the    */
+                          /* per-segment binning is dycg_group_updates's      */
   uint64_t hbm_graph_budget_bytes; /* cap on adjacency bytes resident in HBM  */
   uint32_t cache_policy;  /* DYCG_CACHE_*                                     */
   uint32_t symmetric;     /* 1: graph and every batch are symmetric, the      */

@@ -341,7 +341,40 @@ class Engine:
             raise DycgError(-1, "source differs from the engine's configured source")
 
     # -- batches ---------------------------------------------------------------
+    # -- the reference's update files (Engine::get_update_file / GetUpdateBatchCount,
+    #    include/framework/framework.cuh:2387-2415) ----------------------------------
+    def get_update_file(self, updates, sizes=None):
+        """Read an update stream for del_edge(b) / add_edge(b): a binary
+        DYCGUPD1 file, or a text stream with its sizes file (split as the
+        reference's Loader splits it). Returns the number of snapshots."""
+        from . import formats
+        with open(updates, "rb") as f:
+            binary = f.read(8) == formats.UPD_MAGIC
+        if binary:
+            self._updates = formats.read_updates(updates)
+        elif sizes is None:
+            raise DycgError(-1, "a text update stream needs its sizes file")
+        else:
+            self._updates = formats.read_text_updates(updates, sizes)
+        return len(self._updates)
+
+    def GetUpdateBatchCount(self):
+        return len(getattr(self, "_updates", None) or [])
+
+    def _snapshot(self, b):
+        ups = getattr(self, "_updates", None)
+        if ups is None:
+            raise DycgError(-1, "no update stream read (get_update_file)")
+        if not 0 <= int(b) < len(ups):
+            raise DycgError(-1, f"snapshot {b} out of range (0..{len(ups) - 1})")
+        return ups[int(b)]
+
     def delete_edges(self, dels):
+        """Delete one live occurrence per record; dels is a list of (u, v[, w])
+        or, after get_update_file, a snapshot index (the reference's
+        del_edge(offsets, b))."""
+        if isinstance(dels, (int, np.integer)):
+            dels = self._snapshot(dels)[0]
         arr = edges_array(dels)
         st = BatchStats()
         self._check(lib().dycg_delete_edges(self._h, arr.ctypes.data_as(ctypes.POINTER(Edge)),
@@ -350,6 +383,10 @@ class Engine:
         return self.last_stats
 
     def insert_edges(self, adds):
+        """Append one occurrence per record; adds is a list of (u, v[, w]) or,
+        after get_update_file, a snapshot index (the reference's add_edge)."""
+        if isinstance(adds, (int, np.integer)):
+            adds = self._snapshot(adds)[1]
         arr = edges_array(adds)
         st = BatchStats()
         self._check(lib().dycg_insert_edges(self._h, arr.ctypes.data_as(ctypes.POINTER(Edge)),
@@ -471,6 +508,22 @@ class Engine:
     compute_hot_vertices_sssp = cache_maintenance
     LoadCache = cache_maintenance
 
+    def CacheRefreshRequired(self):
+        """The refresh gate runs inside cache_maintenance; a driver that asks is
+        told to go on to LoadCache."""
+        return True
+
+    def confirm_candidate_batch(self, *args, **kwargs):
+        """Candidate confirmation, eviction, compaction and publication happen
+        inside cache_maintenance (compute_hot_vertices_sssp / LoadCache); the
+        reference's separate calls have nothing left to do."""
+        return None
+
+    TraceCacheCandidates = confirm_candidate_batch
+    MarkCachePublished = confirm_candidate_batch
+    evication_cache = confirm_candidate_batch
+    compact_cache = confirm_candidate_batch
+
     # -- results ---------------------------------------------------------------
     def gather(self):
         v = np.empty(self.n, np.uint32)
@@ -484,6 +537,36 @@ class Engine:
 
     def GatherParent(self):
         return self.gather()[1]
+
+    def GatherBuffer(self):
+        """The reference's per-vertex buffer: equal to the value once a repair
+        has finished (SSSP/BFS/CC); the residuals for PageRank."""
+        if self.algo == ALGOS["pr"]:
+            return self.gather_ranks()[1]
+        return self.gather()[0]
+
+    def GetGraphDatum(self):
+        """Sizes and memory layout of the graph (the reference returns its
+        GraphDatum)."""
+        return self.info()
+
+    def ChunkStore(self):
+        """The live outgoing adjacency as CSR (offsets, dst, w)."""
+        return self.csr()
+
+    def SetOptions(self, **options):
+        """Options are fixed when the engine is created (dycg_create takes them):
+        values equal to the engine's are accepted, any other is an error."""
+        names = {"algo": ALGOS, "weight_mode": WEIGHTS, "cache_policy": CACHE}
+        for k, v in options.items():
+            if not hasattr(self.options, k) or k == "reserved":
+                raise DycgError(-1, f"unknown option {k}")
+            if isinstance(v, str) and k in names:
+                v = names[k][v]
+            cur = getattr(self.options, k)
+            same = abs(cur - v) <= 1e-6 * max(1.0, abs(v)) if isinstance(cur, float) else cur == v
+            if not same:
+                raise DycgError(-1, f"option {k} is fixed at creation ({cur}), not {v}")
 
     # -- many-query forms --------------------------------------------------------
     QUERY_MODES = {"batched": 0, "per_query": 1}

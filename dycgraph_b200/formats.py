@@ -69,12 +69,12 @@ def read_updates(path):
     return out
 
 
-def text_updates_to_binary(update_path, sizes_path, out_path):
-    """Text update stream -> DYCGUPD1, split as the reference's Loader splits it
-    (include/framework/Loader.h:30-101): each sizes line "adds dels" takes the
-    next adds 'a' records and the next dels 'd' records in file order; an update
-    line is "t u v [w]" (t in {a, d}; w defaults to 1, other lines are skipped).
-    Returns the number of snapshots written."""
+def read_text_updates(update_path, sizes_path):
+    """Text update stream -> [(dels, adds), ...] per snapshot, split as the
+    reference's Loader splits it (include/framework/Loader.h:30-101): each
+    sizes line "adds dels" takes the next adds 'a' records and the next dels
+    'd' records in file order; an update line is "t u v [w]" (t in {a, d}; w
+    defaults to 1, other lines are skipped)."""
     sizes = []
     with open(sizes_path) as f:
         for line in f:
@@ -95,6 +95,13 @@ def text_updates_to_binary(update_path, sizes_path, out_path):
                         np.asarray(recs["a"][ia:ia + na], np.uint32).reshape(-1, 3)))
         ia += na
         idl += nd
+    return batches
+
+
+def text_updates_to_binary(update_path, sizes_path, out_path):
+    """Text update stream + sizes file -> DYCGUPD1 (read_text_updates' split).
+    Returns the number of snapshots written."""
+    batches = read_text_updates(update_path, sizes_path)
     write_updates(out_path, batches)
     return len(batches)
 

@@ -160,3 +160,42 @@ def test_text_updates_convert_to_the_binary_stream(tmp_path):
     for (d, a), (wd, wa) in zip(back, want):
         assert [tuple(r) for r in d.tolist()] == [(u, v, weight[(u, v)]) for u, v in wd]
         assert [tuple(r) for r in a.tolist()] == [(u, v, weight[(u, v)]) for u, v in wa]
+
+
+def test_reference_engine_names_and_update_files(tmp_path):
+    """The mirror answers to every Engine method the reference's sample drivers
+    call; the update-file ones work without a GPU (an engine object made
+    without a device handle)."""
+    from dycgraph_b200 import formats
+    names = ["LoadGraph", "SetOptions", "InitGraph", "Start", "compute_hot_vertices_sssp",
+             "confirm_candidate_batch", "TraceCacheCandidates", "LoadCache", "MarkCachePublished",
+             "get_update_file", "GetUpdateBatchCount", "del_edge", "add_edge",
+             "CacheRefreshRequired", "evication_cache", "compact_cache", "GatherValue",
+             "GatherParent", "GatherBuffer", "GetGraphDatum", "ChunkStore", "StartPageRank",
+             "UpdatePageRank"]
+    assert [n for n in names if not hasattr(dg.Engine, n)] == []
+    e = dg.Engine.__new__(dg.Engine)
+    e._h = None
+    e.options = dg.engine.Options()
+    dg.lib().dycg_options_default(ctypes.byref(e.options))
+    assert e.GetUpdateBatchCount() == 0
+    with pytest.raises(dg.DycgError):
+        e._snapshot(0)
+    (tmp_path / "u.txt").write_text("a 1 2 3\nd 4 5\na 6 7\n")
+    (tmp_path / "s.txt").write_text("1 1\n1 0\n")
+    assert e.get_update_file(tmp_path / "u.txt", tmp_path / "s.txt") == 2
+    d, a = e._snapshot(1)
+    assert d.shape == (0, 3) and a.tolist() == [[6, 7, 1]]
+    with pytest.raises(dg.DycgError):
+        e._snapshot(2)
+    with pytest.raises(dg.DycgError):
+        e.get_update_file(tmp_path / "u.txt")  # text needs its sizes file
+    formats.write_updates(tmp_path / "u.bin", [(np.array([[4, 5, 1]]), np.array([[1, 2, 3]]))])
+    assert e.get_update_file(tmp_path / "u.bin") == 1 and e.GetUpdateBatchCount() == 1
+    assert e._snapshot(0)[1].tolist() == [[1, 2, 3]]
+    assert e.CacheRefreshRequired() is True and e.compact_cache() is None
+    e.SetOptions(algo="sssp", alpha=0.85, max_rounds=100)
+    with pytest.raises(dg.DycgError):
+        e.SetOptions(algo="bfs")
+    with pytest.raises(dg.DycgError):
+        e.SetOptions(no_such_option=1)

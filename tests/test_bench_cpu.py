@@ -158,3 +158,22 @@ def test_link_transaction_bound():
     assert bench.link_transaction_bound(0, 1.0)["min_transactions"] == 0
     assert bench.link_transaction_bound(-5.0, 1.0)["bound_ms"] == 0
     assert bench.link_transaction_bound(1000, 0)["frac"] is None
+
+
+def test_rmat_snapshots_are_disjoint_live_deletions_and_rmat_insertions():
+    import numpy as np
+    import bench
+    import oracle
+    n, off, dst, w = oracle.rmat_csr(12, 8, 4)
+    nd, na, nb = 200, 150, 4
+    batches = bench.make_batches(12, nb, nd, na, 9, bench._cpu_sampler(off, dst, w), "rmat26",
+                                 rmat_fn=oracle.gen_rmat_edges)
+    src = np.repeat(np.arange(n), np.diff(off.astype(np.int64)))
+    live = set((src * n + dst).tolist())
+    seen = set()
+    adds_all = oracle.gen_rmat_edges(12, nb * na, 10)
+    for i, (d, a) in enumerate(batches):
+        keys = (d[:, 0].astype(np.int64) * n + d[:, 1]).tolist()
+        assert len(d) == nd and set(keys) <= live and len(set(keys)) == nd and not set(keys) & seen
+        seen |= set(keys)
+        assert (a == adds_all[i * na:(i + 1) * na]).all()

@@ -199,3 +199,16 @@ def test_reference_engine_names_and_update_files(tmp_path):
         e.SetOptions(algo="bfs")
     with pytest.raises(dg.DycgError):
         e.SetOptions(no_such_option=1)
+
+
+def test_smoke_fails_loudly_without_a_gpu():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is visible")
+    except ImportError:
+        pass
+    import __graft_entry__
+    with pytest.raises(dg.DycgError) as ei:
+        __graft_entry__.smoke()
+    assert ei.value.code == -8  # DYCG_ENOGPU: no CPU fallback

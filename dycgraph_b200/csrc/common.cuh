@@ -22,6 +22,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include "../../include/dycg_operators.h"
 
 namespace dycg {
 
@@ -268,13 +269,12 @@ __device__ __forceinline__ bool write_slot(const Adj &a, u64 p, uint32_t d, uint
   return cs != PAGE_NONE;
 }
 
-// Edge weight by algorithm: BFS 1, CC 0, SSSP stored or (u+v)%128+1
-// (the reference's TraversalEdgeWeight, include/framework/variants/api.cuh:26-28).
+// Edge weight by algorithm (BFS 1, CC 0, SSSP (u+v)%128+1 unless weights are
+// stored): the operator's TraversalEdgeWeight (the reference's,
+// include/framework/variants/api.cuh:26-28).
 template <uint32_t ALGO>
 __device__ __forceinline__ uint32_t rule_weight(uint32_t u, uint32_t v) {
-  if (ALGO == ALGO_BFS) return 1;
-  if (ALGO == ALGO_CC) return 0;
-  return (uint32_t)(((u64)u + v) % 128 + 1);
+  return dycg_ops::ForAlgo<ALGO>::type::TraversalEdgeWeight(u, v);
 }
 
 }  // namespace dycg

@@ -75,3 +75,43 @@ def test_documented_examples_compile_against_the_header(tmp_path):
     src.write_text(shim)
     subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I",
                     os.path.join(ROOT, "include"), str(src)], check=True, capture_output=True)
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
+def test_operator_structs_state_the_python_operators(tmp_path):
+    """include/dycg_operators.h (the kernels' edge-weight rule) and
+    dycgraph_b200/operators.py state the same traits and rules."""
+    import numpy as np
+    from dycgraph_b200 import operators
+    rng = np.random.default_rng(5)
+    pts = [(int(a), int(b)) for a, b in rng.integers(0, 1 << 32, (40, 2))] + [(0, 0), (7, 7), (1, 2)]
+    src = ['#include <cstdio>', '#include "dycg_operators.h"', "using namespace dycg_ops;",
+           "template <class O> void dump(const char *n, unsigned long long u, unsigned long long v) {",
+           '  std::printf("%s %llu %llu %u %u %u %u %d %d %d %d %d\\n", n, u, v,',
+           "    O::TraversalEdgeWeight(u, v), O::DeletionEdgeWeight(u, v),",
+           "    O::GetInitBuffer(u, v), O::GetInitValue(u, v),",
+           "    (int)O::kSupportsGpuDeletionRepair, (int)O::kVertexSeeds,",
+           "    (int)O::kRootedDeletionWitness, (int)O::kSignedResidual,",
+           "    (int)O::IsDeletionDependency(u, v, u % 5, v % 5, v % 5, u, false));", "}",
+           "int main() {"]
+    for u, v in pts:
+        for name in ("SSSP", "BFS", "CC", "PR"):
+            src.append(f'  dump<{name}>("{name}", {u}ull, {v}ull);')
+    src += ["  return 0;", "}"]
+    (tmp_path / "ops.cpp").write_text("\n".join(src) + "\n")
+    exe = tmp_path / "ops"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+                    str(tmp_path / "ops.cpp"), "-o", str(exe)], check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    for line in out.splitlines():
+        name, u, v, tw, dw, ib, iv, gpu, seeds, witness, signed, dep = line.split()
+        u, v = int(u), int(v)
+        O = operators.BY_NAME[name.lower()]
+        assert int(tw) == O.TraversalEdgeWeight(u, v) % (1 << 32), line
+        assert int(dw) == O.DeletionEdgeWeight(u, v) % (1 << 32), line
+        want_ib = O.GetInitBuffer(u, v) if hasattr(O, "GetInitBuffer") else operators.INF
+        assert int(ib) == want_ib and int(iv) == O.GetInitValue(u, v), line
+        assert (int(gpu), int(seeds), int(witness), int(signed)) == (
+            O.kSupportsGpuDeletionRepair, O.kVertexSeeds, O.kRootedDeletionWitness,
+            O.kSignedResidual), line
+        assert bool(int(dep)) == bool(O.IsDeletionDependency(u, v, u % 5, v % 5, v % 5, u, False)), line

@@ -46,11 +46,20 @@ def test_reference_arm_other_ranks_exit_without_work():
     assert not [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
 
 
-def test_reference_arm_declines_forms_without_a_reference_counterpart():
-    p = _run(["--impl", "reference", "--config", "batched", "--steps", "2", "--warmup", "3"])
+def test_reference_arm_declines_the_learned_form():
+    p = _run(["--impl", "reference", "--config", "learned", "--steps", "2", "--warmup", "3"])
     assert p.returncode == 0, p.stderr[-2000:]
     d = json.loads([ln for ln in p.stdout.splitlines() if ln.startswith("{")][-1])
     assert d["impl"] == "reference" and d["unavailable"]
+
+
+def test_reference_arm_batched_form_charges_every_query():
+    p = _run(["--impl", "reference", "--config", "batched", "--scale", "12", "--queries", "8",
+              "--batch-max", "5000", "--steps", "3", "--warmup", "3"])
+    assert p.returncode == 0, p.stderr[-2000:]
+    d = json.loads([ln for ln in p.stdout.splitlines() if ln.startswith("{")][-1])
+    assert d["value"] > 0 and d["metric"].endswith("all 8 queries repaired per snapshot")
+    assert "charged 8 times" in d["cpu_baseline"]["sample"] and d["steps"] == 3
 
 
 class _OracleEngine:

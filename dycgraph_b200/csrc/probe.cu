@@ -19,7 +19,102 @@ __global__ void zero_copy_read_kernel(const uint4 *src, u64 n16, unsigned long l
   if (acc == 0x9E3779B9u) atomicAdd(sink, 1ull);  // keeps the loads alive
 }
 
+// Random host-link transactions: every thread (op_bytes 4, 8 or 16) or every
+// warp (op_bytes 128, one 4-byte word per lane) makes `per` accesses at
+// op_bytes-aligned offsets drawn by a hash, reads or writes; the accesses of
+// one thread are independent, so many are in flight. Offsets are
+// line * op_bytes with line < lines = bytes / op_bytes: always inside the
+// buffer.
+__global__ void random_ops_kernel(uint8_t *base, u64 lines, uint32_t op_bytes, int write,
+                                  uint32_t per, u64 seed, unsigned long long *sink) {
+  const u64 tid = blockIdx.x * (u64)blockDim.x + threadIdx.x;
+  const bool warp_op = op_bytes == 128;
+  const u64 who = warp_op ? tid >> 5 : tid;  // warp-uniform for 128-byte lines
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t acc = 0;
+#pragma unroll 4
+  for (uint32_t i = 0; i < per; i++) {
+    const u64 line = mix64(seed ^ (who * per + i)) % lines;
+    uint8_t *p = base + line * op_bytes;
+    // __ldcv / __stwt: uncached loads and write-through stores, so every
+    // access goes over the link
+    if (warp_op) {
+      unsigned int *q = reinterpret_cast<unsigned int *>(p) + lane;
+      if (write) __stwt(q, i);
+      else acc ^= __ldcv(q);
+    } else if (op_bytes == 16) {
+      uint4 *q = reinterpret_cast<uint4 *>(p);
+      if (write) {
+        __stwt(q, make_uint4(i, i, i, i));
+      } else {
+        const uint4 v = __ldcv(q);
+        acc ^= v.x ^ v.w;
+      }
+    } else if (op_bytes == 8) {
+      uint2 *q = reinterpret_cast<uint2 *>(p);
+      if (write) {
+        __stwt(q, make_uint2(i, i));
+      } else {
+        const uint2 v = __ldcv(q);
+        acc ^= v.x ^ v.y;
+      }
+    } else {
+      unsigned int *q = reinterpret_cast<unsigned int *>(p);
+      if (write) __stwt(q, i);
+      else acc ^= __ldcv(q);
+    }
+  }
+  if (acc == 0x9E3779B9u) atomicAdd(sink, 1ull);  // keeps the loads alive
+}
+
 }  // namespace dycg
+
+extern "C" int dycg_measure_host_random(int device, uint64_t bytes, uint32_t op_bytes, int write,
+                                        uint64_t ops, double *ns_per_op) {
+  if (op_bytes != 4 && op_bytes != 8 && op_bytes != 16 && op_bytes != 128) return DYCG_EINVAL;
+  if (bytes < (1u << 20) || ops == 0 || !ns_per_op) return DYCG_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) return DYCG_ENOGPU;
+  bytes &= ~127ull;
+  void *h = nullptr, *hd = nullptr;
+  unsigned long long *sink = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  int rc = DYCG_OK;
+  if (cudaHostAlloc(&h, bytes, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess ||
+      cudaMalloc(&sink, 8) != cudaSuccess || cudaHostGetDevicePointer(&hd, h, 0) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+    rc = DYCG_ENOMEM;
+  } else {
+    memset(h, 1, bytes);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const uint32_t blocks = (uint32_t)sms * 8, threads = 256;
+    const uint64_t actors =
+        op_bytes == 128 ? (uint64_t)blocks * threads / 32 : (uint64_t)blocks * threads;
+    const uint32_t per = (uint32_t)std::min<uint64_t>((ops + actors - 1) / actors, 1u << 20);
+    const uint64_t lines = bytes / op_bytes;
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {  // the first run warms up
+      float ms = 0;
+      cudaEventRecord(a, s);
+      dycg::random_ops_kernel<<<blocks, threads, 0, s>>>((uint8_t *)hd, lines, op_bytes, write,
+                                                        per, 0x5EEDull + rep, sink);
+      cudaEventRecord(b, s);
+      cudaEventSynchronize(b);
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep) best = std::min(best, ms);
+    }
+    if (cudaGetLastError() != cudaSuccess) rc = DYCG_ECUDA;
+    *ns_per_op = best * 1e6 / ((double)actors * per);
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (s) cudaStreamDestroy(s);
+  if (sink) cudaFree(sink);
+  if (h) cudaFreeHost(h);
+  return rc;
+}
 
 extern "C" int dycg_measure_host_link(int device, uint64_t bytes, double *h2d_gbs,
                                       double *zero_copy_gbs) {

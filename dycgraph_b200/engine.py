@@ -148,6 +148,7 @@ def lib():
         "dycg_stream": (I, [P, ctypes.POINTER(P)]),
         "dycg_measure_host_link": (I, [I, u64, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_double)]),
+        "dycg_measure_host_random": (I, [I, u64, u32, I, u64, ctypes.POINTER(ctypes.c_double)]),
         "dycg_group_updates": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
         "dycg_group_updates_noalloc": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
         "dycg_set_queries": (I, [P, u32p, u32, u32]),
@@ -222,6 +223,17 @@ def measure_host_link(device=0, nbytes=1 << 30):
     if rc:
         raise DycgError(rc, "dycg_measure_host_link")
     return a.value, b.value
+
+
+def measure_host_random(device=0, nbytes=8 << 30, op_bytes=128, write=False, ops=1 << 24):
+    """Device time (ns) per random host-link access of op_bytes over an
+    nbytes pinned buffer (reads, or writes with write=True)."""
+    ns = ctypes.c_double(0)
+    rc = lib().dycg_measure_host_random(device, nbytes, op_bytes, int(write), ops,
+                                        ctypes.byref(ns))
+    if rc:
+        raise DycgError(rc, "dycg_measure_host_random")
+    return ns.value
 
 
 def hash_weight(seed, u, v, wlo=1, whi=64):

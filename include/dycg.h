@@ -286,6 +286,15 @@ uint32_t dycg_hash_weight(uint64_t seed, uint32_t u, uint32_t v, uint32_t wlo,
  * loads (best of 5 each, GB/s). */
 int dycg_measure_host_link(int device, uint64_t bytes, double *h2d_gbs, double *zero_copy_gbs);
 
+/* Measurement helper (no reference counterpart): cost of random host-link
+ * transactions on `device` -- `ops` reads (write = 0) or writes of op_bytes
+ * (4, 8 or 16 per thread, or 128 per warp) at random aligned offsets of a
+ * `bytes`-sized pinned, mapped buffer, many in flight; *ns_per_op is the
+ * device time per access (best of 3 after a warm-up). The bound of kernels
+ * that touch rows of a multi-GB arena at random. */
+int dycg_measure_host_random(int device, uint64_t bytes, uint32_t op_bytes, int write,
+                             uint64_t ops, double *ns_per_op);
+
 /* Replaces GroupedUpdateBatch (include/framework/effective_update_batch.h:
  * 36-207) as a standalone device step. Device pointers throughout; stream is a
  * cudaStream_t (NULL = default stream). Records with an endpoint >=

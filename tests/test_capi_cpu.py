@@ -212,3 +212,20 @@ def test_smoke_fails_loudly_without_a_gpu():
     with pytest.raises(dg.DycgError) as ei:
         __graft_entry__.smoke()
     assert ei.value.code == -8  # DYCG_ENOGPU: no CPU fallback
+
+
+def test_random_link_probe_checks_its_arguments_before_the_device():
+    L = dg.lib()
+    ns = ctypes.c_double(0)
+    for op in (0, 3, 32, 256):
+        assert L.dycg_measure_host_random(0, 1 << 26, op, 0, 1000, ctypes.byref(ns)) == -1
+    assert L.dycg_measure_host_random(0, 1 << 10, 128, 0, 1000, ctypes.byref(ns)) == -1
+    assert L.dycg_measure_host_random(0, 1 << 26, 128, 0, 0, ctypes.byref(ns)) == -1
+    assert L.dycg_measure_host_random(0, 1 << 26, 128, 0, 1000, None) == -1
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return
+    except ImportError:
+        pass
+    assert L.dycg_measure_host_random(0, 1 << 26, 16, 1, 1000, ctypes.byref(ns)) == -8

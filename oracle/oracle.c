@@ -439,6 +439,9 @@ static void push_closure(orc *o, uint64_t head, uint64_t tail) {
   }
 }
 
+/* Initial solve (Engine::Start, include/framework/framework.cuh:1963-2005):
+ * every vertex at its initial value, the seeds (the source, or every vertex
+ * for CC) queued, then the closure. */
 static void solve_from_scratch(orc *o) {
   uint32_t n = o->n;
   uint64_t tail = 0;
@@ -721,6 +724,9 @@ static int insert_phase(orc *o, const orc_edge *adds, size_t na) {
   return 0;
 }
 
+/* Records with an endpoint outside [0, n): the replay tool rejects such
+ * additions and counts them (src/topology_replay.cpp:165-167); here both
+ * phases drop and count them. */
 static uint64_t count_invalid(const orc *o, const orc_edge *e, size_t k) {
   uint64_t c = 0;
   for (size_t i = 0; i < k; i++) c += (e[i].u >= o->n || e[i].v >= o->n);
@@ -925,6 +931,8 @@ int orc_static_sssp(uint32_t n, const uint64_t *off, const uint32_t *dst,
   return 0;
 }
 
+/* FIFO BFS levels from source (the from-scratch oracle of
+ * tests/bfs_dynamic_smoke.py:16-40, its unweighted branch :33-40). */
 int orc_static_bfs(uint32_t n, const uint64_t *off, const uint32_t *dst,
                    uint32_t source, uint32_t *level) {
   for (uint32_t v = 0; v < n; v++) level[v] = ORC_INF;
@@ -1034,6 +1042,8 @@ uint64_t orc_bellman_check(uint32_t n, const uint64_t *off, const uint32_t *dst,
   return relax;
 }
 
+/* DistanceChecksum (samples/hybrid_sssp/hybrid_sssp.cu:335-347): FNV-style
+ * fold over the reachable vertices. */
 uint64_t orc_distance_checksum(const uint32_t *values, uint32_t n) {
   uint64_t c = 1469598103934665603ull;
   for (uint32_t v = 0; v < n; v++) {

@@ -26,6 +26,11 @@ What it records (all small JSON, committed):
                           graph, deletions, affected set, repaired distances and
                           the verifier's report, plus one planted mistake that
                           it must catch.
+  replay_random.json   -- a seeded random multigraph and update stream (repeated
+                          pairs, absent deletions, self-loops) replayed by the
+                          reference's topology_replay (per-source degrees and
+                          multiset hashes) and by its chunk store through
+                          chunk_store_replay --pageable (per-batch counts).
   group_updates.json   -- seeded update batches grouped by the reference's own
                           GroupedUpdateBatch (effective_update_batch.h, driven
                           by oracle/ref_group_updates.cpp, built by
@@ -346,6 +351,58 @@ def i16_case(ref):
             "origin": "src/i16_repair_oracle.cpp + include/framework/i16_repair_snapshot.h"}
 
 
+def replay_random_case(ref):
+    import tempfile
+    subprocess.run(["make", "-s", "-C", str(REPO / "oracle"), f"REF={ref}"], check=True)
+    rng = random.Random(20261204)
+    n = 400
+    graph = [[rng.randrange(n), rng.randrange(n)] for _ in range(2500)]
+    graph += graph[:200]                                   # parallel occurrences
+    graph += [[v, v] for v in range(0, n, 97)]             # self-loops
+    live = [tuple(e) for e in graph]
+    updates, sizes = [], []
+    for _ in range(6):
+        dels = [list(live[rng.randrange(len(live))]) for _ in range(60)]
+        dels += dels[:5]                                       # second request, same pair
+        dels += [[rng.randrange(n), rng.randrange(n)] for _ in range(10)]  # mostly absent
+        adds = [[rng.randrange(n), rng.randrange(n)] for _ in range(60)]
+        adds += [list(live[rng.randrange(len(live))]) for _ in range(10)]  # parallel
+        recs = [("d", u, v) for u, v in dels] + [("a", u, v) for u, v in adds]
+        rng.shuffle(recs)                                      # the Loader splits by type
+        updates += recs
+        sizes.append([len(adds), len(dels)])
+        live += [tuple(e) for e in adds]
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        (td / "g.txt").write_text("".join(f"{u} {v}\n" for u, v in graph))
+        (td / "u.txt").write_text("".join(f"{t} {u} {v} 1\n" for t, u, v in updates))
+        (td / "s.txt").write_text("".join(f"{a} {d}\n" for a, d in sizes))
+        args = ["--graph", str(td / "g.txt"), "--updates", str(td / "u.txt"),
+                "--batch-sizes", str(td / "s.txt")]
+        topo = subprocess.run([str(REPO / "oracle/_ref/topology_replay"), *args,
+                               "--dump-sources"], check=True, capture_output=True,
+                              text=True).stdout
+        chunk = subprocess.run([str(REPO / "oracle/_ref/chunk_store_replay"), *args,
+                                "--pageable"], check=True, capture_output=True, text=True).stdout
+
+    def rows(text, tag, keys=None):
+        out = []
+        for line in text.splitlines():
+            if line.startswith(tag):
+                d = dict((k, int(v)) for k, v in re.findall(r"(\w+)=(\d+)(?=\s|$)", line))
+                out.append({k: d[k] for k in keys} if keys else d)
+        return out
+    count_keys = ["batch", "touched_sources", "changed_sources", "missing_deletes",
+                  "invalid_additions", "graph_edges"]
+    return {"graph": graph, "updates": [list(r) for r in updates], "sizes": sizes,
+            "replay_batches": rows(topo, "[TOPOLOGY-REPLAY-BATCH]"),
+            "replay_sources": rows(topo, "[TOPOLOGY-REPLAY-SOURCE]"),
+            "chunk_store_batches": rows(chunk, "[CHUNK-STORE-BATCH]", count_keys),
+            "origin": "src/topology_replay.cpp --dump-sources and src/chunk_store_replay.cpp "
+                      "--pageable (include/framework/source_local_chunk_store.h) on a seeded "
+                      "stream made by tests/golden/make_golden.py"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("DYCG_REFERENCE", "/root/reference"))
@@ -357,7 +414,7 @@ def main():
     makers = {"smoke_bfs_sssp.json": bfs_sssp_case, "smoke_cc.json": cc_case,
               "smoke_pr.json": pr_case, "pr_probe.json": pr_probe_case,
               "topology_replay.json": topology_case, "group_updates.json": group_case,
-              "i16_repair.json": i16_case}
+              "i16_repair.json": i16_case, "replay_random.json": replay_random_case}
     cases = {name: make(ref) for name, make in makers.items()
              if args.only is None or name in args.only}
     for name, data in cases.items():

@@ -188,3 +188,39 @@ def test_deletion_repair_matches_the_reference_verifier():
             assert [int(vals[x]) for x in s["affected"]] == s["after"]
             if "planted_report" in s:
                 assert s["planted_report"]["distance_mismatches"] == 1
+
+
+def test_random_multigraph_stream_matches_the_reference_chunk_store():
+    """A seeded multigraph with parallel edges and self-loops, and an update
+    stream with repeated, absent and parallel records, replayed by the oracle:
+    per batch the same missing deletions and edge count as the reference's
+    replay model and its chunk store, the same changed-source count as the
+    chunk store (a source that lost or gained an occurrence,
+    source_local_chunk_store.h:291-311), and per touched source the same degree
+    and multiset hash as the replay model's dump. (The replay model counts a
+    source as changed only when its row's digest differs, so a deletion and
+    re-insertion that restore the same sequence counts there as unchanged:
+    the two reference tools differ by one source in two of this stream's six
+    batches.)"""
+    case = cases.load("replay_random.json")
+    n = 1 + max(max(max(e) for e in case["graph"]),
+                max(max(u, v) for _, u, v in case["updates"]))
+    off, dst, _ = cases.csr(n, case["graph"])
+    orc = oracle.Oracle(oracle.SSSP, n, off, dst)
+    batches = cases.replay_batches(case["updates"], case["sizes"])
+    assert len(batches) == len(case["replay_batches"]) == len(case["chunk_store_batches"]) == 6
+    sources = {}
+    for s in case["replay_sources"]:
+        sources.setdefault(s["batch"], []).append(s)
+    for bi, (dels, adds) in enumerate(batches):
+        orc.mutate(cases.triples(dels), cases.triples(adds))
+        st = orc.stats()
+        for want in (case["replay_batches"][bi], case["chunk_store_batches"][bi]):
+            assert st["missing_deletes"] == want["missing_deletes"], (bi, want)
+            assert orc.live_edges() == want["graph_edges"], (bi, want)
+        assert st["changed_sources"] == case["chunk_store_batches"][bi]["changed_sources"], bi
+        assert st["changed_sources"] - case["replay_batches"][bi]["changed_sources"] in (0, 1)
+        assert len(sources[bi]) == case["replay_batches"][bi]["touched_sources"]
+        for s in sources[bi]:
+            assert orc.row_degree(s["source"]) == s["after_degree"]
+            assert orc.row_multiset_hash(s["source"]) == s["multiset_hash"]

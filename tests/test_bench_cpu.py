@@ -186,3 +186,27 @@ def test_rmat_snapshots_are_disjoint_live_deletions_and_rmat_insertions():
         assert len(d) == nd and set(keys) <= live and len(set(keys)) == nd and not set(keys) & seen
         seen |= set(keys)
         assert (a == adds_all[i * na:(i + 1) * na]).all()
+
+
+def test_clock_samples_inside_the_timed_region_give_median_and_reasons():
+    import bench
+
+    class FakeProc:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout=None):
+            return 0
+
+    c = bench.Clocks(0)
+    c.proc = FakeProc()
+    row = "0, {sm}, 1965, 900.0, 0x0, {hw}, Not Active, Not Active, {cap}"
+    c.lines = [(0.5, row.format(sm=1200, hw="Active", cap="Not Active")),     # before the window
+               (1.0, row.format(sm=1965, hw="Not Active", cap="Not Active")),
+               (1.5, row.format(sm=1950, hw="Not Active", cap="Active")),
+               (2.0, row.format(sm=1965, hw="Not Active", cap="Not Active")),
+               (3.5, row.format(sm=300, hw="Active", cap="Not Active"))]     # after it
+    c.mark(1.0, 2.0)
+    out = c.stop()
+    assert out["sm_mhz"] == 1965.0 and out["sm_max_mhz"] == 1965.0
+    assert out["reasons"] == ["sw_power_cap"] and out["samples_inside_timed_region"] == 3

@@ -2,10 +2,11 @@
 
 oracle/Makefile compiles a few of the reference's CPU tools into oracle/_ref/
 when the reference checkout is present (the update grouping driver, the
-topology replay model, the chunk store replay). Where they are built, these
-tests draw fresh seeded batches and streams and compare the grouping checker
-and the oracle's mutation with the reference's output; elsewhere they skip
-(the committed fixtures in tests/golden/ carry a fixed sample of the same).
+topology replay model, the chunk store replay, the deletion-repair verifier).
+Where they are built, these tests draw fresh seeded batches, streams and
+deletion phases and compare the grouping checker, the oracle's mutation and
+its deletion repair with the reference's output; elsewhere they skip (the
+committed fixtures in tests/golden/ carry a fixed sample of the same).
 """
 import collections
 import os
@@ -119,3 +120,60 @@ def test_oracle_mutation_matches_reference_chunk_store_live(seed, tmp_path):
         for s in (s for s in src if s["batch"] == bi):
             assert orc.row_degree(s["source"]) == s["after_degree"]
             assert orc.row_multiset_hash(s["source"]) == s["multiset_hash"]
+
+
+def _make_golden():
+    import importlib.util
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "make_golden.py")
+    spec = importlib.util.spec_from_file_location("make_golden", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@pytest.mark.parametrize("seed", range(3))
+def test_deletion_repair_passes_reference_verifier_live(seed, tmp_path):
+    """Fresh deletion phases repaired by the oracle, each checked by the
+    reference's CPU verifier (Dijkstra over the affected subgraph seeded from
+    its boundary): no distance mismatch, no change outside the affected set."""
+    import json
+    tool = _tool("i16_repair_oracle")
+    mg = _make_golden()
+    rng = np.random.default_rng(500 + seed)
+    n = int(rng.integers(50, 400))
+    m = int(rng.integers(3, 9)) * n
+    u, v = rng.integers(0, n, m), rng.integers(0, n, m)
+    off, dst, _ = oracle.csr_from_edges(n, [(int(a), int(b), 1) for a, b in zip(u, v) if a != b])
+    orc = oracle.Oracle(oracle.SSSP, n, off, dst, source=0)
+    orc.init()
+    for b in range(3):
+        vals0, par0 = orc.values()
+        o, d, _ = orc.csr()
+        src = np.repeat(np.arange(n), np.diff(o.astype(np.int64)))
+        pick = rng.choice(len(d), size=min(len(d), 30), replace=False)
+        dels = [(int(src[i]), int(d[i]), 1) for i in pick]
+        aff = mg.i16_affected(n, par0, dels, 0)
+        orc.delete_edges(dels)
+        assert orc.stats()["affected"] == len(aff)
+        vals1, par1 = orc.values()
+        o, d, _ = orc.csr()
+        src = np.repeat(np.arange(n), np.diff(o.astype(np.int64)))
+        idx = {x: i for i, x in enumerate(aff)}
+        inc = [[] for _ in aff]
+        for s_, t_ in zip(src.tolist(), d.tolist()):
+            if t_ in idx:
+                inc[idx[t_]].append(s_)
+        inc_off = np.zeros(len(aff) + 1, np.uint64)
+        inc_off[1:] = np.cumsum([len(x) for x in inc])
+        flat = [s_ for row in inc for s_ in row]
+        listed = sorted(set(aff) | set(flat))
+        inf = oracle.INF
+        before = [(x, inf, inf, inf) if x in idx else (x, int(vals0[x]), int(vals0[x]), int(par0[x]))
+                  for x in listed]
+        after = [(x, int(vals1[x]), int(vals1[x]), int(par1[x])) for x in listed]
+        mg.i16_snapshot(tmp_path / "s.bin", b, 0, n, aff, inc_off, flat, before, after)
+        r = subprocess.run([tool, str(tmp_path / "s.bin"), str(tmp_path / "r.json")],
+                           capture_output=True, text=True)
+        rep = json.loads(r.stdout)
+        assert r.returncode == 0 and rep["distance_mismatches"] == 0, rep
+        assert rep["external_state_changes"] == 0

@@ -50,7 +50,13 @@ extern "C" {
 /* ---- edge weights (SSSP) ----------------------------------------------- */
 /* HASH128: w(u,v) = (u+v) % 128 + 1, the reference's TraversalEdgeWeight
  * (include/framework/variants/api.cuh:26-28); file weights are ignored.
- * STORED: every adjacency slot carries the weight given at load/insert time. */
+ * STORED: every adjacency slot carries the weight given at load/insert time.
+ *   A deletion record matches an occurrence by (u, v) alone, as in the
+ *   reference; its w is ignored. When parallel occurrences of (u, v) carry
+ *   different weights, which one a deletion removes is not specified, so
+ *   results can depend on it. Giving every occurrence of (u, v) the same
+ *   weight (the loaders and the benchmark hash it from (seed, u, v)) keeps
+ *   results independent of it. */
 #define DYCG_WEIGHT_HASH128 0
 #define DYCG_WEIGHT_STORED 1
 

@@ -947,9 +947,14 @@ def run_batched(args):
                    "parallelism": f"replicas x{world}", "load_s": round(t_load, 2),
                    "static_solve_s": round(t_init, 2)},
         "clocks": clk,
+        # e2e runs on the E snapshots drawn after the timed ones (other
+        # log-uniform sizes): compare per-update rates with their mean sizes
         "e2e": {"value": round(e2e_value, 1) if e2e_value else None, "unit": UNIT,
                 "h2d_bytes_per_step": int(e2e_updates * 12 / max(E, 1)),
-                "d2h_bytes_per_step": 256, "steps": E},
+                "d2h_bytes_per_step": 256, "steps": E,
+                "mean_updates_per_step": int(e2e_updates / max(E, 1)),
+                "timed_mean_updates_per_step": int(timed_updates / max(K, 1)),
+                "snapshots": "the e2e steps' own snapshots, drawn after the timed ones"},
         "gpu_launches": launches,
         "roofline": roofline,
         "per_step": per_step,

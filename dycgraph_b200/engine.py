@@ -183,6 +183,8 @@ def edges_array(edges):
         arr = np.ascontiguousarray(edges, dtype=np.uint32)
         if arr.ndim == 1:
             arr = arr.reshape(-1, 3)
+        if arr.ndim != 2 or arr.shape[1] not in (2, 3):
+            raise ValueError(f"edge records must be (k, 2) or (k, 3), not {edges.shape}")
         if arr.shape[1] == 2:
             arr = np.concatenate([arr, np.ones((arr.shape[0], 1), np.uint32)], axis=1)
         return np.ascontiguousarray(arr)

@@ -229,3 +229,17 @@ def test_random_link_probe_checks_its_arguments_before_the_device():
     except ImportError:
         pass
     assert L.dycg_measure_host_random(0, 1 << 26, 16, 1, 1000, ctypes.byref(ns)) == -8
+
+
+def test_edge_records_reach_the_abi_as_12_byte_rows():
+    from dycgraph_b200.engine import edges_array
+    assert edges_array([]).shape == (0, 3)
+    assert edges_array([(1, 2), (3, 4, 5)]).tolist() == [[1, 2, 1], [3, 4, 5]]
+    assert edges_array(np.array([[1, 2], [3, 4]])).tolist() == [[1, 2, 1], [3, 4, 1]]
+    assert edges_array(np.arange(6)).tolist() == [[0, 1, 2], [3, 4, 5]]
+    a = edges_array(np.array([[7, 8, 9]], np.int64))
+    assert a.dtype == np.uint32 and a.flags["C_CONTIGUOUS"] and a.strides == (12, 4)
+    with pytest.raises(ValueError):
+        edges_array(np.zeros((2, 4)))
+    with pytest.raises(ValueError):
+        edges_array(np.zeros((2, 3, 1)))

@@ -293,6 +293,9 @@ void Engine::load_csr(uint32_t n, const uint64_t *off, const uint32_t *dst, cons
   if (loaded_) throw Error(DYCG_ESTATE, "graph already loaded");
   if (n == 0 || n >= 0x7FFFFFFFu) throw Error(DYCG_EINVAL, "vertex count out of range");
   if (!off || (!dst && off[n] != 0)) throw Error(DYCG_EINVAL, "null CSR array");
+  if (off[0] != 0) throw Error(DYCG_EINVAL, "CSR offsets must start at 0");
+  for (uint32_t v = 0; v < n; v++)
+    if (off[v] > off[v + 1]) throw Error(DYCG_EINVAL, "CSR offsets must not decrease");
   n_ = n;
   const u64 m = off[n];
   for (u64 e = 0; e < m; e++)

@@ -192,6 +192,20 @@ def edges_array(edges):
     return np.asarray(rows, dtype=np.uint32).reshape(-1, 3)
 
 
+def csr_arrays(n, offsets, dst, w=None):
+    """CSR arrays as the C ABI reads them (offsets u64 [n+1], dst/w u32 [m]),
+    with the lengths the ABI cannot check itself."""
+    off = np.ascontiguousarray(offsets, np.uint64)
+    d = np.ascontiguousarray(dst, np.uint32)
+    ww = None if w is None else np.ascontiguousarray(w, np.uint32)
+    if off.ndim != 1 or off.shape[0] != n + 1:
+        raise ValueError(f"offsets must have n + 1 = {n + 1} entries, not {off.shape}")
+    m = int(off[-1]) if n >= 0 and off.shape[0] else 0
+    if d.shape[0] < m or (ww is not None and ww.shape[0] < m):
+        raise ValueError(f"dst/w hold fewer than offsets[n] = {m} entries")
+    return off, d, ww
+
+
 def gen_rmat_edges(scale, count, seed, first=0, a=0.57, b=0.19, c=0.19, wlo=1, whi=64):
     out = np.empty((count, 3), np.uint32)
     rc = lib().dycg_gen_rmat_edges(scale, a, b, c, seed, first, count, wlo, whi,
@@ -312,9 +326,7 @@ class Engine:
 
     # -- loading (Engine::LoadGraph) ------------------------------------------
     def load_csr(self, n, offsets, dst, w=None):
-        off = np.ascontiguousarray(offsets, np.uint64)
-        d = np.ascontiguousarray(dst, np.uint32)
-        ww = None if w is None else np.ascontiguousarray(w, np.uint32)
+        off, d, ww = csr_arrays(n, offsets, dst, w)
         self._check(lib().dycg_load_graph_csr(self._h, n, _ptr(off, ctypes.c_uint64),
                                               _ptr(d, ctypes.c_uint32), _ptr(ww, ctypes.c_uint32)),
                     "load_csr")

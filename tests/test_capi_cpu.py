@@ -243,3 +243,15 @@ def test_edge_records_reach_the_abi_as_12_byte_rows():
         edges_array(np.zeros((2, 4)))
     with pytest.raises(ValueError):
         edges_array(np.zeros((2, 3, 1)))
+
+
+def test_csr_arrays_are_length_checked_before_the_abi():
+    from dycgraph_b200.engine import csr_arrays
+    off, d, w = csr_arrays(3, [0, 2, 2, 3], [1, 2, 0], [5, 6, 7])
+    assert off.dtype == np.uint64 and d.dtype == np.uint32 and w.dtype == np.uint32
+    with pytest.raises(ValueError):
+        csr_arrays(3, [0, 2, 3], [1, 2, 0])          # offsets too short
+    with pytest.raises(ValueError):
+        csr_arrays(3, [0, 2, 2, 3], [1, 2])          # dst too short
+    with pytest.raises(ValueError):
+        csr_arrays(3, [0, 2, 2, 3], [1, 2, 0], [5])  # weights too short

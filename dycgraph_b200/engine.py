@@ -470,13 +470,14 @@ class Engine:
 
     def policy_set_params(self, params):
         p = np.ascontiguousarray(params, dtype=np.float32)
-        assert p.shape == (POLICY_PARAMS,)
+        if p.shape != (POLICY_PARAMS,):
+            raise ValueError(f"expected {POLICY_PARAMS} parameters, got shape {p.shape}")
         self._check(lib().dycg_policy_set_params(self._h, _ptr(p, ctypes.c_float)),
                     "policy_set_params")
 
     def sample_row_edges(self, sources, seed):
         """One live out-edge per source; rows (INF, INF, 0) for empty rows."""
-        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        src = np.ascontiguousarray(np.ravel(sources), dtype=np.uint32)
         out = np.empty((len(src), 3), np.uint32)
         self._check(lib().dycg_sample_row_edges(self._h, _ptr(src, ctypes.c_uint32), len(src), seed,
                                                 out.ctypes.data_as(ctypes.POINTER(Edge))),
@@ -601,7 +602,7 @@ class Engine:
         """Keep the results of every source in `sources` (SSSP/BFS, up to 256):
         "batched" repairs all of them in one launch per snapshot, "per_query"
         launches the single-source repair once per query. Call before start()."""
-        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        src = np.ascontiguousarray(np.ravel(sources), dtype=np.uint32)
         self._check(lib().dycg_set_queries(self._h, _ptr(src, ctypes.c_uint32), len(src),
                                            self.QUERY_MODES[mode]), "set_queries")
         self.queries = len(src)

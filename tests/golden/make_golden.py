@@ -407,7 +407,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get("DYCG_REFERENCE", "/root/reference"))
     ap.add_argument("--only", nargs="*", default=None, help="regenerate only these fixtures")
+    ap.add_argument("--out", default=None, help="write here instead of tests/golden/")
     args = ap.parse_args()
+    out_dir = Path(args.out) if args.out else HERE
     ref = Path(args.ref)
     if not (ref / "tests/bfs_dynamic_smoke.py").exists():
         sys.exit(f"reference checkout not found at {ref}")
@@ -418,8 +420,8 @@ def main():
     cases = {name: make(ref) for name, make in makers.items()
              if args.only is None or name in args.only}
     for name, data in cases.items():
-        (HERE / name).write_text(json.dumps(data, separators=(",", ":")) + "\n")
-        print(name, (HERE / name).stat().st_size, "bytes")
+        (out_dir / name).write_text(json.dumps(data, separators=(",", ":")) + "\n")
+        print(name, (out_dir / name).stat().st_size, "bytes")
 
 
 if __name__ == "__main__":

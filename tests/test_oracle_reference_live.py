@@ -177,3 +177,20 @@ def test_deletion_repair_passes_reference_verifier_live(seed, tmp_path):
         rep = json.loads(r.stdout)
         assert r.returncode == 0 and rep["distance_mismatches"] == 0, rep
         assert rep["external_state_changes"] == 0
+
+
+def test_reference_tool_fixtures_regenerate_identically(tmp_path):
+    """The committed fixtures made with the reference's own tools come back
+    byte for byte when regenerated from the reference checkout."""
+    import sys
+    ref = os.environ.get("DYCG_REFERENCE", "/root/reference")
+    if not os.path.exists(os.path.join(ref, "tests", "bfs_dynamic_smoke.py")):
+        pytest.skip("no reference checkout here")
+    for name in ("group_updates", "i16_repair_oracle", "chunk_store_replay"):
+        _tool(name)
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    names = ["group_updates.json", "i16_repair.json", "replay_random.json"]
+    subprocess.run([sys.executable, os.path.join(golden, "make_golden.py"), "--ref", ref,
+                    "--out", str(tmp_path), "--only", *names], check=True, capture_output=True)
+    for name in names:
+        assert (tmp_path / name).read_bytes() == open(os.path.join(golden, name), "rb").read(), name

@@ -33,22 +33,22 @@ __global__ void group_heads_kernel(const u64 *k, uint32_t cnt, uint32_t *head) {
     head[i] = k[i] != KEY_INF && (i == 0 || k[i - 1] != k[i]);
 }
 
-__global__ void group_emit_kernel(const u64 *k, const uint32_t *head, const uint32_t *pos,
-                                  uint32_t cnt, uint32_t *out_uv, uint32_t *out_mult,
-                                  const uint32_t *seg_ends, uint32_t nseg, uint32_t *seg_counts,
-                                  uint32_t *counts) {
+// Run heads in key order: the run number o of head i is pos[i]; record its
+// first index, emit its (u, v) and bin it into its segment.
+__global__ void group_starts_kernel(const u64 *k, const uint32_t *head, const uint32_t *pos,
+                                    uint32_t cnt, uint32_t *start, uint32_t *out_uv,
+                                    const uint32_t *seg_ends, uint32_t nseg,
+                                    uint32_t *seg_counts, uint32_t *counts) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
        i += gridDim.x * blockDim.x) {
     if (i == cnt - 1) counts[0] = pos[i] + head[i];
     if (!head[i]) continue;
     const u64 key = k[i];
-    uint32_t j = i + 1;
-    while (j < cnt && k[j] == key) j++;
     const uint32_t o = pos[i];
     const uint32_t u = (uint32_t)(key >> 32);
+    start[o] = i;
     out_uv[2 * o] = u;
     out_uv[2 * o + 1] = (uint32_t)key;
-    out_mult[o] = j - i;
     if (seg_counts && nseg) {
       uint32_t lo = 0, hi = nseg;  // first segment whose end is > u
       while (lo < hi) {
@@ -57,6 +57,21 @@ __global__ void group_emit_kernel(const u64 *k, const uint32_t *head, const uint
       }
       if (lo < nseg) atomicAdd(seg_counts + lo, 1u);
     }
+  }
+}
+
+// Multiplicity of run o = distance to the next run's first index; the last
+// run ends at the number of valid keys (invalid ones sort last as KEY_INF).
+// One thread per run whatever its length, so a batch of one repeated record
+// costs the same as a batch of distinct ones.
+__global__ void group_mult_kernel(const uint32_t *start, uint32_t cnt, const uint32_t *counts,
+                                  uint32_t *out_mult) {
+  const uint32_t runs = counts[0];
+  const uint32_t valid = cnt - counts[1];
+  for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < runs;
+       o += gridDim.x * blockDim.x) {
+    const uint32_t end = o + 1 < runs ? start[o + 1] : valid;
+    out_mult[o] = end - start[o];
   }
 }
 
@@ -95,8 +110,9 @@ cudaError_t group_run(const dycg_edge *d_records, uint32_t n, uint32_t num_verti
   tb = S.temp_bytes;
   e = cub::DeviceScan::ExclusiveSum(S.temp, tb, S.head, S.pos, (int)n, s);
   if (e != cudaSuccess) return e;
-  group_emit_kernel<<<grid_for(n), BLOCK, 0, s>>>(S.keys_b, S.head, S.pos, n, out_uv, out_mult,
-                                                  seg_ends, nseg, seg_counts, counts);
+  group_starts_kernel<<<grid_for(n), BLOCK, 0, s>>>(S.keys_b, S.head, S.pos, n, S.start, out_uv,
+                                                    seg_ends, nseg, seg_counts, counts);
+  group_mult_kernel<<<grid_for(n), BLOCK, 0, s>>>(S.start, n, counts, out_mult);
   return cudaGetLastError();
 }
 

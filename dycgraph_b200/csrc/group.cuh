@@ -8,6 +8,7 @@ namespace dycg {
 struct GroupScratch {
   u64 *keys_a, *keys_b;  // unsorted / sorted (row << 32 | neighbour) keys
   uint32_t *head, *pos;  // run heads and their exclusive prefix
+  uint32_t *start;       // first sorted index of every run
   void *temp;            // CUB temporary storage
   size_t temp_bytes;
 };
@@ -24,12 +25,14 @@ inline void group_carve(void *base, uint32_t m, GroupScratch &S) {
   p += up((size_t)m * 4);
   S.pos = (uint32_t *)p;
   p += up((size_t)m * 4);
+  S.start = (uint32_t *)p;
+  p += up((size_t)m * 4);
   S.temp = p;
 }
 
 inline size_t group_scratch_bytes(uint32_t m, size_t temp_bytes) {
   auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
-  return 256 + 2 * up((size_t)m * 8) + 2 * up((size_t)m * 4) + temp_bytes;
+  return 256 + 2 * up((size_t)m * 8) + 3 * up((size_t)m * 4) + temp_bytes;
 }
 
 size_t group_temp_bytes(uint32_t n);

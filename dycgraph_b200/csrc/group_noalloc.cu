@@ -15,10 +15,12 @@
 // streams without ordering, or different host threads) race and must not be
 // issued concurrently; calls ordered on one stream are safe.
 //
-// The first call on a device resolves the array's device address with
-// cudaGetSymbolAddress (the host-side name of a __device__ array is only a
-// stand-in and must never be handed to a kernel); that first call should be
-// made before any stream capture begins.
+// Set-up: the host-side name of a __device__ array is only a stand-in and must
+// never be handed to a kernel, so a call resolves the array's device address
+// with cudaGetSymbolAddress on the current device. The first call on a device
+// does this set-up and should come before any stream capture. Later calls
+// resolve it again whenever their stream is not capturing, so the address
+// stays valid after a device reset has reloaded the module.
 #include <cstdio>
 #include <mutex>
 
@@ -31,12 +33,13 @@ constexpr uint32_t kMax = DYCG_GROUP_NOALLOC_MAX_RECORDS;
 constexpr size_t kTemp = 4u << 20;  // CUB sort/scan temporary storage
 constexpr size_t kUp8 = ((size_t)kMax * 8 + 255) & ~(size_t)255;
 constexpr size_t kUp4 = ((size_t)kMax * 4 + 255) & ~(size_t)255;
-constexpr size_t kBytes = 256 + 2 * kUp8 + 2 * kUp4 + kTemp;
+constexpr size_t kBytes = 256 + 2 * kUp8 + 3 * kUp4 + kTemp;
 
 __device__ __align__(256) unsigned char g_group_scratch[kBytes];
 
 std::mutex g_mu;
 void *g_addr[128] = {};  // device address of g_group_scratch, per device ordinal
+int g_temp_ok = -1;      // CUB's storage need for kMax records fits kTemp (checked once)
 
 }  // namespace
 
@@ -57,20 +60,38 @@ extern "C" int dycg_group_updates_noalloc(const dycg_edge *d_records, size_t n,
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return DYCG_ENOGPU;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing((cudaStream_t)stream, &cap) != cudaSuccess) return DYCG_ECUDA;
   void *base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
+    if (g_temp_ok < 0) {
+      // a build whose CUB needs more temporary storage than the array holds is
+      // a configuration error, not an oversized batch
+      g_temp_ok = dycg::group_temp_bytes(kMax) <= kTemp ? 1 : 0;
+      if (!g_temp_ok)
+        std::fprintf(stderr,
+                     "dycg_group_updates_noalloc: CUB needs %zu bytes of temporary storage "
+                     "for %u records, more than the fixed %zu (kTemp); rebuild with a larger "
+                     "kTemp\n",
+                     dycg::group_temp_bytes(kMax), kMax, kTemp);
+    }
+    if (!g_temp_ok) return DYCG_ESTATE;
+    if (cap == cudaStreamCaptureStatusNone) {
       void *p = nullptr;
       const cudaError_t e = cudaGetSymbolAddress(&p, g_group_scratch);
       if (e != cudaSuccess || !p) return DYCG_ECUDA;
       g_addr[dev] = p;
+    } else if (!g_addr[dev]) {
+      std::fprintf(stderr,
+                   "dycg_group_updates_noalloc: the first call on a device must not be "
+                   "captured (the scratch address is resolved outside capture)\n");
+      return DYCG_ESTATE;
     }
     base = g_addr[dev];
   }
   dycg::GroupScratch S{};
   S.temp_bytes = kTemp;
-  if (dycg::group_temp_bytes(kMax) > kTemp) return DYCG_ECAPACITY;  // size query only
   dycg::group_carve(base, kMax, S);
   const cudaError_t e =
       dycg::group_run(d_records, (uint32_t)n, num_vertices, d_segment_ends, num_segments,

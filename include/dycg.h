@@ -322,11 +322,12 @@ int dycg_group_updates(const dycg_edge *d_records, size_t n, uint32_t num_vertic
  * synchronise the device, processes whose device memory is held by another
  * allocator, hosts that must not own GPU allocations). Its scratch is a fixed
  * file-scope device array sized for DYCG_GROUP_NOALLOC_MAX_RECORDS records
- * (about 10 MiB, held on every GPU that loads the library until exit); larger
+ * (about 11 MiB, held on every GPU that loads the library until exit); larger
  * batches return DYCG_ECAPACITY. All calls share that array: calls that
  * overlap on the GPU race, calls ordered on one stream are safe. The first
  * call on a device looks up the array's device address and should come
- * before any stream capture. */
+ * before any stream capture; later calls whose stream is not capturing look
+ * it up again, so a device reset leaves no stale address behind. */
 #define DYCG_GROUP_NOALLOC_MAX_RECORDS 262144u
 int dycg_group_updates_noalloc(const dycg_edge *d_records, size_t n, uint32_t num_vertices,
                                const uint32_t *d_segment_ends, uint32_t num_segments,

@@ -51,3 +51,30 @@ def test_group_updates_matches_numpy(n):
     uk, cnt, rbad, rseg = group_ref(rec, nv, ends)
     assert (keys == uk).all() and (mult == cnt).all()
     assert bad == rbad and (seg == rseg).all()
+
+
+def _hub_records(n, nv, seed):
+    """One hub row: every record has the same source and one of three
+    destinations (runs of ~n/3 copies), plus a few out-of-range records."""
+    rng = np.random.default_rng(seed)
+    rec = np.empty((n, 3), np.uint32)
+    rec[:, 0] = 17
+    rec[:, 1] = rng.choice(np.array([5, 6, nv - 1], np.uint32), size=n)
+    rec[:, 2] = 1
+    rec[rng.integers(0, n, size=8), 0] = nv + 3
+    return rec
+
+
+@pytest.mark.parametrize("fn", ["dycg_group_updates", "dycg_group_updates_noalloc"])
+def test_group_updates_single_hub_batch(fn):
+    """A batch of 262,144 records for one hub row: run lengths come from the
+    run starts, so each run of ~87K copies costs one thread, not a walk."""
+    nv = 5000
+    rec = _hub_records(262_144, nv, 11)
+    ends = np.array([16, 18, nv], np.uint32)
+    rc, keys, mult, bad, seg = run_group(getattr(dg.lib(), fn), rec, nv, ends)
+    assert rc == 0
+    uk, cnt, rbad, rseg = group_ref(rec, nv, ends)
+    assert (keys == uk).all() and (mult == cnt).all()
+    assert bad == rbad and (seg == rseg).all()
+    assert int(mult.sum()) == 262_144 - rbad

@@ -59,6 +59,38 @@ def test_noalloc_matches_allocating_entry_point_on_calls_in_a_row():
             assert np.array_equal(a, b)
 
 
+def _numpy_group(rec, nv, ends):
+    ok = (rec[:, 0] < nv) & (rec[:, 1] < nv)
+    keys = rec[ok, 0].astype(np.uint64) << np.uint64(32) | rec[ok, 1].astype(np.uint64)
+    uk, cnt = np.unique(keys, return_counts=True)
+    u = (uk >> np.uint64(32)).astype(np.uint32)
+    seg = np.bincount(np.searchsorted(ends, u, side="right"), minlength=len(ends))[:len(ends)]
+    uv = np.stack([u, (uk & np.uint64(0xFFFFFFFF)).astype(np.uint32)], 1).reshape(-1)
+    return uv, cnt.astype(np.uint32), int((~ok).sum()), seg.astype(np.uint32)
+
+
+def test_noalloc_full_capacity_single_hub_matches_numpy():
+    """Every record of a full-capacity batch in one hub row (one source, three
+    destinations, so three runs of ~87K copies), all in one segment: the
+    multiplicities and segment counts must be numpy's, on two calls in a row."""
+    L = dg.lib()
+    nv = 70_000
+    rng = np.random.default_rng(5)
+    rec = np.empty((MAX_RECORDS, 3), np.uint32)
+    rec[:, 0] = 40_000
+    rec[:, 1] = rng.choice(np.array([3, 39_999, 69_999], np.uint32), size=MAX_RECORDS)
+    rec[:, 2] = 7
+    ends = np.array([10_000, 30_000, 50_000, nv], np.uint32)
+    uv, mult, bad, seg = _numpy_group(rec, nv, ends)
+    for _ in range(2):
+        rc, guv, gmult, cnt, gseg = _group(L.dycg_group_updates_noalloc, rec, nv, ends)
+        assert rc == 0
+        assert int(cnt[0]) == len(mult) and int(cnt[1]) == bad
+        assert np.array_equal(guv.astype(np.uint32), uv)
+        assert np.array_equal(gmult.astype(np.uint32), mult)
+        assert np.array_equal(gseg.astype(np.uint32), seg)
+
+
 def test_noalloc_rejects_batches_above_capacity():
     import torch
     L = dg.lib()

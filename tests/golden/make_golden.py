@@ -1,8 +1,9 @@
 """Generate the golden fixtures in tests/golden/ from the reference's own tests.
 
-Run in a container that has the reference checkout (default /root/reference):
+Run where the reference checkout is present, naming it with --ref or the
+DYCG_REFERENCE environment variable:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>
 
 What it records (all small JSON, committed):
   smoke_bfs_sssp.json  -- the graph/update stream that tests/bfs_dynamic_smoke.py
@@ -405,7 +406,9 @@ def replay_random_case(ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=os.environ.get("DYCG_REFERENCE", "/root/reference"))
+    ap.add_argument("--ref", default=os.environ.get("DYCG_REFERENCE"),
+                    required="DYCG_REFERENCE" not in os.environ,
+                    help="reference checkout (default: $DYCG_REFERENCE)")
     ap.add_argument("--only", nargs="*", default=None, help="regenerate only these fixtures")
     ap.add_argument("--out", default=None, help="write here instead of tests/golden/")
     args = ap.parse_args()

@@ -52,29 +52,18 @@ def test_ctypes_mirrors_match_the_c_header(tmp_path):
             assert got[(cname, f)] == (d.offset, d.size), (cname, f)
 
 
-def _code_blocks(path, lang):
-    import re
-    text = open(os.path.join(ROOT, path)).read()
-    return re.findall(r"```" + lang + r"\n(.*?)```", text, re.S)
-
-
 @pytest.mark.skipif(shutil.which("gcc") is None or shutil.which("g++") is None,
                     reason="no C/C++ compiler")
-def test_documented_examples_compile_against_the_header(tmp_path):
-    """The README's C example and INTEGRATION.md's C++ shim use only names and
+def test_examples_compile_against_the_header():
+    """The C usage example and the reference-side C++ shim (tests/examples/,
+    the code the README and the integration guide show) use only names and
     signatures that include/dycg.h declares (syntax and type check, no link)."""
-    (c_example,) = _code_blocks("README.md", "c")
-    src = tmp_path / "readme.c"
-    src.write_text('#include "dycg.h"\n'
-                   "int example(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na,\n"
-                   "            uint32_t *dist, uint32_t *parent) {\n" + c_example + "  return 0;\n}\n")
-    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-fsyntax-only", "-I",
-                    os.path.join(ROOT, "include"), str(src)], check=True, capture_output=True)
-    (shim,) = _code_blocks("INTEGRATION.md", "cpp")
-    src = tmp_path / "shim.cpp"
-    src.write_text(shim)
-    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I",
-                    os.path.join(ROOT, "include"), str(src)], check=True, capture_output=True)
+    ex = os.path.join(ROOT, "tests", "examples")
+    inc = os.path.join(ROOT, "include")
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-fsyntax-only", "-I", inc,
+                    os.path.join(ex, "readme_example.c")], check=True, capture_output=True)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", inc,
+                    os.path.join(ex, "integration_shim.cpp")], check=True, capture_output=True)
 
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")

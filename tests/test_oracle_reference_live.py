@@ -183,9 +183,9 @@ def test_reference_tool_fixtures_regenerate_identically(tmp_path):
     """The committed fixtures made with the reference's own tools come back
     byte for byte when regenerated from the reference checkout."""
     import sys
-    ref = os.environ.get("DYCG_REFERENCE", "/root/reference")
-    if not os.path.exists(os.path.join(ref, "tests", "bfs_dynamic_smoke.py")):
-        pytest.skip("no reference checkout here")
+    ref = os.environ.get("DYCG_REFERENCE", "")
+    if not ref or not os.path.exists(os.path.join(ref, "tests", "bfs_dynamic_smoke.py")):
+        pytest.skip("no reference checkout named by DYCG_REFERENCE")
     for name in ("group_updates", "i16_repair_oracle", "chunk_store_replay"):
         _tool(name)
     golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")

@@ -45,31 +45,70 @@ __global__ void flag_kernel(const uint32_t *ids, const float *sc, uint32_t npage
   }
 }
 
+// Admission plan of one maintenance round, computed on the device from the
+// flag scans (admit candidates among the top K, eviction candidates among the
+// rest) and the free-slot count, so no host round trip sits between ranking
+// and staging: the refresh gate skips rounds with fewer than `gate` missing
+// top pages, at most `cap` pages are admitted, and only as many resident
+// pages are evicted (the lowest ranked first) as the free slots cannot cover.
+__global__ void plan_kernel(const uint32_t *sa, const uint32_t *fa, const uint32_t *se,
+                            const uint32_t *fe, uint32_t npages, uint32_t gate, uint32_t cap,
+                            CachePlan *plan, u64 *stat_loaded, u64 *stat_evicted) {
+  if (threadIdx.x || blockIdx.x) return;
+  const uint32_t n_admit = npages ? sa[npages - 1] + fa[npages - 1] : 0;
+  const uint32_t n_evict = npages ? se[npages - 1] + fe[npages - 1] : 0;
+  const uint32_t free0 = plan->free_count;
+  uint32_t admit = 0, evict = 0;
+  if (n_admit >= gate && n_admit) {
+    admit = min(n_admit, cap);
+    const uint32_t need = admit > free0 ? admit - free0 : 0u;
+    evict = min(n_evict, need);
+    admit = min(admit, free0 + evict);
+  }
+  plan->candidates = n_admit;
+  plan->admit = admit;
+  plan->evict = evict;
+  plan->first_rank = n_evict - evict;
+  plan->free_base = free0;
+  plan->top = free0 + evict;
+  plan->free_count = free0 + evict - admit;
+  plan->loaded += admit;
+  plan->evicted += evict;
+  if (stat_loaded && admit) atomicAdd(stat_loaded, (u64)admit);
+  if (stat_evicted && evict) atomicAdd(stat_evicted, (u64)evict);
+}
+
 __global__ void evict_kernel(const uint32_t *ids, uint32_t npages, const uint32_t *fe,
-                             const uint32_t *se, uint32_t first_rank, uint32_t *page_slot,
-                             uint32_t *free_list, uint32_t free_base) {
+                             const uint32_t *se, const CachePlan *plan, uint32_t *page_slot,
+                             uint32_t *free_list) {
+  const uint32_t evict = plan->evict, first_rank = plan->first_rank, base = plan->free_base;
+  if (!evict) return;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npages;
        i += gridDim.x * blockDim.x) {
     if (!fe[i] || se[i] < first_rank) continue;
     const uint32_t p = ids[i];
-    free_list[free_base + (se[i] - first_rank)] = page_slot[p];
+    free_list[base + (se[i] - first_rank)] = page_slot[p];
     page_slot[p] = PAGE_NONE;
   }
 }
 
 __global__ void admit_list_kernel(const uint32_t *ids, uint32_t npages, const uint32_t *fa,
-                                  const uint32_t *sa, uint32_t limit, uint32_t *admit) {
+                                  const uint32_t *sa, const CachePlan *plan, uint32_t *admit) {
+  const uint32_t limit = plan->admit;
+  if (!limit) return;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npages;
        i += gridDim.x * blockDim.x)
     if (fa[i] && sa[i] < limit) admit[sa[i]] = ids[i];
 }
 
 // CTA per page: copy the page's slot words from the host arena into its cache
-// slot with 16-byte loads, then publish it in the page table.
-__global__ void fill_kernel(const uint32_t *admit, uint32_t count, const uint32_t *free_list,
-                            uint32_t free_top, uint32_t *page_slot, const uint32_t *h_out,
+// slot with 16-byte loads, then publish it in the page table. The grid is
+// fixed; the page count comes from the plan.
+__global__ void fill_kernel(const uint32_t *admit, const CachePlan *plan,
+                            const uint32_t *free_list, uint32_t *page_slot, const uint32_t *h_out,
                             const uint32_t *h_in, uint32_t pages_out, uint32_t page_shift,
                             uint32_t stride, uint32_t *cdst) {
+  const uint32_t count = plan->admit, free_top = plan->top;
   const u64 words = (u64)stride << page_shift;
   for (uint32_t j = blockIdx.x; j < count; j += gridDim.x) {
     const uint32_t p = admit[j];
@@ -107,11 +146,6 @@ cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay, f
   bytes = W.temp_bytes;
   e = cub::DeviceScan::ExclusiveSum(W.temp, bytes, W.fe, W.se, (int)npages, s);
   if (e != cudaSuccess) return e;
-  // totals = last scan value + last flag
-  cudaMemcpyAsync(W.h_counts + 0, W.sa + npages - 1, 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(W.h_counts + 1, W.fa + npages - 1, 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(W.h_counts + 2, W.se + npages - 1, 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(W.h_counts + 3, W.fe + npages - 1, 4, cudaMemcpyDeviceToHost, s);
   return cudaGetLastError();
 }
 
@@ -129,10 +163,6 @@ cudaError_t cache_rank_given(CacheWork &W, uint32_t npages, uint32_t K, float mi
   bytes = W.temp_bytes;
   e = cub::DeviceScan::ExclusiveSum(W.temp, bytes, W.fe, W.se, (int)npages, s);
   if (e != cudaSuccess) return e;
-  cudaMemcpyAsync(W.h_counts + 0, W.sa + npages - 1, 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(W.h_counts + 1, W.fa + npages - 1, 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(W.h_counts + 2, W.se + npages - 1, 4, cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(W.h_counts + 3, W.fe + npages - 1, 4, cudaMemcpyDeviceToHost, s);
   return cudaGetLastError();
 }
 
@@ -146,22 +176,17 @@ size_t cache_temp_bytes(uint32_t npages) {
   return a > b ? a : b;
 }
 
-cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t n_evict_cand, uint32_t evict,
-                        uint32_t admit, uint32_t *page_slot, uint32_t *free_list,
-                        uint32_t free_count, const CachePages &pg, cudaStream_t s) {
-  if (evict) {
-    evict_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, npages, W.fe, W.se,
-                                                    n_evict_cand - evict, page_slot, free_list,
-                                                    free_count);
-  }
-  if (admit) {
-    admit_list_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, npages, W.fa, W.sa,
-                                                         admit, W.admit);
-    const uint32_t top = free_count + evict;
-    fill_kernel<<<(int)std::min<uint32_t>(admit, 148 * 8), BLOCK, 0, s>>>(
-        W.admit, admit, free_list, top, page_slot, pg.h_out, pg.h_in, pg.pages_out,
-        pg.page_shift, pg.stride, pg.cdst);
-  }
+cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t gate, uint32_t cap,
+                        uint32_t *page_slot, uint32_t *free_list, const CachePages &pg,
+                        u64 *stat_loaded, u64 *stat_evicted, cudaStream_t s) {
+  plan_kernel<<<1, 32, 0, s>>>(W.sa, W.fa, W.se, W.fe, npages, gate, cap, W.plan, stat_loaded,
+                               stat_evicted);
+  evict_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, npages, W.fe, W.se, W.plan,
+                                                  page_slot, free_list);
+  admit_list_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, npages, W.fa, W.sa, W.plan,
+                                                       W.admit);
+  fill_kernel<<<148 * 8, BLOCK, 0, s>>>(W.admit, W.plan, free_list, page_slot, pg.h_out, pg.h_in,
+                                        pg.pages_out, pg.page_shift, pg.stride, pg.cdst);
   return cudaGetLastError();
 }
 

@@ -221,6 +221,10 @@ int dycg_set_query_mapping(dycg_engine *e, uint32_t qratio, uint32_t heavy, uint
   return guard(e, [&](Engine &g) { g.set_query_mapping(qratio, heavy, tile); });
 }
 
+int dycg_set_query_queue(dycg_engine *e, uint32_t scheme) {
+  return guard(e, [&](Engine &g) { g.set_query_queue(scheme); });
+}
+
 int dycg_gather_query(dycg_engine *e, uint32_t q, uint32_t *values, uint32_t *parents) {
   return guard(e, [&](Engine &g) { g.gather_query(q, values, parents); });
 }

@@ -133,12 +133,16 @@ struct Ctl {
   uint32_t snap_vmin;
   uint32_t wave_tag;     // running wave tag (never reused)
   uint32_t waves;        // waves run in this launch
-  uint32_t pad[2];
+  uint32_t pad[2];       // PageRank: carried frontier (queue parity, length)
+  uint32_t grab;         // claimed-item counter of a phase (reset by its barriers)
+  uint32_t pad2;
   u64 stat[20];
   u64 tphase[8];         // batched repair: global timer at phase boundaries (ns)
   // grid-barrier arrival groups, one 128-byte line each (frontier.cuh)
   uint32_t bar_sub[BAR_GROUPS * 32];
 };
+// read back to the host once per snapshot (dycgraph_b200/engine.py CTL_BYTES)
+static_assert(sizeof(Ctl) == 2360, "Ctl layout changed: update CTL_BYTES in engine.py");
 
 enum StatIdx {
   ST_LINK_BYTES = 0,

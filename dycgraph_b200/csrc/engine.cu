@@ -234,7 +234,6 @@ void Engine::finish_load() {
     std::vector<uint32_t> fl(cache_slots_);
     for (uint32_t i = 0; i < cache_slots_; i++) fl[i] = cache_slots_ - 1 - i;
     CK(cudaMemcpyAsync(free_list_, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice, st_));
-    free_count_ = cache_slots_;
     cwk_.hits = page_hits_;
     cwk_.score = (float *)dmalloc((u64)npages_ * 4);
     cwk_.score_sorted = (float *)dmalloc((u64)npages_ * 4);
@@ -248,10 +247,14 @@ void Engine::finish_load() {
     CK(cudaMemsetAsync(cwk_.score, 0, (u64)npages_ * 4, st_));
     cwk_.temp_bytes = cache_temp_bytes(npages_);
     cwk_.temp = dmalloc(cwk_.temp_bytes);
+    cwk_.plan = (CachePlan *)dmalloc(sizeof(CachePlan));
     void *hc = nullptr;
-    CK(cudaHostAlloc(&hc, 64, cudaHostAllocDefault));
+    CK(cudaHostAlloc(&hc, sizeof(CachePlan), cudaHostAllocDefault));
     hallocs_.push_back(hc);
-    cwk_.h_counts = (uint32_t *)hc;
+    cwk_.h_plan = (CachePlan *)hc;
+    std::memset(cwk_.h_plan, 0, sizeof(CachePlan));
+    cwk_.h_plan->free_count = cache_slots_;
+    CK(cudaMemcpyAsync(cwk_.plan, cwk_.h_plan, sizeof(CachePlan), cudaMemcpyHostToDevice, st_));
   }
   // vertex state
   key_ = (u64 *)dmalloc((n + 1ull) * 8);
@@ -813,8 +816,8 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
   if (!capture) CK(cudaEventRecord(ev_[2], st_));
   // learned admission / trace features, between mutation and repair: rows
   // that moved to new blocks in this snapshot are seen at their new pages
-  if (!capture && feat_ && (policy_ == DYCG_CACHE_LEARNED || trace_n_ < trace_cap_))
-    policy_prefetch(nd, na);
+  if (feat_ && (policy_ == DYCG_CACHE_LEARNED || (!capture && trace_n_ < trace_cap_)))
+    policy_prefetch(nd, na, capture);
   // ---- repair
   if (opt_.algo == DYCG_ALGO_PR) {
     PL.phases = (nd + na) ? (PR_AMEND | PR_CONVERGE) : PR_CONVERGE;
@@ -858,6 +861,8 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
     launches_++;
   }
   if (!capture) CK(cudaEventRecord(ev_[3], st_));
+  // a replayed snapshot keeps its cache maintenance inside the graph
+  if (capture) maintenance_device();
 }
 
 void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na,
@@ -1055,6 +1060,13 @@ void Engine::set_query_mapping(uint32_t qratio, uint32_t heavy, uint32_t tile) {
   drop_graphs();  // captured graphs hold the old mapping
 }
 
+void Engine::set_query_queue(uint32_t scheme) {
+  if (scheme != DYCG_QUEUE_STATIC && scheme != DYCG_QUEUE_CLAIMED)
+    throw Error(DYCG_EINVAL, "unknown frontier-queue scheme");
+  sched_ = scheme;
+  drop_graphs();  // captured graphs hold the old scheme
+}
+
 MultiLaunch Engine::multi_launch(uint32_t phases, uint32_t n_add, u64 timeout) {
   MultiLaunch L{};
   L.out = adj(out_);
@@ -1088,6 +1100,7 @@ MultiLaunch Engine::multi_launch(uint32_t phases, uint32_t n_add, u64 timeout) {
   L.pull_qratio = pull_qratio_;
   L.heavy = heavy_;
   L.tile = tile_;
+  L.sched = sched_;
   L.timeout_ns = timeout;
   L.algo = opt_.algo;
   L.stored = stored_;
@@ -1259,14 +1272,15 @@ void Engine::tune_repair(uint32_t nd, uint32_t na, u64 timeout) {
   static const uint32_t kPull[] = {0, 1, 2, 8};
   static const uint32_t kTile[] = {1024, 4096, 16384};
   tried_.clear();
-  const uint32_t tile0 = tile_;
-  dycg_query_mapping best{qratio_, heavy_, tile_, pull_qratio_, 1e30f};
-  auto trial = [&](uint32_t r, uint32_t h, uint32_t pr, uint32_t t) {
+  const uint32_t tile0 = tile_, sched0 = sched_;
+  dycg_query_mapping best{qratio_, heavy_, tile_, pull_qratio_, sched_, 1e30f};
+  auto trial = [&](uint32_t r, uint32_t h, uint32_t pr, uint32_t t, uint32_t q) {
     if (!tried_.empty()) restore();
     qratio_ = r;
     heavy_ = h;
     pull_qratio_ = pr;
     tile_ = t;
+    sched_ = q;
     CK(cudaEventRecord(sc.a, st_));
     CK(launch_multi(multi_launch(phases, na, timeout), st_));
     CK(cudaEventRecord(sc.b, st_));
@@ -1279,25 +1293,30 @@ void Engine::tune_repair(uint32_t nd, uint32_t na, u64 timeout) {
     }
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, sc.a, sc.b));
-    tried_.push_back({r, h, t, pr, ms});
+    tried_.push_back({r, h, t, pr, q, ms});
     if (ms < best.repair_ms) best = tried_.back();
     launches_++;
   };
   // coordinate search: (qratio, heavy) with the pull phase on the same rule,
-  // then the pull phase's own ratio, then the slots per query-lane tile
+  // then the pull phase's own ratio, then the slots per query-lane tile, then
+  // the frontier-queue scheme
   for (uint32_t r : kRatio)
-    for (uint32_t h : kHeavy) trial(r, h, r, tile0);
+    for (uint32_t h : kHeavy) trial(r, h, r, tile0, sched0);
   const dycg_query_mapping first = best;
   for (uint32_t pr : kPull)
-    if (pr != first.qratio) trial(first.qratio, first.heavy, pr, tile0);
+    if (pr != first.qratio) trial(first.qratio, first.heavy, pr, tile0, sched0);
   const dycg_query_mapping second = best;
   for (uint32_t t : kTile)
-    if (t != second.tile) trial(second.qratio, second.heavy, second.pull_qratio, t);
+    if (t != second.tile) trial(second.qratio, second.heavy, second.pull_qratio, t, sched0);
+  const dycg_query_mapping third = best;
+  for (uint32_t q : {DYCG_QUEUE_STATIC, DYCG_QUEUE_CLAIMED})
+    if (q != third.queue) trial(third.qratio, third.heavy, third.pull_qratio, third.tile, q);
   restore();
   qratio_ = best.qratio;
   heavy_ = best.heavy;
   pull_qratio_ = best.pull_qratio;
   tile_ = best.tile;
+  sched_ = best.queue;
   drop_graphs();
   CK(cudaEventRecord(ev_[2], st_));  // the stage boundary of the kept run
   CK(launch_multi(multi_launch(phases, na, timeout), st_));
@@ -1366,10 +1385,12 @@ void Engine::apply_batches(const dycg_edge *dels, const uint64_t *nd, const dycg
     mx = std::max<u64>(mx, std::max(nd[i], na[i]));
   }
   if ((td && !dels) || (ta && !adds)) throw Error(DYCG_EINVAL, "null update array");
-  if (!(nq_ && qmode_ == DYCG_QUERIES_BATCHED) || policy_ == DYCG_CACHE_LEARNED ||
-      trace_n_ < trace_cap_) {
-    // other forms, the learned policy (its admission synchronises with the
-    // host mid-snapshot) and trace recording: one ordinary apply per snapshot
+  // trace recording (and the snapshots whose page reads still complete the
+  // traced snapshots' targets) needs the host between snapshots
+  const bool tracing =
+      trace_n_ < trace_cap_ || (trace_cap_ && trace_post_ + 1 < (uint32_t)POLICY_HORIZON);
+  if (!(nq_ && qmode_ == DYCG_QUERIES_BATCHED) || tracing) {
+    // other forms and trace recording: one ordinary apply per snapshot
     u64 od = 0, oa = 0;
     for (uint32_t i = 0; i < count; i++) {
       apply(dels + od, nd[i], adds + oa, na[i], device_ptrs, 0, true, stats ? stats + i : nullptr);
@@ -1474,6 +1495,13 @@ void Engine::apply_batches(const dycg_edge *dels, const uint64_t *nd, const dycg
       s->mutate_link_bytes = c.stat[ST_MUT_LINK_BYTES];
       s->mutate_hbm_bytes = c.stat[ST_MUT_HBM_BYTES];
       s->state_bytes = c.stat[ST_STATE_BYTES] + s->expanded * 16 + s->improvements * 16;
+      s->cache_pages_loaded = c.stat[ST_PAGES_LOADED];
+      s->cache_pages_evicted = c.stat[ST_PAGES_EVICTED];
+      {
+        const u64 page_bytes = (4ull << page_shift_) * out_.stride;
+        s->link_bytes += c.stat[ST_PAGES_LOADED] * page_bytes;
+        s->hbm_adj_bytes += c.stat[ST_PAGES_LOADED] * page_bytes;
+      }
       s->kernel_launches = graphs_.count(cls[i]) ? graphs_[cls[i]].kernels : 0;
       float ms = 0;
       cudaEventElapsedTime(&ms, bev_[2 * i], bev_[2 * i + 1]);
@@ -1483,19 +1511,6 @@ void Engine::apply_batches(const dycg_edge *dels, const uint64_t *nd, const dycg
         s->ms_repair = (c.stat[ST_T_END] - c.stat[ST_T_START]) * 1e-6;
       fill_phases(s, c);
     }
-  }
-  // cache maintenance once, after the last snapshot
-  dycg_batch_stats last{};
-  cache_maintenance(false, stats ? &last : nullptr);
-  if (stats && count) {
-    dycg_batch_stats *s = stats + count - 1;
-    s->ms_cache = last.ms_cache;
-    s->ms_total += last.ms_cache;
-    s->cache_pages_loaded = last.cache_pages_loaded;
-    s->cache_pages_evicted = last.cache_pages_evicted;
-    s->link_bytes += last.link_bytes;
-    s->hbm_adj_bytes += last.hbm_adj_bytes;
-    s->kernel_launches += 8;
   }
 }
 
@@ -1511,6 +1526,11 @@ void Engine::policy_alloc() {
   prows_ = (uint32_t *)dmalloc(np * 4);
   pmax_ = (uint32_t *)dmalloc(np * 4);
   pdelta_ = (uint32_t *)dmalloc(np * 4);
+  pperiod_ = (uint32_t *)dmalloc(8);
+  {
+    const uint32_t per[2] = {0, 8};
+    CK(cudaMemcpyAsync(pperiod_, per, 8, cudaMemcpyHostToDevice, st_));
+  }
   CK(cudaMemsetAsync(hist_, 0, np * 16, st_));
   CK(cudaMemsetAsync(age_, 0xFF, np, st_));
   params_ = (float *)dmalloc(POLICY_PARAMS * 4);
@@ -1566,21 +1586,24 @@ void Engine::policy_trace(uint32_t snapshots) {
   drop_graphs();
 }
 
-// Features of the snapshot being applied (after ingest, before mutation);
-// under the learned policy, admit the pages the network ranks highest.
-void Engine::policy_prefetch(size_t nd, size_t na) {
+// Features of the snapshot being applied (after its mutation, before its
+// repair); under the learned policy, admit the pages the network ranks
+// highest. Everything runs on the device (no host synchronisation), so the
+// same sequence is recorded into the replayed snapshot graphs (capture: no
+// stage events, no trace recording).
+void Engine::policy_prefetch(size_t nd, size_t na, bool capture) {
   const u64 np = npages_;
-  CK(cudaEventRecord(pev_[0], st_));
+  if (!capture) CK(cudaEventRecord(pev_[0], st_));
   CK(cudaMemsetAsync(pdelta_, 0, np * 4, st_));
-  if (prefetch_count_++ % 8 == 0) {
-    // the row-layout features (rows per page, longest row) drift slowly with
-    // relocations: refreshed every 8 snapshots
-    CK(cudaMemsetAsync(prows_, 0, np * 4, st_));
-    CK(cudaMemsetAsync(pmax_, 0, np * 4, st_));
-    CK(launch_page_rows(out_.off, out_.len, n_, out_.page_base, page_shift_, prows_, pmax_, st_));
-    if (has_in_)
-      CK(launch_page_rows(in_.off, in_.len, n_, in_.page_base, page_shift_, prows_, pmax_, st_));
-  }
+  // the row-layout features (rows per page, longest row) drift slowly with
+  // relocations: refreshed every 8th snapshot (counter on the device)
+  CK(launch_page_rows_clear(prows_, pmax_, npages_, pperiod_, st_));
+  CK(launch_page_rows(out_.off, out_.len, n_, out_.page_base, page_shift_, prows_, pmax_, pperiod_,
+                      st_));
+  if (has_in_)
+    CK(launch_page_rows(in_.off, in_.len, n_, in_.page_base, page_shift_, prows_, pmax_, pperiod_,
+                        st_));
+  CK(launch_period_step(pperiod_, st_));
   if (nd) {
     CK(launch_page_delta(k_del_out_, (uint32_t)nd, out_.off, out_.page_base, page_shift_, pdelta_,
                          st_));
@@ -1596,43 +1619,30 @@ void Engine::policy_prefetch(size_t nd, size_t na) {
                            st_));
   }
   CK(launch_features(page_hits_, hist_, age_, pdelta_, prows_, pmax_, npages_, feat_, st_));
-  launches_ += 3 + (has_in_ ? 1 : 0) + (nd ? 1 : 0) * (has_in_ ? 2 : 1) +
+  launches_ += 5 + (has_in_ ? 1 : 0) + (nd ? 1 : 0) * (has_in_ ? 2 : 1) +
                (na ? 1 : 0) * (has_in_ ? 2 : 1);
-  trace_pending_ = trace_n_ < trace_cap_;
+  trace_pending_ = !capture && trace_n_ < trace_cap_;
   if (trace_pending_) {
     CK(cudaMemcpyAsync((char *)tx_ + (u64)trace_n_ * np * POLICY_F * 2, feat_,
                        np * POLICY_F * 2, cudaMemcpyDeviceToDevice, st_));
     CK(cudaMemsetAsync(ty_ + (u64)trace_n_ * np, 0, np * 4, st_));
   }
-  prefetch_loaded_ = prefetch_evicted_ = 0;
   if (policy_ == DYCG_CACHE_LEARNED && cache_slots_) {
     CK(launch_mlp_infer(feat_, npages_, params_, cwk_.score, cwk_.ids, st_));
-    // admit pages predicted to be read at least ~64 times in this snapshot
+    // admit pages predicted to be read at least ~64 times in this snapshot,
+    // at most cache_slots / learned_cap_div_ per snapshot (no refresh gate)
     CK(cache_rank_given(cwk_, npages_, cache_slots_, std::log1p(64.f), page_slot_, st_));
-    launches_ += 6;
-    sync_check("learned rank");
-    const uint32_t n_admit = cwk_.h_counts[0] + cwk_.h_counts[1];
-    const uint32_t n_evict_cand = cwk_.h_counts[2] + cwk_.h_counts[3];
+    CachePages pg{out_.d_dst, has_in_ ? in_.d_dst : nullptr, out_.pages, page_shift_,
+                  out_.stride, cdst_};
     const uint32_t cap = std::max<uint32_t>(cache_slots_ / learned_cap_div_, 256u);
-    uint32_t admit = std::min(n_admit, cap);
-    const uint32_t need = admit > free_count_ ? admit - free_count_ : 0u;
-    const uint32_t evict = std::min(n_evict_cand, need);
-    admit = std::min(admit, free_count_ + evict);
-    if (admit) {
-      CachePages pg{out_.d_dst, has_in_ ? in_.d_dst : nullptr, out_.pages, page_shift_,
-                    out_.stride, cdst_};
-      CK(cache_apply(cwk_, npages_, n_evict_cand, evict, admit, page_slot_, free_list_,
-                     free_count_, pg, st_));
-      free_count_ = free_count_ + evict - admit;
-      pages_loaded_ += admit;
-      pages_evicted_ += evict;
-      launches_ += 3;
-    }
-    prefetch_loaded_ = admit;
-    prefetch_evicted_ = evict;
+    CK(cache_apply(cwk_, npages_, 1, cap, page_slot_, free_list_, pg,
+                   &ctl_->stat[ST_PAGES_LOADED], &ctl_->stat[ST_PAGES_EVICTED], st_));
+    launches_ += 9;
   }
-  CK(cudaEventRecord(pev_[1], st_));
-  prefetched_ = true;
+  if (!capture) {
+    CK(cudaEventRecord(pev_[1], st_));
+    prefetched_ = true;
+  }
 }
 
 void Engine::policy_train(uint32_t epochs, float lr, uint32_t batch, uint64_t seed,
@@ -1752,15 +1762,17 @@ void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
     // admission ran before the repair (policy_prefetch); the call ends here
     CK(cudaEventRecord(ev_[5], st_));
     if (prefetched_ && stats) {
+      CK(cudaMemcpyAsync(cwk_.h_plan, cwk_.plan, sizeof(CachePlan), cudaMemcpyDeviceToHost, st_));
       sync_check("learned maintenance");
       float ms = 0;
       cudaEventElapsedTime(&ms, pev_[0], pev_[1]);
       stats->ms_cache = ms;
-      stats->cache_pages_loaded = prefetch_loaded_;
-      stats->cache_pages_evicted = prefetch_evicted_;
+      const CachePlan &pl = *cwk_.h_plan;
+      stats->cache_pages_loaded = pl.admit;
+      stats->cache_pages_evicted = pl.evict;
       const u64 page_bytes = (4ull << page_shift_) * out_.stride;
-      stats->link_bytes += (u64)prefetch_loaded_ * page_bytes;
-      stats->hbm_adj_bytes += (u64)prefetch_loaded_ * page_bytes;
+      stats->link_bytes += (u64)pl.admit * page_bytes;
+      stats->hbm_adj_bytes += (u64)pl.admit * page_bytes;
     }
     prefetched_ = false;
     return;
@@ -1771,44 +1783,55 @@ void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
     return;
   }
   CK(cudaEventRecord(ev_[4], st_));
-  // a page must have been read at least kMinScore times (decayed) before it
-  // displaces a resident one: single random probes do not churn the cache
-  const float kMinScore = initial ? 0.f : 64.f;
-  CK(cache_rank(cwk_, npages_, cache_slots_, 0.75f, kMinScore, page_slot_, st_));
-  sync_check("cache rank");
-  const uint32_t n_admit = cwk_.h_counts[0] + cwk_.h_counts[1];
-  const uint32_t n_evict_cand = cwk_.h_counts[2] + cwk_.h_counts[3];
-  // refresh gate: skip unless enough top-K pages are missing
-  const uint32_t gate = initial ? 1u : std::max<uint32_t>(1u, cache_slots_ / 1024);
-  uint32_t admit = 0, evict = 0;
-  if (n_admit >= gate) {
-    const uint32_t cap = initial ? cache_slots_ : std::max<uint32_t>(cache_slots_ / 512, 64u);
-    admit = std::min(n_admit, cap);
-    const uint32_t need = admit > free_count_ ? admit - free_count_ : 0u;
-    evict = std::min(n_evict_cand, need);
-    admit = std::min(admit, free_count_ + evict);
-    CachePages pg{out_.d_dst, has_in_ ? in_.d_dst : nullptr, out_.pages, page_shift_,
-                  out_.stride, cdst_};
-    CK(cache_apply(cwk_, npages_, n_evict_cand, evict, admit, page_slot_, free_list_, free_count_,
-                   pg, st_));
-    free_count_ = free_count_ + evict - admit;
-    pages_loaded_ += admit;
-    pages_evicted_ += evict;
-    launches_ += 3;
-  }
-  launches_ += 5;
+  hotness_round(initial);
   CK(cudaEventRecord(ev_[5], st_));
+  CK(cudaMemcpyAsync(cwk_.h_plan, cwk_.plan, sizeof(CachePlan), cudaMemcpyDeviceToHost, st_));
   sync_check("cache apply");
   if (stats) {
     float ms = 0;
     cudaEventElapsedTime(&ms, ev_[4], ev_[5]);
+    const CachePlan &pl = *cwk_.h_plan;
     stats->ms_cache = ms;
-    stats->cache_pages_loaded = admit;
-    stats->cache_pages_evicted = evict;
+    stats->cache_pages_loaded = pl.admit;
+    stats->cache_pages_evicted = pl.evict;
     const u64 page_bytes = (4ull << page_shift_) * out_.stride;
-    stats->link_bytes += (u64)admit * page_bytes;
-    stats->hbm_adj_bytes += (u64)admit * page_bytes;
+    stats->link_bytes += (u64)pl.admit * page_bytes;
+    stats->hbm_adj_bytes += (u64)pl.admit * page_bytes;
   }
+}
+
+// One hotness round on the device: decayed page scores, top-K ranking, the
+// refresh gate, eviction and staging. A page must have been read at least
+// kMinScore times (decayed) before it displaces a resident one, so single
+// random probes do not churn the cache; the initial load admits the whole
+// top K.
+void Engine::hotness_round(bool initial) {
+  const float kMinScore = initial ? 0.f : 64.f;
+  CK(cache_rank(cwk_, npages_, cache_slots_, 0.75f, kMinScore, page_slot_, st_));
+  const uint32_t gate = initial ? 1u : std::max<uint32_t>(1u, cache_slots_ / 1024);
+  const uint32_t cap = initial ? cache_slots_ : std::max<uint32_t>(cache_slots_ / 512, 64u);
+  CachePages pg{out_.d_dst, has_in_ ? in_.d_dst : nullptr, out_.pages, page_shift_, out_.stride,
+                cdst_};
+  CK(cache_apply(cwk_, npages_, gate, cap, page_slot_, free_list_, pg,
+                 &ctl_->stat[ST_PAGES_LOADED], &ctl_->stat[ST_PAGES_EVICTED], st_));
+  launches_ += 9;
+}
+
+// Per-snapshot cache maintenance recorded into a replayed snapshot graph:
+// the learned policy's page history (its admission ran before the repair),
+// or a hotness round, or for an engine without cache the counter reset.
+void Engine::maintenance_device() {
+  if (feat_) {
+    const bool clear = policy_ != DYCG_CACHE_HOTNESS || !cache_slots_;
+    CK(launch_history(page_hits_, hist_, age_, npages_, TargetRefs{}, clear, st_));
+    launches_++;
+  }
+  if (policy_ == DYCG_CACHE_LEARNED) return;
+  if (!cache_slots_) {
+    CK(cudaMemsetAsync(page_hits_, 0, (u64)npages_ * 4, st_));
+    return;
+  }
+  hotness_round(false);
 }
 
 void Engine::gather(uint32_t *values, uint32_t *parents) {
@@ -1904,6 +1927,8 @@ void Engine::info(dycg_graph_info *out) {
   u64 top_out = 0, top_in = 0;
   CK(cudaMemcpyAsync(&top_out, out_.top, 8, cudaMemcpyDeviceToHost, st_));
   if (has_in_) CK(cudaMemcpyAsync(&top_in, in_.top, 8, cudaMemcpyDeviceToHost, st_));
+  if (cache_slots_)
+    CK(cudaMemcpyAsync(cwk_.h_plan, cwk_.plan, sizeof(CachePlan), cudaMemcpyDeviceToHost, st_));
   sync_check("info");
   u64 m = 0;
   for (uint32_t x : l) m += x;
@@ -1912,7 +1937,7 @@ void Engine::info(dycg_graph_info *out) {
   out->arena_used = top_out + top_in;
   out->pages = npages_;
   out->cache_slots = cache_slots_;
-  out->cached_pages = cache_slots_ - free_count_;
+  out->cached_pages = cache_slots_ ? cache_slots_ - cwk_.h_plan->free_count : 0;
   out->host_bytes = out->arena_slots * 4 * out_.stride;
   out->device_bytes = (u64)n_ * (8 + 4 * 6) + (u64)n_ * (has_in_ ? 48 : 24) +
                       ((u64)cache_slots_ << page_shift_) * 4 * out_.stride + index_bytes_ +

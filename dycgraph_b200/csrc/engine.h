@@ -69,6 +69,7 @@ class Engine {
   // many-query forms (SSSP/BFS): set after loading, before init
   void set_queries(const uint32_t *sources, uint32_t count, uint32_t mode);
   void set_query_mapping(uint32_t qratio, uint32_t heavy, uint32_t tile);
+  void set_query_queue(uint32_t scheme);
   void gather_query(uint32_t q, uint32_t *values, uint32_t *parents);
   void tune(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size_t na,
             dycg_query_mapping *tried, uint32_t cap, uint32_t *n_tried, dycg_batch_stats *stats);
@@ -112,7 +113,9 @@ class Engine {
   void delete_direction(const Adj &A, const uint2 *uv, const uint32_t *mult,
                         const uint32_t *n_ptr, uint32_t nd, uint32_t *found, int count_missing,
                         bool capture);
-  void policy_prefetch(size_t nd, size_t na);
+  void policy_prefetch(size_t nd, size_t na, bool capture);
+  void hotness_round(bool initial);
+  void maintenance_device();
   void init_queries(u64 timeout);
   void repair_queries(uint32_t nd, uint32_t na, u64 timeout);
   MultiLaunch multi_launch(uint32_t phases, uint32_t n_add, u64 timeout);
@@ -130,10 +133,9 @@ class Engine {
   std::vector<void *> hallocs_;
 
   // cache
-  uint32_t page_shift_ = 12, npages_ = 0, cache_slots_ = 0, free_count_ = 0;
+  uint32_t page_shift_ = 12, npages_ = 0, cache_slots_ = 0;
   uint32_t *page_slot_ = nullptr, *page_hits_ = nullptr, *cdst_ = nullptr, *free_list_ = nullptr;
   CacheWork cwk_{};
-  uint64_t pages_loaded_ = 0, pages_evicted_ = 0;
   u64 index_bytes_ = 0;
 
   // vertex state
@@ -159,7 +161,7 @@ class Engine {
   Ctl *qctl_ = nullptr, *h_qctl_ = nullptr;     // per-query control blocks
   uint4 *mtiles_ = nullptr;
   uint32_t mtile_cap_ = 0;
-  uint32_t qratio_ = 4, heavy_ = 64, tile_ = 4096, pull_qratio_ = 4;
+  uint32_t qratio_ = 4, heavy_ = 64, tile_ = 4096, pull_qratio_ = 4, sched_ = 0;
   u64 qbytes_ = 0;
   bool tune_ = false;
   std::vector<dycg_query_mapping> tried_;
@@ -184,8 +186,8 @@ class Engine {
   float *ty_ = nullptr;
   uint32_t trace_cap_ = 0, trace_n_ = 0, trace_post_ = 0;
   bool trace_pending_ = false, prefetched_ = false;
-  uint32_t prefetch_loaded_ = 0, prefetch_evicted_ = 0, learned_cap_div_ = 256;
-  uint64_t prefetch_count_ = 0;
+  uint32_t learned_cap_div_ = 256;
+  uint32_t *pperiod_ = nullptr;  // device {snapshot counter, refresh period} of the layout features
   cudaEvent_t pev_[2] = {};
   u64 policy_bytes_ = 0;
 

@@ -63,6 +63,7 @@ struct MultiLaunch {
   uint32_t pull_qratio;         // the same rule for the pull phase
   uint32_t heavy;               // rows with more work (warp iterations) are tiled
   uint32_t tile;                // tile size, in slots
+  uint32_t sched;               // item distribution: 0 static, 1 claimed one at a time
   u64 timeout_ns;
   uint32_t algo;
   bool stored;
@@ -176,13 +177,27 @@ cudaError_t launch_touched(const u64 *k, uint32_t cnt, uint32_t *tag, uint32_t e
                            uint32_t *list, uint32_t *n_out, Ctl *ctl, cudaStream_t s);
 
 // cache
+// Device-resident admission state: the free-slot count and the plan of the
+// last maintenance round (cache.cu plan_kernel), so that ranking, eviction
+// and staging run without a host round trip (inside captured graphs too).
+struct CachePlan {
+  uint32_t free_count;   // free cache slots: free_list[0, free_count)
+  uint32_t candidates;   // last round: top-K pages not resident
+  uint32_t admit, evict; // last round: pages staged / evicted
+  uint32_t first_rank;   // last round: first evicted rank among the candidates
+  uint32_t free_base;    // last round: free count before eviction
+  uint32_t top;          // last round: free count after eviction
+  uint32_t pad;
+  u64 loaded, evicted;   // totals
+};
 struct CacheWork {
   uint32_t *hits;        // == page_hits
   float *score, *score_sorted;
   uint32_t *ids, *ids_sorted, *fa, *fe, *sa, *se, *admit;
   void *temp;
   size_t temp_bytes;
-  uint32_t *h_counts;    // pinned host [4]
+  CachePlan *plan;       // device
+  CachePlan *h_plan;     // pinned host copy (read after a synchronisation)
 };
 struct CachePages {
   const uint32_t *h_out, *h_in;  // host arena words (device-mapped)
@@ -192,9 +207,11 @@ struct CachePages {
 size_t cache_temp_bytes(uint32_t npages);
 cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay, float min_score,
                        const uint32_t *page_slot, cudaStream_t s);
-cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t n_evict_cand, uint32_t evict,
-                        uint32_t admit, uint32_t *page_slot, uint32_t *free_list,
-                        uint32_t free_count, const CachePages &pg, cudaStream_t s);
+// plan (refresh gate, at most cap admissions), evict, stage; admissions and
+// evictions are also added to the optional device counters
+cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t gate, uint32_t cap,
+                        uint32_t *page_slot, uint32_t *free_list, const CachePages &pg,
+                        u64 *stat_loaded, u64 *stat_evicted, cudaStream_t s);
 
 // cache given precomputed scores (W.score, W.ids filled): sort, flags, counts
 cudaError_t cache_rank_given(CacheWork &W, uint32_t npages, uint32_t K, float min_score,
@@ -205,9 +222,14 @@ constexpr int POLICY_F = 8, POLICY_H = 64;
 constexpr int POLICY_PARAMS = POLICY_F * POLICY_H + POLICY_H + POLICY_H * POLICY_H + POLICY_H +
                               POLICY_H + 1;
 size_t mlp_grad_smem();
+// Row-layout features (rows starting in each page, longest of them). With
+// period = {counter, every}: only when counter % every == 0 (device values).
 cudaError_t launch_page_rows(const u64 *off, const uint32_t *len, uint32_t n, uint32_t page_base,
                              uint32_t page_shift, uint32_t *rows, uint32_t *maxlen,
-                             cudaStream_t s);
+                             const uint32_t *period, cudaStream_t s);
+cudaError_t launch_page_rows_clear(uint32_t *rows, uint32_t *maxlen, uint32_t npages,
+                                   const uint32_t *period, cudaStream_t s);
+cudaError_t launch_period_step(uint32_t *period, cudaStream_t s);
 cudaError_t launch_page_delta(const u64 *keys, uint32_t cnt, const u64 *off, uint32_t page_base,
                               uint32_t page_shift, uint32_t *delta, cudaStream_t s);
 cudaError_t launch_features(const uint32_t *hits, const float *hist, const uint8_t *age,

@@ -56,6 +56,7 @@ struct MultiParams {
   const uint3 *add_uvw;
   uint32_t n_add;
   uint32_t n, phases, max_waves, qratio, pull_qratio, heavy, tile;
+  uint32_t sched;  // item distribution: 0 static, 1 claimed (dycg_query_mapping.queue)
   u64 timeout_ns;
 };
 
@@ -329,8 +330,23 @@ __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t 
   const uint32_t lane = lane_id();
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t i = gw; i < cnt; i += nw) {
+  // Item distribution: static (warp w takes items w, w + nw, ...) or claimed
+  // one at a time from a per-phase counter, so that a warp that drew long rows
+  // does not hold the wave's barrier while the others idle (the counter is
+  // reset by the barriers that end the phase).
+  uint32_t i = gw;
+  if (P.sched) {
+    if (lane == 0) i = atomicAdd(&ctl->grab, 1u);
+    i = __shfl_sync(0xffffffffu, i, 0);
+  }
+  for (; i < cnt;) {
     const uint32_t v = items[i];
+    if (P.sched) {
+      if (lane == 0) i = atomicAdd(&ctl->grab, 1u);
+      i = __shfl_sync(0xffffffffu, i, 0);
+    } else {
+      i += nw;
+    }
     uint32_t m[NB];
     if (!prep(v, m)) continue;
     const uint32_t len = A.len[v];
@@ -360,12 +376,27 @@ __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t 
     }
     expand_vertex<NB, WITH_W>(A, v, m, 0, len, 32, ql, ph, s, acc);
   }
-  if (!grid_sync(ctl, reset_flags, P.timeout_ns)) return false;
+  if (!grid_sync(ctl, reset_flags | SYNC_RESET_GRAB, P.timeout_ns)) return false;
   const uint32_t nt = min(*(volatile uint32_t *)&ctl->snap_tiles, P.tiles.cap);
   if (nt == 0) return true;
   const uint32_t wib = threadIdx.x >> 5;
-  for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
+  __shared__ uint32_t s_tile;
+  uint32_t t = blockIdx.x;
+  if (P.sched) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(&ctl->grab, 1u);
+    __syncthreads();
+    t = s_tile;
+  }
+  while (t < nt) {
     const uint4 tl = P.tiles.tiles[t];
+    if (P.sched) {
+      __syncthreads();  // every warp has read s_tile
+      if (threadIdx.x == 0) s_tile = atomicAdd(&ctl->grab, 1u);
+      __syncthreads();
+      t = s_tile;
+    } else {
+      t += gridDim.x;
+    }
     uint32_t m[NB];
 #pragma unroll
     for (int k = 0; k < NB; k++) m[k] = P.cmask[(u64)tl.x * NB + k];
@@ -379,7 +410,7 @@ __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t 
       staged_pairs<NB>(tl.x, m, tl.z - tl.y, stage, ph, s, acc);
     }
   }
-  return grid_sync(ctl, SYNC_RESET_TILES, P.timeout_ns);
+  return grid_sync(ctl, SYNC_RESET_TILES | SYNC_RESET_GRAB, P.timeout_ns);
 }
 
 // Children y of a newly affected (x, q) with parent_q(y) == x become affected.
@@ -851,6 +882,7 @@ static cudaError_t launch_multi_t(const MultiLaunch &L, cudaStream_t s) {
   P.pull_qratio = L.pull_qratio;
   P.heavy = std::max(L.heavy, 1u);
   P.tile = std::max(L.tile, MULTI_MIN_TILE);
+  P.sched = L.sched;
   P.timeout_ns = L.timeout_ns;
   static int blocks_per_sm = -1;
   if (blocks_per_sm < 0) {

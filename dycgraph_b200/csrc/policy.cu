@@ -66,7 +66,8 @@ int grid_for(u64 threads) {
 // adds once.
 __global__ void page_rows_kernel(const u64 *off, const uint32_t *len, uint32_t n,
                                  uint32_t page_base, uint32_t page_shift, uint32_t *rows,
-                                 uint32_t *maxlen) {
+                                 uint32_t *maxlen, const uint32_t *period) {
+  if (period && period[0] % period[1]) return;  // not a refresh snapshot
   const uint32_t lane = threadIdx.x & 31;
   for (uint32_t v0 = blockIdx.x * blockDim.x + threadIdx.x - lane; v0 < n;
        v0 += gridDim.x * blockDim.x) {  // warp-uniform
@@ -426,10 +427,39 @@ size_t mlp_grad_smem() {
   return sizeof(float) * (POLICY_PARAMS + TS * F + 2 * TS * HP + TS);
 }
 
+// Clears the row-layout features on refresh snapshots (period[0] % period[1]
+// == 0); the refresh decision is read on the device so it survives graph
+// replay.
+__global__ void page_rows_clear_kernel(uint32_t *rows, uint32_t *maxlen, uint32_t npages,
+                                       const uint32_t *period) {
+  if (period[0] % period[1]) return;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npages;
+       p += gridDim.x * blockDim.x) {
+    rows[p] = 0;
+    maxlen[p] = 0;
+  }
+}
+
+__global__ void period_step_kernel(uint32_t *period) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) period[0]++;
+}
+
 cudaError_t launch_page_rows(const u64 *off, const uint32_t *len, uint32_t n, uint32_t page_base,
                              uint32_t page_shift, uint32_t *rows, uint32_t *maxlen,
-                             cudaStream_t s) {
-  page_rows_kernel<<<grid_for(n), BLOCK, 0, s>>>(off, len, n, page_base, page_shift, rows, maxlen);
+                             const uint32_t *period, cudaStream_t s) {
+  page_rows_kernel<<<grid_for(n), BLOCK, 0, s>>>(off, len, n, page_base, page_shift, rows, maxlen,
+                                                 period);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_page_rows_clear(uint32_t *rows, uint32_t *maxlen, uint32_t npages,
+                                   const uint32_t *period, cudaStream_t s) {
+  page_rows_clear_kernel<<<grid_for(npages), BLOCK, 0, s>>>(rows, maxlen, npages, period);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_period_step(uint32_t *period, cudaStream_t s) {
+  period_step_kernel<<<1, 32, 0, s>>>(period);
   return cudaGetLastError();
 }
 

@@ -55,6 +55,11 @@ _STAT_TAIL = ["mutate_link_bytes", "mutate_hbm_bytes"]
 _STAT_PHASE = ["ms_phase_invalidate", "ms_phase_pull", "ms_phase_seed", "ms_phase_closure"]
 
 
+# Bytes of the engine's per-snapshot device control block, which every
+# snapshot call reads back to the host (static_assert in csrc/common.cuh).
+CTL_BYTES = 2360
+
+
 class BatchStats(ctypes.Structure):
     _fields_ = ([(k, ctypes.c_uint64) for k in _STAT_U64] + [(k, ctypes.c_double) for k in _STAT_F64]
                 + [(k, ctypes.c_uint64) for k in _STAT_TAIL]
@@ -66,7 +71,8 @@ class BatchStats(ctypes.Structure):
 
 class QueryMapping(ctypes.Structure):
     _fields_ = [("qratio", ctypes.c_uint32), ("heavy", ctypes.c_uint32), ("tile", ctypes.c_uint32),
-                ("pull_qratio", ctypes.c_uint32), ("repair_ms", ctypes.c_float)]
+                ("pull_qratio", ctypes.c_uint32), ("queue", ctypes.c_uint32),
+                ("repair_ms", ctypes.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -153,6 +159,7 @@ def lib():
         "dycg_group_updates_noalloc": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
         "dycg_set_queries": (I, [P, u32p, u32, u32]),
         "dycg_set_query_mapping": (I, [P, u32, u32, u32]),
+        "dycg_set_query_queue": (I, [P, u32]),
         "dycg_gather_query": (I, [P, u32, u32p, u32p]),
         "dycg_set_cache_policy": (I, [P, u32]),
         "dycg_policy_trace": (I, [P, u32]),
@@ -613,6 +620,16 @@ class Engine:
         slots; rows above `heavy` warp iterations are tiled (tile slots)."""
         self._check(lib().dycg_set_query_mapping(self._h, qratio, heavy, tile),
                     "set_query_mapping")
+
+    QUEUE_SCHEMES = {"static": 0, "claimed": 1}
+
+    def set_query_queue(self, scheme="static"):
+        """Batched form's frontier-queue scheme (speed only): "static" (warp w
+        takes items w, w + warps, ...) or "claimed" (warps claim items one at
+        a time)."""
+        self._check(lib().dycg_set_query_queue(
+            self._h, self.QUEUE_SCHEMES[scheme] if isinstance(scheme, str) else int(scheme)),
+            "set_query_queue")
 
     def gather_query(self, q):
         v = np.empty(self.n, np.uint32)

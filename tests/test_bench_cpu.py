@@ -5,6 +5,7 @@ import json
 import os
 import subprocess
 import sys
+import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -58,7 +59,8 @@ def test_reference_arm_batched_form_charges_every_query():
               "--batch-max", "5000", "--steps", "3", "--warmup", "3"])
     assert p.returncode == 0, p.stderr[-2000:]
     d = json.loads([ln for ln in p.stdout.splitlines() if ln.startswith("{")][-1])
-    assert d["value"] > 0 and d["metric"].endswith("all 8 queries repaired per snapshot")
+    import bench
+    assert d["value"] > 0 and d["metric"] == bench.METRIC_HEADLINE
     assert "charged 8 times" in d["cpu_baseline"]["sample"] and d["steps"] == 3
 
 
@@ -141,7 +143,7 @@ def test_grid_snapshots_mix_grid_edges_and_shortcuts():
     side = 256
     n, off, dst, w = oracle.grid_csr(side, 10, 8, 11, 1, 1000)
     nd, na, nb = 100, 100, 3
-    batches = bench.make_batches(8, nb, nd, na, 5, bench._cpu_sampler(off, dst, w), "grid", 1000)
+    batches = bench.make_batches(8, nb, nd, na, 5, bench._engine_sampler(off, dst, w), "grid", 1000)
     live = set((np.repeat(np.arange(n), np.diff(off.astype(np.int64))) * n + dst).tolist())
     seen = set()
     for d, a in batches:
@@ -161,12 +163,13 @@ def test_grid_snapshots_mix_grid_edges_and_shortcuts():
 
 def test_link_transaction_bound():
     import bench
-    b = bench.link_transaction_bound(4_150_000, 0.98)
+    b = bench.link_transaction_bound(4_150_000, 0.98, 14.0)
     assert b["min_transactions"] == 32_422  # ceil(4.15 MB / 128 B)
     assert abs(b["bound_ms"] - 32_422 * 14e-6) < 1e-3 and 0 < b["frac"] < 1
-    assert bench.link_transaction_bound(0, 1.0)["min_transactions"] == 0
-    assert bench.link_transaction_bound(-5.0, 1.0)["bound_ms"] == 0
-    assert bench.link_transaction_bound(1000, 0)["frac"] is None
+    assert b["ns_per_transaction"] == 14.0
+    assert bench.link_transaction_bound(0, 1.0, 14.0)["min_transactions"] == 0
+    assert bench.link_transaction_bound(-5.0, 1.0, 14.0)["bound_ms"] == 0
+    assert bench.link_transaction_bound(1000, 0, 14.0)["frac"] is None
 
 
 def test_rmat_snapshots_are_disjoint_live_deletions_and_rmat_insertions():
@@ -175,7 +178,7 @@ def test_rmat_snapshots_are_disjoint_live_deletions_and_rmat_insertions():
     import oracle
     n, off, dst, w = oracle.rmat_csr(12, 8, 4)
     nd, na, nb = 200, 150, 4
-    batches = bench.make_batches(12, nb, nd, na, 9, bench._cpu_sampler(off, dst, w), "rmat26",
+    batches = bench.make_batches(12, nb, nd, na, 9, bench._engine_sampler(off, dst, w), "rmat26",
                                  rmat_fn=oracle.gen_rmat_edges)
     src = np.repeat(np.arange(n), np.diff(off.astype(np.int64)))
     live = set((src * n + dst).tolist())
@@ -210,3 +213,27 @@ def test_clock_samples_inside_the_timed_region_give_median_and_reasons():
     out = c.stop()
     assert out["sm_mhz"] == 1965.0 and out["sm_max_mhz"] == 1965.0
     assert out["reasons"] == ["sw_power_cap"] and out["samples_inside_timed_region"] == 3
+
+
+def test_engine_sampler_restatement():
+    """The reference arm's restatement of the engine's edge sampler draws
+    distinct live edges of the CSR, deterministically per seed, in the
+    engine's order of draws (counter hash, first occurrences kept)."""
+    import bench
+    import oracle
+    n, off, dst, w = oracle.rmat_csr(10, 8, 3, wlo=1, whi=64, with_w=True)
+    smp = bench._engine_sampler(off, dst, w)
+    a = smp(3000, 77)
+    assert a.shape == (3000, 3)
+    assert np.array_equal(a, smp(3000, 77)) and not np.array_equal(a, smp(3000, 78))
+    keys = a[:, 0].astype(np.uint64) << np.uint64(32) | a[:, 1].astype(np.uint64)
+    assert len(np.unique(keys)) == 3000  # distinct (the graph has no parallel edges)
+    for u, v, ww in a[:200]:
+        row = dst[off[u]:off[u + 1]]
+        k = np.searchsorted(row, v)
+        assert row[k] == v and w[int(off[u]) + int(k)] == ww
+    # the first draws are the hash of the draw index, as in the engine
+    total = np.uint64(len(dst))
+    s0 = bench._mix64(np.uint64(77))
+    r0 = int(bench._mix64(s0 ^ bench._mix64(np.uint64(0xA24BAED4963EE407))) % total)
+    assert a[0, 0] == np.searchsorted(off, r0, side="right") - 1 and a[0, 1] == dst[r0]

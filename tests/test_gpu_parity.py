@@ -266,6 +266,72 @@ def test_random_pr_fused():
     _assert_pr_close(x, r, oracle.static_pr(n, cur_off, cur_dst))
 
 
+def _pr_reference_check(x, r, off, dst, eps, alpha=0.85):
+    """The reference's own PageRank acceptance check (samples/hybrid_pr/
+    hybrid_pr_host.cu:9-54) restated in float64: an independent Jacobi fixed
+    point of x = 0.15 + 0.85 P^T x; the L1 error of the ranks must stay within
+    (n*eps + roundoff) / 0.15 (substochastic P: |x - x*|_1 <= |r|_1 / (1 - alpha)),
+    the invariant x + r = 0.15 + 0.85 P^T x must hold within roundoff, and
+    every residual must be at most eps (in float32). Returns its figures and
+    the same errors on the normalised scale (ranks / n)."""
+    n = len(x)
+    ref = oracle.static_pr(n, off, dst, alpha=alpha)
+    xd, rd = x.astype(np.float64), r.astype(np.float64)
+    src = np.repeat(np.arange(n), np.diff(off).astype(np.int64))
+    deg = np.diff(off).astype(np.float64)
+    nxt = np.full(n, 1.0 - alpha)
+    np.add.at(nxt, dst.astype(np.int64), alpha * xd[src] / deg[src])
+    err = np.abs(xd - ref)
+    mass = float(np.sum(np.abs(ref)))
+    roundoff = 64 * float(np.finfo(np.float32).eps) * max(1.0, mass)
+    out = {"l1_error": float(err.sum()), "bound": (n * eps + roundoff) / (1 - alpha),
+           "max_error": float(err.max()), "invariant_l1": float(np.abs(nxt - xd - rd).sum()),
+           "max_residual": float(np.abs(rd).max()), "roundoff": roundoff,
+           "max_error_normalized": float(err.max()) / n, "l1_error_normalized": float(err.sum()) / n}
+    out["ok"] = (bool(np.isfinite(xd).all() and np.isfinite(rd).all() and (xd >= -eps).all())
+                 and out["l1_error"] <= out["bound"] and out["invariant_l1"] <= roundoff
+                 and out["max_residual"] <= float(np.float32(eps)))
+    return out
+
+
+def _pr_run(eps, scale=12, seed=23, batches=3):
+    n, off, dst, _ = cases.small_rmat(scale, 8, seed)
+    e = engine_for("pr", n, off, dst, epsilon=eps, max_rounds=100000)
+    orc = oracle.Oracle(oracle.PR, n, off, dst)
+    cur_off, cur_dst = off, dst
+    for bi in range(batches):
+        dels, adds = cases.random_batch(n, cur_off, cur_dst, None, 300, 300, 700 + bi)
+        e.apply_batch(dels, adds)
+        orc.mutate(dels, adds)
+        cur_off, cur_dst, _ = orc.csr()
+    x, r = e.gather_ranks()
+    e.close()
+    return _pr_reference_check(x, r, cur_off, cur_dst, eps)
+
+
+def test_pr_reference_acceptance_at_epsilon_1e4():
+    """Reference-parity mode at the configurations' threshold (epsilon 1e-4):
+    the reference's own acceptance check passes, and the error is reported."""
+    c = _pr_run(1e-4)
+    print(f"[PR-CHECK] epsilon=1e-4 {c}")
+    assert c["ok"], c
+    # on the normalised scale (ranks / n) the bound is epsilon / 0.15
+    assert c["l1_error_normalized"] <= 1e-4 / 0.15 + c["roundoff"] / (0.15 * 4096), c
+
+
+def test_pr_normalised_max_abs_within_1e6():
+    """Acceptance on the normalised scale (ranks / n, which sum to at most 1):
+    with the push threshold scaled so that the L1 bound n*eps/0.15/n = eps/0.15
+    is at most 1e-6 (eps = 1.5e-7), the FP32 ranks are within max-abs 1e-6 of
+    the FP64 oracle (and within L1 1e-6 plus the FP32 roundoff allowance)."""
+    eps = 1.5e-7
+    c = _pr_run(eps)
+    print(f"[PR-CHECK] epsilon=1.5e-7 {c}")
+    assert c["ok"], c
+    assert c["max_error_normalized"] <= 1e-6, c
+    assert c["l1_error_normalized"] <= 1e-6 + c["roundoff"] / (0.15 * 4096), c
+
+
 # ---- edge cases ---------------------------------------------------------------
 
 def test_empty_batches_and_invalid_ids():

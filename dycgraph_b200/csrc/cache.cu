@@ -176,11 +176,15 @@ size_t cache_temp_bytes(uint32_t npages) {
   return a > b ? a : b;
 }
 
-cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t gate, uint32_t cap,
-                        uint32_t *page_slot, uint32_t *free_list, const CachePages &pg,
-                        u64 *stat_loaded, u64 *stat_evicted, cudaStream_t s) {
+cudaError_t cache_plan(CacheWork &W, uint32_t npages, uint32_t gate, uint32_t cap,
+                       u64 *stat_loaded, u64 *stat_evicted, cudaStream_t s) {
   plan_kernel<<<1, 32, 0, s>>>(W.sa, W.fa, W.se, W.fe, npages, gate, cap, W.plan, stat_loaded,
                                stat_evicted);
+  return cudaGetLastError();
+}
+
+cudaError_t cache_stage(CacheWork &W, uint32_t npages, uint32_t *page_slot, uint32_t *free_list,
+                        const CachePages &pg, cudaStream_t s) {
   evict_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, npages, W.fe, W.se, W.plan,
                                                   page_slot, free_list);
   admit_list_kernel<<<grid_for(npages), BLOCK, 0, s>>>(W.ids_sorted, npages, W.fa, W.sa, W.plan,
@@ -188,6 +192,14 @@ cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t gate, uint32_t c
   fill_kernel<<<148 * 8, BLOCK, 0, s>>>(W.admit, W.plan, free_list, page_slot, pg.h_out, pg.h_in,
                                         pg.pages_out, pg.page_shift, pg.stride, pg.cdst);
   return cudaGetLastError();
+}
+
+cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t gate, uint32_t cap,
+                        uint32_t *page_slot, uint32_t *free_list, const CachePages &pg,
+                        u64 *stat_loaded, u64 *stat_evicted, cudaStream_t s) {
+  cudaError_t e = cache_plan(W, npages, gate, cap, stat_loaded, stat_evicted, s);
+  if (e != cudaSuccess) return e;
+  return cache_stage(W, npages, page_slot, free_list, pg, s);
 }
 
 }  // namespace dycg

@@ -17,10 +17,14 @@ struct dycg_engine {
 
 namespace {
 
+// Runs f on the engine and turns exceptions into status codes. join: the
+// engine stream first waits for side-stream page staging of an earlier call;
+// the snapshot calls pass false and join after their ingest instead.
 template <class F>
-int guard(dycg_engine *e, F &&f) {
+int guard(dycg_engine *e, F &&f, bool join = true) {
   if (!e || !e->impl) return DYCG_EINVAL;
   try {
+    if (join) e->impl->join();
     f(*e->impl);
     return DYCG_OK;
   } catch (const Error &x) {
@@ -114,11 +118,11 @@ int dycg_init(dycg_engine *e) {
 }
 
 int dycg_delete_edges(dycg_engine *e, const dycg_edge *dels, size_t nd, dycg_batch_stats *stats) {
-  return guard(e, [&](Engine &g) { g.apply(dels, nd, nullptr, 0, false, 1, false, stats); });
+  return guard(e, [&](Engine &g) { g.apply(dels, nd, nullptr, 0, false, 1, false, stats); }, false);
 }
 
 int dycg_insert_edges(dycg_engine *e, const dycg_edge *adds, size_t na, dycg_batch_stats *stats) {
-  return guard(e, [&](Engine &g) { g.apply(nullptr, 0, adds, na, false, 2, false, stats); });
+  return guard(e, [&](Engine &g) { g.apply(nullptr, 0, adds, na, false, 2, false, stats); }, false);
 }
 
 int dycg_cache_maintenance(dycg_engine *e, dycg_batch_stats *stats) {
@@ -131,12 +135,12 @@ int dycg_reserve_batch(dycg_engine *e, size_t max_records) {
 
 int dycg_apply_batch(dycg_engine *e, const dycg_edge *dels, size_t nd, const dycg_edge *adds,
                      size_t na, dycg_batch_stats *stats) {
-  return guard(e, [&](Engine &g) { g.apply(dels, nd, adds, na, false, 0, true, stats); });
+  return guard(e, [&](Engine &g) { g.apply(dels, nd, adds, na, false, 0, true, stats); }, false);
 }
 
 int dycg_apply_batch_device(dycg_engine *e, const dycg_edge *d_dels, size_t nd,
                             const dycg_edge *d_adds, size_t na, dycg_batch_stats *stats) {
-  return guard(e, [&](Engine &g) { g.apply(d_dels, nd, d_adds, na, true, 0, true, stats); });
+  return guard(e, [&](Engine &g) { g.apply(d_dels, nd, d_adds, na, true, 0, true, stats); }, false);
 }
 
 int dycg_gather(dycg_engine *e, uint32_t *values, uint32_t *parents) {

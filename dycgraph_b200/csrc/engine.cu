@@ -53,14 +53,19 @@ Engine::Engine(const dycg_options &opt) : opt_(opt) {
   CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev_));
   if (!coop) throw Error(DYCG_ENOGPU, "device lacks cooperative launch");
   CK(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&fst_, cudaStreamNonBlocking));
   for (auto &e : ev_) CK(cudaEventCreate(&e));
+  for (auto &e : fev_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   if (opt_.cache_policy > DYCG_CACHE_LEARNED) throw Error(DYCG_EINVAL, "unknown cache policy");
+  if (opt_.frontier_queue > DYCG_QUEUE_CLAIMED)
+    throw Error(DYCG_EINVAL, "unknown frontier-queue scheme");
   policy_ = opt_.cache_policy;
   stored_ = opt_.algo == DYCG_ALGO_SSSP && opt_.weight_mode == DYCG_WEIGHT_STORED;
   has_in_ = !opt_.symmetric && opt_.algo != DYCG_ALGO_PR;
 }
 
 Engine::~Engine() {
+  if (fst_) cudaStreamSynchronize(fst_);
   if (st_) cudaStreamSynchronize(st_);
   drop_graphs();
   for (cudaEvent_t e : bev_) cudaEventDestroy(e);
@@ -78,7 +83,16 @@ Engine::~Engine() {
   for (void *p : hallocs_) cudaFreeHost(p);
   for (auto &e : ev_)
     if (e) cudaEventDestroy(e);
+  for (auto &e : fev_)
+    if (e) cudaEventDestroy(e);
+  if (fst_) cudaStreamDestroy(fst_);
   if (st_) cudaStreamDestroy(st_);
+}
+
+void Engine::join_staging() {
+  if (!staging_) return;
+  CK(cudaStreamWaitEvent(st_, fev_[1], 0));
+  staging_ = false;
 }
 
 void *Engine::dmalloc(size_t bytes) {
@@ -559,6 +573,7 @@ void Engine::init() {
     L.algo = opt_.algo;
     L.stored = stored_;
     L.num_sms = num_sms_;
+    L.sched = opt_.frontier_queue;
     CK(launch_repair(L, st_));
     launches_ += 2;
   }
@@ -766,6 +781,9 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
     launches_ += (nd ? 1 : 0) + (na ? 1 : 0);
   }
   if (!capture) CK(cudaEventRecord(ev_[1], st_));
+  // the previous call's page staging (side stream) ends before this snapshot
+  // reads or writes adjacency (a capture begins only after a join)
+  if (!capture) join_staging();
   const u64 timeout = 60ull * 1000000000ull;
   PrLaunch PL{};
   if (opt_.algo == DYCG_ALGO_PR) {
@@ -857,6 +875,7 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
     L.algo = opt_.algo;
     L.stored = stored_;
     L.num_sms = num_sms_;
+    L.sched = opt_.frontier_queue;
     CK(launch_repair(L, st_));
     launches_++;
   }
@@ -1160,6 +1179,7 @@ void Engine::init_queries(u64 timeout) {
     L.algo = opt_.algo;
     L.stored = stored_;
     L.num_sms = num_sms_;
+    L.sched = opt_.frontier_queue;
     CK(launch_repair(L, st_));
     launches_ += 2;
   }
@@ -1213,6 +1233,7 @@ void Engine::repair_queries(uint32_t nd, uint32_t na, u64 timeout) {
     L.algo = opt_.algo;
     L.stored = stored_;
     L.num_sms = num_sms_;
+    L.sched = opt_.frontier_queue;
     CK(launch_repair(L, st_));
     launches_++;
   }
@@ -1351,6 +1372,7 @@ void Engine::drop_graphs() {
 const Engine::SnapshotGraph &Engine::graph_for(uint32_t cls) {
   auto it = graphs_.find(cls);
   if (it != graphs_.end()) return it->second;
+  join_staging();
   cudaGraph_t g = nullptr;
   const uint64_t l0 = launches_;
   CK(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
@@ -1783,7 +1805,9 @@ void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
     return;
   }
   CK(cudaEventRecord(ev_[4], st_));
-  hotness_round(initial);
+  // the staging (eviction, fills) of a later round runs on the side stream,
+  // hidden behind the next snapshot's record staging and ingest
+  hotness_round(initial, !initial);
   CK(cudaEventRecord(ev_[5], st_));
   CK(cudaMemcpyAsync(cwk_.h_plan, cwk_.plan, sizeof(CachePlan), cudaMemcpyDeviceToHost, st_));
   sync_check("cache apply");
@@ -1805,15 +1829,25 @@ void Engine::cache_maintenance(bool initial, dycg_batch_stats *stats) {
 // kMinScore times (decayed) before it displaces a resident one, so single
 // random probes do not churn the cache; the initial load admits the whole
 // top K.
-void Engine::hotness_round(bool initial) {
+void Engine::hotness_round(bool initial, bool side) {
   const float kMinScore = initial ? 0.f : 64.f;
   CK(cache_rank(cwk_, npages_, cache_slots_, 0.75f, kMinScore, page_slot_, st_));
   const uint32_t gate = initial ? 1u : std::max<uint32_t>(1u, cache_slots_ / 1024);
   const uint32_t cap = initial ? cache_slots_ : std::max<uint32_t>(cache_slots_ / 512, 64u);
   CachePages pg{out_.d_dst, has_in_ ? in_.d_dst : nullptr, out_.pages, page_shift_, out_.stride,
                 cdst_};
-  CK(cache_apply(cwk_, npages_, gate, cap, page_slot_, free_list_, pg,
-                 &ctl_->stat[ST_PAGES_LOADED], &ctl_->stat[ST_PAGES_EVICTED], st_));
+  CK(cache_plan(cwk_, npages_, gate, cap, &ctl_->stat[ST_PAGES_LOADED],
+                &ctl_->stat[ST_PAGES_EVICTED], st_));
+  if (side) {
+    // staging on the side stream, after the plan; the engine stream goes on
+    CK(cudaEventRecord(fev_[0], st_));
+    CK(cudaStreamWaitEvent(fst_, fev_[0], 0));
+    CK(cache_stage(cwk_, npages_, page_slot_, free_list_, pg, fst_));
+    CK(cudaEventRecord(fev_[1], fst_));
+    staging_ = true;
+  } else {
+    CK(cache_stage(cwk_, npages_, page_slot_, free_list_, pg, st_));
+  }
   launches_ += 9;
 }
 

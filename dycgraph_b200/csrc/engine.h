@@ -85,6 +85,9 @@ class Engine {
   void policy_set_params(const float *in);
   void sample_row_edges(const uint32_t *sources, uint64_t count, uint64_t seed, dycg_edge *out);
   cudaStream_t stream() const { return st_; }
+  // make the engine stream wait for side-stream page staging (every call
+  // that reads adjacency or the page table starts with this)
+  void join() { join_staging(); }
 
   std::string last_error;
   bool failed = false;
@@ -114,7 +117,8 @@ class Engine {
                         const uint32_t *n_ptr, uint32_t nd, uint32_t *found, int count_missing,
                         bool capture);
   void policy_prefetch(size_t nd, size_t na, bool capture);
-  void hotness_round(bool initial);
+  void hotness_round(bool initial, bool side = false);
+  void join_staging();
   void maintenance_device();
   void init_queries(u64 timeout);
   void repair_queries(uint32_t nd, uint32_t na, u64 timeout);
@@ -126,6 +130,12 @@ class Engine {
   int dev_ = 0, num_sms_ = 148;
   cudaStream_t st_ = nullptr;
   cudaEvent_t ev_[6] = {};
+  // side stream of the hotness path's page staging (eviction, admission list,
+  // fills), overlapped with the next call's staging and ingest; joined
+  // before anything reads the page table or the cached pages again
+  cudaStream_t fst_ = nullptr;
+  cudaEvent_t fev_[2] = {};
+  bool staging_ = false;
   uint32_t n_ = 0;
   bool loaded_ = false, inited_ = false, has_in_ = false, stored_ = false;
   Arena out_, in_;

@@ -186,15 +186,30 @@ struct Tiles {
 // Expand the rows of items[0..cnt) over adjacency A. Ends with a grid barrier
 // that also applies `reset_flags` (with the tile reset). Returns false when
 // the launch has failed (error flag set).
+// Items are taken statically (warp w: items w, w + warps, ...) or, with
+// `claimed`, one at a time from the control block's claim counter (reset by
+// the barriers that end the phase), so a warp that drew long rows does not
+// hold the wave's barrier while the others idle.
 template <bool WITH_W, class Op>
 __device__ bool expand_rows(const Adj &A, const uint32_t *items, uint32_t cnt, Op &op,
                             Acc &acc, Tiles T, Ctl *ctl, uint32_t reset_flags,
-                            u64 timeout_ns) {
+                            u64 timeout_ns, bool claimed = false) {
   const uint32_t lane = lane_id();
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t i = gw; i < cnt; i += nw) {
+  uint32_t i = gw;
+  if (claimed) {
+    if (lane == 0) i = atomicAdd(&ctl->grab, 1u);
+    i = __shfl_sync(0xffffffffu, i, 0);
+  }
+  while (i < cnt) {
     const uint32_t v = items[i];
+    if (claimed) {
+      if (lane == 0) i = atomicAdd(&ctl->grab, 1u);
+      i = __shfl_sync(0xffffffffu, i, 0);
+    } else {
+      i += nw;
+    }
     const uint32_t len = A.len[v];
     if (len > HEAVY) {
       if (lane == 0) {
@@ -214,15 +229,30 @@ __device__ bool expand_rows(const Adj &A, const uint32_t *items, uint32_t cnt, O
   // The items have been consumed: the queue resets can apply here. When no row
   // was heavy this barrier's snapshot already holds every append of the
   // expansion and the tile phase (and its barrier) is skipped.
-  if (!grid_sync(ctl, reset_flags, timeout_ns)) return false;
+  if (!grid_sync(ctl, reset_flags | SYNC_RESET_GRAB, timeout_ns)) return false;
   const uint32_t nt = min(*(volatile uint32_t *)&ctl->snap_tiles, T.cap);
   if (nt == 0) return true;
   const uint32_t wib = threadIdx.x >> 5;
-  for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
+  __shared__ uint32_t s_tile;
+  uint32_t t = blockIdx.x;
+  if (claimed) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(&ctl->grab, 1u);
+    __syncthreads();
+    t = s_tile;
+  }
+  while (t < nt) {
     const uint4 tl = T.tiles[t];
+    if (claimed) {
+      __syncthreads();  // every warp has read s_tile
+      if (threadIdx.x == 0) s_tile = atomicAdd(&ctl->grab, 1u);
+      __syncthreads();
+      t = s_tile;
+    } else {
+      t += gridDim.x;
+    }
     warp_slots<WITH_W>(A, tl.x, A.off[tl.x], tl.y + wib * 32, tl.z, blockDim.x, op, acc);
   }
-  return grid_sync(ctl, SYNC_RESET_TILES, timeout_ns);
+  return grid_sync(ctl, SYNC_RESET_TILES | SYNC_RESET_GRAB, timeout_ns);
 }
 
 __device__ __forceinline__ u64 ld_key(const u64 *p) {

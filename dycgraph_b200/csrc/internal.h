@@ -36,6 +36,7 @@ struct RepairLaunch {
   uint32_t algo;
   bool stored;
   int num_sms;
+  uint32_t sched;     // frontier items: 0 static, 1 claimed one at a time
 };
 cudaError_t launch_repair(const RepairLaunch &L, cudaStream_t s);
 cudaError_t launch_init_state(uint32_t algo, u64 *key, uint32_t n, uint32_t source,
@@ -208,7 +209,13 @@ size_t cache_temp_bytes(uint32_t npages);
 cudaError_t cache_rank(CacheWork &W, uint32_t npages, uint32_t K, float decay, float min_score,
                        const uint32_t *page_slot, cudaStream_t s);
 // plan (refresh gate, at most cap admissions), evict, stage; admissions and
-// evictions are also added to the optional device counters
+// evictions are also added to the optional device counters. cache_plan and
+// cache_stage are its two halves (the staging may run on another stream,
+// ordered after the plan).
+cudaError_t cache_plan(CacheWork &W, uint32_t npages, uint32_t gate, uint32_t cap,
+                       u64 *stat_loaded, u64 *stat_evicted, cudaStream_t s);
+cudaError_t cache_stage(CacheWork &W, uint32_t npages, uint32_t *page_slot, uint32_t *free_list,
+                        const CachePages &pg, cudaStream_t s);
 cudaError_t cache_apply(CacheWork &W, uint32_t npages, uint32_t gate, uint32_t cap,
                         uint32_t *page_slot, uint32_t *free_list, const CachePages &pg,
                         u64 *stat_loaded, u64 *stat_evicted, cudaStream_t s);

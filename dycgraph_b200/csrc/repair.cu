@@ -49,6 +49,7 @@ struct RepairParams {
   uint32_t *tag_dev;        // non-null: wave tags start at *tag_dev, which the
                             // launch advances past the tags it used
   u64 timeout_ns;
+  bool claimed;             // waves' items claimed one at a time (else static)
 };
 
 template <uint32_t ALGO>
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
         if (hi == lo) break;
         InvalidateOp<ALGO> op{&P};
         if (!expand_rows<false>(P.out, P.aff + lo, hi - lo, op, acc, P.tiles, ctl, 0,
-                                P.timeout_ns))
+                                P.timeout_ns, P.claimed))
           goto done;
         lo = hi;
       }
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
       if (!grid_sync(ctl, 0, P.timeout_ns)) goto done;
       // 4. pull over incoming rows
       PullOp<ALGO, STORED> op{&P};
-      if (!expand_rows<STORED>(P.in, P.aff, na, op, acc, P.tiles, ctl, 0, P.timeout_ns))
+      if (!expand_rows<STORED>(P.in, P.aff, na, op, acc, P.tiles, ctl, 0, P.timeout_ns, P.claimed))
         goto done;
       // 5a. frontier from affected vertices with a finite value
       for (uint32_t i0 = gtid - lane; i0 < na; i0 += gstride) {
@@ -277,7 +278,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
       const uint32_t nb = *(volatile uint32_t *)&ctl->snap_q[2];
       RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag};
       if (!expand_rows<STORED>(P.out, P.q2, nb, op, acc, P.tiles, ctl, SYNC_RESET_Q2,
-                               P.timeout_ns))
+                               P.timeout_ns, P.claimed))
         goto done;
       if (gtid == 0) ctl->waves = wave + 1;
       cur ^= 1;
@@ -293,7 +294,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
       }
       RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag_base + 1 + wave};
       if (!expand_rows<STORED>(P.out, P.q[cur], cnt, op, acc, P.tiles, ctl,
-                               cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.timeout_ns))
+                               cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.timeout_ns, P.claimed))
         goto done;
       if (gtid == 0) ctl->waves = wave + 1;
       cur ^= 1;
@@ -359,6 +360,7 @@ static cudaError_t launch_one(const RepairLaunch &L, cudaStream_t s) {
   P.q2 = L.q2;
   P.tag_dev = L.tag_dev;
   P.timeout_ns = L.timeout_ns;
+  P.claimed = L.sched != 0;
   static int blocks_per_sm = -1;
   if (blocks_per_sm < 0) {
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(

@@ -99,7 +99,11 @@ typedef struct dycg_options {
   uint32_t arena_headroom_permille; /* spare arena slots for row growth, per   */
                           /* mille of the loaded slots (0: 125, the reference's */
                           /* 1/8; at least 2^20 slots either way)              */
-  uint32_t reserved[5];
+  uint32_t frontier_queue; /* single-source repair: DYCG_QUEUE_STATIC (0) or   */
+                          /* DYCG_QUEUE_CLAIMED, how warps share a wave's rows */
+                          /* (the batched form's scheme is tuned, see          */
+                          /* dycg_tune_query_mapping)                          */
+  uint32_t reserved[4];
 } dycg_options;
 
 /* Per-call counters. Byte counts are algorithmic: every adjacency slot read
@@ -398,12 +402,14 @@ int dycg_tune_query_mapping(dycg_engine *e, const dycg_edge *dels, size_t nd,
  * The records of snapshot i follow those of snapshot i-1: del_counts[i]
  * deletions in dels, add_counts[i] insertions in adds. stats: one entry per
  * snapshot, or NULL. In the batched many-query form each snapshot is one
- * replay of a CUDA graph (ingest, mutation, repair) captured once per batch
- * size class (powers of two >= 1024; records are padded with out-of-range
- * entries that ingest drops), with no host synchronisation between
- * snapshots, and cache maintenance runs once, after the last snapshot;
- * per-stage times are then not split (ms_total per snapshot). Other forms
- * apply the snapshots one by one. */
+ * replay of a CUDA graph (ingest, mutation, learned admission when that
+ * policy is set, repair, cache maintenance) captured once per batch size
+ * class (powers of two >= 1024; records are padded with out-of-range entries
+ * that ingest drops), with no host synchronisation between snapshots; the
+ * admission plan is computed on the device. Per-stage times are then not
+ * split (ms_total per snapshot, ms_repair from the repair kernel's own
+ * stamps). Other forms, and an engine still recording policy traces, apply
+ * the snapshots one by one. */
 int dycg_apply_batches(dycg_engine *e, const dycg_edge *dels, const uint64_t *del_counts,
                        const dycg_edge *adds, const uint64_t *add_counts, uint32_t snapshots,
                        dycg_batch_stats *stats);
@@ -482,7 +488,11 @@ int dycg_mlp_loss_grad(const void *d_x, const float *d_y, uint32_t n, const floa
 int dycg_sample_row_edges(dycg_engine *e, const uint32_t *sources, uint64_t count,
                           uint64_t seed, dycg_edge *out);
 
-/* cudaStream_t the engine launches on (for CUDA-event timing by callers). */
+/* cudaStream_t the engine launches on (for CUDA-event timing by callers).
+ * Like every call other than the snapshot calls, it first makes that stream
+ * wait for the engine's side-stream work of earlier calls (the hotness
+ * policy's page staging), so an event recorded on the stream afterwards
+ * covers all the work of those calls. */
 int dycg_stream(dycg_engine *e, void **stream);
 
 /* Copy of the last error message into buf (always NUL-terminated). */

@@ -136,13 +136,16 @@ struct Ctl {
   uint32_t pad[2];       // PageRank: carried frontier (queue parity, length)
   uint32_t grab;         // claimed-item counter of a phase (reset by its barriers)
   uint32_t pad2;
+  // range-ordered wave queues (batched form): entries per vertex range, per
+  // queue parity (reset with the parity's queue count)
+  uint32_t qrange[2][64];
   u64 stat[20];
   u64 tphase[8];         // batched repair: global timer at phase boundaries (ns)
   // grid-barrier arrival groups, one 128-byte line each (frontier.cuh)
   uint32_t bar_sub[BAR_GROUPS * 32];
 };
 // read back to the host once per snapshot (dycgraph_b200/engine.py CTL_BYTES)
-static_assert(sizeof(Ctl) == 2360, "Ctl layout changed: update CTL_BYTES in engine.py");
+static_assert(sizeof(Ctl) == 2872, "Ctl layout changed: update CTL_BYTES in engine.py");
 
 enum StatIdx {
   ST_LINK_BYTES = 0,

@@ -276,8 +276,10 @@ void Engine::finish_load() {
   wtag_ = (uint32_t *)dmalloc((n + 1ull) * 4);
   touch_ = (uint32_t *)dmalloc((n + 1ull) * 4);
   aff_ = (uint32_t *)dmalloc((n + 1ull) * 4);
-  q0_ = (uint32_t *)dmalloc((n + 1ull) * 4);
-  q1_ = (uint32_t *)dmalloc((n + 1ull) * 4);
+  // wave queues: n + 64 entries, enough for the batched form's 64
+  // range-ordered regions of ceil(n / 64) entries each
+  q0_ = (uint32_t *)dmalloc((n + 64ull) * 4);
+  q1_ = (uint32_t *)dmalloc((n + 64ull) * 4);
   q2_ = opt_.ordered_delta ? (uint32_t *)dmalloc((n + 1ull) * 4) : nullptr;
   CK(cudaMemsetAsync(mark_, 0, (n + 1ull) * 4, st_));
   CK(cudaMemsetAsync(wtag_, 0, (n + 1ull) * 4, st_));
@@ -1080,7 +1082,7 @@ void Engine::set_query_mapping(uint32_t qratio, uint32_t heavy, uint32_t tile) {
 }
 
 void Engine::set_query_queue(uint32_t scheme) {
-  if (scheme != DYCG_QUEUE_STATIC && scheme != DYCG_QUEUE_CLAIMED)
+  if (scheme > (DYCG_QUEUE_CLAIMED | DYCG_QUEUE_RANGES))
     throw Error(DYCG_EINVAL, "unknown frontier-queue scheme");
   sched_ = scheme;
   drop_graphs();  // captured graphs hold the old scheme
@@ -1140,7 +1142,8 @@ static RepairLaunch query_launch(const Adj &out, const Adj &in, u64 *key, uint32
 // Static solve of every query.
 void Engine::init_queries(u64 timeout) {
   if (qmode_ == DYCG_QUERIES_BATCHED) {
-    CK(launch_multi_init(qkey_, n_, qnb_, d_sources_, nmask_[0], q0_, wtag_, seq_, ctl_, st_));
+    CK(launch_multi_init(qkey_, n_, qnb_, d_sources_, nmask_[0], q0_, wtag_, seq_, ctl_, sched_,
+                         st_));
     CK(launch_multi(multi_launch(PH_CLOSE, 0, timeout), st_));
     launches_ += 3;
     CK(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(Ctl), cudaMemcpyDeviceToHost, st_));
@@ -1330,7 +1333,8 @@ void Engine::tune_repair(uint32_t nd, uint32_t na, u64 timeout) {
   for (uint32_t t : kTile)
     if (t != second.tile) trial(second.qratio, second.heavy, second.pull_qratio, t, sched0);
   const dycg_query_mapping third = best;
-  for (uint32_t q : {DYCG_QUEUE_STATIC, DYCG_QUEUE_CLAIMED})
+  for (uint32_t q : {DYCG_QUEUE_STATIC, DYCG_QUEUE_CLAIMED, DYCG_QUEUE_RANGES,
+                     DYCG_QUEUE_CLAIMED | DYCG_QUEUE_RANGES})
     if (q != third.queue) trial(third.qratio, third.heavy, third.pull_qratio, third.tile, q);
   restore();
   qratio_ = best.qratio;

@@ -51,8 +51,14 @@ __device__ __forceinline__ bool grid_sync(Ctl *c, uint32_t flags, u64 timeout_ns
     int ok = 1;
     if (last) {
       if (flags & SYNC_RESET_TILES) c->tile_count = 0;
-      if (flags & SYNC_RESET_Q0) c->q_count[0] = 0;
-      if (flags & SYNC_RESET_Q1) c->q_count[1] = 0;
+      if (flags & SYNC_RESET_Q0) {
+        c->q_count[0] = 0;
+        for (int b = 0; b < 64; b++) c->qrange[0][b] = 0;
+      }
+      if (flags & SYNC_RESET_Q1) {
+        c->q_count[1] = 0;
+        for (int b = 0; b < 64; b++) c->qrange[1][b] = 0;
+      }
       if (flags & SYNC_RESET_Q2) c->q_count[2] = 0;
       if (flags & SYNC_RESET_GRAB) c->grab = 0;
       c->snap_aff = *(volatile uint32_t *)&c->n_aff;

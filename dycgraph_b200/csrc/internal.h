@@ -64,7 +64,8 @@ struct MultiLaunch {
   uint32_t pull_qratio;         // the same rule for the pull phase
   uint32_t heavy;               // rows with more work (warp iterations) are tiled
   uint32_t tile;                // tile size, in slots
-  uint32_t sched;               // item distribution: 0 static, 1 claimed one at a time
+  uint32_t sched;               // frontier-queue scheme (DYCG_QUEUE_* bits): claimed items,
+                                // range-ordered wave queues
   u64 timeout_ns;
   uint32_t algo;
   bool stored;
@@ -73,7 +74,7 @@ struct MultiLaunch {
 cudaError_t launch_multi(const MultiLaunch &L, cudaStream_t s);
 cudaError_t launch_multi_init(u64 *key, uint32_t n, uint32_t nb, const uint32_t *sources,
                               uint32_t *nmask0, uint32_t *q0, uint32_t *wtag, const uint32_t *seq,
-                              Ctl *ctl, cudaStream_t s);
+                              Ctl *ctl, uint32_t sched, cudaStream_t s);
 // values/parents of query q out of the vertex-major (Q = 32*nb) or
 // query-major (Q = 0: key already offset to the query) key array
 cudaError_t launch_multi_gather(const u64 *key, uint32_t n, uint32_t Q, uint32_t q,

@@ -35,6 +35,7 @@
 namespace dycg {
 
 constexpr uint32_t WARPS = BLOCK / 32;
+constexpr uint32_t QRANGES = 64;  // vertex ranges of a range-ordered wave queue
 
 struct MultiParams {
   Adj out, in;
@@ -56,7 +57,9 @@ struct MultiParams {
   const uint3 *add_uvw;
   uint32_t n_add;
   uint32_t n, phases, max_waves, qratio, pull_qratio, heavy, tile;
-  uint32_t sched;  // item distribution: 0 static, 1 claimed (dycg_query_mapping.queue)
+  uint32_t sched;   // item distribution: 0 static, 1 claimed (dycg_query_mapping.queue bit 0)
+  bool ranges;      // wave queues ordered by vertex range (dycg_query_mapping.queue bit 1)
+  uint32_t rsize;   // vertices per range: ceil(n / QRANGES)
   u64 timeout_ns;
 };
 
@@ -93,12 +96,26 @@ __device__ __forceinline__ bool lower_key(u64 *addr, u64 cand) {
   return lower_from<STRICT>(addr, cand, ldk(addr));
 }
 
-__device__ __forceinline__ void enqueue_once(const MultiParams &P, uint32_t *q, uint32_t *count,
-                                             uint32_t y, uint32_t tag) {
+// Append y to the wave queue of parity par once per wave (tag). With range
+// ordering the queue is cut into QRANGES regions of P.rsize slots, region b
+// holding the vertices of [b * rsize, (b + 1) * rsize); a vertex enters a
+// wave's queue at most once, so no region overflows. The queue count is kept
+// either way (it ends the waves).
+__device__ __forceinline__ void enqueue_once(const MultiParams &P, uint32_t par, uint32_t y,
+                                             uint32_t tag) {
   if (atomicExch(P.wtag + y, tag) != tag) {
-    const uint32_t s = atomicAdd(count, 1u);
-    if (s < P.n) q[s] = y;
-    else atomicCAS(&P.ctl->err, 0u, ERR_QUEUE);
+    Ctl *c = P.ctl;
+    const uint32_t s = atomicAdd(&c->q_count[par], 1u);
+    if (P.ranges) {
+      const uint32_t b = y / P.rsize;
+      const uint32_t k = atomicAdd(&c->qrange[par][b], 1u);
+      if (b < QRANGES && k < P.rsize) P.q[par][b * P.rsize + k] = y;
+      else atomicCAS(&c->err, 0u, ERR_QUEUE);
+    } else if (s < P.n) {
+      P.q[par][s] = y;
+    } else {
+      atomicCAS(&c->err, 0u, ERR_QUEUE);
+    }
   }
 }
 
@@ -322,12 +339,45 @@ __device__ __forceinline__ void staged_pairs(uint32_t v, const uint32_t (&m)[NB]
 // range, w = mapping) that whole CTAs process after a grid barrier; their
 // masks travel through cmask. Ends with a barrier that applies reset_flags.
 // Returns false when the launch has failed.
+constexpr uint32_t NO_QUEUE = 0xFFFFFFFFu;
+
 template <int NB, bool WITH_W, class Prep, class Ph>
 __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t *items,
                              uint32_t cnt, Prep &prep, Ph &ph, u64 *s, uint2 *stage, Acc &acc,
-                             uint32_t reset_flags, uint32_t qratio) {
+                             uint32_t qpar, uint32_t reset_flags, uint32_t qratio) {
   Ctl *ctl = P.ctl;
   const uint32_t lane = lane_id();
+  // a range-ordered wave queue (qpar: its parity) is read range by range:
+  // item i is entry i - pre[b] of region b, pre = prefix of the range counts
+  __shared__ uint32_t s_pre[QRANGES + 1];
+  const bool ranged = P.ranges && qpar != NO_QUEUE;
+  if (ranged) {
+    if (threadIdx.x < 32) {
+      uint32_t x = ctl->qrange[qpar][lane], y = ctl->qrange[qpar][lane + 32];
+      for (int o = 1; o < 32; o <<= 1) {  // inclusive warp scans of both halves
+        const uint32_t xa = __shfl_up_sync(0xffffffffu, x, o);
+        const uint32_t ya = __shfl_up_sync(0xffffffffu, y, o);
+        if ((int)lane >= o) {
+          x += xa;
+          y += ya;
+        }
+      }
+      const uint32_t tot_a = __shfl_sync(0xffffffffu, x, 31);
+      s_pre[lane + 1] = x;
+      s_pre[lane + 33] = tot_a + y;
+      if (lane == 0) s_pre[0] = 0;
+    }
+    __syncthreads();
+  }
+  auto item = [&](uint32_t i) -> uint32_t {
+    if (!ranged) return items[i];
+    uint32_t lo = 0, hi = QRANGES;  // last b with s_pre[b] <= i
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) / 2;
+      if (s_pre[mid] <= i) lo = mid; else hi = mid;
+    }
+    return items[lo * P.rsize + (i - s_pre[lo])];
+  };
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   // Item distribution: static (warp w takes items w, w + nw, ...) or claimed
@@ -340,7 +390,7 @@ __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t 
     i = __shfl_sync(0xffffffffu, i, 0);
   }
   for (; i < cnt;) {
-    const uint32_t v = items[i];
+    const uint32_t v = item(i);
     if (P.sched) {
       if (lane == 0) i = atomicAdd(&ctl->grab, 1u);
       i = __shfl_sync(0xffffffffu, i, 0);
@@ -417,7 +467,8 @@ __device__ bool multi_expand(const MultiParams &P, const Adj &A, const uint32_t 
 template <int NB>
 struct InvalidatePh {
   const MultiParams *P;
-  uint32_t *inew_next, *nq, *nc;
+  uint32_t *inew_next;
+  uint32_t qpar;  // parity of the next wave's queue
   uint32_t tag, epoch;
   __device__ void mark(uint32_t y, uint32_t k, uint32_t bits) {
     const uint32_t old = atomicOr(P->affm + (u64)y * NB + k, bits);
@@ -425,7 +476,7 @@ struct InvalidatePh {
     if (fresh) {
       atomicOr(inew_next + (u64)y * NB + k, fresh);
       note_affected(*P, y, epoch);
-      enqueue_once(*P, nq, nc, y, tag);
+      enqueue_once(*P, qpar, y, tag);
     }
   }
   __device__ void beginQ(uint32_t, int, uint32_t, u64 &) {}
@@ -545,7 +596,8 @@ struct PullPh {
 template <uint32_t ALGO, bool STORED, int NB>
 struct RelaxPh {
   const MultiParams *P;
-  uint32_t *nmask_next, *nq, *nc;
+  uint32_t *nmask_next;
+  uint32_t qpar;  // parity of the next wave's queue
   uint32_t tag;
   static constexpr bool STRICT = Strict<ALGO, STORED>::value;
   __device__ void beginQ(uint32_t x, int k, uint32_t mk, u64 &dx) {
@@ -581,7 +633,7 @@ struct RelaxPh {
         any = true;
       }
     }
-    if (lane == 0 && any) enqueue_once(*P, nq, nc, y, tag);
+    if (lane == 0 && any) enqueue_once(*P, qpar, y, tag);
   }
   __device__ void endQ(uint32_t, int, uint32_t, u64 &) {}
   __device__ void beginE(uint32_t x, int k, uint32_t mk, u64 *s) {
@@ -614,7 +666,7 @@ struct RelaxPh {
       if (lower_from<STRICT>(P->key + (u64)y * NB * 32 + q, pack_key((uint32_t)c[u], x + 1u),
                              cur[u])) {
         atomicOr(nmask_next + (u64)y * NB + (q >> 5), 1u << (q & 31));
-        enqueue_once(*P, nq, nc, y, tag);
+        enqueue_once(*P, qpar, y, tag);
         acc.improved++;
       }
     }
@@ -681,7 +733,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
       }
       if (lane == 0 && any) {
         note_affected(P, e.y, epoch);
-        enqueue_once(P, P.q[0], &ctl->q_count[0], e.y, tag0);
+        enqueue_once(P, 0, e.y, tag0);
       }
     }
     if (!grid_sync(ctl, 0, P.timeout_ns)) goto done;
@@ -696,10 +748,10 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
           break;
         }
         const uint32_t par = wave & 1;
-        InvalidatePh<NB> ph{&P, P.inew[par ^ 1], P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag++, epoch};
+        InvalidatePh<NB> ph{&P, P.inew[par ^ 1], cur ^ 1, tag++, epoch};
         uint32_t *src = P.inew[par];
         auto prep = [&](uint32_t v, uint32_t (&m)[NB]) { return take_masks<NB>(src, v, true, m); };
-        if (!multi_expand<NB, false>(P, P.out, P.q[cur], cnt, prep, ph, s, s_stage, acc,
+        if (!multi_expand<NB, false>(P, P.out, P.q[cur], cnt, prep, ph, s, s_stage, acc, cur,
                                      cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.qratio))
           goto done;
         waves++;
@@ -722,7 +774,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
       // 4. pull over in-rows
       PullPh<ALGO, STORED, NB> ph{&P};
       auto prep = [&](uint32_t v, uint32_t (&m)[NB]) { return take_masks<NB>(P.affm, v, false, m); };
-      if (!multi_expand<NB, STORED>(P, P.in, P.aff, na, prep, ph, s, s_stage, acc, 0,
+      if (!multi_expand<NB, STORED>(P, P.in, P.aff, na, prep, ph, s, s_stage, acc, NO_QUEUE, 0,
                                     P.pull_qratio))
         goto done;
       if (gtid == 0) ctl->tphase[1] = globaltimer_ns();  // reset + pull done
@@ -747,7 +799,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
             any = true;
           }
         }
-        if (lane == 0 && any) enqueue_once(P, P.q[0], &ctl->q_count[0], v, ftag);
+        if (lane == 0 && any) enqueue_once(P, 0, v, ftag);
       }
     }
     if (P.phases & PH_INSERT) {
@@ -771,7 +823,7 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
             any = true;
           }
         }
-        if (lane == 0 && any) enqueue_once(P, P.q[0], &ctl->q_count[0], e.y, ftag);
+        if (lane == 0 && any) enqueue_once(P, 0, e.y, ftag);
       }
     }
   }
@@ -788,10 +840,10 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(Mu
         break;
       }
       const uint32_t par = wave & 1;
-      RelaxPh<ALGO, STORED, NB> ph{&P, P.nmask[par ^ 1], P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag++};
+      RelaxPh<ALGO, STORED, NB> ph{&P, P.nmask[par ^ 1], cur ^ 1, tag++};
       uint32_t *src = P.nmask[par];
       auto prep = [&](uint32_t v, uint32_t (&m)[NB]) { return take_masks<NB>(src, v, true, m); };
-      if (!multi_expand<NB, STORED>(P, P.out, P.q[cur], cnt, prep, ph, s, s_stage, acc,
+      if (!multi_expand<NB, STORED>(P, P.out, P.q[cur], cnt, prep, ph, s, s_stage, acc, cur,
                                     cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.qratio))
         goto done;
       waves++;
@@ -828,15 +880,24 @@ __global__ void multi_init_kernel(u64 *key, u64 total) {
 
 __global__ void multi_seed_kernel(u64 *key, uint32_t n, uint32_t nb, const uint32_t *sources,
                                   uint32_t *nmask0, uint32_t *q0, uint32_t *wtag,
-                                  const uint32_t *seq, Ctl *ctl) {
+                                  const uint32_t *seq, Ctl *ctl, bool ranges) {
   const uint32_t Q = nb * 32;
   const uint32_t tag = seq[1];
+  const uint32_t rsize = (n + QRANGES - 1) / QRANGES;
   for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < Q; q += gridDim.x * blockDim.x) {
     const uint32_t s = sources[q];
     if (s >= n) continue;
     key[(u64)s * Q + q] = pack_key(0, 0);
     atomicOr(nmask0 + (u64)s * nb + q / 32, 1u << (q % 32));
-    if (atomicExch(wtag + s, tag) != tag) q0[atomicAdd(&ctl->q_count[0], 1u)] = s;
+    if (atomicExch(wtag + s, tag) != tag) {
+      const uint32_t k = atomicAdd(&ctl->q_count[0], 1u);
+      if (ranges) {
+        const uint32_t b = s / rsize;
+        q0[b * rsize + atomicAdd(&ctl->qrange[0][b], 1u)] = s;
+      } else {
+        q0[k] = s;
+      }
+    }
   }
 }
 
@@ -882,7 +943,9 @@ static cudaError_t launch_multi_t(const MultiLaunch &L, cudaStream_t s) {
   P.pull_qratio = L.pull_qratio;
   P.heavy = std::max(L.heavy, 1u);
   P.tile = std::max(L.tile, MULTI_MIN_TILE);
-  P.sched = L.sched;
+  P.sched = L.sched & 1u;
+  P.ranges = (L.sched & 2u) != 0;
+  P.rsize = (L.n + QRANGES - 1) / QRANGES;
   P.timeout_ns = L.timeout_ns;
   static int blocks_per_sm = -1;
   if (blocks_per_sm < 0) {
@@ -926,9 +989,10 @@ cudaError_t launch_multi(const MultiLaunch &L, cudaStream_t s) {
 
 cudaError_t launch_multi_init(u64 *key, uint32_t n, uint32_t nb, const uint32_t *sources,
                               uint32_t *nmask0, uint32_t *q0, uint32_t *wtag, const uint32_t *seq,
-                              Ctl *ctl, cudaStream_t s) {
+                              Ctl *ctl, uint32_t sched, cudaStream_t s) {
   multi_init_kernel<<<148 * 16, BLOCK, 0, s>>>(key, (u64)n * nb * 32);
-  multi_seed_kernel<<<1, BLOCK, 0, s>>>(key, n, nb, sources, nmask0, q0, wtag, seq, ctl);
+  multi_seed_kernel<<<1, BLOCK, 0, s>>>(key, n, nb, sources, nmask0, q0, wtag, seq, ctl,
+                                        (sched & 2u) != 0);
   return cudaGetLastError();
 }
 

@@ -373,13 +373,18 @@ typedef struct dycg_query_mapping {
   float repair_ms;
 } dycg_query_mapping;
 
-/* Frontier-queue schemes of the batched form: how the warps of the repair
- * launch share a wave's frontier items (vertices with per-query masks).
- * STATIC: warp w takes items w, w + warps, ... (no shared counter);
- * CLAIMED: warps claim items one at a time from a counter of the wave, so
- * warps that drew long rows do not hold the wave's barrier. */
+/* Frontier-queue schemes of the batched form: how a wave's frontier items
+ * (vertices with per-query masks) are queued and shared by the warps of the
+ * repair launch. STATIC: warp w takes items w, w + warps, ... (no shared
+ * counter); CLAIMED: warps claim items one at a time from a counter of the
+ * wave, so warps that drew long rows do not hold the wave's barrier.
+ * RANGES (a flag, combined with either): each wave queue is cut into 64
+ * regions by vertex range and read region by region, so the warps in flight
+ * read rows from a narrow window of the host arena (fewer address
+ * translations per host transaction) instead of from all of it. */
 #define DYCG_QUEUE_STATIC 0u
 #define DYCG_QUEUE_CLAIMED 1u
+#define DYCG_QUEUE_RANGES 2u
 int dycg_set_query_queue(dycg_engine *e, uint32_t scheme);
 
 /* Autotuner of the batched form's work mapping (no reference counterpart):
@@ -387,8 +392,8 @@ int dycg_set_query_queue(dycg_engine *e, uint32_t scheme);
  * candidate mapping (qratio in {2,4,8,2^20} x heavy in {16,64,256} with the
  * pull phase on the same ratio, then the best of those with the pull phase's
  * ratio in {0,1,2,8}, then the best so far with query-lane tiles of
- * {1024,4096,16384} slots, then the best so far under the other
- * frontier-queue scheme), each from the same saved state, keeps the fastest
+ * {1024,4096,16384} slots, then the best so far under the other three
+ * frontier-queue schemes), each from the same saved state, keeps the fastest
  * mapping for later snapshots
  * and leaves the state of one ordinary repair. Needs HBM for one extra copy
  * of the query results while it runs. tried (cap entries, may be NULL)

@@ -1009,7 +1009,8 @@ def run_batched(args):
                    "updates_timed": L["upd"],
                    "snapshot_sizes": [int(x) for x in sizes[1 + T + W:1 + T + W + K]],
                    "weights": "uint32 uniform [1,64] stored" if algo == "sssp" else "rule",
-                   "mapping": {k: mapping.get(k) for k in ("qratio", "heavy", "tile", "pull_qratio")},
+                   "mapping": {k: mapping.get(k) for k in ("qratio", "heavy", "tile", "pull_qratio",
+                                                            "queue")},
                    "mapping_tuned_on": (f"one {args.tune_batch}-update snapshot, "
                                         f"{len(L['tried'])} candidates") if L["tried"] else "not tuned",
                    "replay": "one dycg_apply_batches_device call for the timed snapshots "
@@ -1042,8 +1043,9 @@ def run_batched(args):
                                "hit_rate": {"learned": L["hit_rate"], "hotness": H["hit_rate"]}},
         "training": L["report"],
         "results_equal": exact,
-        # [qratio, heavy, pull ratio, query-lane tile slots, repair ms] per trial
-        "mapping_candidates": [[x["qratio"], x["heavy"], x["pull_qratio"], x["tile"],
+        # [qratio, heavy, pull ratio, query-lane tile slots, frontier-queue scheme
+        # (DYCG_QUEUE_* bits: 1 claimed, 2 ranges), repair ms] per trial
+        "mapping_candidates": [[x["qratio"], x["heavy"], x["pull_qratio"], x["tile"], x["queue"],
                                 round(x["repair_ms"], 3)] for x in L["tried"]],
     }
     if cpu:

@@ -694,8 +694,15 @@ __device__ __forceinline__ bool take_masks(uint32_t *src, uint32_t v, bool consu
   return any;
 }
 
+// CTAs per SM the register allocation is sized for at 8 blocks of queries
+// (at 3 the compiler spills ~140 bytes per thread)
+#ifndef DYCG_MULTI_MIN_BLOCKS
+#define DYCG_MULTI_MIN_BLOCKS 2
+#endif
+
 template <uint32_t ALGO, bool STORED, int NB>
-__global__ void __launch_bounds__(BLOCK, NB >= 8 ? 2 : 3) multi_repair_kernel(MultiParams P) {
+__global__ void __launch_bounds__(BLOCK, NB >= 8 ? DYCG_MULTI_MIN_BLOCKS : 3)
+    multi_repair_kernel(MultiParams P) {
   Ctl *ctl = P.ctl;
   Acc acc = {0, 0, 0, 0, 0, 0};
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;

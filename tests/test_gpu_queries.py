@@ -46,7 +46,7 @@ def tight_parents(algo, stored, off, dst, w, vals, par, src):
 
 def run_queries(algo, nq, mode, scale=10, batches=3, nd=300, na=300, seed=7, stored=False,
                 budget=0, qratio=4, heavy=64, tile=4096, split=False, ef=8,
-                parent_every=16):
+                parent_every=16, queue=None):
     n, off, dst, w = cases.small_rmat(scale, ef, seed)
     rng = np.random.default_rng(seed)
     # sources: distinct vertices with out-edges (plus vertex 0)
@@ -59,6 +59,8 @@ def run_queries(algo, nq, mode, scale=10, batches=3, nd=300, na=300, seed=7, sto
     e.set_queries(sources, mode)
     if mode == "batched":
         e.set_query_mapping(qratio, heavy, tile)
+        if queue is not None:
+            e.set_query_queue(queue)
     e.start()
     orc = oracle.Oracle(ALGO[algo], n, off, dst, w if stored else None,
                         weight_mode=oracle.WEIGHT_STORED if stored else oracle.WEIGHT_HASH128)
@@ -105,6 +107,15 @@ def test_batched_work_mappings(qratio, heavy):
     # qratio 0: every row on query lanes; 2^20: every row on edge lanes;
     # heavy 1: every row tiled (CTA splits); 2^30: no row tiled
     run_queries("sssp", 64, "batched", stored=True, qratio=qratio, heavy=heavy, seed=9)
+
+
+@pytest.mark.parametrize("queue", ["static", "claimed", "ranges", "claimed+ranges"])
+def test_batched_frontier_queue_schemes(queue):
+    # every frontier-queue scheme (static or claimed items, plain or
+    # range-ordered wave queues) gives the static recompute's results, heavy
+    # rows and tiles included
+    run_queries("sssp", 64, "batched", scale=12, ef=16, batches=2, nd=800, na=800, seed=21,
+                stored=True, heavy=4, tile=1024, queue=queue, parent_every=32)
 
 
 def test_batched_256_queries_split_phases():
@@ -187,9 +198,10 @@ def test_tune_mapping_keeps_results():
     tried = e.tune_query_mapping(dels, adds)
     orc.mutate(dels, adds)
     cur = orc.csr()
-    # 12 (qratio x heavy) + 3-4 pull ratios + 2-3 tile sizes
-    assert 12 < len(tried) <= 19 and all(t["repair_ms"] > 0 for t in tried)
+    # 12 (qratio x heavy) + 3-4 pull ratios + 2-3 tile sizes + 3 frontier-queue schemes
+    assert 12 < len(tried) <= 22 and all(t["repair_ms"] > 0 for t in tried)
     assert {t["tile"] for t in tried} == {1024, 4096, 16384}
+    assert {t["queue"] for t in tried} == {0, 1, 2, 3}
     _check_all(e, n, cur, src)
     for bi in range(2):  # later snapshots under the kept mapping
         dels, adds = cases.random_batch(n, *cur, 400, 400, 2310 + bi)
@@ -235,3 +247,42 @@ def test_apply_batches_invalid_records_and_empty_snapshots():
     assert stats[1]["invalid_updates"] == 2 and stats[0]["invalid_updates"] == 0
     orc.mutate(dels, adds)
     _check_all(e, n, orc.csr(), src)
+
+
+@pytest.mark.parametrize("policy", ["hotness", "learned"])
+def test_replayed_snapshots_with_cache_admission_inside_the_graph(policy):
+    """Snapshots replayed from captured graphs with the cache admission
+    (hotness round after the repair, or the learned admission between the
+    mutation and the repair, with its page history) recorded inside each
+    graph: results equal the static recompute and the one-by-one engine's, and
+    pages are admitted along the way."""
+    a, (n, off, dst, w), src = _engine_and_sources(12, 32, 37, budget=2 << 20)
+    b, _, _ = _engine_and_sources(12, 32, 37, budget=2 << 20)
+    if policy == "learned":
+        # a network that predicts log1p(reads) = 10 for every page (above the
+        # admission threshold log1p(64)), so pages are admitted every snapshot
+        p = np.zeros(dg.POLICY_PARAMS, np.float32)
+        p[-1] = 10.0
+        a.policy_set_params(p)
+        a.set_cache_policy("learned")
+    orc = oracle.Oracle(oracle.SSSP, n, off, dst, w, weight_mode=oracle.WEIGHT_STORED)
+    cur = (off, dst, w)
+    loaded = 0
+    for rnd in range(3):
+        snaps = []
+        for i, sz in enumerate((900, 2500, 40)):
+            dels, adds = cases.random_batch(n, *cur, sz // 2, sz - sz // 2, 3700 + 10 * rnd + i)
+            snaps.append((dels, adds))
+            orc.mutate(dels, adds)
+            cur = orc.csr()
+        stats = a.apply_batches(snaps)
+        loaded += sum(s["cache_pages_loaded"] for s in stats)
+        for d, ad in snaps:
+            b.apply_batch(d, ad)
+    _check_all(a, n, cur, src)
+    for q in range(len(src)):
+        assert (a.gather_query(q)[0] == b.gather_query(q)[0]).all()
+    info = a.info()
+    assert 0 < info["cached_pages"] <= info["cache_slots"]
+    if policy == "learned":
+        assert loaded > 0

@@ -78,6 +78,8 @@ def parse():
                     help="bucketed closure width (default: 0 on R-MAT, on the grid 256 for SSSP "
                          "and 1 for BFS/CC)")
     ap.add_argument("--json-out", default=None)
+    ap.add_argument("--mutation-ctas", type=int, default=0,
+                    help="CTAs of the deletion/append kernels (0: the library default)")
     ap.add_argument("--queries", type=int, default=256, help="batched config: sources")
     ap.add_argument("--plain-queries", type=int, default=None,
                     help="batched config: queries timed on the per-query path (default all)")
@@ -288,7 +290,8 @@ def run_dycg(args):
     eng = dg.Engine(algo, weight_mode="stored" if algo == "sssp" else "hash128",
                     hbm_graph_budget_bytes=budget,
                     symmetric=(algo == "cc" and args.config != "grid"), epsilon=1e-4,
-                    device=local, ordered_delta=args.ordered_delta if algo != "pr" else 0)
+                    device=local, mutation_ctas=args.mutation_ctas,
+                    ordered_delta=args.ordered_delta if algo != "pr" else 0)
     wmax = 1000 if args.config == "grid" else 64
     if args.config == "grid":
         eng.load_grid(1 << args.scale, 10, 8, seed=args.seed, wlo=1, whi=wmax)
@@ -824,7 +827,8 @@ def run_batched(args):
 
     def build():
         eng = dg.Engine(algo, weight_mode="stored" if algo == "sssp" else "hash128",
-                        hbm_graph_budget_bytes=budget, cache_policy="hotness", device=local)
+                        hbm_graph_budget_bytes=budget, cache_policy="hotness", device=local,
+                        mutation_ctas=args.mutation_ctas)
         eng.load_rmat(args.scale, args.edge_factor, seed=args.seed, wlo=1, whi=64)
         return eng
 
@@ -1214,7 +1218,7 @@ def run_learned(args):
         eng = dg.Engine(algo, weight_mode="stored" if algo == "sssp" else "hash128",
                         hbm_graph_budget_bytes=0 if policy == "none" else budget,
                         cache_policy="none" if policy == "none" else "hotness", epsilon=1e-4,
-                        device=local)
+                        device=local, mutation_ctas=args.mutation_ctas)
         eng.load_rmat(args.scale, args.edge_factor, seed=args.seed, wlo=1, whi=64)
         t_load = time.time() - t0
         t0 = time.time()

@@ -59,6 +59,7 @@ Engine::Engine(const dycg_options &opt) : opt_(opt) {
   if (opt_.cache_policy > DYCG_CACHE_LEARNED) throw Error(DYCG_EINVAL, "unknown cache policy");
   if (opt_.frontier_queue > DYCG_QUEUE_CLAIMED)
     throw Error(DYCG_EINVAL, "unknown frontier-queue scheme");
+  mut_ctas_ = opt_.mutation_ctas ? opt_.mutation_ctas : 2u * (uint32_t)num_sms_;
   policy_ = opt_.cache_policy;
   stored_ = opt_.algo == DYCG_ALGO_SSSP && opt_.weight_mode == DYCG_WEIGHT_STORED;
   has_in_ = !opt_.symmetric && opt_.algo != DYCG_ALGO_PR;
@@ -692,12 +693,13 @@ void Engine::delete_direction(const Adj &A, const uint2 *uv, const uint32_t *mul
                               const uint32_t *n_ptr, uint32_t nd, uint32_t *found,
                               int count_missing, bool capture) {
   if (capture) {
-    CK(launch_delete_rows(A, uv, mult, n_ptr, nd, found, ctl_, count_missing, tombs_, st_));
+    CK(launch_delete_rows(A, uv, mult, n_ptr, nd, found, ctl_, count_missing, tombs_, mut_ctas_,
+                          st_));
     launches_ += 2;
     return;
   }
   CK(launch_delete_prefix(A, uv, mult, n_ptr, nd, found, ctl_, count_missing, tombs_, defer_,
-                          st_));
+                          mut_ctas_, st_));
   CK(cudaMemcpyAsync(h_dpacked_, defer_.packed, 8, cudaMemcpyDeviceToHost, st_));
   sync_check("deferred deletions");
   const u64 pk = *h_dpacked_;
@@ -825,11 +827,11 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
   }
   if (na) {
     CK(launch_add_rows(A_out, k_add_out_, w_add_out_, seg_out_, counts_ + 2, (uint32_t)na,
-                       reloc_, ctl_, st_));
+                       reloc_, ctl_, mut_ctas_, st_));
     launches_ += 3;
     if (has_in_) {
       CK(launch_add_rows(A_in, k_add_in_, w_add_in_, seg_in_, counts_ + 3, (uint32_t)na, reloc_,
-                         ctl_, st_));
+                         ctl_, mut_ctas_, st_));
       launches_ += 3;
     }
   }

@@ -128,6 +128,7 @@ class Engine {
 
   dycg_options opt_;
   int dev_ = 0, num_sms_ = 148;
+  uint32_t mut_ctas_ = 296;  // CTAs of the warp-per-record mutation kernels
   cudaStream_t st_ = nullptr;
   cudaEvent_t ev_[6] = {};
   // side stream of the hotness path's page staging (eviction, admission list,

@@ -123,9 +123,11 @@ struct Tombs {
   uint32_t *count;
   uint32_t cap;
 };
+// ctas: CTAs of the warp-per-record mutation kernels (0: one warp per record,
+// up to the grid cap)
 cudaError_t launch_delete_rows(const Adj &A, const uint2 *uv, const uint32_t *mult,
                                const uint32_t *n_ptr, uint32_t max_n, uint32_t *found, Ctl *ctl,
-                               int count_missing, const Tombs &T, cudaStream_t s);
+                               int count_missing, const Tombs &T, uint32_t ctas, cudaStream_t s);
 // Deletions in rows whose unsorted suffix exceeds DEFER_SUFFIX slots are
 // matched by sort-merge (gather the live suffix slots once, stable sort by
 // (row, neighbour), binary search per record) instead of a suffix scan per
@@ -149,7 +151,7 @@ struct DeferBufs {
 cudaError_t launch_delete_prefix(const Adj &A, const uint2 *uv, const uint32_t *mult,
                                  const uint32_t *n_ptr, uint32_t max_n, uint32_t *found, Ctl *ctl,
                                  int count_missing, const Tombs &T, const DeferDel &D,
-                                 cudaStream_t s);
+                                 uint32_t ctas, cudaStream_t s);
 size_t delete_sort_temp_bytes(u64 total);
 // sort-merge of the deferred suffixes (total gathered slots, nrows rows), then
 // the tombstones of all found occurrences
@@ -172,7 +174,7 @@ struct Reloc {
 };
 cudaError_t launch_add_rows(const Adj &A, const u64 *k, const uint32_t *w, const uint3 *seg,
                             const uint32_t *n_ptr, uint32_t max_n, const Reloc &R, Ctl *ctl,
-                            cudaStream_t s);
+                            uint32_t ctas, cudaStream_t s);
 cudaError_t launch_keys_to_uvw(const u64 *k, const uint32_t *w, uint32_t cnt, uint3 *out,
                                cudaStream_t s);
 cudaError_t launch_touched(const u64 *k, uint32_t cnt, uint32_t *tag, uint32_t epoch,

@@ -484,6 +484,16 @@ static int grid_for(u64 threads) {
   return (int)b;
 }
 
+// Grid of a warp-per-record mutation kernel: the records are in row order
+// (sorted by ingest) and the rows in arena order, so the warps in flight work
+// on a window of consecutive records; capping the CTAs (ctas > 0) narrows
+// that window of the host arena, and the host link serves transactions in a
+// narrow window several times faster than ones spread over a multi-GB arena.
+static int mut_grid(u64 records, uint32_t ctas) {
+  const int g = grid_for(records * 32);
+  return ctas ? std::min<int>(g, (int)ctas) : g;
+}
+
 cudaError_t launch_prep_keys(const dycg_edge_dev *e, uint32_t cnt, uint32_t n, u64 *kout,
                              u64 *kin, uint32_t *w, u64 *invalid, cudaStream_t s) {
   if (!cnt) return cudaSuccess;
@@ -542,12 +552,12 @@ cudaError_t launch_row_segments(const u64 *k, uint32_t cnt, uint3 *seg, uint32_t
 
 cudaError_t launch_delete_rows(const Adj &A, const uint2 *uv, const uint32_t *mult,
                                const uint32_t *n_ptr, uint32_t max_n, uint32_t *found, Ctl *ctl,
-                               int count_missing, const Tombs &T, cudaStream_t s) {
+                               int count_missing, const Tombs &T, uint32_t ctas, cudaStream_t s) {
   if (!max_n) return cudaSuccess;
   cudaMemsetAsync(T.count, 0, 4, s);
   DeferDel off{};
-  delete_rows_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, uv, mult, n_ptr, found, ctl,
-                                                                 count_missing, T, off);
+  delete_rows_kernel<<<mut_grid(max_n, ctas), BLOCK, 0, s>>>(A, uv, mult, n_ptr, found, ctl,
+                                                             count_missing, T, off);
   tombstone_kernel<<<grid_for(max_n), BLOCK, 0, s>>>(A, T, ctl);
   return cudaGetLastError();
 }
@@ -555,12 +565,12 @@ cudaError_t launch_delete_rows(const Adj &A, const uint2 *uv, const uint32_t *mu
 cudaError_t launch_delete_prefix(const Adj &A, const uint2 *uv, const uint32_t *mult,
                                  const uint32_t *n_ptr, uint32_t max_n, uint32_t *found, Ctl *ctl,
                                  int count_missing, const Tombs &T, const DeferDel &D,
-                                 cudaStream_t s) {
+                                 uint32_t ctas, cudaStream_t s) {
   if (!max_n) return cudaSuccess;
   cudaMemsetAsync(T.count, 0, 4, s);
   cudaMemsetAsync(D.packed, 0, 8, s);
-  delete_rows_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, uv, mult, n_ptr, found, ctl,
-                                                                 count_missing, T, D);
+  delete_rows_kernel<<<mut_grid(max_n, ctas), BLOCK, 0, s>>>(A, uv, mult, n_ptr, found, ctl,
+                                                             count_missing, T, D);
   return cudaGetLastError();
 }
 
@@ -595,12 +605,12 @@ cudaError_t launch_delete_suffix(const Adj &A, const uint2 *uv, const uint32_t *
 
 cudaError_t launch_add_rows(const Adj &A, const u64 *k, const uint32_t *w, const uint3 *seg,
                             const uint32_t *n_ptr, uint32_t max_n, const Reloc &R, Ctl *ctl,
-                            cudaStream_t s) {
+                            uint32_t ctas, cudaStream_t s) {
   if (!max_n) return cudaSuccess;
   cudaMemsetAsync(R.n_reloc, 0, 4, s);
   cudaMemsetAsync(R.n_chunks, 0, 4, s);
   const uint32_t *wv = A.stride == 2 ? w : nullptr;
-  add_rows_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, k, wv, seg, n_ptr, R, ctl);
+  add_rows_kernel<<<mut_grid(max_n, ctas), BLOCK, 0, s>>>(A, k, wv, seg, n_ptr, R, ctl);
   relocate_copy_kernel<<<148 * 16, BLOCK, 0, s>>>(A, R, ctl);
   relocate_append_kernel<<<grid_for((u64)max_n * 32), BLOCK, 0, s>>>(A, k, wv, seg, R);
   return cudaGetLastError();

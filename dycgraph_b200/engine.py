@@ -43,7 +43,8 @@ class Options(ctypes.Structure):
                 ("alpha", ctypes.c_float), ("max_rounds", ctypes.c_uint32),
                 ("device", ctypes.c_int32), ("page_shift", ctypes.c_uint32),
                 ("ordered_delta", ctypes.c_uint32), ("arena_headroom_permille", ctypes.c_uint32),
-                ("frontier_queue", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 4)]
+                ("frontier_queue", ctypes.c_uint32), ("mutation_ctas", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 3)]
 
 
 _STAT_U64 = ["deletions", "insertions", "missing_deletes", "invalid_updates", "touched_sources",
@@ -277,7 +278,7 @@ class Engine:
     def __init__(self, algo="sssp", weight_mode="hash128", source=0, segments=1,
                  hbm_graph_budget_bytes=0, cache_policy=None, symmetric=False, epsilon=1e-6,
                  alpha=0.85, max_rounds=100, device=0, page_shift=12, ordered_delta=0,
-                 arena_headroom_permille=0, frontier_queue="static"):
+                 arena_headroom_permille=0, frontier_queue="static", mutation_ctas=0):
         L = lib()
         opt = Options()
         L.dycg_options_default(ctypes.byref(opt))
@@ -299,6 +300,7 @@ class Engine:
         opt.arena_headroom_permille = arena_headroom_permille
         opt.frontier_queue = (self.QUEUE_SCHEMES[frontier_queue] if isinstance(frontier_queue, str)
                               else int(frontier_queue))
+        opt.mutation_ctas = int(mutation_ctas)
         self.algo = opt.algo
         self.options = opt
         self._h = ctypes.c_void_p()

@@ -103,7 +103,12 @@ typedef struct dycg_options {
                           /* DYCG_QUEUE_CLAIMED, how warps share a wave's rows */
                           /* (the batched form's scheme is tuned, see          */
                           /* dycg_tune_query_mapping)                          */
-  uint32_t reserved[4];
+  uint32_t mutation_ctas; /* CTAs of the deletion / append kernels (0: two    */
+                          /* per SM). They take a snapshot's records in row   */
+                          /* order, so fewer CTAs in flight keep their host   */
+                          /* transactions in a narrower window of the arena,  */
+                          /* which the host link serves several times faster */
+  uint32_t reserved[3];
 } dycg_options;
 
 /* Per-call counters. Byte counts are algorithmic: every adjacency slot read

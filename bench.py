@@ -181,7 +181,9 @@ class Clocks:
 # workloads hold tens of GB on the device, too large for a multi-metric
 # capture); the line's `traffic` scales it by the run's own algorithmic bytes.
 # None where no capture was taken.
-NCU_TRAFFIC_RATIO = {}
+# batched repair kernel, R-MAT 20 / 256 queries, the two timed launches of
+# profiles/ncu_multi_repair_rmat20_q256.md: 2,443 MB DRAM / 567.6 MB algorithmic
+NCU_TRAFFIC_RATIO = {("batched", "sssp"): 4.3}
 
 # Random host-link transactions cost about the same whatever their size up to
 # 128 bytes, so a kernel whose host-link bytes move in transactions of at most

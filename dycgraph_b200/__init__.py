@@ -10,7 +10,7 @@ a CUDA device is missing.
 """
 from .engine import (  # noqa: F401
     Engine, DycgError, BatchStats, GraphInfo, Edge, lib, library_path, edges_array,
-    gen_rmat_edges, hash_weight, measure_host_link, measure_host_random, mlp_infer, mlp_loss_grad,
+    gen_rmat_edges, hash_weight, measure_host_link, measure_host_random, measure_host_sweep, mlp_infer, mlp_loss_grad,
     ALGOS, STATUS, POLICY_F, POLICY_H, POLICY_PARAMS, CTL_BYTES,
 )
 from . import operators  # noqa: F401

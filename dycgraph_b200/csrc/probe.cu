@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
+#include <vector>
 
 #include "../../include/dycg.h"
 #include "common.cuh"
@@ -67,7 +69,86 @@ __global__ void random_ops_kernel(uint8_t *base, u64 lines, uint32_t op_bytes, i
   if (acc == 0x9E3779B9u) atomicAdd(sink, 1ull);  // keeps the loads alive
 }
 
+// Accesses at the given byte offsets, in the order given (sorted by the
+// caller), one per thread (8-byte words) or per warp (128-byte lines); the
+// grid strides over them, so the accesses in flight are consecutive ones.
+__global__ void sweep_ops_kernel(uint8_t *base, const u64 *off, u64 n, uint32_t op_bytes,
+                                 int write, unsigned long long *sink) {
+  const u64 tid = blockIdx.x * (u64)blockDim.x + threadIdx.x;
+  const u64 nthreads = (u64)gridDim.x * blockDim.x;
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t acc = 0;
+  if (op_bytes == 128) {
+    for (u64 i = tid >> 5; i < n; i += nthreads >> 5) {
+      unsigned int *q = reinterpret_cast<unsigned int *>(base + off[i]) + lane;
+      if (write) __stwt(q, (uint32_t)i);
+      else acc ^= __ldcv(q);
+    }
+  } else {
+    for (u64 i = tid; i < n; i += nthreads) {
+      uint2 *q = reinterpret_cast<uint2 *>(base + off[i]);
+      if (write) {
+        __stwt(q, make_uint2((uint32_t)i, 0u));
+      } else {
+        const uint2 v = __ldcv(q);
+        acc ^= v.x ^ v.y;
+      }
+    }
+  }
+  if (acc == 0x9E3779B9u) atomicAdd(sink, 1ull);  // keeps the loads alive
+}
+
 }  // namespace dycg
+
+extern "C" int dycg_measure_host_sweep(int device, uint64_t bytes, uint32_t op_bytes, int write,
+                                       uint64_t ops, uint32_t ctas, double *ns_per_op) {
+  if (op_bytes != 8 && op_bytes != 128) return DYCG_EINVAL;
+  if (bytes < (1u << 20) || ops == 0 || ops > (1ull << 28) || ctas == 0 || !ns_per_op)
+    return DYCG_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) return DYCG_ENOGPU;
+  bytes &= ~127ull;
+  // offsets: random lines of op_bytes, sorted ascending (inside the buffer)
+  const uint64_t lines = bytes / op_bytes;
+  std::vector<uint64_t> off(ops);
+  for (uint64_t i = 0; i < ops; i++) off[i] = (dycg::mix64(0x5EED5ull ^ i) % lines) * op_bytes;
+  std::sort(off.begin(), off.end());
+  void *h = nullptr, *hd = nullptr;
+  uint64_t *d_off = nullptr;
+  unsigned long long *sink = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  int rc = DYCG_OK;
+  if (cudaHostAlloc(&h, bytes, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess ||
+      cudaMalloc(&sink, 8) != cudaSuccess || cudaMalloc(&d_off, ops * 8) != cudaSuccess ||
+      cudaHostGetDevicePointer(&hd, h, 0) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+    rc = DYCG_ENOMEM;
+  } else {
+    memset(h, 1, bytes);
+    cudaMemcpyAsync(d_off, off.data(), ops * 8, cudaMemcpyHostToDevice, s);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {  // the first run warms up
+      float ms = 0;
+      cudaEventRecord(a, s);
+      dycg::sweep_ops_kernel<<<ctas, 256, 0, s>>>((uint8_t *)hd, (const dycg::u64 *)d_off, ops,
+                                                  op_bytes, write, sink);
+      cudaEventRecord(b, s);
+      cudaEventSynchronize(b);
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep) best = std::min(best, ms);
+    }
+    if (cudaGetLastError() != cudaSuccess) rc = DYCG_ECUDA;
+    *ns_per_op = best * 1e6 / (double)ops;
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  if (s) cudaStreamDestroy(s);
+  if (sink) cudaFree(sink);
+  if (d_off) cudaFree(d_off);
+  if (h) cudaFreeHost(h);
+  return rc;
+}
 
 extern "C" int dycg_measure_host_random(int device, uint64_t bytes, uint32_t op_bytes, int write,
                                         uint64_t ops, double *ns_per_op) {

@@ -156,6 +156,7 @@ def lib():
         "dycg_measure_host_link": (I, [I, u64, ctypes.POINTER(ctypes.c_double),
                                        ctypes.POINTER(ctypes.c_double)]),
         "dycg_measure_host_random": (I, [I, u64, u32, I, u64, ctypes.POINTER(ctypes.c_double)]),
+        "dycg_measure_host_sweep": (I, [I, u64, u32, I, u64, u32, ctypes.POINTER(ctypes.c_double)]),
         "dycg_group_updates": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
         "dycg_group_updates_noalloc": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
         "dycg_set_queries": (I, [P, u32p, u32, u32]),
@@ -257,6 +258,18 @@ def measure_host_random(device=0, nbytes=8 << 30, op_bytes=128, write=False, ops
                                         ctypes.byref(ns))
     if rc:
         raise DycgError(rc, "dycg_measure_host_random")
+    return ns.value
+
+
+def measure_host_sweep(device=0, nbytes=32 << 30, op_bytes=128, write=False, ops=1 << 20,
+                       ctas=148):
+    """Device time (ns) per host-link access of op_bytes at random offsets of
+    an nbytes pinned buffer, issued in ascending address order by `ctas` CTAs."""
+    ns = ctypes.c_double(0)
+    rc = lib().dycg_measure_host_sweep(device, nbytes, op_bytes, int(write), ops, ctas,
+                                       ctypes.byref(ns))
+    if rc:
+        raise DycgError(rc, "dycg_measure_host_sweep")
     return ns.value
 
 

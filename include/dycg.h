@@ -310,6 +310,16 @@ int dycg_measure_host_link(int device, uint64_t bytes, double *h2d_gbs, double *
 int dycg_measure_host_random(int device, uint64_t bytes, uint32_t op_bytes, int write,
                              uint64_t ops, double *ns_per_op);
 
+/* Measurement helper (no reference counterpart): the same accesses as
+ * dycg_measure_host_random (op_bytes 8 per thread or 128 per warp, reads or
+ * writes, `ops` random aligned offsets of a `bytes`-sized pinned buffer) but
+ * issued in ascending address order by `ctas` CTAs of 256 threads taking
+ * them in turn, the way the mutation kernels take their row-ordered records:
+ * the warps in flight then touch a narrow window of the buffer. Needs
+ * ops * 8 bytes of device memory for the sorted offsets. */
+int dycg_measure_host_sweep(int device, uint64_t bytes, uint32_t op_bytes, int write,
+                            uint64_t ops, uint32_t ctas, double *ns_per_op);
+
 /* Replaces GroupedUpdateBatch (include/framework/effective_update_batch.h:
  * 36-207) as a standalone device step. Device pointers throughout; stream is a
  * cudaStream_t (NULL = default stream). Records with an endpoint >=

@@ -139,13 +139,17 @@ struct Ctl {
   // range-ordered wave queues (batched form): entries per vertex range, per
   // queue parity (reset with the parity's queue count)
   uint32_t qrange[2][64];
+  // asynchronous worklist (batched form): ring claim / append positions, items
+  // pushed and not yet finished, mask records and tile items handed out
+  u64 a_head, a_tail;
+  uint32_t a_pend, a_pool, a_tiles, a_pad;
   u64 stat[20];
   u64 tphase[8];         // batched repair: global timer at phase boundaries (ns)
   // grid-barrier arrival groups, one 128-byte line each (frontier.cuh)
   uint32_t bar_sub[BAR_GROUPS * 32];
 };
 // read back to the host once per snapshot (dycgraph_b200/engine.py CTL_BYTES)
-static_assert(sizeof(Ctl) == 2872, "Ctl layout changed: update CTL_BYTES in engine.py");
+static_assert(sizeof(Ctl) == 2904, "Ctl layout changed: update CTL_BYTES in engine.py");
 
 enum StatIdx {
   ST_LINK_BYTES = 0,

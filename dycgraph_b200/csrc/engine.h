@@ -128,7 +128,7 @@ class Engine {
 
   dycg_options opt_;
   int dev_ = 0, num_sms_ = 148;
-  uint32_t mut_ctas_ = 296;  // CTAs of the warp-per-record mutation kernels
+  uint32_t mut_ctas_ = 148;  // CTAs of the warp-per-record mutation kernels
   cudaStream_t st_ = nullptr;
   cudaEvent_t ev_[6] = {};
   // side stream of the hotness path's page staging (eviction, admission list,
@@ -172,6 +172,10 @@ class Engine {
   Ctl *qctl_ = nullptr, *h_qctl_ = nullptr;     // per-query control blocks
   uint4 *mtiles_ = nullptr;
   uint32_t mtile_cap_ = 0;
+  // asynchronous worklist of the batched form (DYCG_QUEUE_ASYNC)
+  u64 *aring_ = nullptr;
+  uint32_t aring_cap_ = 0, apool_cap_ = 0;
+  uint32_t *ainq_ = nullptr, *apool_ = nullptr;
   uint32_t qratio_ = 4, heavy_ = 64, tile_ = 4096, pull_qratio_ = 4, sched_ = 0;
   u64 qbytes_ = 0;
   bool tune_ = false;

@@ -18,6 +18,7 @@ constexpr uint32_t SYNC_RESET_Q1 = 4;
 constexpr uint32_t SYNC_RESET_Q2 = 8;
 constexpr uint32_t SYNC_RESET_VMIN = 16;
 constexpr uint32_t SYNC_RESET_GRAB = 32;
+constexpr uint32_t SYNC_RESET_ASYNC = 64;
 
 // Back-off of a block waiting at the grid barrier between polls (ns).
 #ifndef DYCG_SPIN_NS
@@ -61,6 +62,13 @@ __device__ __forceinline__ bool grid_sync(Ctl *c, uint32_t flags, u64 timeout_ns
       }
       if (flags & SYNC_RESET_Q2) c->q_count[2] = 0;
       if (flags & SYNC_RESET_GRAB) c->grab = 0;
+      if (flags & SYNC_RESET_ASYNC) {
+        c->a_head = 0;
+        c->a_tail = 0;
+        c->a_pend = 0;
+        c->a_pool = 0;
+        c->a_tiles = 0;
+      }
       c->snap_aff = *(volatile uint32_t *)&c->n_aff;
       c->snap_q[0] = *(volatile uint32_t *)&c->q_count[0];
       c->snap_q[1] = *(volatile uint32_t *)&c->q_count[1];

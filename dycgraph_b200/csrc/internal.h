@@ -65,7 +65,12 @@ struct MultiLaunch {
   uint32_t heavy;               // rows with more work (warp iterations) are tiled
   uint32_t tile;                // tile size, in slots
   uint32_t sched;               // frontier-queue scheme (DYCG_QUEUE_* bits): claimed items,
-                                // range-ordered wave queues
+                                // range-ordered wave queues, asynchronous worklist
+  u64 *ring;                    // asynchronous worklist ring (ring_cap items)
+  uint32_t ring_cap;
+  uint32_t *inq;                // per vertex: an item waits in the ring
+  uint32_t *pool;               // mask records of split heavy rows (pool_cap x nb words)
+  uint32_t pool_cap;
   u64 timeout_ns;
   uint32_t algo;
   bool stored;

@@ -59,9 +59,23 @@ struct MultiParams {
   uint32_t n, phases, max_waves, qratio, pull_qratio, heavy, tile;
   uint32_t sched;   // item distribution: 0 static, 1 claimed (dycg_query_mapping.queue bit 0)
   bool ranges;      // wave queues ordered by vertex range (dycg_query_mapping.queue bit 1)
+  bool async;       // invalidation and closure on the asynchronous worklist (bit 2)
   uint32_t rsize;   // vertices per range: ceil(n / QRANGES)
+  u64 *ring;        // asynchronous worklist: ring_cap items, A_EMPTY when free
+  uint32_t ring_cap;
+  uint32_t *inq;    // per vertex: an item of it is in the ring and not yet taken
+  uint32_t *pool;   // mask records of split heavy rows, NB words each
+  uint32_t pool_cap;
   u64 timeout_ns;
 };
+
+// Asynchronous worklist items: vertex v in the low 32 bits; a tile of a
+// split heavy row carries its mask record + 1 (bits 32-47) and its tile index
+// (bits 48-63).
+constexpr u64 A_EMPTY = ~0ull;
+constexpr uint32_t A_TILE_CAP = 1u << 20;   // tile items outstanding at once
+constexpr uint32_t A_MAX_TILES = 1u << 16;  // tiles of one split row
+constexpr uint32_t QPAR_ASYNC = 2;          // Ph queue parity that means "the worklist"
 
 template <uint32_t ALGO, bool STORED>
 __device__ __forceinline__ uint32_t mweight(uint32_t u, uint32_t v, uint32_t w) {
@@ -101,8 +115,18 @@ __device__ __forceinline__ bool lower_key(u64 *addr, u64 cand) {
 // holding the vertices of [b * rsize, (b + 1) * rsize); a vertex enters a
 // wave's queue at most once, so no region overflows. The queue count is kept
 // either way (it ends the waves).
+__device__ bool async_push(const MultiParams &P, u64 item);
+
 __device__ __forceinline__ void enqueue_once(const MultiParams &P, uint32_t par, uint32_t y,
                                              uint32_t tag) {
+  if (par == QPAR_ASYNC) {
+    // asynchronous worklist: y's new mask bits are set; one item per vertex
+    // until a consumer takes it (the fence orders the mask update before the
+    // flag, the consumer clears the flag before it takes the masks)
+    __threadfence();
+    if (atomicExch(P.inq + y, 1u) == 0u) async_push(P, y);
+    return;
+  }
   if (atomicExch(P.wtag + y, tag) != tag) {
     Ctl *c = P.ctl;
     const uint32_t s = atomicAdd(&c->q_count[par], 1u);
@@ -694,6 +718,163 @@ __device__ __forceinline__ bool take_masks(uint32_t *src, uint32_t v, bool consu
   return any;
 }
 
+// ---- asynchronous worklist ----------------------------------------------------
+// Invalidation and closure without wave barriers: producers set a vertex's
+// mask bits and, unless an item of the vertex is already waiting, append the
+// vertex to a ring; every warp claims ring positions in order and processes
+// what arrives there. a_pend counts items appended and not yet finished (an
+// item's own appends come before its completion), so once it reaches zero no
+// item can appear any more and the waiting warps leave. Every wait is bounded
+// by the launch's time limit (ERR_BARRIER).
+
+__device__ bool async_push(const MultiParams &P, u64 item) {
+  Ctl *c = P.ctl;
+  atomicAdd(&c->a_pend, 1u);
+  const u64 t = atomicAdd(&c->a_tail, 1ull);
+  u64 *slot = P.ring + (t % P.ring_cap);
+  // the position is free unless the item of the previous lap is still being
+  // read by the warp that claimed it
+  const u64 t0 = globaltimer_ns();
+  while (atomicCAS(slot, A_EMPTY, item) != A_EMPTY) {
+    if (*(volatile uint32_t *)&c->err) return false;
+    if (globaltimer_ns() - t0 > P.timeout_ns) {
+      atomicCAS(&c->err, 0u, ERR_BARRIER);
+      return false;
+    }
+    __nanosleep(64);
+  }
+  return true;
+}
+
+// Lane 0 claims the next ring position and waits for its item; A_EMPTY when
+// the worklist has drained (or the launch failed). Warp-uniform result.
+__device__ __forceinline__ u64 async_pop(const MultiParams &P) {
+  // (the caller's lanes read the item's mask record after this returns: the
+  // fence below orders those reads after the item's arrival)
+  Ctl *c = P.ctl;
+  u64 item = A_EMPTY;
+  if (lane_id() == 0) {
+    const u64 h = atomicAdd(&c->a_head, 1ull);
+    u64 *slot = P.ring + (h % P.ring_cap);
+    const u64 t0 = globaltimer_ns();
+    for (;;) {
+      const u64 x = *(volatile u64 *)slot;
+      if (x != A_EMPTY) {
+        atomicExch(slot, A_EMPTY);
+        item = x;
+        break;
+      }
+      if (*(volatile uint32_t *)&c->a_pend == 0u || *(volatile uint32_t *)&c->err) break;
+      if (globaltimer_ns() - t0 > P.timeout_ns) {
+        atomicCAS(&c->err, 0u, ERR_BARRIER);
+        break;
+      }
+      __nanosleep(32);
+    }
+  }
+  item = __shfl_sync(0xffffffffu, item, 0);
+  __threadfence();
+  return item;
+}
+
+// Masks of v taken atomically from pend (producers may set bits meanwhile).
+template <int NB>
+__device__ __forceinline__ bool take_masks_atomic(uint32_t *pend, uint32_t v, uint32_t (&m)[NB]) {
+  const uint32_t lane = lane_id();
+  uint32_t x = 0;
+  if (lane < (uint32_t)NB) x = atomicExch(pend + (u64)v * NB + lane, 0u);
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < NB; k++) {
+    m[k] = __shfl_sync(0xffffffffu, x, k);
+    any |= m[k] != 0;
+  }
+  return any;
+}
+
+// One asynchronous phase over adjacency A: the vertices items[0..cnt) (their
+// masks already in pend) are appended, a barrier, then every warp drains the
+// worklist; rows whose work exceeds P.heavy are split into tile items with
+// their masks in a pool record (or expanded by the warp itself when the pool
+// or the tile budget is exhausted). Ends with a barrier that resets the ring.
+template <int NB, bool WITH_W, class Ph>
+__device__ bool async_phase(const MultiParams &P, const Adj &A, const uint32_t *items,
+                            uint32_t cnt, uint32_t *pend, Ph &ph, u64 *s, Acc &acc,
+                            uint32_t qratio) {
+  Ctl *c = P.ctl;
+  const uint32_t lane = lane_id();
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint32_t i = gtid; i < cnt; i += gridDim.x * blockDim.x) {
+    const uint32_t v = items[i];
+    if (atomicExch(P.inq + v, 1u) == 0u) async_push(P, v);
+  }
+  if (!grid_sync(c, SYNC_RESET_Q0 | SYNC_RESET_Q1, P.timeout_ns)) return false;
+  for (;;) {
+    const u64 item = async_pop(P);
+    if (item == A_EMPTY) break;
+    const uint32_t v = (uint32_t)item;
+    const uint32_t rec1 = (uint32_t)(item >> 32) & 0xFFFFu;
+    uint32_t m[NB];
+    const uint32_t len = A.len[v];
+    if (rec1) {  // one tile of a split row
+      const uint32_t t = (uint32_t)(item >> 48);
+      uint32_t x = 0;
+      if (lane < (uint32_t)NB) x = P.pool[(u64)(rec1 - 1) * NB + lane];
+      uint32_t act = 0;
+#pragma unroll
+      for (int k = 0; k < NB; k++) {
+        m[k] = __shfl_sync(0xffffffffu, x, k);
+        act += __popc(m[k]);
+      }
+      const bool ql = use_query_lanes(act, len, qratio);
+      const uint32_t ts = ql ? P.tile : MULTI_MIN_TILE;
+      expand_vertex<NB, WITH_W>(A, v, m, t * ts, min(len, (t + 1) * ts), 32, ql, ph, s, acc);
+      if (lane == 0) atomicSub(&c->a_tiles, 1u);
+    } else {
+      if (lane == 0) atomicExch(P.inq + v, 0u);
+      __threadfence();
+      __syncwarp();
+      if (take_masks_atomic<NB>(pend, v, m) && len) {
+        uint32_t act = 0;
+#pragma unroll
+        for (int k = 0; k < NB; k++) act += __popc(m[k]);
+        const bool ql = use_query_lanes(act, len, qratio);
+        const u64 work = ql ? len : (u64)((len + 31) / 32) * act;
+        const uint32_t ts = ql ? P.tile : MULTI_MIN_TILE;
+        const uint32_t nt = (len + ts - 1) / ts;
+        bool split = false;
+        if (work > P.heavy && nt > 1 && nt <= A_MAX_TILES) {
+          uint32_t rec = 0;
+          if (lane == 0) {
+            rec = atomicAdd(&c->a_pool, 1u);
+            if (rec < P.pool_cap && atomicAdd(&c->a_tiles, nt) + nt <= A_TILE_CAP) {
+              split = true;
+            } else if (rec < P.pool_cap) {
+              atomicSub(&c->a_tiles, nt);
+            }
+          }
+          split = __shfl_sync(0xffffffffu, split, 0);
+          rec = __shfl_sync(0xffffffffu, rec, 0);
+          if (split) {
+#pragma unroll
+            for (int k = 0; k < NB; k++)
+              if (lane == (uint32_t)k) P.pool[(u64)rec * NB + k] = m[k];
+            __threadfence();
+            __syncwarp();
+            for (uint32_t t = lane; t < nt; t += 32)
+              async_push(P, (u64)v | ((u64)(rec + 1) << 32) | ((u64)t << 48));
+          }
+        }
+        if (!split) expand_vertex<NB, WITH_W>(A, v, m, 0, len, 32, ql, ph, s, acc);
+      }
+    }
+    __syncwarp();
+    __threadfence();
+    if (lane == 0) atomicSub(&c->a_pend, 1u);
+  }
+  return grid_sync(c, SYNC_RESET_ASYNC | SYNC_RESET_Q0 | SYNC_RESET_Q1, P.timeout_ns);
+}
+
 // CTAs per SM the register allocation is sized for at 8 blocks of queries:
 // 3 (85 registers, ~140 bytes of spills per thread) measured ~3% faster on
 // the R-MAT 24 / 256-query workload than 2 (104 registers, no spills)
@@ -745,8 +926,14 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? DYCG_MULTI_MIN_BLOCKS : 3)
       }
     }
     if (!grid_sync(ctl, 0, P.timeout_ns)) goto done;
-    // 2. invalidation waves
-    {
+    // 2. invalidation waves (or one asynchronous phase)
+    if (P.async) {
+      const uint32_t cnt = *(volatile uint32_t *)&ctl->snap_q[0];
+      InvalidatePh<NB> ph{&P, P.inew[0], QPAR_ASYNC, tag++, epoch};
+      if (!async_phase<NB, false>(P, P.out, P.q[0], cnt, P.inew[0], ph, s, acc, P.qratio))
+        goto done;
+      waves++;
+    } else {
       uint32_t cur = 0;
       for (uint32_t wave = 0;; wave++) {
         const uint32_t cnt = *(volatile uint32_t *)&ctl->snap_q[cur];
@@ -837,8 +1024,14 @@ __global__ void __launch_bounds__(BLOCK, NB >= 8 ? DYCG_MULTI_MIN_BLOCKS : 3)
   }
   if (!grid_sync(ctl, 0, P.timeout_ns)) goto done;
   if (gtid == 0) ctl->tphase[2] = globaltimer_ns();  // frontier + insertion seeds done
-  // 6. closure waves
-  if (P.phases & PH_CLOSE) {
+  // 6. closure waves (or one asynchronous phase)
+  if ((P.phases & PH_CLOSE) && P.async) {
+    const uint32_t cnt = *(volatile uint32_t *)&ctl->snap_q[0];
+    RelaxPh<ALGO, STORED, NB> ph{&P, P.nmask[0], QPAR_ASYNC, tag++};
+    if (!async_phase<NB, STORED>(P, P.out, P.q[0], cnt, P.nmask[0], ph, s, acc, P.qratio))
+      goto done;
+    waves++;
+  } else if (P.phases & PH_CLOSE) {
     uint32_t cur = 0;
     for (uint32_t wave = 0;; wave++) {
       const uint32_t cnt = *(volatile uint32_t *)&ctl->snap_q[cur];
@@ -898,7 +1091,7 @@ __global__ void multi_seed_kernel(u64 *key, uint32_t n, uint32_t nb, const uint3
     key[(u64)s * Q + q] = pack_key(0, 0);
     atomicOr(nmask0 + (u64)s * nb + q / 32, 1u << (q % 32));
     if (atomicExch(wtag + s, tag) != tag) {
-      const uint32_t k = atomicAdd(&ctl->q_count[0], 1u);
+      const uint32_t k = atomicAdd(&ctl->q_count[0], 1u);  // ranges: seeds into their regions
       if (ranges) {
         const uint32_t b = s / rsize;
         q0[b * rsize + atomicAdd(&ctl->qrange[0][b], 1u)] = s;
@@ -952,7 +1145,13 @@ static cudaError_t launch_multi_t(const MultiLaunch &L, cudaStream_t s) {
   P.heavy = std::max(L.heavy, 1u);
   P.tile = std::max(L.tile, MULTI_MIN_TILE);
   P.sched = L.sched & 1u;
-  P.ranges = (L.sched & 2u) != 0;
+  P.async = (L.sched & 4u) != 0;
+  P.ranges = (L.sched & 2u) != 0 && !P.async;  // the worklist reads the plain queue
+  P.ring = L.ring;
+  P.ring_cap = L.ring_cap;
+  P.inq = L.inq;
+  P.pool = L.pool;
+  P.pool_cap = L.pool_cap;
   P.rsize = (L.n + QRANGES - 1) / QRANGES;
   P.timeout_ns = L.timeout_ns;
   static int blocks_per_sm = -1;
@@ -1000,7 +1199,7 @@ cudaError_t launch_multi_init(u64 *key, uint32_t n, uint32_t nb, const uint32_t 
                               Ctl *ctl, uint32_t sched, cudaStream_t s) {
   multi_init_kernel<<<148 * 16, BLOCK, 0, s>>>(key, (u64)n * nb * 32);
   multi_seed_kernel<<<1, BLOCK, 0, s>>>(key, n, nb, sources, nmask0, q0, wtag, seq, ctl,
-                                        (sched & 2u) != 0);
+                                        (sched & 2u) != 0 && (sched & 4u) == 0);
   return cudaGetLastError();
 }
 

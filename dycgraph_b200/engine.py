@@ -58,7 +58,7 @@ _STAT_PHASE = ["ms_phase_invalidate", "ms_phase_pull", "ms_phase_seed", "ms_phas
 
 # Bytes of the engine's per-snapshot device control block, which every
 # snapshot call reads back to the host (static_assert in csrc/common.cuh).
-CTL_BYTES = 2872
+CTL_BYTES = 2904
 
 
 class BatchStats(ctypes.Structure):
@@ -638,12 +638,14 @@ class Engine:
         self._check(lib().dycg_set_query_mapping(self._h, qratio, heavy, tile),
                     "set_query_mapping")
 
-    QUEUE_SCHEMES = {"static": 0, "claimed": 1, "ranges": 2, "claimed+ranges": 3}
+    QUEUE_SCHEMES = {"static": 0, "claimed": 1, "ranges": 2, "claimed+ranges": 3, "async": 4,
+                     "async+claimed": 5}
 
     def set_query_queue(self, scheme="static"):
         """Batched form's frontier-queue scheme (speed only): "static" (warp w
         takes items w, w + warps, ...), "claimed" (warps claim items one at a
-        time), with "+ranges" the wave queues read by vertex range."""
+        time), with "+ranges" the wave queues read by vertex range; "async"
+        runs the invalidation and the closure on a worklist without waves."""
         self._check(lib().dycg_set_query_queue(
             self._h, self.QUEUE_SCHEMES[scheme] if isinstance(scheme, str) else int(scheme)),
             "set_query_queue")

@@ -103,11 +103,11 @@ typedef struct dycg_options {
                           /* DYCG_QUEUE_CLAIMED, how warps share a wave's rows */
                           /* (the batched form's scheme is tuned, see          */
                           /* dycg_tune_query_mapping)                          */
-  uint32_t mutation_ctas; /* CTAs of the deletion / append kernels (0: two    */
+  uint32_t mutation_ctas; /* CTAs of the deletion / append kernels (0: one    */
                           /* per SM). They take a snapshot's records in row   */
                           /* order, so fewer CTAs in flight keep their host   */
                           /* transactions in a narrower window of the arena,  */
-                          /* which the host link serves several times faster */
+                          /* which the host link serves faster                */
   uint32_t reserved[3];
 } dycg_options;
 
@@ -396,10 +396,17 @@ typedef struct dycg_query_mapping {
  * RANGES (a flag, combined with either): each wave queue is cut into 64
  * regions by vertex range and read region by region, so the warps in flight
  * read rows from a narrow window of the host arena (fewer address
- * translations per host transaction) instead of from all of it. */
+ * translations per host transaction) instead of from all of it.
+ * ASYNC (a flag; RANGES is then ignored): the invalidation and the push
+ * closure run without waves: a vertex whose masks gain bits is appended to a
+ * ring unless it already waits there, and every warp takes ring items in
+ * turn until none is left and none is being processed (label-correcting
+ * order, same fixpoint); heavy rows are split into tile items. The pull
+ * phase (one pass) keeps the static or claimed distribution. */
 #define DYCG_QUEUE_STATIC 0u
 #define DYCG_QUEUE_CLAIMED 1u
 #define DYCG_QUEUE_RANGES 2u
+#define DYCG_QUEUE_ASYNC 4u
 int dycg_set_query_queue(dycg_engine *e, uint32_t scheme);
 
 /* Autotuner of the batched form's work mapping (no reference counterpart):
@@ -407,8 +414,9 @@ int dycg_set_query_queue(dycg_engine *e, uint32_t scheme);
  * candidate mapping (qratio in {2,4,8,2^20} x heavy in {16,64,256} with the
  * pull phase on the same ratio, then the best of those with the pull phase's
  * ratio in {0,1,2,8}, then the best so far with query-lane tiles of
- * {1024,4096,16384} slots, then the best so far under the other three
- * frontier-queue schemes), each from the same saved state, keeps the fastest
+ * {1024,4096,16384} slots, then the best so far under the other
+ * frontier-queue schemes: static, claimed, ranges, claimed + ranges, async,
+ * async + claimed), each from the same saved state, keeps the fastest
  * mapping for later snapshots
  * and leaves the state of one ordinary repair. Needs HBM for one extra copy
  * of the query results while it runs. tried (cap entries, may be NULL)

@@ -109,7 +109,8 @@ def test_batched_work_mappings(qratio, heavy):
     run_queries("sssp", 64, "batched", stored=True, qratio=qratio, heavy=heavy, seed=9)
 
 
-@pytest.mark.parametrize("queue", ["static", "claimed", "ranges", "claimed+ranges"])
+@pytest.mark.parametrize("queue", ["static", "claimed", "ranges", "claimed+ranges", "async",
+                                   "async+claimed"])
 def test_batched_frontier_queue_schemes(queue):
     # every frontier-queue scheme (static or claimed items, plain or
     # range-ordered wave queues) gives the static recompute's results, heavy
@@ -198,10 +199,10 @@ def test_tune_mapping_keeps_results():
     tried = e.tune_query_mapping(dels, adds)
     orc.mutate(dels, adds)
     cur = orc.csr()
-    # 12 (qratio x heavy) + 3-4 pull ratios + 2-3 tile sizes + 3 frontier-queue schemes
-    assert 12 < len(tried) <= 22 and all(t["repair_ms"] > 0 for t in tried)
+    # 12 (qratio x heavy) + 3-4 pull ratios + 2-3 tile sizes + 5 frontier-queue schemes
+    assert 12 < len(tried) <= 24 and all(t["repair_ms"] > 0 for t in tried)
     assert {t["tile"] for t in tried} == {1024, 4096, 16384}
-    assert {t["queue"] for t in tried} == {0, 1, 2, 3}
+    assert {t["queue"] for t in tried} == {0, 1, 2, 3, 4, 5}
     _check_all(e, n, cur, src)
     for bi in range(2):  # later snapshots under the kept mapping
         dels, adds = cases.random_batch(n, *cur, 400, 400, 2310 + bi)

@@ -1675,9 +1675,12 @@ void Engine::policy_prefetch(size_t nd, size_t na, bool capture) {
   }
   if (policy_ == DYCG_CACHE_LEARNED && cache_slots_) {
     CK(launch_mlp_infer(feat_, npages_, params_, cwk_.score, cwk_.ids, st_));
-    // admit pages predicted to be read at least ~64 times in this snapshot,
+    // admit a page only when its predicted reads over the training horizon
+    // (log1p of slot reads) pay back at least half of its fill: a fill moves
+    // all 2^page_shift slots over the host link, a cached read saves one slot;
     // at most cache_slots / learned_cap_div_ per snapshot (no refresh gate)
-    CK(cache_rank_given(cwk_, npages_, cache_slots_, std::log1p(64.f), page_slot_, st_));
+    const float payback = std::log1p((float)(1u << page_shift_) * 0.5f);
+    CK(cache_rank_given(cwk_, npages_, cache_slots_, payback, page_slot_, st_));
     CachePages pg{out_.d_dst, has_in_ ? in_.d_dst : nullptr, out_.pages, page_shift_,
                   out_.stride, cdst_};
     const uint32_t cap = std::max<uint32_t>(cache_slots_ / learned_cap_div_, 256u);

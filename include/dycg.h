@@ -462,8 +462,9 @@ int dycg_gather_query(dycg_engine *e, uint32_t q, uint32_t *values, uint32_t *pa
  * read score, update records of this batch whose row starts in the page,
  * snapshots since the last read, rows starting in the page and the longest of
  * them -- these two refreshed every 8 snapshots), and stages the pages it
- * predicts to be read most (predicted reads >= 64) before the repair, up to
- * cache pages/256 per snapshot. Which pages are cached never changes results.
+ * predicts to be read most before the repair, when the predicted reads over
+ * the horizon cover at least half the page's slots (half its fill over the
+ * host link), up to cache pages/256 per snapshot. Which pages are cached never changes results.
  * The network predicts log1p(page reads over this snapshot and the next
  * two) and is trained on traces the engine records, by the library's own
  * forward/backward and Adam kernels on the GPU; one of its history features

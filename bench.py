@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--json-out", default=None)
     ap.add_argument("--mutation-ctas", type=int, default=0,
                     help="CTAs of the deletion/append kernels (0: the library default)")
+    ap.add_argument("--frontier-queue", default="static", choices=["static", "claimed"],
+                    help="single-source repair: how warps share a wave's rows")
     ap.add_argument("--queries", type=int, default=256, help="batched config: sources")
     ap.add_argument("--plain-queries", type=int, default=None,
                     help="batched config: queries timed on the per-query path (default all)")
@@ -200,6 +202,18 @@ def link_transaction_bound(link_bytes, launch_ms, ns_per_tx):
             "frac": round(bound_ms / launch_ms, 4) if launch_ms > 0 else None}
 
 
+def mutation_bound(updates, algo, ms, ns_per_tx):
+    """Lower bound on the mutation kernels' time per snapshot: one random host
+    transaction per update record (append or deletion window) and adjacency
+    direction (two where the incoming adjacency is kept: SSSP/BFS)."""
+    dirs = 2 if algo in ("sssp", "bfs") else 1
+    tx = int(updates) * dirs
+    bound_ms = tx * ns_per_tx / 1e6
+    return {"ns_per_transaction": ns_per_tx, "transactions": tx, "bound_ms": round(bound_ms, 4),
+            "ns_per_transaction_achieved": round(ms * 1e6 / tx, 2) if tx else None,
+            "frac": round(bound_ms / ms, 4) if ms > 0 else None}
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -293,6 +307,7 @@ def run_dycg(args):
                     hbm_graph_budget_bytes=budget,
                     symmetric=(algo == "cc" and args.config != "grid"), epsilon=1e-4,
                     device=local, mutation_ctas=args.mutation_ctas,
+                    frontier_queue=args.frontier_queue,
                     ordered_delta=args.ordered_delta if algo != "pr" else 0)
     wmax = 1000 if args.config == "grid" else 64
     if args.config == "grid":
@@ -396,8 +411,12 @@ def run_dycg(args):
                       "frac": round(ach_link / link_zc, 5),
                       "transaction_bound": link_transaction_bound(rep_link, float(rep_ms), tx_ns)},
         "roofline_time_frac": round(t_bound / (rep_ms / 1e3), 5),
+        # deletion search + appends: at least one random host transaction per
+        # appended occurrence and per deletion record, in each adjacency direction
         "mutation_kernels": {"ms": round(float(mut_ms), 4), "link_bytes": int(mut_bytes_link),
-                             "hbm_bytes": int(mut_bytes_hbm)},
+                             "hbm_bytes": int(mut_bytes_hbm),
+                             "transaction_bound": mutation_bound(per_step_updates, algo,
+                                                                 float(mut_ms), tx_ns)},
     }
     launches = int(sum(p["kernel_launches"] for p in per))
     out = {

@@ -104,23 +104,38 @@ struct PullOp {
   }
 };
 
-// Push relaxation of the out-edges of a frontier vertex.
+// Push relaxation of the out-edges of a frontier vertex. In the ordered
+// closure (vmin set) a vertex whose value is not below `thr` is carried to
+// the next wave's queue instead of expanded, and every carried value and
+// every improvement lowers *vmin, the next wave's minimum.
 template <uint32_t ALGO, bool STORED>
 struct RelaxOp {
   const RepairParams *P;
   uint32_t *outq;
   uint32_t *outc;
   uint32_t tag;
+  uint32_t thr;    // ordered closure: expand only values below this
+  uint32_t *vmin;  // ordered closure: running minimum of the next wave (or null)
   struct Row {
     uint32_t dv;
   };
   __device__ bool begin(uint32_t x, Row &r) {
     // one read, broadcast: the key may change under concurrent relaxations
     r.dv = __shfl_sync(0xffffffffu, key_value(ld_key(P->key + x)), 0);
+    if (vmin && r.dv != INF32 && r.dv >= thr) {
+      bool fresh = false;
+      if (lane_id() == 0) {
+        fresh = atomicExch(P->wtag + x, tag) != tag;
+        atomicMin(vmin, r.dv);
+      }
+      warp_append(outq, outc, P->n, fresh, x, &P->ctl->err);
+      return false;
+    }
     return r.dv != INF32;
   }
   __device__ void edge(uint32_t x, uint32_t y, uint32_t w, bool valid, Row &r, Acc &acc) {
     bool want = false;
+    uint32_t imp = INF32;  // value this lane lowered y to
     if (valid) {
       const u64 c = (u64)r.dv + (STORED ? w : rule_weight<ALGO>(x, y));
       if (c < INF32) {
@@ -134,10 +149,15 @@ struct RelaxOp {
         if (lowered) {
           acc.improved++;
           want = atomicExch(P->wtag + y, tag) != tag;
+          imp = (uint32_t)c;
         }
       }
     }
     warp_append(outq, outc, P->n, want, y, &P->ctl->err);
+    if (vmin) {
+      imp = (uint32_t)warp_min(imp);
+      if (lane_id() == 0 && imp != INF32) atomicMin(vmin, imp);
+    }
   }
   __device__ void end(uint32_t, Row &) {}
 };
@@ -241,8 +261,22 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
     // the reference's ordered insertion schedule (framework.cuh:537-556):
     // each wave expands only the frontier vertices whose value is below the
     // wave's minimum + delta and carries the rest to the next wave, so a
-    // vertex is expanded about once instead of once per improvement.
+    // vertex is expanded about once instead of once per improvement. One
+    // grid barrier per wave: the expansion pass carries the vertices at or
+    // above the threshold itself, and the next wave's minimum is kept on the
+    // fly (carried values and improvements lower ctl->vmin, which the wave's
+    // closing barrier snapshots and resets). Only the first wave's minimum
+    // needs a reduction pass.
     uint32_t cur = 0;
+    {
+      const uint32_t cnt = *(volatile uint32_t *)&ctl->snap_q[0];
+      uint32_t m = INF32;
+      for (uint32_t i = gtid; i < cnt; i += gstride)
+        m = min(m, key_value(ld_key(P.key + P.q[0][i])));
+      for (int o = 16; o; o >>= 1) m = min(m, __shfl_down_sync(0xffffffffu, m, o));
+      if (lane == 0 && m != INF32) atomicMin(&ctl->vmin, m);
+      if (!grid_sync(ctl, SYNC_RESET_VMIN, P.timeout_ns)) goto done;
+    }
     for (uint32_t wave = 0;; wave++) {
       const uint32_t cnt = *(volatile uint32_t *)&ctl->snap_q[cur];
       if (cnt == 0) break;
@@ -251,33 +285,11 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
         break;
       }
       const uint32_t tag = tag_base + 1 + wave;
-      uint32_t m = INF32;
-      for (uint32_t i = gtid; i < cnt; i += gstride)
-        m = min(m, key_value(ld_key(P.key + P.q[cur][i])));
-      for (int o = 16; o; o >>= 1) m = min(m, __shfl_down_sync(0xffffffffu, m, o));
-      if (lane == 0 && m != INF32) atomicMin(&ctl->vmin, m);
-      if (!grid_sync(ctl, 0, P.timeout_ns)) goto done;
       const uint32_t vm = *(volatile uint32_t *)&ctl->snap_vmin;
       const uint32_t thr = vm > INF32 - P.delta ? INF32 : vm + P.delta;
-      // split: values below thr form this wave's bucket, the rest carry over
-      for (uint32_t i0 = gtid - lane; i0 < cnt; i0 += gstride) {
-        const uint32_t i = i0 + lane;
-        uint32_t v = 0;
-        bool now = false, carry = false;
-        if (i < cnt) {
-          v = P.q[cur][i];
-          const uint32_t d = key_value(ld_key(P.key + v));
-          now = d < thr;
-          carry = !now && d != INF32 && atomicExch(P.wtag + v, tag) != tag;
-        }
-        warp_append(P.q2, &ctl->q_count[2], P.n, now, v, &ctl->err);
-        warp_append(P.q[cur ^ 1], &ctl->q_count[cur ^ 1], P.n, carry, v, &ctl->err);
-      }
-      if (!grid_sync(ctl, (cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0) | SYNC_RESET_VMIN, P.timeout_ns))
-        goto done;
-      const uint32_t nb = *(volatile uint32_t *)&ctl->snap_q[2];
-      RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag};
-      if (!expand_rows<STORED>(P.out, P.q2, nb, op, acc, P.tiles, ctl, SYNC_RESET_Q2,
+      RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag, thr, &ctl->vmin};
+      if (!expand_rows<STORED>(P.out, P.q[cur], cnt, op, acc, P.tiles, ctl,
+                               (cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0) | SYNC_RESET_VMIN,
                                P.timeout_ns, P.claimed))
         goto done;
       if (gtid == 0) ctl->waves = wave + 1;
@@ -292,7 +304,8 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
         if (gtid == 0) atomicCAS(&ctl->err, 0u, ERR_WAVES);
         break;
       }
-      RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag_base + 1 + wave};
+      RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag_base + 1 + wave,
+                               INF32, nullptr};
       if (!expand_rows<STORED>(P.out, P.q[cur], cnt, op, acc, P.tiles, ctl,
                                cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.timeout_ns, P.claimed))
         goto done;

@@ -157,6 +157,7 @@ def lib():
                                        ctypes.POINTER(ctypes.c_double)]),
         "dycg_measure_host_random": (I, [I, u64, u32, I, u64, ctypes.POINTER(ctypes.c_double)]),
         "dycg_measure_host_sweep": (I, [I, u64, u32, I, u64, u32, ctypes.POINTER(ctypes.c_double)]),
+        "dycg_check_bounded_wait": (I, [I, u32, u32p, u32p]),
         "dycg_group_updates": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
         "dycg_group_updates_noalloc": (I, [P, sz, u32, P, u32, P, P, P, P, P]),
         "dycg_set_queries": (I, [P, u32p, u32, u32]),

@@ -301,6 +301,19 @@ uint32_t dycg_hash_weight(uint64_t seed, uint32_t u, uint32_t v, uint32_t wlo,
  * loads (best of 5 each, GB/s). */
 int dycg_measure_host_link(int device, uint64_t bytes, double *h2d_gbs, double *zero_copy_gbs);
 
+/* Failure-detection check (no reference counterpart): every wait of the
+ * persistent repair kernels (grid barriers, worklist waits) is bounded by a
+ * time limit after which the kernel records an error status and returns, so
+ * a rank or block that never arrives is reported to the host instead of
+ * hanging the GPU. This runs the library's grid barrier in a cooperative
+ * launch of 8 blocks in which block 0 never arrives (it waits, bounded, on a
+ * flag that nothing sets): *status_absent receives the status the waiting
+ * blocks recorded (1, the barrier time-limit error, expected); then a launch
+ * in which every block arrives runs on the same context: *status_all (0
+ * expected). limit_ms in [1, 10000]. */
+int dycg_check_bounded_wait(int device, uint32_t limit_ms, uint32_t *status_absent,
+                            uint32_t *status_all);
+
 /* Measurement helper (no reference counterpart): cost of random host-link
  * transactions on `device` -- `ops` reads (write = 0) or writes of op_bytes
  * (4, 8 or 16 per thread, or 128 per warp) at random aligned offsets of a

@@ -105,16 +105,14 @@ struct PullOp {
 };
 
 // Push relaxation of the out-edges of a frontier vertex. In the ordered
-// closure (vmin set) a vertex whose value is not below `thr` is carried to
-// the next wave's queue instead of expanded, and every carried value and
-// every improvement lowers *vmin, the next wave's minimum.
+// closure (vmin set) every improvement also lowers *vmin, the next wave's
+// running minimum.
 template <uint32_t ALGO, bool STORED>
 struct RelaxOp {
   const RepairParams *P;
   uint32_t *outq;
   uint32_t *outc;
   uint32_t tag;
-  uint32_t thr;    // ordered closure: expand only values below this
   uint32_t *vmin;  // ordered closure: running minimum of the next wave (or null)
   struct Row {
     uint32_t dv;
@@ -122,15 +120,6 @@ struct RelaxOp {
   __device__ bool begin(uint32_t x, Row &r) {
     // one read, broadcast: the key may change under concurrent relaxations
     r.dv = __shfl_sync(0xffffffffu, key_value(ld_key(P->key + x)), 0);
-    if (vmin && r.dv != INF32 && r.dv >= thr) {
-      bool fresh = false;
-      if (lane_id() == 0) {
-        fresh = atomicExch(P->wtag + x, tag) != tag;
-        atomicMin(vmin, r.dv);
-      }
-      warp_append(outq, outc, P->n, fresh, x, &P->ctl->err);
-      return false;
-    }
     return r.dv != INF32;
   }
   __device__ void edge(uint32_t x, uint32_t y, uint32_t w, bool valid, Row &r, Acc &acc) {
@@ -161,6 +150,64 @@ struct RelaxOp {
   }
   __device__ void end(uint32_t, Row &) {}
 };
+
+// One wave of the ordered closure in a single pass: a warp takes 32
+// consecutive queue items, its lanes split them by value (below thr: expand
+// now; at or above: carry to the next queue, with the carried values' minimum
+// lowering the next wave's running minimum, one atomic per warp), then the
+// warp expands the items kept for now one by one (rows longer than HEAVY as
+// CTA tiles after the barrier, as expand_rows does).
+template <bool WITH_W, class Op>
+__device__ bool expand_ordered(const RepairParams &P, const uint32_t *items, uint32_t cnt,
+                               uint32_t thr, Op &op, Acc &acc, Ctl *ctl, uint32_t reset_flags) {
+  const Adj &A = P.out;
+  const uint32_t lane = lane_id();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i0 = gw * 32; i0 < cnt; i0 += nw * 32) {
+    const uint32_t i = i0 + lane;
+    uint32_t v = 0, dv = INF32;
+    if (i < cnt) {
+      v = items[i];
+      dv = key_value(ld_key(P.key + v));
+    }
+    const bool now = dv < thr;
+    const bool carry = dv != INF32 && !now && atomicExch(P.wtag + v, op.tag) != op.tag;
+    warp_append(op.outq, op.outc, P.n, carry, v, &ctl->err);
+    const uint32_t cm = (uint32_t)warp_min(carry ? dv : INF32);
+    if (lane == 0 && cm != INF32) atomicMin(op.vmin, cm);
+    unsigned todo = __ballot_sync(0xffffffffu, now);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint32_t x = __shfl_sync(0xffffffffu, v, src);
+      const uint32_t len = A.len[x];
+      if (len > HEAVY) {
+        if (lane == 0) {
+          const uint32_t nt = (len + TILE - 1) / TILE;
+          const uint32_t base = atomicAdd(&ctl->tile_count, nt);
+          if (base + nt > P.tiles.cap) {
+            atomicCAS(&ctl->err, 0u, ERR_TILES);
+          } else {
+            for (uint32_t t = 0; t < nt; t++)
+              P.tiles.tiles[base + t] = make_uint4(x, t * TILE, min(len, (t + 1) * TILE), 0);
+          }
+        }
+        continue;
+      }
+      warp_slots<WITH_W>(A, x, A.off[x], 0, len, 32, op, acc);
+    }
+  }
+  if (!grid_sync(ctl, reset_flags, P.timeout_ns)) return false;
+  const uint32_t nt = min(*(volatile uint32_t *)&ctl->snap_tiles, P.tiles.cap);
+  if (nt == 0) return true;
+  const uint32_t wib = threadIdx.x >> 5;
+  for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
+    const uint4 tl = P.tiles.tiles[t];
+    warp_slots<WITH_W>(A, tl.x, A.off[tl.x], tl.y + wib * 32, tl.z, blockDim.x, op, acc);
+  }
+  return grid_sync(ctl, SYNC_RESET_TILES, P.timeout_ns);
+}
 
 template <uint32_t ALGO, bool STORED>
 __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
@@ -287,10 +334,9 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
       const uint32_t tag = tag_base + 1 + wave;
       const uint32_t vm = *(volatile uint32_t *)&ctl->snap_vmin;
       const uint32_t thr = vm > INF32 - P.delta ? INF32 : vm + P.delta;
-      RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag, thr, &ctl->vmin};
-      if (!expand_rows<STORED>(P.out, P.q[cur], cnt, op, acc, P.tiles, ctl,
-                               (cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0) | SYNC_RESET_VMIN,
-                               P.timeout_ns, P.claimed))
+      RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag, &ctl->vmin};
+      if (!expand_ordered<STORED>(P, P.q[cur], cnt, thr, op, acc, ctl,
+                                  (cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0) | SYNC_RESET_VMIN))
         goto done;
       if (gtid == 0) ctl->waves = wave + 1;
       cur ^= 1;
@@ -305,7 +351,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
         break;
       }
       RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag_base + 1 + wave,
-                               INF32, nullptr};
+                               nullptr};
       if (!expand_rows<STORED>(P.out, P.q[cur], cnt, op, acc, P.tiles, ctl,
                                cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.timeout_ns, P.claimed))
         goto done;

@@ -308,12 +308,15 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
     // the reference's ordered insertion schedule (framework.cuh:537-556):
     // each wave expands only the frontier vertices whose value is below the
     // wave's minimum + delta and carries the rest to the next wave, so a
-    // vertex is expanded about once instead of once per improvement. One
-    // grid barrier per wave: the expansion pass carries the vertices at or
-    // above the threshold itself, and the next wave's minimum is kept on the
-    // fly (carried values and improvements lower ctl->vmin, which the wave's
-    // closing barrier snapshots and resets). Only the first wave's minimum
-    // needs a reduction pass.
+    // vertex is expanded about once instead of once per improvement. The
+    // next wave's minimum is kept on the fly (carried values and every
+    // improvement lower ctl->vmin, which the wave's closing barrier snapshots
+    // and resets), so only the first wave needs a reduction pass. SSSP and
+    // BFS split each wave's queue into a compact bucket first (a barrier),
+    // which spreads the bucket's rows over all warps (their buckets hold
+    // runs of consecutive queue entries); CC splits and expands in one pass
+    // (its waves are mostly carried entries, for which the split barrier is
+    // the larger cost).
     uint32_t cur = 0;
     {
       const uint32_t cnt = *(volatile uint32_t *)&ctl->snap_q[0];
@@ -335,9 +338,31 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
       const uint32_t vm = *(volatile uint32_t *)&ctl->snap_vmin;
       const uint32_t thr = vm > INF32 - P.delta ? INF32 : vm + P.delta;
       RelaxOp<ALGO, STORED> op{&P, P.q[cur ^ 1], &ctl->q_count[cur ^ 1], tag, &ctl->vmin};
-      if (!expand_ordered<STORED>(P, P.q[cur], cnt, thr, op, acc, ctl,
-                                  (cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0) | SYNC_RESET_VMIN))
-        goto done;
+      const uint32_t close = (cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0) | SYNC_RESET_VMIN;
+      if (ALGO == ALGO_CC) {
+        if (!expand_ordered<STORED>(P, P.q[cur], cnt, thr, op, acc, ctl, close)) goto done;
+      } else {
+        // split: values below thr form this wave's bucket, the rest carry over
+        for (uint32_t i0 = gtid - lane; i0 < cnt; i0 += gstride) {
+          const uint32_t i = i0 + lane;
+          uint32_t v = 0, d = INF32;
+          if (i < cnt) {
+            v = P.q[cur][i];
+            d = key_value(ld_key(P.key + v));
+          }
+          const bool now = d < thr;
+          const bool carry = !now && d != INF32 && atomicExch(P.wtag + v, tag) != tag;
+          warp_append(P.q2, &ctl->q_count[2], P.n, now, v, &ctl->err);
+          warp_append(P.q[cur ^ 1], &ctl->q_count[cur ^ 1], P.n, carry, v, &ctl->err);
+          const uint32_t cm = (uint32_t)warp_min(carry ? d : INF32);
+          if (lane == 0 && cm != INF32) atomicMin(&ctl->vmin, cm);
+        }
+        if (!grid_sync(ctl, cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.timeout_ns)) goto done;
+        const uint32_t nb = *(volatile uint32_t *)&ctl->snap_q[2];
+        if (!expand_rows<STORED>(P.out, P.q2, nb, op, acc, P.tiles, ctl,
+                                 SYNC_RESET_Q2 | SYNC_RESET_VMIN, P.timeout_ns, P.claimed))
+          goto done;
+      }
       if (gtid == 0) ctl->waves = wave + 1;
       cur ^= 1;
     }

@@ -75,7 +75,7 @@ def parse():
     ap.add_argument("--cpu-baseline-batches", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ordered-delta", type=int, default=None,
-                    help="bucketed closure width (default: 0 on R-MAT, on the grid 256 for SSSP "
+                    help="bucketed closure width (default: 0 on R-MAT, on the grid 2048 for SSSP "
                          "and 1 for BFS/CC)")
     ap.add_argument("--json-out", default=None)
     ap.add_argument("--mutation-ctas", type=int, default=0,
@@ -100,7 +100,9 @@ def parse():
     ap.add_argument("--batch-max", type=int, default=1_000_000)
     args = ap.parse_args()
     if args.ordered_delta is None:
-        args.ordered_delta = 0 if args.config != "grid" else (256 if args.algo == "sssp" else 1)
+        # grid SSSP (weights [1,1000]): delta 2048 took 330 ms per 10K snapshot against
+        # 611 ms at 256 (fewer waves, 8% more row expansions)
+        args.ordered_delta = 0 if args.config != "grid" else (2048 if args.algo == "sssp" else 1)
     defaults = {"rmat26": (26, 100_000, 4.0), "rmat16": (16, 2_000, 0.0),
                 "grid": (12, 10_000, 0.25), "batched": (24, 0, 2.0),
                 "learned": (27, 1_000_000, 8.0)}[args.config]

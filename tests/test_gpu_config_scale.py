@@ -3,7 +3,7 @@ from-scratch static recomputes on the host cores:
 
   * road-like grid 4096x4096 + 1% shortcuts within radius 8, HBM graph budget
     256 MB, one 10K-update snapshot (70% of the deletions on grid edges):
-    SSSP (weights [1,1000], ordered closure, delta 256), BFS and CC (ordered,
+    SSSP (weights [1,1000], ordered closure, delta 2048), BFS and CC (ordered,
     delta 1); the library's grid generator equals the host restatement the
     reference arm repairs, edge for edge;
   * R-MAT scale 26 (67.1M vertices, ~1.07B edges), HBM graph budget 4 GB, one
@@ -32,7 +32,7 @@ SEED = 20261203
 
 
 def _grid_engine(algo):
-    delta = 256 if algo == "sssp" else 1
+    delta = 2048 if algo == "sssp" else 1
     e = dg.Engine(algo, weight_mode="stored" if algo == "sssp" else "hash128",
                   hbm_graph_budget_bytes=256 << 20, ordered_delta=delta, device=0)
     e.load_grid(1 << GRID_LOG, 10, 8, seed=SEED, wlo=1, whi=1000)

@@ -284,7 +284,7 @@ int dycg_mlp_infer(const void *d_x, uint32_t n, const float *d_params, float *d_
   if (!d_params) return DYCG_EINVAL;
   if (!n) return DYCG_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  if (dycg::launch_mlp_infer(d_x, n, d_params, d_out, nullptr, s) != cudaSuccess)
+  if (dycg::launch_mlp_infer(d_x, n, d_params, d_out, nullptr, nullptr, s) != cudaSuccess)
     return DYCG_ECUDA;
   return cudaStreamSynchronize(s) == cudaSuccess ? DYCG_OK : DYCG_ECUDA;
 }

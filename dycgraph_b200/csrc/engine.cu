@@ -1674,7 +1674,7 @@ void Engine::policy_prefetch(size_t nd, size_t na, bool capture) {
     CK(cudaMemsetAsync(ty_ + (u64)trace_n_ * np, 0, np * 4, st_));
   }
   if (policy_ == DYCG_CACHE_LEARNED && cache_slots_) {
-    CK(launch_mlp_infer(feat_, npages_, params_, cwk_.score, cwk_.ids, st_));
+    CK(launch_mlp_infer(feat_, npages_, params_, cwk_.score, cwk_.ids, &ctl_->err, st_));
     // admit a page only when its predicted reads over the training horizon
     // (log1p of slot reads) pay back at least half of its fill: a fill moves
     // all 2^page_shift slots over the host link, a cached read saves one slot;

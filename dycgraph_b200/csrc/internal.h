@@ -257,8 +257,10 @@ struct TargetRefs {
 cudaError_t launch_history(uint32_t *hits, float *hist, uint8_t *age, uint32_t npages,
                            const TargetRefs &tg, bool clear, cudaStream_t s);
 cudaError_t launch_log1p(const float *in, float *out, u64 n, cudaStream_t s);
+// tcgen05 inference; err (optional) receives ERR_BARRIER if a tensor-core
+// completion wait ran out
 cudaError_t launch_mlp_infer(const void *x, uint32_t n, const float *params, float *score,
-                             uint32_t *ids, cudaStream_t s);
+                             uint32_t *ids, uint32_t *err, cudaStream_t s);
 cudaError_t launch_mlp_grad(const void *x, const float *y, uint64_t total, uint32_t count,
                             uint64_t sample_seed, const float *params, float scale, float *grad,
                             float *loss, cudaStream_t s);

@@ -23,9 +23,10 @@
 // accumulation and FP32 master weights; loss = mean squared error.
 //
 // The MLP is 4.7K multiply-adds per page. Inference runs every snapshot over
-// every page (1.85M pages at R-MAT 27, ~9 GMAC): it runs on the tensor cores
-// (mma.sync BF16 tiles of 16 pages), where the FP32-FMA version took ~1.2 ms
-// per snapshot. Training runs once per trained network on FP32 FMA tiles.
+// every page (1.85M pages at R-MAT 27, ~9 GMAC): it runs on the 5th-generation
+// tensor cores (tcgen05.mma, 128-page tiles, accumulators in tensor memory),
+// where the FP32-FMA version took ~1.2 ms per snapshot. Training runs once per
+// trained network on FP32 FMA tiles.
 #include <cuda_bf16.h>
 
 #include <atomic>
@@ -150,127 +151,223 @@ __global__ void log1p_kernel(const float *in, float *out, u64 n) {
 
 // ---- inference -----------------------------------------------------------------
 
-// Tensor-core fragments (mma.sync, BF16 operands, FP32 accumulation). In a
-// warp, g = lane / 4 and t = lane % 4; a 16 x K A fragment holds rows g and
-// g + 8, columns 2t, 2t + 1 (and 2t + 8, 2t + 9 for K = 16); a K x 8 B
-// fragment holds rows 2t, 2t + 1 (and 2t + 8, 2t + 9) of column g; the 16 x 8
-// FP32 accumulator holds rows g and g + 8, columns 2t and 2t + 1.
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
   __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);  // lo in the low half
   return *reinterpret_cast<uint32_t *>(&v);
 }
 
-__device__ __forceinline__ void mma_k8(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
-  asm("mma.sync.aligned.m16n8k8.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a0), "r"(a1), "r"(b0));
+// ---- inference on the 5th-generation tensor cores (tcgen05) ---------------------
+
+// A CTA of 4 warps serves 128 pages per tile: layer 1 and layer 2 are
+// tcgen05.mma products (M = 128 pages, N = 64 hidden units, K = 16 per
+// instruction, BF16 operands from shared memory, FP32 accumulators in tensor
+// memory), issued by one thread; each thread then reads its page's row of
+// the accumulator back with tcgen05.ld (warp w owns tensor-memory lanes
+// 32w..32w+31) for the bias / ReLU epilogue, the BF16 hi + lo split of the
+// layer-1 activations (both parts go through layer 2, so the activations keep
+// FP32-level precision: h = hi + lo to ~2^-17 relative, while a single BF16
+// rounding missed the float64 oracle's tolerance by 60-190x) and the final
+// FP32 dot product. Operands sit in shared
+// memory in the no-swizzle K-major layout of 8-row x 16-byte core matrices:
+// element (row, k) of an operand with KC chunks of 8 along K lives at
+// ((row / 8) * KC + k / 8) * 128 + (row % 8) * 16 + (k % 8) * 2 bytes, so the
+// descriptor's leading byte offset (next core matrix along K) is 128 and its
+// stride byte offset (next 8 rows) is KC * 128.
+namespace tc {
+constexpr uint32_t M = 128, N = 64;
+constexpr uint32_t SM_A1 = 0;                  // 128 x 16 (KC 2): 4 KB
+constexpr uint32_t SM_B1 = SM_A1 + 4096;       // 64 x 16 (KC 2): 2 KB
+constexpr uint32_t SM_A2H = SM_B1 + 2048;      // 128 x 64 (KC 8): 16 KB
+constexpr uint32_t SM_A2L = SM_A2H + 16384;    // 16 KB
+constexpr uint32_t SM_B2 = SM_A2L + 16384;     // 64 x 64 (KC 8): 8 KB
+constexpr uint32_t SM_BAR = SM_B2 + 8192;      // mbarrier (8 B) + tensor-memory address (4 B)
+constexpr uint32_t SM_BYTES = SM_BAR + 16;
+// idesc: D FP32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both
+// K-major, N >> 3 in bits 17-22, M >> 4 in bits 24-28
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+
+__device__ __forceinline__ uint32_t off(uint32_t row, uint32_t k, uint32_t kc) {
+  return ((row >> 3) * kc + (k >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
-
-__device__ __forceinline__ void mma_k16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
-                                        uint32_t b1) {
-  asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-      "{%8,%9}, {%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+// shared-memory matrix descriptor: start >> 4 (bits 0-13), leading byte
+// offset >> 4 (bits 16-29), stride byte offset >> 4 (bits 32-45), version 1
+// (bits 46-47), no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ u64 sdesc(uint32_t saddr, uint32_t sbo) {
+  return (u64)((saddr >> 4) & 0x3FFF) | ((u64)(128 >> 4) << 16) | ((u64)((sbo >> 4) & 0x3FFF) << 32) |
+         (1ull << 46);
 }
-
-constexpr int IB = 128;  // inference block: 4 warps
-
-// score[p] = MLP(x[p]); ids[p] = p (for the admission sort). A warp runs 16
-// pages per tile: layer 1 as eight m16n8k8 products (K = the 8 features),
-// layer 2 as m16n8k16 products over the 64 hidden units, layer 3 as an FP32
-// dot product reduced over each lane quad. The first layer's FP32 outputs are
-// split into BF16 hi + lo parts (h = hi + lo to ~2^-17 relative) and both parts
-// go through layer 2, so activations keep FP32-level precision while the
-// operands stay BF16; the weight fragments live in registers for the whole
-// kernel.
-__global__ void __launch_bounds__(IB, 3) mlp_infer_kernel(const __nv_bfloat16 *x, uint32_t n,
-                                                          const float *params, float *score,
-                                                          uint32_t *ids) {
-  __shared__ __align__(16) float w[POLICY_PARAMS];
-  load_params(params, w);
-  const uint32_t lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-  uint32_t b1f[8];
-#pragma unroll
-  for (int j = 0; j < 8; j++)
-    b1f[j] = pack2(w[OFF_W1 + (2 * t) * H + 8 * j + g], w[OFF_W1 + (2 * t + 1) * H + 8 * j + g]);
-  uint32_t b2f[4][8][2];
-#pragma unroll
-  for (int kk = 0; kk < 4; kk++)
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const int k0 = 16 * kk + 2 * t, c = OFF_W2 + 8 * j + g;
-      b2f[kk][j][0] = pack2(w[c + k0 * H], w[c + (k0 + 1) * H]);
-      b2f[kk][j][1] = pack2(w[c + (k0 + 8) * H], w[c + (k0 + 9) * H]);
-    }
-  const float b3 = w[OFF_B3];
-  const uint32_t *xw = reinterpret_cast<const uint32_t *>(x);  // F = 8 BF16 = 4 words per page
-  const uint32_t tiles = (n + 15) / 16;
-  const uint32_t nwarps = gridDim.x * (IB / 32);
-  uint32_t tile = (blockIdx.x * IB + threadIdx.x) >> 5;
-  auto load_row = [&](uint32_t r) { return r < n ? __ldg(xw + (u64)r * 4 + t) : 0u; };
-  uint32_t na0 = load_row(tile * 16 + g), na1 = load_row(tile * 16 + g + 8);
-  for (; tile < tiles; tile += nwarps) {
-    const uint32_t a0 = na0, a1 = na1;
-    const uint32_t r0 = tile * 16 + g, r1 = r0 + 8;
-    if (tile + nwarps < tiles) {  // next tile's inputs in flight during this one
-      na0 = load_row(r0 + nwarps * 16);
-      na1 = load_row(r1 + nwarps * 16);
-    }
-    float c2[8][4];
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const float2 b = *reinterpret_cast<const float2 *>(&w[OFF_B2 + 8 * j + 2 * t]);
-      c2[j][0] = b.x, c2[j][1] = b.y, c2[j][2] = b.x, c2[j][3] = b.y;
-    }
-#pragma unroll
-    for (int kk = 0; kk < 4; kk++) {
-      // hidden units 16kk .. 16kk+15 of layer 1 = the A fragment of layer 2
-      uint32_t hi[4], lo[4];
-#pragma unroll
-      for (int half = 0; half < 2; half++) {
-        const int j1 = 2 * kk + half;
-        const float2 b = *reinterpret_cast<const float2 *>(&w[OFF_B1 + 8 * j1 + 2 * t]);
-        float c[4] = {b.x, b.y, b.x, b.y};
-        mma_k8(c, a0, a1, b1f[j1]);
-        float h[4], r[4];
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-          const float v = fmaxf(c[e], 0.f);
-          h[e] = bf(v);
-          r[e] = v - h[e];  // exact in FP32
-        }
-        hi[2 * half] = pack2(h[0], h[1]);
-        hi[2 * half + 1] = pack2(h[2], h[3]);
-        lo[2 * half] = pack2(r[0], r[1]);
-        lo[2 * half + 1] = pack2(r[2], r[3]);
-      }
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        mma_k16(c2[j], hi, b2f[kk][j][0], b2f[kk][j][1]);
-        mma_k16(c2[j], lo, b2f[kk][j][0], b2f[kk][j][1]);
-      }
-    }
-    float y0 = 0.f, y1 = 0.f;
-#pragma unroll
-    for (int j = 0; j < 8; j++) {
-      const float2 w3 = *reinterpret_cast<const float2 *>(&w[OFF_W3 + 8 * j + 2 * t]);
-      y0 = fmaf(fmaxf(c2[j][0], 0.f), w3.x, y0);
-      y0 = fmaf(fmaxf(c2[j][1], 0.f), w3.y, y0);
-      y1 = fmaf(fmaxf(c2[j][2], 0.f), w3.x, y1);
-      y1 = fmaf(fmaxf(c2[j][3], 0.f), w3.y, y1);
-    }
-    y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
-    y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
-    y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
-    y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
-    if (t == 0) {
-      if (r0 < n) score[r0] = y0 + b3;
-      if (r1 < n) score[r1] = y1 + b3;
-    }
-    if (ids && lane < 16 && tile * 16 + lane < n) ids[tile * 16 + lane] = tile * 16 + lane;
+__device__ __forceinline__ void mma(uint32_t d_tmem, u64 a, u64 b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+      :
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(0u));
+}
+__device__ __forceinline__ void commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :
+               : "r"(bar)
+               : "memory");
+}
+// bounded wait on the mbarrier's phase; false when the limit ran out
+__device__ __forceinline__ bool wait(uint32_t bar, uint32_t phase) {
+  const u64 t0 = globaltimer_ns();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+    if (globaltimer_ns() - t0 > 1000000000ull) return false;
   }
+}
+// 64 FP32 columns of this thread's tensor-memory lane, in two 32-column loads
+__device__ __forceinline__ void ld64(uint32_t taddr, float (&v)[64]) {
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+        "%28, %29, %30, %31}, [%32];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr + 32 * h));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[32 * h + i] = __uint_as_float(r[i]);
+  }
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+}  // namespace tc
+
+__global__ void __launch_bounds__(128, 1) mlp_infer_tc_kernel(const __nv_bfloat16 *x, uint32_t n,
+                                                              const float *params, float *score,
+                                                              uint32_t *ids, uint32_t *err) {
+  extern __shared__ __align__(1024) uint8_t sm_tc[];
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm_tc);
+  const uint32_t bar = sbase + tc::SM_BAR;
+  uint32_t *taddr_slot = reinterpret_cast<uint32_t *>(sm_tc + tc::SM_BAR + 8);
+  // the weights as the B operands (N = hidden unit, K = input), BF16; the
+  // padding columns 8..15 of layer 1 are zero; biases and W3 in registers
+  for (uint32_t i = tid; i < tc::N * 16; i += blockDim.x) {
+    const uint32_t nn = i / 16, k = i % 16;
+    const float wv = k < (uint32_t)F ? params[OFF_W1 + k * H + nn] : 0.f;
+    *reinterpret_cast<__nv_bfloat16 *>(sm_tc + tc::SM_B1 + tc::off(nn, k, 2)) = __float2bfloat16_rn(wv);
+  }
+  for (uint32_t i = tid; i < tc::N * (uint32_t)H; i += blockDim.x) {
+    const uint32_t nn = i / H, k = i % H;
+    *reinterpret_cast<__nv_bfloat16 *>(sm_tc + tc::SM_B2 + tc::off(nn, k, 8)) =
+        __float2bfloat16_rn(params[OFF_W2 + k * H + nn]);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {  // 128 tensor-memory columns: layer 1 in 0..63, layer 2 in 64..127
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;" ::"r"(
+        sbase + tc::SM_BAR + 8));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = *taddr_slot;
+  const uint32_t lane_base = (32 * warp) << 16;  // this warp's tensor-memory lanes
+  const float b3 = bf(params[OFF_B3]);
+  uint32_t phase = 0;
+  bool ok = true;
+  const uint32_t tiles = (n + tc::M - 1) / tc::M;
+  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    const uint32_t row = tile * tc::M + tid;
+    // A1: this page's 8 BF16 features, zero padding to K = 16
+    {
+      uint4 f = make_uint4(0, 0, 0, 0);
+      if (row < n) f = __ldg(reinterpret_cast<const uint4 *>(x) + row);
+      *reinterpret_cast<uint4 *>(sm_tc + tc::SM_A1 + tc::off(tid, 0, 2)) = f;
+      *reinterpret_cast<uint4 *>(sm_tc + tc::SM_A1 + tc::off(tid, 8, 2)) = make_uint4(0, 0, 0, 0);
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (tid == 0) {
+      tc::mma(tmem, tc::sdesc(sbase + tc::SM_A1, 256), tc::sdesc(sbase + tc::SM_B1, 256), 0);
+      tc::commit(bar);
+    }
+    ok = tc::wait(bar, phase);
+    phase ^= 1;
+    tc::fence_after();
+    float v[64];
+    tc::ld64(tmem + lane_base, v);
+    // layer-1 epilogue: bias, ReLU, BF16 hi + lo parts as the A operands of layer 2
+#pragma unroll
+    for (int h = 0; h < H; h += 8) {
+      uint32_t hw[4], lw[4];
+#pragma unroll
+      for (int e = 0; e < 8; e += 2) {
+        const float a0 = fmaxf(v[h + e] + bf(params[OFF_B1 + h + e]), 0.f);
+        const float a1 = fmaxf(v[h + e + 1] + bf(params[OFF_B1 + h + e + 1]), 0.f);
+        const float h0 = bf(a0), h1 = bf(a1);
+        hw[e / 2] = pack2(h0, h1);
+        lw[e / 2] = pack2(a0 - h0, a1 - h1);
+      }
+      *reinterpret_cast<uint4 *>(sm_tc + tc::SM_A2H + tc::off(tid, h, 8)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+      *reinterpret_cast<uint4 *>(sm_tc + tc::SM_A2L + tc::off(tid, h, 8)) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (tid == 0 && ok) {
+#pragma unroll
+      for (uint32_t s = 0; s < (uint32_t)H / 16; s++) {
+        const uint32_t kb = s * 256;  // 16 K-elements = two core matrices along K
+        tc::mma(tmem + tc::N, tc::sdesc(sbase + tc::SM_A2H + kb, 1024),
+                tc::sdesc(sbase + tc::SM_B2 + kb, 1024), s > 0);
+        tc::mma(tmem + tc::N, tc::sdesc(sbase + tc::SM_A2L + kb, 1024),
+                tc::sdesc(sbase + tc::SM_B2 + kb, 1024), 1);
+      }
+      tc::commit(bar);
+    }
+    if (ok) ok = tc::wait(bar, phase);
+    phase ^= 1;
+    tc::fence_after();
+    tc::ld64(tmem + lane_base + tc::N, v);
+    float y = 0.f;
+#pragma unroll
+    for (int h = 0; h < H; h++)
+      y = fmaf(fmaxf(v[h] + bf(params[OFF_B2 + h]), 0.f), bf(params[OFF_W3 + h]), y);
+    if (row < n) {
+      score[row] = y + b3;
+      if (ids) ids[row] = row;
+    }
+    tc::fence_before();
+    __syncthreads();  // every lane's reads of the accumulators are done before the next tile
+    tc::fence_after();
+  }
+  if (!ok && err && tid == 0) atomicCAS(err, 0u, ERR_BARRIER);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tmem));
 }
 
 // ---- training ------------------------------------------------------------------
@@ -490,13 +587,14 @@ cudaError_t launch_log1p(const float *in, float *out, u64 n, cudaStream_t s) {
 }
 
 cudaError_t launch_mlp_infer(const void *x, uint32_t n, const float *params, float *score,
-                             uint32_t *ids, cudaStream_t s) {
-  const u64 warps = ((u64)n + 15) / 16;
-  const int grid = (int)std::max<u64>(1, std::min<u64>((warps + 3) / 4, 148ull * 3));
-  mlp_infer_kernel<<<grid, IB, 0, s>>>((const __nv_bfloat16 *)x, n, params, score, ids);
+                             uint32_t *ids, uint32_t *err, cudaStream_t s) {
+  if (!n) return cudaSuccess;
+  const uint32_t tiles = (n + tc::M - 1) / tc::M;
+  const int grid = (int)std::min<uint32_t>(tiles, 148u * 2);
+  mlp_infer_tc_kernel<<<grid, 128, tc::SM_BYTES, s>>>((const __nv_bfloat16 *)x, n, params, score,
+                                                      ids, err);
   return cudaGetLastError();
 }
-
 cudaError_t launch_mlp_grad(const void *x, const float *y, uint64_t total, uint32_t count,
                             uint64_t sample_seed, const float *params, float scale, float *grad,
                             float *loss, cudaStream_t s) {

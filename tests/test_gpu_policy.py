@@ -37,8 +37,9 @@ def test_mlp_gradient_matches_oracle(n):
     assert np.max(np.abs(gg - go)) <= tol, (np.max(np.abs(gg - go)), tol)
 
 
-def test_mlp_inference_matches_oracle():
-    n = 3001
+@pytest.mark.parametrize("n", [1, 127, 3001, 100_037])
+def test_mlp_inference_matches_oracle(n):
+    # tcgen05 inference: 128 pages per tile, partial last tiles, several tiles per CTA
     x, _, xd, _ = _device_inputs(n, 7)
     p = mlp.glorot_params(7)
     out = torch.empty(n, dtype=torch.float32, device="cuda")

@@ -180,7 +180,8 @@ constexpr uint32_t SM_B1 = SM_A1 + 4096;       // 64 x 16 (KC 2): 2 KB
 constexpr uint32_t SM_A2H = SM_B1 + 2048;      // 128 x 64 (KC 8): 16 KB
 constexpr uint32_t SM_A2L = SM_A2H + 16384;    // 16 KB
 constexpr uint32_t SM_B2 = SM_A2L + 16384;     // 64 x 64 (KC 8): 8 KB
-constexpr uint32_t SM_BAR = SM_B2 + 8192;      // mbarrier (8 B) + tensor-memory address (4 B)
+constexpr uint32_t SM_BIAS = SM_B2 + 8192;     // b1, b2, W3 (BF16-rounded, FP32): 768 B
+constexpr uint32_t SM_BAR = SM_BIAS + 768;     // mbarrier (8 B) + tensor-memory address (4 B)
 constexpr uint32_t SM_BYTES = SM_BAR + 16;
 // idesc: D FP32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both
 // K-major, N >> 3 in bits 17-22, M >> 4 in bits 24-28
@@ -255,7 +256,7 @@ __device__ __forceinline__ void fence_after() {
 }
 }  // namespace tc
 
-__global__ void __launch_bounds__(128, 1) mlp_infer_tc_kernel(const __nv_bfloat16 *x, uint32_t n,
+__global__ void __launch_bounds__(128, 4) mlp_infer_tc_kernel(const __nv_bfloat16 *x, uint32_t n,
                                                               const float *params, float *score,
                                                               uint32_t *ids, uint32_t *err) {
   extern __shared__ __align__(1024) uint8_t sm_tc[];
@@ -275,6 +276,9 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_tc_kernel(const __nv_bfloat1
     *reinterpret_cast<__nv_bfloat16 *>(sm_tc + tc::SM_B2 + tc::off(nn, k, 8)) =
         __float2bfloat16_rn(params[OFF_W2 + k * H + nn]);
   }
+  float *bias = reinterpret_cast<float *>(sm_tc + tc::SM_BIAS);  // b1[64], b2[64], W3[64]
+  for (uint32_t i = tid; i < 3 * (uint32_t)H; i += blockDim.x)
+    bias[i] = bf(params[(i < (uint32_t)H ? OFF_B1 : i < 2u * H ? OFF_B2 - H : OFF_W3 - 2 * H) + i]);
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -322,8 +326,8 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_tc_kernel(const __nv_bfloat1
       uint32_t hw[4], lw[4];
 #pragma unroll
       for (int e = 0; e < 8; e += 2) {
-        const float a0 = fmaxf(v[h + e] + bf(params[OFF_B1 + h + e]), 0.f);
-        const float a1 = fmaxf(v[h + e + 1] + bf(params[OFF_B1 + h + e + 1]), 0.f);
+        const float a0 = fmaxf(v[h + e] + bias[h + e], 0.f);
+        const float a1 = fmaxf(v[h + e + 1] + bias[h + e + 1], 0.f);
         const float h0 = bf(a0), h1 = bf(a1);
         hw[e / 2] = pack2(h0, h1);
         lw[e / 2] = pack2(a0 - h0, a1 - h1);
@@ -353,7 +357,7 @@ __global__ void __launch_bounds__(128, 1) mlp_infer_tc_kernel(const __nv_bfloat1
     float y = 0.f;
 #pragma unroll
     for (int h = 0; h < H; h++)
-      y = fmaf(fmaxf(v[h] + bf(params[OFF_B2 + h]), 0.f), bf(params[OFF_W3 + h]), y);
+      y = fmaf(fmaxf(v[h] + bias[H + h], 0.f), bias[2 * H + h], y);
     if (row < n) {
       score[row] = y + b3;
       if (ids) ids[row] = row;
@@ -590,7 +594,9 @@ cudaError_t launch_mlp_infer(const void *x, uint32_t n, const float *params, flo
                              uint32_t *ids, uint32_t *err, cudaStream_t s) {
   if (!n) return cudaSuccess;
   const uint32_t tiles = (n + tc::M - 1) / tc::M;
-  const int grid = (int)std::min<uint32_t>(tiles, 148u * 2);
+  // up to 4 CTAs per SM (4 x 128 tensor-memory columns = all 512), so an SM
+  // overlaps the MMA and epilogue latencies of four tiles
+  const int grid = (int)std::min<uint32_t>(tiles, 148u * 4);
   mlp_infer_tc_kernel<<<grid, 128, tc::SM_BYTES, s>>>((const __nv_bfloat16 *)x, n, params, score,
                                                       ids, err);
   return cudaGetLastError();

@@ -82,6 +82,9 @@ def parse():
                     help="CTAs of the deletion/append kernels (0: the library default)")
     ap.add_argument("--frontier-queue", default="static", choices=["static", "claimed"],
                     help="single-source repair: how warps share a wave's rows")
+    ap.add_argument("--page-shift", type=int, default=12,
+                    help="single-source lines: log2 adjacency slots per cache page (8-20); "
+                         "20 approximates the reference's SEGMENT-sized chunks")
     ap.add_argument("--queries", type=int, default=256, help="batched config: sources")
     ap.add_argument("--plain-queries", type=int, default=None,
                     help="batched config: queries timed on the per-query path (default all)")
@@ -309,7 +312,7 @@ def run_dycg(args):
                     hbm_graph_budget_bytes=budget,
                     symmetric=(algo == "cc" and args.config != "grid"), epsilon=1e-4,
                     device=local, mutation_ctas=args.mutation_ctas,
-                    frontier_queue=args.frontier_queue,
+                    frontier_queue=args.frontier_queue, page_shift=args.page_shift,
                     ordered_delta=args.ordered_delta if algo != "pr" else 0)
     wmax = 1000 if args.config == "grid" else 64
     if args.config == "grid":
@@ -436,6 +439,7 @@ def run_dycg(args):
                    "inserts_per_step": na, "weights": f"uint32 uniform [1,{wmax}] stored"
                    if algo == "sssp" else "rule", "graph_host_bytes": info["host_bytes"],
                    "cached_pages": info["cached_pages"], "cache_slots": info["cache_slots"],
+                   "page_slots": 1 << args.page_shift,
                    "l2": "inputs larger than L2 (graph in pinned host memory, vertex state "
                          f"{info['nodes'] * 40 / 1e9:.1f} GB in HBM)",
                    "parallelism": f"replicas x{world}", "ordered_delta": args.ordered_delta,
@@ -450,8 +454,11 @@ def run_dycg(args):
         "per_step": {k: round(float(np.mean([p[k] for p in per])), 4) for k in
                      ("ms_ingest", "ms_mutate", "ms_repair", "ms_cache", "ms_total", "affected",
                       "expanded", "edges_scanned", "improvements", "waves", "relocated_rows",
-                      "missing_deletes", "cache_pages_loaded")},
+                      "missing_deletes", "cache_pages_loaded", "link_bytes", "hbm_adj_bytes")},
     }
+    _hb = float(np.sum([p["hbm_adj_bytes"] for p in per]))
+    out["per_step"]["adjacency_hit_rate"] = round(
+        _hb / max(1.0, _hb + float(np.sum([p["link_bytes"] for p in per]))), 4)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         if algo == "cc" and args.config == "grid":
             out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(),
@@ -726,8 +733,9 @@ def run_reference_batched(args):
     T = args.trace_snapshots
     E = args.e2e_steps if args.e2e_steps is not None else min(K, 8)
     rng = np.random.default_rng(args.seed + 41)
-    sizes = np.exp(rng.uniform(np.log(args.batch_min), np.log(args.batch_max), T + W + K + E))
+    sizes = np.exp(rng.uniform(np.log(args.batch_min), np.log(args.batch_max), T + W + K))
     sizes = np.maximum(2, sizes.astype(np.int64))
+    sizes = np.concatenate([sizes, sizes[T + W:T + W + E]])
     sizes = np.concatenate([[args.tune_batch], sizes])
     nd = sizes // 2
     na = sizes - nd
@@ -843,8 +851,11 @@ def run_batched(args):
     Q = args.queries
     budget = int(args.budget_gb * (1 << 30))
     rng = np.random.default_rng(args.seed + 41 + 1000 * rank)
-    sizes = np.exp(rng.uniform(np.log(args.batch_min), np.log(args.batch_max), T + W + K + E))
+    sizes = np.exp(rng.uniform(np.log(args.batch_min), np.log(args.batch_max), T + W + K))
     sizes = np.maximum(2, sizes.astype(np.int64))
+    # the e2e snapshots (new records) repeat the sizes of the first E timed
+    # ones, so e2e and value are rates over the same size mix
+    sizes = np.concatenate([sizes, sizes[T + W:T + W + E]])
     # snapshot 0 tunes the work mapping (untimed); all deletions are disjoint
     sizes = np.concatenate([[args.tune_batch], sizes])
 
@@ -1050,14 +1061,15 @@ def run_batched(args):
                    "parallelism": f"replicas x{world}", "load_s": round(L["load_s"], 2),
                    "static_solve_s": round(L["init_s"], 2)},
         "clocks": L["clk"],
-        # e2e runs on the E snapshots drawn after the timed ones (other
-        # log-uniform sizes): compare per-update rates with their mean sizes
+        # e2e runs on E snapshots drawn after the timed ones, with the sizes
+        # of the first E timed snapshots
         "e2e": {"value": round(e2e_value, 1) if e2e_value else None, "unit": UNIT,
                 "h2d_bytes_per_step": int(L["e2e_upd"] * 12 / max(E, 1)),
                 "d2h_bytes_per_step": int(sizeof_ctl() * 1), "steps": E,
                 "mean_updates_per_step": int(L["e2e_upd"] / max(E, 1)),
                 "timed_mean_updates_per_step": int(L["upd"] / max(K, 1)),
-                "snapshots": "the e2e steps' own snapshots, drawn after the timed ones"},
+                "snapshots": "the e2e steps' own snapshots, drawn after the timed ones, with "
+                             "the sizes of the first E timed snapshots"},
         "gpu_launches": int(sum(p["kernel_launches"] for p in per)),
         "roofline": roofline,
         "per_step": per_step,

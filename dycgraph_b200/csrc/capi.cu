@@ -295,7 +295,8 @@ int dycg_mlp_loss_grad(const void *d_x, const float *d_y, uint32_t n, const floa
   if (!d_params || !d_grad || !d_loss) return DYCG_EINVAL;
   if (!n) return DYCG_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  if (dycg::launch_mlp_grad(d_x, d_y, n, n, 0, d_params, 2.f, d_grad, d_loss, s) != cudaSuccess)
+  if (dycg::launch_mlp_grad(d_x, d_y, n, n, 0, d_params, 2.f, d_grad, d_loss, nullptr, s) !=
+      cudaSuccess)
     return DYCG_ECUDA;
   return cudaStreamSynchronize(s) == cudaSuccess ? DYCG_OK : DYCG_ECUDA;
 }

@@ -544,7 +544,6 @@ void Engine::init() {
     L.n = n_;
     L.cur = 0;
     L.phases = PR_CONVERGE;
-    L.sign = 1.f;
     L.eps = opt_.epsilon;
     L.alpha = opt_.alpha;
     L.max_rounds = opt_.max_rounds;
@@ -610,6 +609,8 @@ void Engine::reserve_batch(size_t max_records) {
     for (uint32_t c = 1024; c <= top; c *= 2) graph_for(c);
   } else {
     ensure_batch(std::max<size_t>(max_records, 1));
+    // deferred deletions: hub rows' unsorted suffixes, a few slots per record
+    ensure_defer(4ull * max_records);
   }
   sync_check("reserve batch");
 }
@@ -707,24 +708,33 @@ void Engine::delete_direction(const Adj &A, const uint2 *uv, const uint32_t *mul
   const u64 pk = *h_dpacked_;
   const uint32_t nrows = (uint32_t)(pk >> 40);
   const u64 total = pk & ((1ull << 40) - 1);
-  if (total > dbuf_cap_) {
-    for (void *p : {(void *)dbufs_.k_in, (void *)dbufs_.k_out, (void *)dbufs_.v_in,
-                    (void *)dbufs_.v_out, dbufs_.temp})
-      cudaFree(p);
-    dbufs_ = DeferBufs{};
-    dbuf_cap_ = 0;
-    const u64 c = total + total / 2;
-    CK(cudaMalloc((void **)&dbufs_.k_in, c * 8));
-    CK(cudaMalloc((void **)&dbufs_.k_out, c * 8));
-    CK(cudaMalloc((void **)&dbufs_.v_in, c * 4));
-    CK(cudaMalloc((void **)&dbufs_.v_out, c * 4));
-    dbufs_.temp_bytes = delete_sort_temp_bytes(c);
-    CK(cudaMalloc(&dbufs_.temp, std::max<size_t>(dbufs_.temp_bytes, 16)));
-    dbuf_cap_ = c;
-  }
+  if (total > dbuf_cap_) ensure_defer(total);
   CK(launch_delete_suffix(A, uv, n_ptr, nd, found, ctl_, count_missing, tombs_, defer_, nrows,
                           total, dbufs_, st_));
   launches_ += 2 + (nrows ? 7 : 0);
+}
+
+// Sort buffers of the deferred deletions, for at least `slots` suffix slots.
+// They grow geometrically (at least doubling), and reserve_batch sizes them
+// ahead, because an allocation between a snapshot's stage events leaves the
+// GPU idle for as long as the driver takes (hundreds of ms when another
+// process holds the driver's locks, e.g. a monitoring query).
+void Engine::ensure_defer(u64 slots) {
+  if (slots <= dbuf_cap_) return;
+  CK(cudaStreamSynchronize(st_));
+  for (void *p : {(void *)dbufs_.k_in, (void *)dbufs_.k_out, (void *)dbufs_.v_in,
+                  (void *)dbufs_.v_out, dbufs_.temp})
+    cudaFree(p);
+  dbufs_ = DeferBufs{};
+  const u64 c = std::max<u64>({slots + slots / 2, dbuf_cap_ * 2, 1ull << 20});
+  dbuf_cap_ = 0;
+  CK(cudaMalloc((void **)&dbufs_.k_in, c * 8));
+  CK(cudaMalloc((void **)&dbufs_.k_out, c * 8));
+  CK(cudaMalloc((void **)&dbufs_.v_in, c * 4));
+  CK(cudaMalloc((void **)&dbufs_.v_out, c * 4));
+  dbufs_.temp_bytes = delete_sort_temp_bytes(c);
+  CK(cudaMalloc(&dbufs_.temp, std::max<size_t>(dbufs_.temp_bytes, 16)));
+  dbuf_cap_ = c;
 }
 
 // Device half of a snapshot on st_: counters reset, ingest, mutation and
@@ -807,15 +817,19 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
     PL.ctl = ctl_;
     PL.n = n_;
     PL.cur = pr_cur_;
-    PL.phases = PR_AMEND;
-    PL.sign = -1.f;
+    PL.del_uv = uv_out_;
+    PL.del_found = found_out_;
+    PL.n_del = counts_ + 0;
+    PL.add_uvw = add_uvw_;
+    PL.n_add = (uint32_t)na;
     PL.eps = opt_.epsilon;
     PL.alpha = opt_.alpha;
     PL.max_rounds = opt_.max_rounds;
     PL.timeout_ns = timeout;
     PL.num_sms = num_sms_;
+    // the amend after the mutation needs each touched source's old degree
     if (nd + na) {
-      CK(launch_pr(PL, st_));
+      CK(launch_pr_old_degree(touched_, counts_ + 4, (uint32_t)(nd + na), out_.live, delta_, st_));
       launches_++;
     }
   }
@@ -845,7 +859,6 @@ void Engine::enqueue_snapshot(const dycg_edge_dev *d_dels, size_t nd, const dycg
   // ---- repair
   if (opt_.algo == DYCG_ALGO_PR) {
     PL.phases = (nd + na) ? (PR_AMEND | PR_CONVERGE) : PR_CONVERGE;
-    PL.sign = 1.f;
     CK(launch_pr(PL, st_));
     launches_++;
   } else if (nq_) {
@@ -1715,7 +1728,7 @@ void Engine::policy_train(uint32_t epochs, float lr, uint32_t batch, uint64_t se
     for (u64 o = 0; o < total; o += (1ull << 30)) {
       const uint32_t c = (uint32_t)std::min<u64>(1ull << 30, total - o);
       CK(launch_mlp_grad((const char *)tx_ + o * POLICY_F * 2, ylog + o, c, c, 0, params_, 0.f,
-                         grad_, ploss_, st_));
+                         grad_, ploss_, &ctl_->err, st_));
     }
     CK(cudaMemsetAsync(grad_, 0, POLICY_PARAMS * 4, st_));
     float l = 0;
@@ -1731,7 +1744,7 @@ void Engine::policy_train(uint32_t epochs, float lr, uint32_t batch, uint64_t se
   const u64 steps = std::max<u64>(1, (u64)epochs * total / batch);
   for (u64 s = 0; s < steps; s++) {
     CK(launch_mlp_grad(tx_, ylog, total, batch, mix64(seed + s + 1) | 1, params_, 2.f / batch,
-                       grad_, ploss_, st_));
+                       grad_, ploss_, &ctl_->err, st_));
     CK(launch_adam(params_, grad_, adam_m_, adam_v_, lr, ++adam_step_, st_));
   }
   const float l1 = eval();

@@ -219,6 +219,7 @@ class Engine {
   Reloc reloc_{};
   Tombs tombs_{};
   DeferDel defer_{};
+  void ensure_defer(u64 slots);
   DeferBufs dbufs_{};
   u64 dbuf_cap_ = 0;
   u64 *h_dpacked_ = nullptr;  // pinned

@@ -89,17 +89,24 @@ struct PrLaunch {
   Adj out;
   float *x, *r, *delta;
   uint32_t *queued, *q0, *q1;
-  const uint32_t *sources, *n_sources;
+  const uint32_t *sources, *n_sources;  // touched sources
+  const uint2 *del_uv;                   // distinct deleted pairs, occurrences found
+  const uint32_t *del_found, *n_del;
+  const uint3 *add_uvw;                  // inserted occurrences
+  uint32_t n_add;
   uint4 *tiles;
   uint32_t tile_cap;
   Ctl *ctl;
   uint32_t n, cur, phases;
-  float sign, eps, alpha;
+  float eps, alpha;
   uint32_t max_rounds;
   u64 timeout_ns;
   int num_sms;
 };
 cudaError_t launch_pr(const PrLaunch &L, cudaStream_t s);
+cudaError_t launch_pr_old_degree(const uint32_t *sources, const uint32_t *n_sources,
+                                 uint32_t max_sources, const uint32_t *live, float *delta,
+                                 cudaStream_t s);
 cudaError_t launch_pr_init(float *x, float *r, uint32_t *queued, uint32_t *q0, uint32_t n,
                            float base, Ctl *ctl, cudaStream_t s);
 
@@ -261,9 +268,10 @@ cudaError_t launch_log1p(const float *in, float *out, u64 n, cudaStream_t s);
 // completion wait ran out
 cudaError_t launch_mlp_infer(const void *x, uint32_t n, const float *params, float *score,
                              uint32_t *ids, uint32_t *err, cudaStream_t s);
+// tcgen05 loss and gradient; err (optional) as for inference
 cudaError_t launch_mlp_grad(const void *x, const float *y, uint64_t total, uint32_t count,
                             uint64_t sample_seed, const float *params, float scale, float *grad,
-                            float *loss, cudaStream_t s);
+                            float *loss, uint32_t *err, cudaStream_t s);
 cudaError_t launch_adam(float *p, float *g, float *m, float *v, float lr, uint32_t step,
                         cudaStream_t s);
 cudaError_t sample_row_edges(const Adj &A, const uint32_t *sources, u64 count, u64 seed,

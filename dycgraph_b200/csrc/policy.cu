@@ -25,8 +25,8 @@
 // The MLP is 4.7K multiply-adds per page. Inference runs every snapshot over
 // every page (1.85M pages at R-MAT 27, ~9 GMAC): it runs on the 5th-generation
 // tensor cores (tcgen05.mma, 128-page tiles, accumulators in tensor memory),
-// where the FP32-FMA version took ~1.2 ms per snapshot. Training runs once per
-// trained network on FP32 FMA tiles.
+// where the FP32-FMA version took ~1.2 ms per snapshot. Training (forward,
+// backward and the gradient sums over samples) runs on them too.
 #include <cuda_bf16.h>
 
 #include <atomic>
@@ -44,12 +44,6 @@ constexpr int OFF_W1 = 0, OFF_B1 = F * H, OFF_W2 = OFF_B1 + H, OFF_B2 = OFF_W2 +
 static_assert(OFF_B3 + 1 == POLICY_PARAMS, "parameter layout");
 
 __device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
-
-// Parameters into shared memory, BF16-rounded (the precision the MLP runs at).
-__device__ __forceinline__ void load_params(const float *p, float *s) {
-  for (int i = threadIdx.x; i < POLICY_PARAMS; i += blockDim.x) s[i] = bf(p[i]);
-  __syncthreads();
-}
 
 int grid_for(u64 threads) {
   u64 b = (threads + BLOCK - 1) / BLOCK;
@@ -197,12 +191,13 @@ __device__ __forceinline__ u64 sdesc(uint32_t saddr, uint32_t sbo) {
   return (u64)((saddr >> 4) & 0x3FFF) | ((u64)(128 >> 4) << 16) | ((u64)((sbo >> 4) & 0x3FFF) << 32) |
          (1ull << 46);
 }
-__device__ __forceinline__ void mma(uint32_t d_tmem, u64 a, u64 b, uint32_t accumulate) {
+__device__ __forceinline__ void mma(uint32_t d_tmem, u64 a, u64 b, uint32_t accumulate,
+                                    uint32_t idesc = IDESC) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
       :
-      : "r"(d_tmem), "l"(a), "l"(b), "r"(IDESC), "r"(accumulate), "r"(0u));
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u));
 }
 __device__ __forceinline__ void commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
@@ -225,25 +220,27 @@ __device__ __forceinline__ bool wait(uint32_t bar, uint32_t phase) {
     if (globaltimer_ns() - t0 > 1000000000ull) return false;
   }
 }
+// 32 FP32 columns of this thread's tensor-memory lane (warp-collective)
+__device__ __forceinline__ void ld32(uint32_t taddr, float *v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+      "%28, %29, %30, %31}, [%32];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
 // 64 FP32 columns of this thread's tensor-memory lane, in two 32-column loads
 __device__ __forceinline__ void ld64(uint32_t taddr, float (&v)[64]) {
-#pragma unroll
-  for (int h = 0; h < 2; h++) {
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
-        "%28, %29, %30, %31}, [%32];\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr + 32 * h));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 32; i++) v[32 * h + i] = __uint_as_float(r[i]);
-  }
+  ld32(taddr, v);
+  ld32(taddr + 32, v + 32);
 }
 __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -374,139 +371,293 @@ __global__ void __launch_bounds__(128, 4) mlp_infer_tc_kernel(const __nv_bfloat1
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" ::"r"(tmem));
 }
 
-// ---- training ------------------------------------------------------------------
+// ---- training on the 5th-generation tensor cores ----------------------------------
 
-constexpr int TS = 128;     // samples per tile
-constexpr int HP = H + 1;   // padded activation row (bank-conflict free)
+// One CTA of 4 warps per SM, 128 samples per tile (thread t = sample t of the
+// tile = tensor-memory lane t). Per tile, four tcgen05.mma products with FP32
+// accumulators in tensor memory, each followed by a per-thread epilogue:
+//   Z1 = X W1             (M 128 samples, N 64, K 16: the 8 features padded)
+//   Z2 = H1 W2            (N 64, K 64; H1 as BF16 hi + lo)
+//   G1 = dH2 W2^T         (N 64, K 64; dH2 as hi + lo) -> dH1 = G1 * [H1 > 0]
+//   G  = A B              (M 128, N 208, K 128 samples), accumulated over the
+//                          CTA's tiles, where the rows of A are H1^T (64), X^T
+//                          (8), a row of ones and dy^T, and the columns of B are
+//                          dH2 (64), dH1 (64), H2 (64) and a column of ones:
+//                          G[H1^T][dH2] = dW2, G[X^T][dH1] = dW1,
+//                          G[ones][dH2 | dH1] = db2 | db1,
+//                          G[dy^T][H2 | ones] = dW3 | db3.
+// FP32 operands (activations, gradients) enter as BF16 hi + lo parts, and G
+// sums hi*hi + hi*lo + lo*hi, so products keep ~2^-16 relative precision, as
+// the FP32 FMA formulation it replaces; X, ones and the BF16-rounded weights
+// are exact in BF16. Operand layout and descriptors as in the inference
+// kernel (no-swizzle K-major core matrices).
+namespace tt {
+constexpr uint32_t TS = 128, GN = 208;        // samples per tile; columns of G
+constexpr uint32_t KG = TS / 8;                // core-matrix chunks along G's K
+constexpr uint32_t SM_A1 = 0;                  // X: 128 x 16 (KC 2), 4 KB
+constexpr uint32_t SM_B1 = 4096;               // W1 as [n = hidden][k = feature], 2 KB
+constexpr uint32_t SM_AH = SM_B1 + 2048;       // H1, then dH2: 128 x 64 hi (KC 8), 16 KB
+constexpr uint32_t SM_AL = SM_AH + 16384;      // ... lo
+constexpr uint32_t SM_B2F = SM_AL + 16384;     // W2 as [n = out][k = in], 8 KB
+constexpr uint32_t SM_B2B = SM_B2F + 8192;     // W2 as [n = in][k = out], 8 KB
+constexpr uint32_t SM_GAH = SM_B2B + 8192;     // A of G: 128 x 128 (KC 16) hi, 32 KB
+constexpr uint32_t SM_GAL = SM_GAH + 32768;    // ... lo
+constexpr uint32_t SM_GBH = SM_GAL + 32768;    // B of G: 208 x 128 (KC 16) hi, 52 KB
+constexpr uint32_t SM_GBL = SM_GBH + GN * TS * 2;  // ... lo
+constexpr uint32_t SM_BIAS = SM_GBL + GN * TS * 2;  // b1, b2, W3, b3 (FP32)
+constexpr uint32_t SM_BAR = SM_BIAS + 784;     // mbarrier + tensor-memory address
+constexpr uint32_t SM_BYTES = SM_BAR + 16;
+static_assert(SM_BYTES <= 232448, "shared memory per block");
+// rows of A and columns (rows of the K-major B) of G
+constexpr uint32_t A_H1 = 0, A_X = 64, A_ONE = 72, A_DY = 73;
+constexpr uint32_t B_DH2 = 0, B_DH1 = 64, B_H2 = 128, B_ONE = 192;
+// tensor-memory columns: Z1 / G1 in 0..63, Z2 in 64..127, G in 128..335
+constexpr uint32_t T_Z1 = 0, T_Z2 = 64, T_G = 128, T_COLS = 512;
+constexpr uint32_t ID64 = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t IDG = (1u << 4) | (1u << 7) | (1u << 10) | ((GN >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void put(uint8_t *sm, uint32_t base, uint32_t row, uint32_t k,
+                                    uint32_t kc, __nv_bfloat16 v) {
+  *reinterpret_cast<__nv_bfloat16 *>(sm + base + tc::off(row, k, kc)) = v;
+}
+// v as BF16 hi + lo at (row, k) of the hi and lo copies of an operand
+__device__ __forceinline__ void put2(uint8_t *sm, uint32_t hi, uint32_t lo, uint32_t row,
+                                     uint32_t k, uint32_t kc, float v) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  put(sm, hi, row, k, kc, h);
+  put(sm, lo, row, k, kc, __float2bfloat16_rn(v - __bfloat162float(h)));
+}
+// 64 values of this thread's sample as hi + lo rows of a sample-major operand
+__device__ __forceinline__ void put_row(uint8_t *sm, uint32_t t, const float (&v)[64]) {
+#pragma unroll
+  for (int h = 0; h < 64; h += 8) {
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int e = 0; e < 8; e += 2) {
+      const float h0 = bf(v[h + e]), h1 = bf(v[h + e + 1]);
+      hw[e / 2] = pack2(h0, h1);
+      lw[e / 2] = pack2(v[h + e] - h0, v[h + e + 1] - h1);
+    }
+    *reinterpret_cast<uint4 *>(sm + SM_AH + tc::off(t, h, 8)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    *reinterpret_cast<uint4 *>(sm + SM_AL + tc::off(t, h, 8)) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+  }
+}
+// all threads' shared-memory operand writes visible to the tensor core, then
+// one thread issues; the caller waits on the mbarrier
+__device__ __forceinline__ void publish() {
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+}
+}  // namespace tt
 
 // Loss and gradient over samples: sample s of the pass is row idx(s) of x
 // (idx = identity, or a seeded draw when sample_seed != 0 and total > 0).
 // Gradients (FP32, w.r.t. the BF16-rounded parameters) and the summed squared
 // error are added into grad[] and *loss. scale multiplies the gradient
 // (2/batch for a mean).
-__global__ void __launch_bounds__(BLOCK) mlp_grad_kernel(const __nv_bfloat16 *x, const float *y,
-                                                         uint64_t total, uint32_t count,
-                                                         uint64_t sample_seed, const float *params,
-                                                         float scale, float *grad, float *loss) {
-  extern __shared__ float sm[];
-  float *w = sm;                          // POLICY_PARAMS
-  float *X = w + POLICY_PARAMS;           // TS x F
-  float *A1 = X + TS * F;                 // TS x HP: H1, then dH1
-  float *A2 = A1 + TS * HP;               // TS x HP: H2, then dH2
-  float *T = A2 + TS * HP;                // TS: target, then dy
-  load_params(params, w);
-  const int t = threadIdx.x;
-  float gW2[H * H / BLOCK] = {}, gW1[F * H / BLOCK] = {};
-  float gb1 = 0, gb2 = 0, gW3 = 0, gb3 = 0, lsum = 0;
-  const uint32_t tiles = (count + TS - 1) / TS;
-  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const uint32_t s0 = tile * TS;
-    const int ns = (int)min((uint32_t)TS, count - s0);
-    // load inputs and targets
-    for (int e = t; e < TS * F; e += BLOCK) {
-      const int s = e / F, k = e % F;
-      float v = 0.f;
-      if (s < ns) {
-        u64 r = s0 + s;
-        if (sample_seed) r = mix64(sample_seed ^ mix64(r)) % total;
-        v = __bfloat162float(x[r * F + k]);
-        if (k == 0) T[s] = y[r];
-      }
-      X[s * F + k] = v;
-    }
-    __syncthreads();
-    // H1 = relu(X W1 + b1)
-    for (int e = t; e < TS * H; e += BLOCK) {
-      const int s = e / H, i = e % H;
-      float a = w[OFF_B1 + i];
-#pragma unroll
-      for (int k = 0; k < F; k++) a = fmaf(X[s * F + k], w[OFF_W1 + k * H + i], a);
-      A1[s * HP + i] = fmaxf(a, 0.f);
-    }
-    __syncthreads();
-    // H2 = relu(H1 W2 + b2)
-    for (int e = t; e < TS * H; e += BLOCK) {
-      const int s = e / H, j = e % H;
-      float a = w[OFF_B2 + j];
-      for (int i = 0; i < H; i++) a = fmaf(A1[s * HP + i], w[OFF_W2 + i * H + j], a);
-      A2[s * HP + j] = fmaxf(a, 0.f);
-    }
-    __syncthreads();
-    // y = H2 W3 + b3; dy = scale * (y - target)
-    if (t < TS) {
-      float d = 0.f;
-      if (t < ns) {
-        float a = w[OFF_B3];
-        for (int j = 0; j < H; j++) a = fmaf(A2[t * HP + j], w[OFF_W3 + j], a);
-        d = a - T[t];
-        lsum += d * d;
-      }
-      T[t] = scale * d;
-    }
-    __syncthreads();
-    // gW3, gb3 (need H2), then dH2 in place
-    if (t < H) {
-      float a = 0.f;
-      for (int s = 0; s < ns; s++) a = fmaf(A2[s * HP + t], T[s], a);
-      gW3 += a;
-    }
-    if (t == 0)
-      for (int s = 0; s < ns; s++) gb3 += T[s];
-    __syncthreads();
-    for (int e = t; e < TS * H; e += BLOCK) {
-      const int s = e / H, j = e % H;
-      A2[s * HP + j] = A2[s * HP + j] > 0.f ? T[s] * w[OFF_W3 + j] : 0.f;
-    }
-    __syncthreads();
-    // gW2[i][j] += sum_s H1[s][i] dH2[s][j]; gb2[j] += sum_s dH2[s][j]
-#pragma unroll
-    for (int r = 0; r < H * H / BLOCK; r++) {
-      const int e = t + r * BLOCK, i = e / H, j = e % H;
-      float a = 0.f;
-      for (int s = 0; s < ns; s++) a = fmaf(A1[s * HP + i], A2[s * HP + j], a);
-      gW2[r] += a;
-    }
-    if (t < H) {
-      float a = 0.f;
-      for (int s = 0; s < ns; s++) a += A2[s * HP + t];
-      gb2 += a;
-    }
-    __syncthreads();
-    // dH1 = mask(H1) * (dH2 W2^T), in place
-    for (int e = t; e < TS * H; e += BLOCK) {
-      const int s = e / H, i = e % H;
-      float a = 0.f;
-      if (A1[s * HP + i] > 0.f)
-        for (int j = 0; j < H; j++) a = fmaf(A2[s * HP + j], w[OFF_W2 + i * H + j], a);
-      A1[s * HP + i] = a;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < F * H / BLOCK; r++) {
-      const int e = t + r * BLOCK, k = e / H, i = e % H;
-      float a = 0.f;
-      for (int s = 0; s < ns; s++) a = fmaf(X[s * F + k], A1[s * HP + i], a);
-      gW1[r] += a;
-    }
-    if (t < H) {
-      float a = 0.f;
-      for (int s = 0; s < ns; s++) a += A1[s * HP + t];
-      gb1 += a;
-    }
-    __syncthreads();
+__global__ void __launch_bounds__(128, 1)
+    mlp_grad_tc_kernel(const __nv_bfloat16 *x, const float *y, uint64_t total, uint32_t count,
+                       uint64_t sample_seed, const float *params, float scale, float *grad,
+                       float *loss, uint32_t *err) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  const uint32_t t = threadIdx.x, warp = t >> 5;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+  const uint32_t bar = sbase + tt::SM_BAR;
+  uint32_t *taddr_slot = reinterpret_cast<uint32_t *>(sm + tt::SM_BAR + 8);
+  // operands that do not change: zeros everywhere (padding rows and columns,
+  // the lo parts of exact values), the weights, the two rows of ones
+  for (uint32_t i = t * 16; i < tt::SM_BIAS; i += 128 * 16)
+    *reinterpret_cast<uint4 *>(sm + i) = make_uint4(0, 0, 0, 0);
+  __syncthreads();
+  for (uint32_t i = t; i < 64 * (uint32_t)F; i += 128) {
+    const uint32_t nn = i / F, k = i % F;
+    tt::put(sm, tt::SM_B1, nn, k, 2, __float2bfloat16_rn(params[OFF_W1 + k * H + nn]));
   }
-#pragma unroll
-  for (int r = 0; r < H * H / BLOCK; r++) atomicAdd(grad + OFF_W2 + t + r * BLOCK, gW2[r]);
-#pragma unroll
-  for (int r = 0; r < F * H / BLOCK; r++) atomicAdd(grad + OFF_W1 + t + r * BLOCK, gW1[r]);
-  if (t < H) {
-    atomicAdd(grad + OFF_B1 + t, gb1);
-    atomicAdd(grad + OFF_B2 + t, gb2);
-    atomicAdd(grad + OFF_W3 + t, gW3);
+  for (uint32_t i = t; i < (uint32_t)(H * H); i += 128) {
+    const uint32_t a = i / H, b = i % H;  // W2[a][b]: input a, output b
+    const __nv_bfloat16 w = __float2bfloat16_rn(params[OFF_W2 + i]);
+    tt::put(sm, tt::SM_B2F, b, a, 8, w);
+    tt::put(sm, tt::SM_B2B, a, b, 8, w);
   }
-  if (t == 0) atomicAdd(grad + OFF_B3, gb3);
+  tt::put(sm, tt::SM_GAH, tt::A_ONE, t, tt::KG, __float2bfloat16_rn(1.f));
+  tt::put(sm, tt::SM_GBH, tt::B_ONE, t, tt::KG, __float2bfloat16_rn(1.f));
+  float *bias = reinterpret_cast<float *>(sm + tt::SM_BIAS);  // b1[64], b2[64], W3[64], b3
+  for (uint32_t i = t; i < 3 * (uint32_t)H; i += 128)
+    bias[i] = bf(params[(i < (uint32_t)H ? OFF_B1 : i < 2u * H ? OFF_B2 - H : OFF_W3 - 2 * H) + i]);
+  if (t == 0) {
+    bias[3 * H] = bf(params[OFF_B3]);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     sbase + tt::SM_BAR + 8),
+                 "n"(tt::T_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tt::publish();
+  const uint32_t tmem = *taddr_slot;
+  const uint32_t lane_base = (32 * warp) << 16;  // this warp's tensor-memory lanes
+  const float *b1 = bias, *b2 = bias + H, *w3 = bias + 2 * H;
+  const float b3 = bias[3 * H];
+  uint32_t phase = 0;
+  bool ok = true;
+  float lsum = 0.f;
+  const uint32_t tiles = (count + tt::TS - 1) / tt::TS;
+  uint32_t done = 0;  // tiles this CTA accumulated into G
+  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, done++) {
+    const uint32_t s0 = tile * tt::TS;
+    const bool valid = t < min(tt::TS, count - s0);
+    // inputs: X row into A1, X^T into G's A, the target
+    uint4 xf = make_uint4(0, 0, 0, 0);
+    float target = 0.f;
+    if (valid) {
+      u64 r = s0 + t;
+      if (sample_seed) r = mix64(sample_seed ^ mix64(r)) % total;
+      xf = __ldg(reinterpret_cast<const uint4 *>(x) + r);
+      target = y[r];
+    }
+    *reinterpret_cast<uint4 *>(sm + tt::SM_A1 + tc::off(t, 0, 2)) = xf;
+    {
+      const __nv_bfloat16 *xv = reinterpret_cast<const __nv_bfloat16 *>(&xf);
+#pragma unroll
+      for (int k = 0; k < F; k++) tt::put(sm, tt::SM_GAH, tt::A_X + k, t, tt::KG, xv[k]);
+    }
+    tt::publish();
+    if (t == 0) {
+      tc::mma(tmem + tt::T_Z1, tc::sdesc(sbase + tt::SM_A1, 256), tc::sdesc(sbase + tt::SM_B1, 256),
+              0, tt::ID64);
+      tc::commit(bar);
+    }
+    ok = tc::wait(bar, phase);
+    phase ^= 1;
+    tc::fence_after();
+    // layer 1: H1 = relu(Z1 + b1), its sign mask, H1 as A of layer 2, H1^T in G's A
+    float v[64];
+    u64 mask1 = 0;
+    tc::ld64(tmem + lane_base + tt::T_Z1, v);
+#pragma unroll
+    for (int i = 0; i < H; i++) {
+      v[i] = fmaxf(v[i] + b1[i], 0.f);
+      if (v[i] > 0.f) mask1 |= 1ull << i;
+      tt::put2(sm, tt::SM_GAH, tt::SM_GAL, tt::A_H1 + i, t, tt::KG, v[i]);
+    }
+    tt::put_row(sm, t, v);
+    tt::publish();
+    if (t == 0 && ok) {
+#pragma unroll
+      for (uint32_t s = 0; s < (uint32_t)H / 16; s++) {
+        const uint32_t kb = s * 256;
+        tc::mma(tmem + tt::T_Z2, tc::sdesc(sbase + tt::SM_AH + kb, 1024),
+                tc::sdesc(sbase + tt::SM_B2F + kb, 1024), s > 0, tt::ID64);
+        tc::mma(tmem + tt::T_Z2, tc::sdesc(sbase + tt::SM_AL + kb, 1024),
+                tc::sdesc(sbase + tt::SM_B2F + kb, 1024), 1, tt::ID64);
+      }
+      tc::commit(bar);
+    }
+    if (ok) ok = tc::wait(bar, phase);
+    phase ^= 1;
+    tc::fence_after();
+    // layer 2 and output: H2, y, dy; dH2 = dy W3 [H2 > 0]
+    tc::ld64(tmem + lane_base + tt::T_Z2, v);
+    float out = b3;
+#pragma unroll
+    for (int j = 0; j < H; j++) {
+      v[j] = fmaxf(v[j] + b2[j], 0.f);
+      out = fmaf(v[j], w3[j], out);
+    }
+    const float d = out - target;
+    const float dy = valid ? scale * d : 0.f;
+    if (valid) lsum = fmaf(d, d, lsum);
+    tt::put2(sm, tt::SM_GAH, tt::SM_GAL, tt::A_DY, t, tt::KG, dy);
+#pragma unroll
+    for (int j = 0; j < H; j++) {
+      tt::put2(sm, tt::SM_GBH, tt::SM_GBL, tt::B_H2 + j, t, tt::KG, v[j]);
+      v[j] = v[j] > 0.f ? dy * w3[j] : 0.f;
+      tt::put2(sm, tt::SM_GBH, tt::SM_GBL, tt::B_DH2 + j, t, tt::KG, v[j]);
+    }
+    tt::put_row(sm, t, v);  // dH2 as A of G1 (layer 2's MMAs are complete)
+    tt::publish();
+    if (t == 0 && ok) {
+#pragma unroll
+      for (uint32_t s = 0; s < (uint32_t)H / 16; s++) {
+        const uint32_t kb = s * 256;
+        tc::mma(tmem + tt::T_Z1, tc::sdesc(sbase + tt::SM_AH + kb, 1024),
+                tc::sdesc(sbase + tt::SM_B2B + kb, 1024), s > 0, tt::ID64);
+        tc::mma(tmem + tt::T_Z1, tc::sdesc(sbase + tt::SM_AL + kb, 1024),
+                tc::sdesc(sbase + tt::SM_B2B + kb, 1024), 1, tt::ID64);
+      }
+      tc::commit(bar);
+    }
+    if (ok) ok = tc::wait(bar, phase);
+    phase ^= 1;
+    tc::fence_after();
+    // dH1 = G1 [H1 > 0] into G's B
+    tc::ld64(tmem + lane_base + tt::T_Z1, v);
+#pragma unroll
+    for (int i = 0; i < H; i++)
+      tt::put2(sm, tt::SM_GBH, tt::SM_GBL, tt::B_DH1 + i, t, tt::KG,
+               (mask1 >> i) & 1ull ? v[i] : 0.f);
+    tt::publish();
+    if (t == 0 && ok) {
+#pragma unroll
+      for (uint32_t s = 0; s < tt::TS / 16; s++) {
+        const uint32_t kb = s * 256;
+        const u64 ah = tc::sdesc(sbase + tt::SM_GAH + kb, tt::KG * 128);
+        const u64 al = tc::sdesc(sbase + tt::SM_GAL + kb, tt::KG * 128);
+        const u64 bh = tc::sdesc(sbase + tt::SM_GBH + kb, tt::KG * 128);
+        const u64 bl = tc::sdesc(sbase + tt::SM_GBL + kb, tt::KG * 128);
+        tc::mma(tmem + tt::T_G, ah, bh, done > 0 || s > 0, tt::IDG);
+        tc::mma(tmem + tt::T_G, ah, bl, 1, tt::IDG);
+        tc::mma(tmem + tt::T_G, al, bh, 1, tt::IDG);
+      }
+      tc::commit(bar);
+    }
+    if (ok) ok = tc::wait(bar, phase);  // the next tile rewrites G's operands
+    phase ^= 1;
+    tc::fence_after();
+  }
+  // G's rows to the gradient: warps 0-1 hold dW2, warp 2 dW1, the biases, dW3
+  if (ok && done) {
+    float g[32];
+    if (warp < 2) {
+#pragma unroll
+      for (uint32_t c = 0; c < 64; c += 32) {
+        tc::ld32(tmem + lane_base + tt::T_G + tt::B_DH2 + c, g);
+#pragma unroll
+        for (int j = 0; j < 32; j++) atomicAdd(grad + OFF_W2 + t * H + c + j, g[j]);
+      }
+    } else if (warp == 2) {
+      for (uint32_t c = 0; c < 224; c += 32) {  // G columns 0..223 (208.. unused)
+        tc::ld32(tmem + lane_base + tt::T_G + c, g);
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          const uint32_t col = c + j;
+          if (t >= tt::A_X && t < tt::A_X + F && col >= tt::B_DH1 && col < tt::B_DH1 + H)
+            atomicAdd(grad + OFF_W1 + (t - tt::A_X) * H + (col - tt::B_DH1), g[j]);
+          else if (t == tt::A_ONE && col < tt::B_DH1)
+            atomicAdd(grad + OFF_B2 + col, g[j]);
+          else if (t == tt::A_ONE && col < tt::B_H2)
+            atomicAdd(grad + OFF_B1 + (col - tt::B_DH1), g[j]);
+          else if (t == tt::A_DY && col >= tt::B_H2 && col < tt::B_ONE)
+            atomicAdd(grad + OFF_W3 + (col - tt::B_H2), g[j]);
+          else if (t == tt::A_DY && col == tt::B_ONE)
+            atomicAdd(grad + OFF_B3, g[j]);
+        }
+      }
+    }
+  }
   for (int o = 16; o; o >>= 1) lsum += __shfl_down_sync(0xffffffffu, lsum, o);
   if ((t & 31) == 0 && lsum != 0.f) atomicAdd(loss, lsum);
+  if (!ok && err && t == 0) atomicCAS(err, 0u, ERR_BARRIER);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "n"(tt::T_COLS));
 }
 
 // Adam on the FP32 master parameters; clears the gradient.
@@ -524,9 +675,7 @@ __global__ void adam_kernel(float *p, float *g, float *m, float *v, float lr, fl
 
 // ---- launchers -----------------------------------------------------------------
 
-size_t mlp_grad_smem() {
-  return sizeof(float) * (POLICY_PARAMS + TS * F + 2 * TS * HP + TS);
-}
+size_t mlp_grad_smem() { return tt::SM_BYTES; }
 
 // Clears the row-layout features on refresh snapshots (period[0] % period[1]
 // == 0); the refresh decision is read on the device so it survives graph
@@ -603,7 +752,7 @@ cudaError_t launch_mlp_infer(const void *x, uint32_t n, const float *params, flo
 }
 cudaError_t launch_mlp_grad(const void *x, const float *y, uint64_t total, uint32_t count,
                             uint64_t sample_seed, const float *params, float scale, float *grad,
-                            float *loss, cudaStream_t s) {
+                            float *loss, uint32_t *err, cudaStream_t s) {
   // the shared-memory opt-in is a per-device setting: once per device used
   constexpr int kMaxDevices = 64;
   static std::atomic<bool> attr[kMaxDevices];
@@ -612,15 +761,18 @@ cudaError_t launch_mlp_grad(const void *x, const float *y, uint64_t total, uint3
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDevices || !attr[dev].load(std::memory_order_acquire)) {
-    e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(mlp_grad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < kMaxDevices) attr[dev].store(true, std::memory_order_release);
   }
-  const uint32_t tiles = (count + TS - 1) / TS;
-  const int grid = (int)std::max<uint32_t>(1, std::min<uint32_t>(tiles, 148 * 2));
-  mlp_grad_kernel<<<grid, BLOCK, smem, s>>>((const __nv_bfloat16 *)x, y, total, count,
-                                            sample_seed, params, scale, grad, loss);
+  if (!count) return cudaSuccess;
+  // one CTA per SM (223 KB of shared memory, 512 tensor-memory columns); every
+  // CTA gets at least one tile
+  const uint32_t tiles = (count + tt::TS - 1) / tt::TS;
+  const int grid = (int)std::min<uint32_t>(tiles, 148);
+  mlp_grad_tc_kernel<<<grid, 128, smem, s>>>((const __nv_bfloat16 *)x, y, total, count,
+                                             sample_seed, params, scale, grad, loss, err);
   return cudaGetLastError();
 }
 

@@ -6,10 +6,19 @@
 // a vertex is in the frontier while |r| > epsilon (Frontier::Add :21-30);
 // Consume (:54-71) moves r into x; Scatter (:74-100) pushes
 // alpha * delta / degree along every live occurrence with FP32 atomics. A
-// batch amends r by -alpha*x[u]/deg_old(u) over the old rows of the touched
-// sources before the topology changes and by +alpha*x[u]/deg_new(u) over the
-// new rows after (Engine::UpdatePageRank, framework.cuh:2692-2736), then
-// converges for at most max_rounds rounds; unfinished work carries over.
+// batch changes r by what the reference's two amend passes add up to
+// (Engine::UpdatePageRank, framework.cuh:2692-2736: -alpha*x[u]/deg_old(u)
+// over the old row of every touched source before the topology changes,
+// +alpha*x[u]/deg_new(u) over the new row after), then converges for at most
+// max_rounds rounds; unfinished work carries over. The sum is pushed in one
+// pass after the mutation: every live occurrence of the new row gets
+// alpha*x[u]*(1/deg_new - 1/deg_old), an inserted occurrence another
+// alpha*x[u]/deg_old, a deleted one -alpha*x[u]/deg_old. The residuals are
+// the same sums (with one rounding instead of two per kept occurrence), but
+// a row whose degree did not change pushes nothing, and a kept neighbour gets
+// a push ~deg times smaller, so far fewer vertices cross epsilon only to be
+// cancelled by the second pass. deg_old is saved per touched source (in the
+// delta array, free between snapshots) before the mutation.
 #include "frontier.cuh"
 #include "internal.h"
 
@@ -24,12 +33,16 @@ struct PrParams {
   uint32_t *q[2];
   const uint32_t *sources;  // touched sources (amend)
   const uint32_t *n_sources;
+  const uint2 *del_uv;      // distinct deleted (u, v) pairs and occurrences found
+  const uint32_t *del_found;
+  const uint32_t *n_del;
+  const uint3 *add_uvw;     // inserted occurrences (u >= n: invalid record)
+  uint32_t n_add;
   Tiles tiles;
   Ctl *ctl;
   uint32_t n;
   uint32_t cur;             // queue holding the frontier
   uint32_t phases;          // PR_AMEND and/or PR_CONVERGE
-  float sign;               // amend sign
   float eps;
   float alpha;
   uint32_t max_rounds;
@@ -44,6 +57,11 @@ __device__ __forceinline__ bool pr_add(const PrParams *P, uint32_t dst, float c)
   return fabsf(old) <= P->eps && fabsf(nv) > P->eps && atomicCAS(P->queued + dst, 0u, 1u) == 0u;
 }
 
+__device__ __forceinline__ uint32_t old_degree(const PrParams *P, uint32_t u) {
+  return __float_as_uint(P->delta[u]);
+}
+
+// The kept-occurrence share of the amend over a touched source's new row.
 struct AmendOp {
   const PrParams *P;
   uint32_t *outq;
@@ -52,11 +70,14 @@ struct AmendOp {
     float c;
   };
   __device__ bool begin(uint32_t u, Row &row) {
-    const uint32_t deg = P->out.live[u];
+    const uint32_t dn = P->out.live[u], dold = old_degree(P, u);
     const float xu = P->x[u];
-    if (!deg || xu == 0.f) return false;
-    row.c = P->sign * P->alpha * xu / (float)deg;
-    return true;
+    if (!dn || dn == dold || xu == 0.f) return false;
+    // alpha x (1/dn - 1/dold) = alpha x (dold - dn) / (dn dold), or alpha x / dn
+    row.c = dold ? P->alpha * xu * ((float)((int64_t)dold - (int64_t)dn) /
+                                    ((float)dn * (float)dold))
+                 : P->alpha * xu / (float)dn;
+    return row.c != 0.f;
   }
   __device__ void edge(uint32_t, uint32_t y, uint32_t, bool valid, Row &row, Acc &acc) {
     bool want = false;
@@ -94,6 +115,43 @@ struct ScatterOp {
   __device__ void end(uint32_t, Row &) {}
 };
 
+// The per-occurrence shares of the amend: -alpha x[u]/deg_old for each
+// deleted occurrence, +alpha x[u]/deg_old for each inserted one (together with
+// the row pass that makes it alpha x[u]/deg_new). Appends into q[cur].
+__device__ void amend_records(const PrParams &P, uint32_t cur, Acc &acc) {
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t gstride = gridDim.x * blockDim.x;
+  uint32_t *q = P.q[cur], *qc = &P.ctl->q_count[cur];
+  const uint32_t nd = *P.n_del;
+  for (uint32_t i = gtid; i < nd; i += gstride) {
+    const uint32_t f = P.del_found[i];
+    bool want = false;
+    const uint2 e = P.del_uv[i];
+    if (f) {
+      const uint32_t dold = old_degree(&P, e.x);
+      const float xu = P.x[e.x];
+      if (dold && xu != 0.f) {
+        want = pr_add(&P, e.y, -P.alpha * xu * (float)f / (float)dold);
+        acc.improved++;
+      }
+    }
+    warp_append(q, qc, P.n, want, e.y, &P.ctl->err);
+  }
+  for (uint32_t i = gtid; i < P.n_add; i += gstride) {
+    const uint3 e = P.add_uvw[i];
+    bool want = false;
+    if (e.x < P.n && e.y < P.n) {
+      const uint32_t dold = old_degree(&P, e.x);
+      const float xu = P.x[e.x];
+      if (dold && xu != 0.f) {
+        want = pr_add(&P, e.y, P.alpha * xu / (float)dold);
+        acc.improved++;
+      }
+    }
+    warp_append(q, qc, P.n, want, e.y, &P.ctl->err);
+  }
+}
+
 __global__ void __launch_bounds__(BLOCK) pr_kernel(PrParams P) {
   Ctl *ctl = P.ctl;
   Acc acc = {0, 0, 0, 0, 0};
@@ -101,6 +159,7 @@ __global__ void __launch_bounds__(BLOCK) pr_kernel(PrParams P) {
   const uint32_t gstride = gridDim.x * blockDim.x;
   uint32_t cur = P.cur;
   if (P.phases & PR_AMEND) {
+    amend_records(P, cur, acc);
     AmendOp op{&P, P.q[cur], &ctl->q_count[cur]};
     if (!expand_rows<false>(P.out, P.sources, *P.n_sources, op, acc, P.tiles, ctl, 0,
                             P.timeout_ns))
@@ -167,12 +226,16 @@ cudaError_t launch_pr(const PrLaunch &L, cudaStream_t s) {
   P.q[1] = L.q1;
   P.sources = L.sources;
   P.n_sources = L.n_sources;
+  P.del_uv = L.del_uv;
+  P.del_found = L.del_found;
+  P.n_del = L.n_del;
+  P.add_uvw = L.add_uvw;
+  P.n_add = L.n_add;
   P.tiles = Tiles{L.tiles, L.tile_cap};
   P.ctl = L.ctl;
   P.n = L.n;
   P.cur = L.cur;
   P.phases = L.phases;
-  P.sign = L.sign;
   P.eps = L.eps;
   P.alpha = L.alpha;
   P.max_rounds = L.max_rounds;
@@ -186,6 +249,26 @@ cudaError_t launch_pr(const PrLaunch &L, cudaStream_t s) {
   void *args[] = {&P};
   return cudaLaunchCooperativeKernel((const void *)pr_kernel, blocks_per_sm * L.num_sms, BLOCK,
                                      args, 0, s);
+}
+
+// deg_old of every touched source, kept in the delta array until the amend
+__global__ void pr_old_degree_kernel(const uint32_t *sources, const uint32_t *n_sources,
+                                     const uint32_t *live, float *delta) {
+  const uint32_t cnt = *n_sources;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
+       i += gridDim.x * blockDim.x) {
+    const uint32_t u = sources[i];
+    delta[u] = __uint_as_float(live[u]);
+  }
+}
+
+cudaError_t launch_pr_old_degree(const uint32_t *sources, const uint32_t *n_sources,
+                                 uint32_t max_sources, const uint32_t *live, float *delta,
+                                 cudaStream_t s) {
+  if (!max_sources) return cudaSuccess;
+  const int grid = (int)std::min<u64>((max_sources + BLOCK - 1) / BLOCK, 148ull * 16);
+  pr_old_degree_kernel<<<grid, BLOCK, 0, s>>>(sources, n_sources, live, delta);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_pr_init(float *x, float *r, uint32_t *queued, uint32_t *q0, uint32_t n,

@@ -8,9 +8,19 @@
 // longer than HEAVY are cut into TILE-slot tiles that whole CTAs process after
 // a grid barrier, so a million-edge hub row spreads over the whole GPU.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace dycg {
+
+// Ops that declare `static constexpr int kBatch` take a lane's UNROLL slots in
+// one call (edges()), so they can issue independent atomics back to back
+// instead of waiting on each before the next.
+template <class T, class = void>
+struct batch_edges : std::false_type {};
+template <class T>
+struct batch_edges<T, std::void_t<decltype(T::kBatch)>> : std::true_type {};
 
 constexpr uint32_t SYNC_RESET_TILES = 1;
 constexpr uint32_t SYNC_RESET_Q0 = 2;
@@ -129,6 +139,7 @@ struct Acc {
 // Op interface (all lanes call every member, keeping the warp converged):
 //   bool begin(uint32_t v, Row&)                  -- false: skip the row
 //   void edge(uint32_t v, uint32_t nb, uint32_t w, bool valid, Row&, Acc&)
+//     or, with kBatch, edges(v, nb[UNROLL], valid[UNROLL], Row&, Acc&)
 //   void end(uint32_t v, Row&)
 template <bool WITH_W, class Op>
 __device__ __forceinline__ void warp_slots(const Adj &A, uint32_t v, u64 off, uint32_t b,
@@ -164,10 +175,14 @@ __device__ __forceinline__ void warp_slots(const Adj &A, uint32_t v, u64 off, ui
         if (slot_deleted(A, p, d[u])) d[u] |= TOMB;
       }
     }
+    bool ok[UNROLL];  // valid slot (every entry set before the loop may break)
+#pragma unroll
+    for (int u = 0; u < UNROLL; u++) ok[u] = false;
 #pragma unroll
     for (int u = 0; u < UNROLL; u++) {
       if (s0 + u * stride >= e) break;  // warp-uniform
       const bool valid = in[u] && !(d[u] & TOMB);
+      ok[u] = valid;
       if (in[u]) {
         if (cached[u]) acc.hbm += valid ? bytes : 4u;
         else acc.link += valid ? bytes : 4u;
@@ -185,7 +200,13 @@ __device__ __forceinline__ void warp_slots(const Adj &A, uint32_t v, u64 off, ui
         hit_n += __popc(same);
       }
       if (in[u] && pg[u] != pg0) atomicAdd(A.page_hits + pg[u], 1u);
-      op.edge(v, d[u] & VMASK, w[u], valid, r, acc);
+      if constexpr (!batch_edges<Op>::value) op.edge(v, d[u] & VMASK, w[u], valid, r, acc);
+    }
+    if constexpr (batch_edges<Op>::value) {
+      uint32_t nb[UNROLL];
+#pragma unroll
+      for (int u = 0; u < UNROLL; u++) nb[u] = d[u] & VMASK;
+      op.edges(v, nb, ok, r, acc);
     }
   }
   if (lane == 0 && hit_n) atomicAdd(A.page_hits + hit_pg, hit_n);

@@ -57,6 +57,29 @@ __device__ __forceinline__ bool pr_add(const PrParams *P, uint32_t dst, float c)
   return fabsf(old) <= P->eps && fabsf(nv) > P->eps && atomicCAS(P->queued + dst, 0u, 1u) == 0u;
 }
 
+// Pushes c to UNROLL targets per lane: the atomics first (independent, in
+// flight together), then Frontier::Add's crossing test on each result.
+template <int U>
+__device__ __forceinline__ void push_batch(const PrParams *P, uint32_t *outq, uint32_t *outc,
+                                           const uint32_t (&y)[U], const bool (&valid)[U], float c,
+                                           Acc &acc) {
+  float old[U];
+#pragma unroll
+  for (int u = 0; u < U; u++) old[u] = valid[u] ? atomicAdd(P->r + y[u], c) : 0.f;
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    bool want = false;
+    if (valid[u]) {
+      const float nv = old[u] + c;
+      if (!isfinite(nv)) atomicCAS(&P->ctl->err, 0u, ERR_NONFINITE);
+      want = fabsf(old[u]) <= P->eps && fabsf(nv) > P->eps &&
+             atomicCAS(P->queued + y[u], 0u, 1u) == 0u;
+      acc.improved++;
+    }
+    warp_append(outq, outc, P->n, want, y[u], &P->ctl->err);
+  }
+}
+
 __device__ __forceinline__ uint32_t old_degree(const PrParams *P, uint32_t u) {
   return __float_as_uint(P->delta[u]);
 }
@@ -79,13 +102,11 @@ struct AmendOp {
                  : P->alpha * xu / (float)dn;
     return row.c != 0.f;
   }
-  __device__ void edge(uint32_t, uint32_t y, uint32_t, bool valid, Row &row, Acc &acc) {
-    bool want = false;
-    if (valid) {
-      want = pr_add(P, y, row.c);
-      acc.improved++;
-    }
-    warp_append(outq, outc, P->n, want, y, &P->ctl->err);
+  static constexpr int kBatch = 1;
+  template <int U>
+  __device__ void edges(uint32_t, const uint32_t (&y)[U], const bool (&valid)[U], Row &row,
+                        Acc &acc) {
+    push_batch(P, outq, outc, y, valid, row.c, acc);
   }
   __device__ void end(uint32_t, Row &) {}
 };
@@ -104,13 +125,11 @@ struct ScatterOp {
     row.c = P->alpha * d / (float)deg;
     return true;
   }
-  __device__ void edge(uint32_t, uint32_t y, uint32_t, bool valid, Row &row, Acc &acc) {
-    bool want = false;
-    if (valid) {
-      want = pr_add(P, y, row.c);
-      acc.improved++;
-    }
-    warp_append(outq, outc, P->n, want, y, &P->ctl->err);
+  static constexpr int kBatch = 1;
+  template <int U>
+  __device__ void edges(uint32_t, const uint32_t (&y)[U], const bool (&valid)[U], Row &row,
+                        Acc &acc) {
+    push_batch(P, outq, outc, y, valid, row.c, acc);
   }
   __device__ void end(uint32_t, Row &) {}
 };

@@ -83,8 +83,8 @@ def parse():
     ap.add_argument("--frontier-queue", default="static", choices=["static", "claimed"],
                     help="single-source repair: how warps share a wave's rows")
     ap.add_argument("--page-shift", type=int, default=12,
-                    help="single-source lines: log2 adjacency slots per cache page (8-20); "
-                         "20 approximates the reference's SEGMENT-sized chunks")
+                    help="log2 adjacency slots per cache page (8-20; single-source and batched "
+                         "lines); 20 approximates the reference's SEGMENT-sized chunks")
     ap.add_argument("--queries", type=int, default=256, help="batched config: sources")
     ap.add_argument("--plain-queries", type=int, default=None,
                     help="batched config: queries timed on the per-query path (default all)")
@@ -862,7 +862,7 @@ def run_batched(args):
     def build():
         eng = dg.Engine(algo, weight_mode="stored" if algo == "sssp" else "hash128",
                         hbm_graph_budget_bytes=budget, cache_policy="hotness", device=local,
-                        mutation_ctas=args.mutation_ctas)
+                        mutation_ctas=args.mutation_ctas, page_shift=args.page_shift)
         eng.load_rmat(args.scale, args.edge_factor, seed=args.seed, wlo=1, whi=64)
         return eng
 
@@ -1047,6 +1047,7 @@ def run_batched(args):
                    "updates_timed": L["upd"],
                    "snapshot_sizes": [int(x) for x in sizes[1 + T + W:1 + T + W + K]],
                    "weights": "uint32 uniform [1,64] stored" if algo == "sssp" else "rule",
+                   "page_slots": 1 << args.page_shift,
                    "mapping": {k: mapping.get(k) for k in ("qratio", "heavy", "tile", "pull_qratio",
                                                             "queue")},
                    "mapping_tuned_on": (f"one {args.tune_batch}-update snapshot, "

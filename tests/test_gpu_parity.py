@@ -332,6 +332,43 @@ def test_pr_normalised_max_abs_within_1e6():
     assert c["l1_error_normalized"] <= 1e-6 + c["roundoff"] / (0.15 * 4096), c
 
 
+def test_pr_amend_degree_edge_cases():
+    """The one-pass amend (every kept occurrence of a touched row gets
+    alpha x (1/deg_new - 1/deg_old), inserted and deleted occurrences their own
+    share) on the degree cases it must get right: a row losing all its edges
+    (deg_new 0), a row gaining edges from none (deg_old 0, with a repeated
+    occurrence), an edge deleted and re-inserted in one batch (degree
+    unchanged: no row pass), one of two parallel occurrences deleted. After
+    each batch the ranks pass the reference's acceptance check, including the
+    invariant x + r = 0.15 + 0.85 P^T x, which the amend alone maintains."""
+    eps = 1e-7
+    n, off, dst, _ = cases.small_rmat(10, 8, 31)
+    deg = np.diff(off.astype(np.int64))
+    e = engine_for("pr", n, off, dst, epsilon=eps, max_rounds=100000)
+    orc = oracle.Oracle(oracle.PR, n, off, dst)
+    rows = lambda v: [int(x) for x in orc.csr()[1][int(orc.csr()[0][v]):int(orc.csr()[0][v + 1])]]
+    a = int(np.argmax(deg))                        # hub: loses every out-edge
+    b = int(np.flatnonzero(deg == 0)[0])           # no out-edges: gains three occurrences
+    c = int(np.flatnonzero(deg >= 3)[1])           # deletes and re-inserts one edge
+    d = int(np.flatnonzero(deg >= 2)[5])           # gets a parallel occurrence, then loses one
+    assert len({a, b, c, d}) == 4
+    ca, cc, cd = rows(a), rows(c), rows(d)
+    batches = [
+        ([(a, y) for y in ca], [(b, ca[0]), (b, ca[1]), (b, ca[0]), (d, cd[0])]),
+        ([(c, cc[0])], [(c, cc[0])]),
+        ([(d, cd[0])], [(a, cc[1])]),
+    ]
+    for dels, adds in batches:
+        e.apply_batch(cases.triples(dels), cases.triples(adds))
+        orc.mutate(cases.triples(dels), cases.triples(adds))
+        cur_off, cur_dst, _ = orc.csr()
+        x, r = e.gather_ranks()
+        chk = _pr_reference_check(x, r, cur_off, cur_dst, eps)
+        assert chk["ok"], chk
+    assert np.diff(cur_off.astype(np.int64))[b] == 3
+    e.close()
+
+
 # ---- edge cases ---------------------------------------------------------------
 
 def test_empty_batches_and_invalid_ids():

@@ -110,6 +110,29 @@ __device__ __forceinline__ bool lower_key(u64 *addr, u64 cand) {
   return lower_from<STRICT>(addr, cand, ldk(addr));
 }
 
+// lower_from split in two so that a lane can issue several independent
+// first attempts before it looks at any result: first_lower issues the first
+// atomic (false: cand cannot lower `seen`, nothing issued) and leaves its
+// result in got; lowered finishes the attempt (the strict form retries from
+// the value it lost to, exactly as lower_from's loop does).
+template <bool STRICT>
+__device__ __forceinline__ bool first_lower(u64 *addr, u64 cand, u64 seen, u64 &got) {
+  if (cand >= seen) return false;
+  if (STRICT) {
+    if (key_value(cand) >= key_value(seen)) return false;
+    got = atomicCAS(addr, seen, cand);
+  } else {
+    got = atomicMin(addr, cand);
+  }
+  return true;
+}
+template <bool STRICT>
+__device__ __forceinline__ bool lowered(u64 *addr, u64 cand, u64 seen, u64 got) {
+  if (!STRICT) return key_value(got) > key_value(cand);
+  if (got == seen) return true;
+  return lower_from<true>(addr, cand, got);
+}
+
 // Append y to the wave queue of parity par once per wave (tag). With range
 // ordering the queue is cut into QRANGES regions of P.rsize slots, region b
 // holding the vertices of [b * rsize, (b + 1) * rsize); a vertex enters a
@@ -516,12 +539,33 @@ struct InvalidatePh {
         acc.state += 8;
       }
     }
+    // lane 0 takes every block's children; their affected-mask atomics are
+    // independent and issued together, the fresh bits handled after
+    uint32_t bits[NB], old[NB];
 #pragma unroll
     for (int k = 0; k < NB; k++) {
+      bits[k] = 0;
       if (!m[k]) continue;
       const bool child = ((m[k] >> lane) & 1u) && key_parent1(cur[k]) == x + 1u;
-      const unsigned bits = __ballot_sync(0xffffffffu, child);
-      if (bits && lane == 0) mark(y, k, bits);
+      bits[k] = __ballot_sync(0xffffffffu, child);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < NB; k++)
+        old[k] = bits[k] ? atomicOr(P->affm + (u64)y * NB + k, bits[k]) : ~0u;
+      bool fresh_any = false;
+#pragma unroll
+      for (int k = 0; k < NB; k++) {
+        const uint32_t fresh = bits[k] & ~old[k];
+        if (fresh) {
+          atomicOr(inew_next + (u64)y * NB + k, fresh);
+          fresh_any = true;
+        }
+      }
+      if (fresh_any) {
+        note_affected(*P, y, epoch);
+        enqueue_once(*P, qpar, y, tag);
+      }
     }
   }
   __device__ void endQ(uint32_t, int, uint32_t, u64 &) {}
@@ -537,11 +581,22 @@ struct InvalidatePh {
         acc.state += 8;
       }
     }
+    // the lane's children (one edge, up to four queries in ascending order),
+    // merged per mask word: one affected-mask atomic per word
+    uint32_t word = ~0u, bits = 0;
 #pragma unroll
     for (uint32_t u = 0; u < 4; u++) {
       const uint32_t q = (qpk >> (8 * u)) & 255;
-      if (u < cnt && valid && key_parent1(cur[u]) == x + 1u) mark(y, q >> 5, 1u << (q & 31));
+      if (u < cnt && valid && key_parent1(cur[u]) == x + 1u) {
+        if ((q >> 5) != word) {
+          if (bits) mark(y, word, bits);
+          word = q >> 5;
+          bits = 0;
+        }
+        bits |= 1u << (q & 31);
+      }
     }
+    if (bits) mark(y, word, bits);
   }
   __device__ void endE(uint32_t, int, uint32_t, u64 *) {}
 };
@@ -683,17 +738,39 @@ struct RelaxPh {
         }
       }
     }
+    // first lowering attempts, independent and issued together
+    u64 cand[4], got[4];
+    bool tried[4];
 #pragma unroll
     for (uint32_t u = 0; u < 4; u++) {
+      tried[u] = false;
+      cand[u] = KEY_INF;
+      got[u] = 0;
       if (c[u] == INF32) continue;
       const uint32_t q = (qpk >> (8 * u)) & 255;
-      if (lower_from<STRICT>(P->key + (u64)y * NB * 32 + q, pack_key((uint32_t)c[u], x + 1u),
-                             cur[u])) {
-        atomicOr(nmask_next + (u64)y * NB + (q >> 5), 1u << (q & 31));
-        enqueue_once(*P, qpar, y, tag);
-        acc.improved++;
-      }
+      cand[u] = pack_key((uint32_t)c[u], x + 1u);
+      tried[u] = first_lower<STRICT>(P->key + (u64)y * NB * 32 + q, cand[u], cur[u], got[u]);
     }
+    // improvements of this edge's queries (ascending), merged per mask word;
+    // y enters the next wave's queue once
+    uint32_t word = ~0u, bits = 0;
+    bool any = false;
+#pragma unroll
+    for (uint32_t u = 0; u < 4; u++) {
+      if (!tried[u]) continue;
+      const uint32_t q = (qpk >> (8 * u)) & 255;
+      if (!lowered<STRICT>(P->key + (u64)y * NB * 32 + q, cand[u], cur[u], got[u])) continue;
+      if ((q >> 5) != word) {
+        if (bits) atomicOr(nmask_next + (u64)y * NB + word, bits);
+        word = q >> 5;
+        bits = 0;
+      }
+      bits |= 1u << (q & 31);
+      acc.improved++;
+      any = true;
+    }
+    if (bits) atomicOr(nmask_next + (u64)y * NB + word, bits);
+    if (any) enqueue_once(*P, qpar, y, tag);
   }
   __device__ void endE(uint32_t, int, uint32_t, u64 *) {}
 };

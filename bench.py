@@ -454,7 +454,9 @@ def run_dycg(args):
         "per_step": {k: round(float(np.mean([p[k] for p in per])), 4) for k in
                      ("ms_ingest", "ms_mutate", "ms_repair", "ms_cache", "ms_total", "affected",
                       "expanded", "edges_scanned", "improvements", "waves", "relocated_rows",
-                      "missing_deletes", "cache_pages_loaded", "link_bytes", "hbm_adj_bytes")},
+                      "missing_deletes", "cache_pages_loaded", "link_bytes", "hbm_adj_bytes",
+                      "ms_phase_invalidate", "ms_phase_pull", "ms_phase_seed",
+                      "ms_phase_closure")},
     }
     _hb = float(np.sum([p["hbm_adj_bytes"] for p in per]))
     out["per_step"]["adjacency_hit_rate"] = round(

@@ -1006,14 +1006,15 @@ void Engine::apply(const dycg_edge *dels, size_t nd, const dycg_edge *adds, size
       // batched: the kernel counts 8 B per (edge, active query) key access
       stats->state_bytes = c.stat[ST_STATE_BYTES] + stats->expanded * 16 + stats->improvements * 16;
       fill_phases(stats, c);
-    }
-    else
+    } else {
       stats->state_bytes = stats->expanded * 24 + stats->edges_scanned * 8 + stats->improvements * 16;
+      if (!nq_ && opt_.algo != DYCG_ALGO_PR) fill_phases(stats, c);
+    }
   }
 }
 
-// Phase times of a batched repair from the kernel's own timer stamps
-// (phases a launch skipped have no stamp and count zero).
+// Phase times of a repair from the kernel's own timer stamps (single-source
+// or batched; phases a launch skipped have no stamp and count zero).
 static void fill_phases(dycg_batch_stats *s, const Ctl &c) {
   const u64 t[4] = {c.tphase[0], c.tphase[1], c.tphase[2], c.tphase[3]};
   double *out[4] = {&s->ms_phase_invalidate, &s->ms_phase_pull, &s->ms_phase_seed,

@@ -217,6 +217,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
   const uint32_t gstride = gridDim.x * blockDim.x;
   const uint32_t lane = lane_id();
   const uint32_t tag_base = P.tag_dev ? *(volatile uint32_t *)P.tag_dev : P.tag_base;
+  if (gtid == 0) ctl->stat[ST_T_START] = globaltimer_ns();
 
   if (P.phases & PH_DELETE) {
     // 1. deletion seeds (warp-uniform loop so appends can aggregate)
@@ -248,6 +249,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
         lo = hi;
       }
     }
+    if (gtid == 0) ctl->tphase[0] = globaltimer_ns();  // seeds + invalidation done
     // 3. reset
     {
       const uint32_t na = *(volatile uint32_t *)&ctl->snap_aff;
@@ -260,6 +262,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
       PullOp<ALGO, STORED> op{&P};
       if (!expand_rows<STORED>(P.in, P.aff, na, op, acc, P.tiles, ctl, 0, P.timeout_ns, P.claimed))
         goto done;
+      if (gtid == 0) ctl->tphase[1] = globaltimer_ns();  // reset + pull done
       // 5a. frontier from affected vertices with a finite value
       for (uint32_t i0 = gtid - lane; i0 < na; i0 += gstride) {
         const uint32_t i = i0 + lane;
@@ -302,6 +305,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
     }
   }
   if (!grid_sync(ctl, SYNC_RESET_VMIN, P.timeout_ns)) goto done;
+  if (gtid == 0) ctl->tphase[2] = globaltimer_ns();  // frontier + insertion seeds done
   // 6. closure waves
   if ((P.phases & PH_CLOSE) && P.delta) {
     // Ordered (bucketed) closure for high-diameter graphs, the B200 form of
@@ -384,6 +388,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
       cur ^= 1;
     }
   }
+  if (gtid == 0) ctl->tphase[3] = globaltimer_ns();  // closure done
 done:
   acc.flush(ctl);
   if (gtid == 0) {

@@ -139,7 +139,8 @@ typedef struct dycg_batch_stats {
   double ms_total;
   uint64_t mutate_link_bytes;  /* mutation kernels' share of link_bytes      */
   uint64_t mutate_hbm_bytes;   /* mutation kernels' share of hbm_adj_bytes    */
-  /* batched many-query form: time inside the repair kernel per phase */
+  /* time inside the repair kernel per phase (SSSP/BFS/CC: one source, or
+     the batched many-query form; zero for PageRank and per-query repairs) */
   double ms_phase_invalidate;  /* deletion seeds + invalidation waves        */
   double ms_phase_pull;        /* reset + pull over in-rows                  */
   double ms_phase_seed;        /* frontier + insertion seeds                 */

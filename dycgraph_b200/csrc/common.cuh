@@ -205,12 +205,14 @@ __device__ __forceinline__ u64 warp_sum(u64 x) {
   return x;
 }
 
-__device__ __forceinline__ u64 warp_min(u64 x) {
-  for (int o = 16; o; o >>= 1) {
-    u64 y = __shfl_down_sync(0xffffffffu, x, o);
-    x = y < x ? y : x;
-  }
-  return x;
+// Minimum of a 64-bit key over the warp, in every lane: the high words'
+// minimum, then the minimum low word among the lanes that hold it (the same
+// order as the 64-bit comparison), each one warp reduction instruction.
+__device__ __forceinline__ u64 warp_min_all(u64 x) {
+  const uint32_t hi = __reduce_min_sync(0xffffffffu, (uint32_t)(x >> 32));
+  const uint32_t lo =
+      __reduce_min_sync(0xffffffffu, (uint32_t)(x >> 32) == hi ? (uint32_t)x : 0xFFFFFFFFu);
+  return ((u64)hi << 32) | lo;
 }
 
 // Slot address through the page table.

@@ -1325,7 +1325,7 @@ void Engine::tune_repair(uint32_t nd, uint32_t na, u64 timeout) {
     CK(cudaMemcpyAsync(ctl_, sc.p[2], sizeof(Ctl), cudaMemcpyDeviceToDevice, st_));
   };
   static const uint32_t kRatio[] = {2, 4, 8, 1u << 20};
-  static const uint32_t kHeavy[] = {16, 64, 256};
+  static const uint32_t kHeavy[] = {4, 8, 16, 64, 256};
   static const uint32_t kPull[] = {0, 1, 2, 8};
   static const uint32_t kTile[] = {1024, 4096, 16384};
   tried_.clear();

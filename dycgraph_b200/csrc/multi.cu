@@ -244,17 +244,42 @@ __device__ __forceinline__ bool use_query_lanes(uint32_t act, uint32_t len, uint
 // Expand slots [b, e) of v's row, `stride` apart per lane, for the queries
 // in masks m (warp-uniform); s is the warp's shared per-query state (Q
 // entries) for the edge-lane mapping.
+// Ask L2 for the key lines of neighbour y that the active queries (masks m,
+// warp-uniform) will read: one 256-byte bulk prefetch per block of 32 queries
+// with any bit set (no registers held, no completion to wait for). A lane's
+// loads for its later query groups, or for the warp's later edges, then find
+// their sectors in L2 instead of waiting on HBM one group after another. The
+// kernel is latency-bound with DRAM bandwidth mostly idle, so fetching whole
+// lines costs nothing it is short of. Each line is 256-byte aligned inside the
+// key array, and y is a live slot's vertex id (< n).
+template <int NB>
+__device__ __forceinline__ void prefetch_keys(const u64 *key, uint32_t y,
+                                              const uint32_t (&m)[NB]) {
+#pragma unroll
+  for (int k = 0; k < NB; k++) {
+    if (!m[k]) continue;  // warp-uniform
+    const u64 *p = key + ((u64)y * NB + k) * 32;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], 256;" ::"l"(p) : "memory");
+  }
+}
+
 template <int NB, bool WITH_W, class Ph>
 __device__ __forceinline__ void expand_vertex(const Adj &A, uint32_t v, const uint32_t (&m)[NB],
                                               uint32_t b, uint32_t e, uint32_t stride, bool qlanes,
                                               Ph &ph, u64 *s, Acc &acc) {
   if (lane_id() == 0 && b == 0) acc.expanded++;
   const u64 off = A.off[v];
+  uint32_t act = 0;
+#pragma unroll
+  for (int k = 0; k < NB; k++) act += __popc(m[k]);
   if (qlanes) {
     u64 st[NB];
 #pragma unroll
     for (int k = 0; k < NB; k++) ph.beginQ(v, k, m[k], st[k]);
     auto visit = [&](uint32_t y, uint32_t w, bool valid) {
+      // the warp takes these edges one at a time: their key lines are asked
+      // for together first
+      if (valid) prefetch_keys<NB>(ph.P->key, y, m);
       unsigned vb = __ballot_sync(0xffffffffu, valid);
       while (vb) {
         const int src = __ffs(vb) - 1;
@@ -274,6 +299,9 @@ __device__ __forceinline__ void expand_vertex(const Adj &A, uint32_t v, const ui
     if (m[k]) ph.beginE(v, k, m[k], s);
   __syncwarp();
   auto visit = [&](uint32_t y, uint32_t w, bool valid) {
+    // more than one group of four queries: the later groups' keys are
+    // asked for before the first group's loads
+    if (act > 4 && valid) prefetch_keys<NB>(ph.P->key, y, m);
     uint32_t qpk = 0, cnt = 0;
 #pragma unroll
     for (int k = 0; k < NB; k++) {
@@ -651,14 +679,17 @@ struct PullPh {
         acc.state += 8;
       }
     }
+    // the four minima over the warp's slots are independent: their
+    // reductions (two single-instruction 32-bit reductions each) overlap
+    u64 mn[4];
 #pragma unroll
-    for (uint32_t u = 0; u < 4; u++) {
-      if (u >= cnt) break;  // warp-uniform
-      const u64 c = cand(v, x, w, cur[u]);
-      if (__any_sync(0xffffffffu, c != KEY_INF)) {
-        const u64 mn = warp_min(c);
+    for (uint32_t u = 0; u < 4; u++)
+      mn[u] = u < cnt ? warp_min_all(cand(v, x, w, cur[u])) : KEY_INF;  // cnt warp-uniform
+    if (lane_id() == 0) {
+#pragma unroll
+      for (uint32_t u = 0; u < 4; u++) {
         const uint32_t q = (qpk >> (8 * u)) & 255;
-        if (lane_id() == 0 && mn < s[q]) s[q] = mn;
+        if (u < cnt && mn[u] < s[q]) s[q] = mn[u];
       }
     }
   }

@@ -96,7 +96,7 @@ struct PullOp {
     r.best = cand < r.best ? cand : r.best;
   }
   __device__ void end(uint32_t v, Row &r) {
-    const u64 m = warp_min(r.best);
+    const u64 m = warp_min_all(r.best);
     if (lane_id() == 0 && m != KEY_INF) {
       if (Strict<ALGO, STORED>::value) strict_lower(P->key + v, m);
       else atomicMin(P->key + v, m);
@@ -144,7 +144,7 @@ struct RelaxOp {
     }
     warp_append(outq, outc, P->n, want, y, &P->ctl->err);
     if (vmin) {
-      imp = (uint32_t)warp_min(imp);
+      imp = __reduce_min_sync(0xffffffffu, imp);
       if (lane_id() == 0 && imp != INF32) atomicMin(vmin, imp);
     }
   }
@@ -174,7 +174,7 @@ __device__ bool expand_ordered(const RepairParams &P, const uint32_t *items, uin
     const bool now = dv < thr;
     const bool carry = dv != INF32 && !now && atomicExch(P.wtag + v, op.tag) != op.tag;
     warp_append(op.outq, op.outc, P.n, carry, v, &ctl->err);
-    const uint32_t cm = (uint32_t)warp_min(carry ? dv : INF32);
+    const uint32_t cm = __reduce_min_sync(0xffffffffu, carry ? dv : INF32);
     if (lane == 0 && cm != INF32) atomicMin(op.vmin, cm);
     unsigned todo = __ballot_sync(0xffffffffu, now);
     while (todo) {
@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(BLOCK) repair_kernel(RepairParams P) {
           const bool carry = !now && d != INF32 && atomicExch(P.wtag + v, tag) != tag;
           warp_append(P.q2, &ctl->q_count[2], P.n, now, v, &ctl->err);
           warp_append(P.q[cur ^ 1], &ctl->q_count[cur ^ 1], P.n, carry, v, &ctl->err);
-          const uint32_t cm = (uint32_t)warp_min(carry ? d : INF32);
+          const uint32_t cm = __reduce_min_sync(0xffffffffu, carry ? d : INF32);
           if (lane == 0 && cm != INF32) atomicMin(&ctl->vmin, cm);
         }
         if (!grid_sync(ctl, cur ? SYNC_RESET_Q1 : SYNC_RESET_Q0, P.timeout_ns)) goto done;

@@ -161,15 +161,17 @@ def test_grid_snapshots_mix_grid_edges_and_shortcuts():
         assert ((cheb <= 8) | (av == (au + 1) % n)).all()
 
 
-def test_link_transaction_bound():
+def test_link_transactions():
     import bench
-    b = bench.link_transaction_bound(4_150_000, 0.98, 14.0)
-    assert b["min_transactions"] == 32_422  # ceil(4.15 MB / 128 B)
-    assert abs(b["bound_ms"] - 32_422 * 14e-6) < 1e-3 and 0 < b["frac"] < 1
-    assert b["ns_per_transaction"] == 14.0
-    assert bench.link_transaction_bound(0, 1.0, 14.0)["min_transactions"] == 0
-    assert bench.link_transaction_bound(-5.0, 1.0, 14.0)["bound_ms"] == 0
-    assert bench.link_transaction_bound(1000, 0, 14.0)["frac"] is None
+    b = bench.link_transactions(4_150_000, 0.98, 14.0)
+    assert b["transactions_128B"] == 32_422  # ceil(4.15 MB / 128 B)
+    assert abs(b["random_cost_ms"] - 32_422 * 14e-6) < 1e-3
+    assert abs(b["ns_per_128B_achieved"] - 0.98e6 / 32_422) < 0.01
+    assert b["ns_per_random_transaction"] == 14.0
+    assert bench.link_transactions(0, 1.0, 14.0)["transactions_128B"] == 0
+    assert bench.link_transactions(0, 1.0, 14.0)["ns_per_128B_achieved"] is None
+    assert bench.link_transactions(-5.0, 1.0, 14.0)["random_cost_ms"] == 0
+    assert bench.link_transactions(1000, 0, 14.0)["ns_per_128B_achieved"] is None
 
 
 def test_rmat_snapshots_are_disjoint_live_deletions_and_rmat_insertions():

@@ -199,8 +199,9 @@ def test_tune_mapping_keeps_results():
     tried = e.tune_query_mapping(dels, adds)
     orc.mutate(dels, adds)
     cur = orc.csr()
-    # 12 (qratio x heavy) + 3-4 pull ratios + 2-3 tile sizes + 5 frontier-queue schemes
-    assert 12 < len(tried) <= 24 and all(t["repair_ms"] > 0 for t in tried)
+    # 20 (qratio x heavy) + 3-4 pull ratios + 2-3 tile sizes + 5 frontier-queue schemes
+    assert 20 < len(tried) <= 32 and all(t["repair_ms"] > 0 for t in tried)
+    assert {t["heavy"] for t in tried} >= {4, 8, 16, 64, 256}
     assert {t["tile"] for t in tried} == {1024, 4096, 16384}
     assert {t["queue"] for t in tried} == {0, 1, 2, 3, 4, 5}
     _check_all(e, n, cur, src)

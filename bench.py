@@ -189,8 +189,8 @@ class Clocks:
 # capture); the line's `traffic` scales it by the run's own algorithmic bytes.
 # None where no capture was taken.
 # batched repair kernel, R-MAT 20 / 256 queries, the two timed launches of
-# profiles/ncu_multi_repair_rmat20_q256.md: 2,443 MB DRAM / 567.6 MB algorithmic
-NCU_TRAFFIC_RATIO = {("batched", "sssp"): 4.3}
+# profiles/ncu_multi_repair_rmat20_q256.md: 2,728 MB DRAM / 589.2 MB algorithmic
+NCU_TRAFFIC_RATIO = {("batched", "sssp"): 4.6}
 
 # Random host-link transactions cost about the same whatever their size up to
 # 128 bytes (dycg_measure_host_random: random 128-byte reads over an 8 GB

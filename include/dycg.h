@@ -425,7 +425,7 @@ int dycg_set_query_queue(dycg_engine *e, uint32_t scheme);
 
 /* Autotuner of the batched form's work mapping (no reference counterpart):
  * applies one snapshot like dycg_apply_batch, but repairs it once per
- * candidate mapping (qratio in {2,4,8,2^20} x heavy in {16,64,256} with the
+ * candidate mapping (qratio in {2,4,8,2^20} x heavy in {4,8,16,64,256} with the
  * pull phase on the same ratio, then the best of those with the pull phase's
  * ratio in {0,1,2,8}, then the best so far with query-lane tiles of
  * {1024,4096,16384} slots, then the best so far under the other
